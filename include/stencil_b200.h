@@ -1,0 +1,131 @@
+/*
+ * stencil_b200.h -- C ABI of the B200-native stencil time-stepper.
+ *
+ * Plain pointers and sizes only.  Device pointers are CUDA device memory owned by
+ * the caller; `stream` is a cudaStream_t (NULL = legacy default stream).  Every
+ * call is asynchronous on that stream unless stated otherwise, returns an int
+ * status (SB200_OK or a negative SB200_ERR_* code) and never allocates device
+ * memory.  sb200_last_error() describes the last failure on the calling thread.
+ *
+ * Field layout (the reference's GridDims, include/stencil/types.hpp:103-140):
+ * extents include a 4-cell halo on every face, z is slowest,
+ * idx = (z*ny + y)*nx + x, the interior is [4, n-4) on each axis and halo cells
+ * are never written (fixed zero walls).
+ */
+#ifndef STENCIL_B200_H
+#define STENCIL_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SB200_OK 0
+#define SB200_ERR_INVALID (-1)     /* bad argument (null pointer, aliasing, bad extents) */
+#define SB200_ERR_CUDA (-2)        /* CUDA runtime / driver error */
+#define SB200_ERR_DEVICE (-3)      /* a kernel's bounded wait gave up (device error word) */
+#define SB200_ERR_UNSUPPORTED (-4) /* shape or alignment this entry point cannot take */
+#define SB200_ERR_MONITOR (-5)     /* stability monitor tripped (non-finite or blow-up) */
+
+/* Grid descriptor: the reference's GridDims (types.hpp:115-140) with an explicit dt. */
+typedef struct sb200_grid {
+    int64_t nx, ny, nz; /* halo-inclusive extents (interior = n - 8) */
+    float dx, dy, dz;   /* grid spacing [m] */
+    float dt;           /* time step [s] */
+} sb200_grid;
+
+/* ── library / errors ─────────────────────────────────────────────────────── */
+int sb200_version(void);
+/* Text of the last failure on the calling thread ("" if none). */
+const char* sb200_last_error(void);
+/* Reads the current device's error word (synchronous); clears it when clear != 0.
+ * Returns the word (0 = no device-side error) or a negative status. */
+int sb200_device_error(int clear);
+
+/* ── reference kernel-launcher API (include/stencil/kernels.cuh:33-83) ───────── */
+
+/* Replaces upload_fd_coefficients() (kernels.cuh:33; stencil_naive.cu:38-46).
+ * The radius-4 weights are compile-time constants of every kernel here, so this
+ * only validates that a CUDA device is usable.  Synchronous. */
+int sb200_upload_fd_coefficients(void);
+
+/* Replaces launch_naive() (kernels.cuh:42-43; stencil_naive.cu:92-114):
+ *   p_next = 2 p_cur - p_prev + dt^2 vel2 lap(p_cur)   on the interior,
+ * evaluated in the reference's operation order without FMA contraction
+ * (bit-identical to its CPU path built with -ffp-contract=off).
+ * p_next must not alias p_cur; p_next == p_prev is allowed (in place). */
+int sb200_launch_naive(const float* p_cur, const float* p_prev, const float* vel2,
+                       float* p_next, const sb200_grid* grid, void* stream);
+
+/* Replaces launch_tiled() (kernels.cuh:54-55; stencil_tiled.cu:147-168): the same
+ * update by the TMA z-marching pencil kernel (FP32, FMA-contracted; within 1e-6
+ * relative L2 of the reference order per step).  Grids whose row pitch is not a
+ * multiple of 16 bytes (nx % 4 != 0) or with pointers not 16-byte aligned run
+ * the naive kernel instead.  Aliasing rules as sb200_launch_naive. */
+int sb200_launch_tiled(const float* p_cur, const float* p_prev, const float* vel2,
+                       float* p_next, const sb200_grid* grid, void* stream);
+
+/* Replaces launch_slab() (kernels.cuh:63-64; stencil_multi_gpu.cu:60-66): on one
+ * GPU a slab whose z-face halos the caller has filled is an ordinary grid, so
+ * this is sb200_launch_tiled. */
+int sb200_launch_slab(const float* p_cur, const float* p_prev, const float* vel2,
+                      float* p_next, const sb200_grid* grid, void* stream);
+
+/* ── solver-step entry points (src/solver/wave_prop.cpp:67-75, heat_diffusion.cpp:103-122) */
+
+/* One acoustic step with centre-source injection (WavePropSolver::step_impl plus
+ * the source rule p_next[src] += (dt^2 vel2[src]) * src_amp after the update).
+ * src_index < 0 disables the source.  p_next may alias p_prev. */
+int sb200_wave_step_f32(const float* p, const float* p_prev, const float* vel2, float* p_next,
+                        const sb200_grid* grid, int64_t src_index, float src_amp,
+                        void* stream);
+
+/* sb200_wave_step_f32 evaluated in the reference's operation order with no FMA
+ * contraction (the kernel behind sb200_launch_naive): bit-identical to the
+ * reference CPU path built with -ffp-contract=off, at about a third of the
+ * pencil kernel's throughput.  For callers that need reproducible bits. */
+int sb200_wave_step_exact_f32(const float* p, const float* p_prev, const float* vel2,
+                              float* p_next, const sb200_grid* grid, int64_t src_index,
+                              float src_amp, void* stream);
+
+/* One explicit heat step u_next = u + alpha*dt*lap(u) with a scalar diffusivity
+ * (HeatDiffusionSolver::step_impl without its vel2 field and D2D copy: 8 B/point).
+ * u_next must not alias u. */
+int sb200_heat_step_f32(const float* u, float* u_next, const sb200_grid* grid, float alpha,
+                        void* stream);
+
+/* ── inputs of the benchmark configurations (host memory; no reference counterpart:
+ *    the reference has only a constant / two-layer velocity and a Gaussian pulse,
+ *    include/stencil/grid.hpp:57-99) ─────────────────────────────────────────── */
+
+/* Seeded layered velocity model written as v^2 into vel2[nz*ny*nx] (host):
+ * n_layers horizontal layers whose interfaces are uniform random depths over the
+ * interior, velocities rising linearly from v_top to v_bottom with depth, times
+ * (1 + perturbation*g) with g a Gaussian-correlated field (correlation function
+ * exp(-r^2/corr_cells^2)) scaled to max|g| = 1.  *v_max_out (optional) receives
+ * the largest velocity.  Deterministic for a given seed on every host. */
+int sb200_model_layered(float* vel2, int64_t nx, int64_t ny, int64_t nz, uint64_t seed,
+                        int n_layers, float v_top, float v_bottom, float perturbation,
+                        float corr_cells, float* v_max_out);
+
+/* Ricker wavelet w(t_n) = (1 - 2 pi^2 f^2 tau^2) exp(-pi^2 f^2 tau^2),
+ * tau = n*dt - t0, n = 0..n_steps-1, evaluated in double and rounded to float. */
+int sb200_ricker(double freq, double t0, double dt, int64_t n_steps, float* out);
+
+/* ── pencil-kernel configuration (used by the tuner and the tests) ──────────── */
+#define SB200_KIND_WAVE_F32 0
+#define SB200_KIND_HEAT_F32 1
+int sb200_pencil_variant_count(int kind);
+const char* sb200_pencil_variant_name(int kind, int variant);
+/* Forces (variant, zchunks) for every later launch of `kind` on this process;
+ * variant < 0 restores automatic selection. */
+int sb200_set_pencil_override(int kind, int variant, int zchunks);
+/* The (variant, zchunks) the next launch of `kind` on `grid` would use. */
+int sb200_pencil_choice(int kind, const sb200_grid* grid, int* variant, int* zchunks);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* STENCIL_B200_H */

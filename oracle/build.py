@@ -1,0 +1,105 @@
+"""Build recipe for the oracle (test infrastructure only).
+
+Produces
+  oracle/liboracle.so                 -- the C restatement (stencil_oracle.c),
+                                         -ffp-contract=off, OpenMP.
+  oracle/_ref/libstencil_ref_*.so     -- the reference's own CPU path, compiled
+                                         from its sources where they lie (only
+                                         when the reference checkout exists):
+      f32_strict : -O3 -ffp-contract=off          (bit-exact pin of the oracle)
+      f32        : -O3 -march=x86-64-v3           (the reference's Release flags
+                                                   with a portable -march so the
+                                                   library runs on any host of
+                                                   the pool; timed CPU baseline)
+      f64        : -O3 -ffp-contract=off -DSTENCIL_FP64   (FP64 CPU oracle)
+The reference sources are never copied into this repository; oracle/_ref/ is
+git-ignored.
+"""
+from __future__ import annotations
+
+import os
+import pathlib
+import subprocess
+import sys
+
+HERE = pathlib.Path(__file__).resolve().parent
+REF_ROOT = pathlib.Path(os.environ.get("STENCIL_REF_ROOT", "/root/reference"))
+
+# Reference translation units that make up its CPU path (kernels + solver + utils).
+REF_SOURCES = [
+    "src/kernels/stencil_naive.cu",
+    "src/kernels/stencil_tiled.cu",
+    "src/utils/grid.cpp",
+    "src/utils/timer.cpp",
+    "src/utils/io.cpp",
+    "src/solver/solver_base.cpp",
+    "src/solver/wave_prop.cpp",
+    "src/solver/heat_diffusion.cpp",
+]
+
+REF_VARIANTS = {
+    "f32_strict": ["-O3", "-ffp-contract=off"],
+    "f32": ["-O3", "-march=x86-64-v3"],
+    "f64": ["-O3", "-ffp-contract=off", "-DSTENCIL_FP64"],
+}
+
+
+def _newer(target: pathlib.Path, deps) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(pathlib.Path(d).stat().st_mtime > t for d in deps)
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("oracle build failed: " + " ".join(map(str, cmd)))
+
+
+def build_oracle(force: bool = False) -> pathlib.Path:
+    out = HERE / "liboracle.so"
+    src = HERE / "stencil_oracle.c"
+    if force or _newer(out, [src]):
+        _run(["gcc", "-O2", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared", "-std=c11",
+              "-Wall", "-Wextra", str(src), "-o", str(out), "-lm"])
+    return out
+
+
+def reference_available() -> bool:
+    return all((REF_ROOT / s).exists() for s in REF_SOURCES)
+
+
+def build_reference(force: bool = False) -> dict:
+    """Compile the reference CPU path; returns {variant: path}. No-op without the checkout."""
+    built = {}
+    if not reference_available():
+        return built
+    outdir = HERE / "_ref"
+    outdir.mkdir(exist_ok=True)
+    shim = HERE / "ref_shim.cpp"
+    srcs = [REF_ROOT / s for s in REF_SOURCES]
+    for name, flags in REF_VARIANTS.items():
+        out = outdir / f"libstencil_ref_{name}.so"
+        if force or _newer(out, [shim, *srcs]):
+            cmd = ["g++", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-w",
+                   "-DSTENCIL_CPU_FALLBACK", *flags, "-I", str(REF_ROOT / "include")]
+            for s in srcs:
+                cmd += ["-x", "c++", str(s)]
+            cmd += ["-x", "c++", str(shim), "-o", str(out)]
+            _run(cmd)
+        built[name] = out
+    return built
+
+
+def build(force: bool = False) -> None:
+    build_oracle(force)
+    build_reference(force)
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv)
+    print("oracle built:", HERE / "liboracle.so")
+    for p in sorted((HERE / "_ref").glob("*.so")) if (HERE / "_ref").exists() else []:
+        print("reference CPU path built:", p)

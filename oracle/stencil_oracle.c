@@ -1,0 +1,192 @@
+/*
+ * oracle/stencil_oracle.c -- CPU restatement of the reference stencil time-stepper.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA path: it is
+ * loaded by tests/, by __graft_entry__.smoke() and by bench.py's cpu_baseline /
+ * reference legs, never by the product library.  It is compiled with
+ * -ffp-contract=off so every multiply and add rounds exactly where the C source
+ * says, which makes the FP32 variant bit-identical to the reference's own CPU
+ * path built with the same flag (pinned in tests/test_oracle.py against the
+ * reference sources compiled into oracle/_ref/, and against tests/golden/).
+ *
+ * Algorithm followed (somya2703/stencil_solver):
+ *   - coefficients: include/stencil/types.hpp:175-181 (FDCoeffs<4>)
+ *   - wave step:    src/kernels/stencil_naive.cu:136-170 (CPU launch_naive)
+ *                   and tests/integration/test_kernel_correctness.cpp:43-75
+ *                   (cpu_reference_step): per axis
+ *                       lap_a  = c0*p*inv_da2
+ *                       lap_a += c_r*(p[+r]+p[-r])*inv_da2      r = 1..4
+ *                   then next = 2*p - prev + dt2*vel2*(lap_x+lap_y+lap_z)
+ *                   over the interior [R, n-R) of each axis; halo never written.
+ *   - heat step:    src/solver/heat_diffusion.cpp:73-122 -- the wave step with
+ *                   prev == cur and vel2 == alpha, dt_eff^2 in place of dt^2.
+ *   - norms:        src/utils/grid.cpp:86-115 (l2_error is an RMS, max_abs_error).
+ * Project-defined pieces (no reference counterpart; identical rule in the CUDA
+ * path): Ricker wavelet samples and the source rule
+ *       next[src] += (dt2*vel2[src]) * w(t_n)    after the update of step n.
+ */
+#include <math.h>
+#include <stddef.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define R 4
+
+/* include/stencil/types.hpp:175-181, evaluated in double then rounded. */
+static const double C0_D = -205.0 / 72.0;
+static const double C_D[R] = {8.0 / 5.0, -1.0 / 5.0, 8.0 / 315.0, -1.0 / 560.0};
+
+void oracle_fd_coefficients(double out[R + 1]) {
+    out[0] = C0_D;
+    for (int r = 0; r < R; ++r) out[r + 1] = C_D[r];
+}
+
+/* One leapfrog step, generic over the element type via a macro so that the
+ * FP32 and FP64 variants share one statement of the arithmetic. */
+#define DEFINE_WAVE_STEP(NAME, T)                                                        \
+    void NAME(const T* cur, const T* prev, const T* vel2, T* next, int64_t nx,          \
+              int64_t ny, int64_t nz, T dx, T dy, T dz, T dt) {                          \
+        const T c0 = (T)C0_D;                                                            \
+        T c[R];                                                                          \
+        for (int r = 0; r < R; ++r) c[r] = (T)C_D[r];                                    \
+        const T inv_dx2 = (T)1 / (dx * dx);                                              \
+        const T inv_dy2 = (T)1 / (dy * dy);                                              \
+        const T inv_dz2 = (T)1 / (dz * dz);                                              \
+        const T dt2 = dt * dt;                                                           \
+        const int64_t sy = nx, sz = nx * ny;                                             \
+        _Pragma("omp parallel for collapse(2) schedule(static)")                         \
+        for (int64_t iz = R; iz < nz - R; ++iz)                                          \
+            for (int64_t iy = R; iy < ny - R; ++iy)                                      \
+                for (int64_t ix = R; ix < nx - R; ++ix) {                                \
+                    const int64_t ci = iz * sz + iy * sy + ix;                           \
+                    const T p = cur[ci];                                                 \
+                    T lx = c0 * p * inv_dx2;                                             \
+                    T ly = c0 * p * inv_dy2;                                             \
+                    T lz = c0 * p * inv_dz2;                                             \
+                    for (int r = 1; r <= R; ++r) {                                       \
+                        lx += c[r - 1] * (cur[ci + r] + cur[ci - r]) * inv_dx2;          \
+                        ly += c[r - 1] * (cur[ci + r * sy] + cur[ci - r * sy]) * inv_dy2; \
+                        lz += c[r - 1] * (cur[ci + r * sz] + cur[ci - r * sz]) * inv_dz2; \
+                    }                                                                    \
+                    next[ci] = (T)2 * p - prev[ci] + dt2 * vel2[ci] * (lx + ly + lz);    \
+                }                                                                        \
+    }
+
+DEFINE_WAVE_STEP(oracle_wave_step_f32, float)
+DEFINE_WAVE_STEP(oracle_wave_step_f64, double)
+
+/* Heat step with a scalar diffusivity, in the reference's arithmetic
+ * (heat_diffusion.cpp:103-118): next = 2*u - u + (dt_eff^2*alpha)*lap(u).
+ * 2*u - u is exact in binary floating point, so this equals
+ * u + (dt_eff^2*alpha)*lap(u) with lap in the reference's per-axis order. */
+#define DEFINE_HEAT_STEP(NAME, T)                                                        \
+    void NAME(const T* u, T* u_next, int64_t nx, int64_t ny, int64_t nz, T dx, T dy,    \
+              T dz, T dt_eff, T alpha) {                                                 \
+        const T c0 = (T)C0_D;                                                            \
+        T c[R];                                                                          \
+        for (int r = 0; r < R; ++r) c[r] = (T)C_D[r];                                    \
+        const T inv_dx2 = (T)1 / (dx * dx);                                              \
+        const T inv_dy2 = (T)1 / (dy * dy);                                              \
+        const T inv_dz2 = (T)1 / (dz * dz);                                              \
+        const T dt2 = dt_eff * dt_eff;                                                   \
+        const int64_t sy = nx, sz = nx * ny;                                             \
+        _Pragma("omp parallel for collapse(2) schedule(static)")                         \
+        for (int64_t iz = R; iz < nz - R; ++iz)                                          \
+            for (int64_t iy = R; iy < ny - R; ++iy)                                      \
+                for (int64_t ix = R; ix < nx - R; ++ix) {                                \
+                    const int64_t ci = iz * sz + iy * sy + ix;                           \
+                    const T p = u[ci];                                                   \
+                    T lx = c0 * p * inv_dx2;                                             \
+                    T ly = c0 * p * inv_dy2;                                             \
+                    T lz = c0 * p * inv_dz2;                                             \
+                    for (int r = 1; r <= R; ++r) {                                       \
+                        lx += c[r - 1] * (u[ci + r] + u[ci - r]) * inv_dx2;              \
+                        ly += c[r - 1] * (u[ci + r * sy] + u[ci - r * sy]) * inv_dy2;    \
+                        lz += c[r - 1] * (u[ci + r * sz] + u[ci - r * sz]) * inv_dz2;    \
+                    }                                                                    \
+                    u_next[ci] = (T)2 * p - p + dt2 * alpha * (lx + ly + lz);            \
+                }                                                                        \
+    }
+
+DEFINE_HEAT_STEP(oracle_heat_step_f32, float)
+DEFINE_HEAT_STEP(oracle_heat_step_f64, double)
+
+/* Project-defined source rule: after the update of step n,
+ *   next[src] += (dt2 * vel2[src]) * w_n,  dt2 = dt*dt in the field's type. */
+void oracle_inject_f32(float* next, const float* vel2, int64_t src, float dt, float w) {
+    const float dt2 = dt * dt;
+    const float k = dt2 * vel2[src];
+    next[src] = next[src] + k * w;
+}
+
+void oracle_inject_f64(double* next, const double* vel2, int64_t src, double dt, double w) {
+    const double dt2 = dt * dt;
+    const double k = dt2 * vel2[src];
+    next[src] = next[src] + k * w;
+}
+
+/* Ricker wavelet w(t) = (1 - 2 pi^2 f^2 tau^2) exp(-pi^2 f^2 tau^2), tau = t - t0,
+ * sampled at t_n = n*dt for n = 0..n_steps-1 (project-defined; t0 = 1/f). */
+void oracle_ricker(double f, double t0, double dt, int64_t n_steps, double* out) {
+    const double pi = 3.14159265358979323846;
+    for (int64_t n = 0; n < n_steps; ++n) {
+        const double tau = (double)n * dt - t0;
+        const double a = pi * pi * f * f * tau * tau;
+        out[n] = (1.0 - 2.0 * a) * exp(-a);
+    }
+}
+
+/* Runs n_steps of the acoustic scheme with a three-level ring, as the reference
+ * solver does (wave_prop.cpp:67-75 + grid.hpp:144-153), with an optional source.
+ * On return, cur holds the final field and prev the one before it.  trace
+ * (optional) receives p at the source cell after every step. */
+#define DEFINE_WAVE_RUN(NAME, STEP, INJ, T)                                             \
+    void NAME(T* cur, T* prev, T* scratch, const T* vel2, int64_t nx, int64_t ny,       \
+              int64_t nz, T dx, T dy, T dz, T dt, int64_t n_steps, int64_t src,          \
+              const double* wavelet, T* trace) {                                         \
+        T* bufs[3] = {prev, cur, scratch};                                               \
+        int ip = 0, ic = 1, in = 2;                                                      \
+        for (int64_t n = 0; n < n_steps; ++n) {                                          \
+            STEP(bufs[ic], bufs[ip], vel2, bufs[in], nx, ny, nz, dx, dy, dz, dt);        \
+            if (src >= 0 && wavelet) INJ(bufs[in], vel2, src, dt, (T)wavelet[n]);        \
+            if (trace && src >= 0) trace[n] = bufs[in][src];                             \
+            const int t = ip;                                                            \
+            ip = ic;                                                                     \
+            ic = in;                                                                     \
+            in = t;                                                                      \
+        }                                                                                \
+        /* (cur, prev) <- (bufs[ic], bufs[ip]); the three names are a permutation  \
+         * of the caller's buffers, so copy through temporaries. */                   \
+        const size_t bytes = (size_t)(nx * ny * nz) * sizeof(T);                         \
+        T* tc = (T*)malloc(bytes);                                                       \
+        T* tp = (T*)malloc(bytes);                                                       \
+        memcpy(tc, bufs[ic], bytes);                                                     \
+        memcpy(tp, bufs[ip], bytes);                                                     \
+        memcpy(cur, tc, bytes);                                                          \
+        memcpy(prev, tp, bytes);                                                         \
+        free(tc);                                                                        \
+        free(tp);                                                                        \
+    }
+
+DEFINE_WAVE_RUN(oracle_wave_run_f32, oracle_wave_step_f32, oracle_inject_f32, float)
+DEFINE_WAVE_RUN(oracle_wave_run_f64, oracle_wave_step_f64, oracle_inject_f64, double)
+
+/* Norms, accumulated in double (src/utils/grid.cpp:86-115). */
+double oracle_rms_diff_f32(const float* a, const float* b, int64_t n) {
+    double s = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        const double d = (double)a[i] - (double)b[i];
+        s += d * d;
+    }
+    return n > 0 ? sqrt(s / (double)n) : 0.0;
+}
+
+double oracle_max_abs_diff_f32(const float* a, const float* b, int64_t n) {
+    double m = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        const double d = fabs((double)a[i] - (double)b[i]);
+        if (d > m) m = d;
+    }
+    return m;
+}

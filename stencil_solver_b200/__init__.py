@@ -1,0 +1,234 @@
+"""B200-native stencil time-stepper (sm_100a) -- Python binding of the C ABI.
+
+The product is the shared library ``lib/libstencil_b200.so`` (CUDA kernels + the
+C ABI declared in ``include/stencil_b200.h``) together with the C++ drop-in API in
+``include/stencil/``.  This module is a thin ctypes layer over the C ABI for
+Python callers, the tests and the benchmark: device buffers are passed as raw
+pointers or as CUDA tensors (anything with ``data_ptr()``), streams as raw
+``cudaStream_t`` values or torch streams.
+
+There is no CPU fallback: if the library is missing, loading fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+from dataclasses import dataclass
+
+PKG = pathlib.Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libstencil_b200.so"
+
+SB200_OK = 0
+SB200_ERR_INVALID = -1
+SB200_ERR_CUDA = -2
+SB200_ERR_DEVICE = -3
+SB200_ERR_UNSUPPORTED = -4
+SB200_ERR_MONITOR = -5
+
+KIND_WAVE_F32 = 0
+KIND_HEAT_F32 = 1
+
+R = 4  # stencil radius (8th order)
+
+
+class StencilError(RuntimeError):
+    """A C-ABI call returned a non-zero status."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+
+
+class sb200_grid(C.Structure):
+    _fields_ = [("nx", C.c_int64), ("ny", C.c_int64), ("nz", C.c_int64),
+                ("dx", C.c_float), ("dy", C.c_float), ("dz", C.c_float), ("dt", C.c_float)]
+
+
+@dataclass
+class Grid:
+    """Halo-inclusive grid (the reference's GridDims with an explicit dt)."""
+    nx: int
+    ny: int
+    nz: int
+    dx: float = 10.0
+    dy: float = 10.0
+    dz: float = 10.0
+    dt: float = 1e-3
+
+    @property
+    def shape(self):
+        return (self.nz, self.ny, self.nx)
+
+    @property
+    def size(self) -> int:
+        return self.nx * self.ny * self.nz
+
+    @property
+    def interior(self) -> int:
+        return max(self.nx - 2 * R, 0) * max(self.ny - 2 * R, 0) * max(self.nz - 2 * R, 0)
+
+    def index(self, x: int, y: int, z: int) -> int:
+        return (z * self.ny + y) * self.nx + x
+
+    def c(self) -> sb200_grid:
+        return sb200_grid(self.nx, self.ny, self.nz, self.dx, self.dy, self.dz, self.dt)
+
+
+_lib: C.CDLL | None = None
+
+_SIGNATURES = {
+    "sb200_version": ([], C.c_int),
+    "sb200_last_error": ([], C.c_char_p),
+    "sb200_device_error": ([C.c_int], C.c_int),
+    "sb200_upload_fd_coefficients": ([], C.c_int),
+    "sb200_launch_naive": ([C.c_void_p] * 4 + [C.POINTER(sb200_grid), C.c_void_p], C.c_int),
+    "sb200_launch_tiled": ([C.c_void_p] * 4 + [C.POINTER(sb200_grid), C.c_void_p], C.c_int),
+    "sb200_launch_slab": ([C.c_void_p] * 4 + [C.POINTER(sb200_grid), C.c_void_p], C.c_int),
+    "sb200_wave_step_f32": ([C.c_void_p] * 4 + [C.POINTER(sb200_grid), C.c_int64, C.c_float,
+                                                C.c_void_p], C.c_int),
+    "sb200_wave_step_exact_f32": ([C.c_void_p] * 4 + [C.POINTER(sb200_grid), C.c_int64,
+                                      C.c_float, C.c_void_p], C.c_int),
+    "sb200_heat_step_f32": ([C.c_void_p, C.c_void_p, C.POINTER(sb200_grid), C.c_float,
+                             C.c_void_p], C.c_int),
+    "sb200_model_layered": ([C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_uint64, C.c_int,
+                             C.c_float, C.c_float, C.c_float, C.c_float,
+                             C.POINTER(C.c_float)], C.c_int),
+    "sb200_ricker": ([C.c_double, C.c_double, C.c_double, C.c_int64, C.c_void_p], C.c_int),
+    "sb200_pencil_variant_count": ([C.c_int], C.c_int),
+    "sb200_pencil_variant_name": ([C.c_int, C.c_int], C.c_char_p),
+    "sb200_set_pencil_override": ([C.c_int, C.c_int, C.c_int], C.c_int),
+    "sb200_pencil_choice": ([C.c_int, C.POINTER(sb200_grid), C.POINTER(C.c_int),
+                             C.POINTER(C.c_int)], C.c_int),
+}
+
+
+def lib() -> C.CDLL:
+    """Loads libstencil_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -c 'import __graft_entry__ as g; "
+                "g.build()'` (requires nvcc); there is no CPU fallback")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (args, res) in _SIGNATURES.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    return sorted(_SIGNATURES)
+
+
+def last_error() -> str:
+    s = lib().sb200_last_error()
+    return s.decode() if s else ""
+
+
+def _check(status: int) -> int:
+    if status < 0:
+        raise StencilError(status, last_error())
+    return status
+
+
+def _ptr(x) -> int | None:
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    raise TypeError(f"expected a device pointer or tensor, got {type(x)!r}")
+
+
+def _stream(s) -> int | None:
+    if s is None:
+        return None
+    if isinstance(s, int):
+        return s
+    if hasattr(s, "cuda_stream"):
+        return s.cuda_stream
+    raise TypeError(f"expected a cudaStream_t or torch stream, got {type(s)!r}")
+
+
+def _g(grid: Grid):
+    return C.byref(grid.c())
+
+
+def upload_fd_coefficients() -> None:
+    _check(lib().sb200_upload_fd_coefficients())
+
+
+def launch_naive(p_cur, p_prev, vel2, p_next, grid: Grid, stream=None) -> None:
+    _check(lib().sb200_launch_naive(_ptr(p_cur), _ptr(p_prev), _ptr(vel2), _ptr(p_next),
+                                    _g(grid), _stream(stream)))
+
+
+def launch_tiled(p_cur, p_prev, vel2, p_next, grid: Grid, stream=None) -> None:
+    _check(lib().sb200_launch_tiled(_ptr(p_cur), _ptr(p_prev), _ptr(vel2), _ptr(p_next),
+                                    _g(grid), _stream(stream)))
+
+
+def launch_slab(p_cur, p_prev, vel2, p_next, grid: Grid, stream=None) -> None:
+    _check(lib().sb200_launch_slab(_ptr(p_cur), _ptr(p_prev), _ptr(vel2), _ptr(p_next),
+                                   _g(grid), _stream(stream)))
+
+
+def wave_step(p, p_prev, vel2, p_next, grid: Grid, src_index: int = -1, src_amp: float = 0.0,
+              stream=None) -> None:
+    _check(lib().sb200_wave_step_f32(_ptr(p), _ptr(p_prev), _ptr(vel2), _ptr(p_next), _g(grid),
+                                     src_index, src_amp, _stream(stream)))
+
+
+def wave_step_exact(p, p_prev, vel2, p_next, grid: Grid, src_index: int = -1,
+                    src_amp: float = 0.0, stream=None) -> None:
+    _check(lib().sb200_wave_step_exact_f32(_ptr(p), _ptr(p_prev), _ptr(vel2), _ptr(p_next),
+                                           _g(grid), src_index, src_amp, _stream(stream)))
+
+
+def heat_step(u, u_next, grid: Grid, alpha: float, stream=None) -> None:
+    _check(lib().sb200_heat_step_f32(_ptr(u), _ptr(u_next), _g(grid), alpha, _stream(stream)))
+
+
+def model_layered(nx: int, ny: int, nz: int, seed: int, n_layers: int = 8,
+                  v_top: float = 1500.0, v_bottom: float = 4500.0, perturbation: float = 0.05,
+                  corr_cells: float = 20.0, out=None):
+    """Seeded layered v^2 model as a (nz, ny, nx) float32 numpy array; returns (vel2, v_max)."""
+    import numpy as np
+
+    if out is None:
+        out = np.empty((nz, ny, nx), np.float32)
+    vmax = C.c_float()
+    _check(lib().sb200_model_layered(out.ctypes.data, nx, ny, nz, seed, n_layers, v_top,
+                                     v_bottom, perturbation, corr_cells, C.byref(vmax)))
+    return out, float(vmax.value)
+
+
+def ricker(freq: float, t0: float, dt: float, n_steps: int):
+    import numpy as np
+
+    out = np.empty(n_steps, np.float32)
+    _check(lib().sb200_ricker(freq, t0, dt, n_steps, out.ctypes.data))
+    return out
+
+
+def device_error(clear: bool = True) -> int:
+    return _check(lib().sb200_device_error(1 if clear else 0))
+
+
+def variant_names(kind: int = KIND_WAVE_F32):
+    n = _check(lib().sb200_pencil_variant_count(kind))
+    return [lib().sb200_pencil_variant_name(kind, i).decode() for i in range(n)]
+
+
+def set_pencil_override(kind: int, variant: int, zchunks: int = 1) -> None:
+    _check(lib().sb200_set_pencil_override(kind, variant, zchunks))
+
+
+def pencil_choice(kind: int, grid: Grid):
+    v, z = C.c_int(), C.c_int()
+    _check(lib().sb200_pencil_choice(kind, _g(grid), C.byref(v), C.byref(z)))
+    return v.value, z.value

@@ -1,0 +1,299 @@
+// C ABI of the library (include/stencil_b200.h): argument checks, kernel choice,
+// tensor-map setup and error reporting around the sm_100a kernels.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <mutex>
+#include <string>
+
+#include "kernels.h"
+#include "stencil_b200.h"
+
+// Library-wide device error word (one per device context); kernels receive its
+// address and record bounded-wait failures in it.
+__device__ int g_sb200_device_error = 0;
+
+namespace sb200 {
+
+namespace {
+
+thread_local std::string t_last_error;
+
+int fail(int code, const std::string& msg) {
+    t_last_error = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+    return fail(SB200_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+std::mutex g_dev_mu;
+int* g_err_ptr[64] = {};
+
+int* device_error_ptr() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(g_dev_mu);
+    if (!g_err_ptr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_sb200_device_error) != cudaSuccess) return nullptr;
+        g_err_ptr[dev] = static_cast<int*>(p);
+    }
+    return g_err_ptr[dev];
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+int to_desc(const sb200_grid* g, GridDesc* d) {
+    if (!g) return fail(SB200_ERR_INVALID, "grid descriptor is NULL");
+    if (g->nx < 0 || g->ny < 0 || g->nz < 0)
+        return fail(SB200_ERR_INVALID, "negative grid extent");
+    if (g->nx > (1 << 30) || g->ny > (1 << 30) || g->nz > (1 << 30))
+        return fail(SB200_ERR_INVALID, "grid extent above 2^30");
+    if (!(g->dx > 0.f) || !(g->dy > 0.f) || !(g->dz > 0.f) || !std::isfinite(g->dx) ||
+        !std::isfinite(g->dy) || !std::isfinite(g->dz))
+        return fail(SB200_ERR_INVALID, "grid spacing must be positive and finite");
+    if (!std::isfinite(g->dt)) return fail(SB200_ERR_INVALID, "dt must be finite");
+    d->nx = g->nx;
+    d->ny = g->ny;
+    d->nz = g->nz;
+    d->dx = g->dx;
+    d->dy = g->dy;
+    d->dz = g->dz;
+    d->dt = g->dt;
+    return SB200_OK;
+}
+
+// ── pencil configuration: override or heuristic ──────────────────────────────
+
+struct Override {
+    int variant = -1;
+    int zchunks = 1;
+};
+std::mutex g_cfg_mu;
+Override g_override[2];
+
+int sm_count() {
+    int dev = 0, n = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n;
+}
+
+// Chooses zchunks so the CTA count fills whole waves (a wave = SMs x resident
+// CTAs), trading the tail of the last wave against the 8 extra halo planes each
+// chunk reads.
+PencilConfig heuristic(int variant, bool heat, const GridDesc& g) {
+    PencilConfig c;
+    c.variant = variant;
+    const int inz = static_cast<int>(g.nz - 8);
+    const double slots = double(sm_count()) * pencil_f32_resident(variant, heat);
+    double best = -1.0;
+    for (int zc = 1; zc <= 16 && zc <= inz; ++zc) {
+        const double ctas = double(pencil_f32_ctas(variant, g, zc));
+        const double waves = std::ceil(ctas / slots);
+        const double fill = ctas / (waves * slots);
+        const int zlen = (inz + zc - 1) / zc;
+        // Each chunk re-reads 8 halo planes of p; p is 1 of 4 streams (acoustic)
+        // or 1 of 2 (heat).
+        const double pshare = heat ? 0.5 : 0.25;
+        const double halo = double(zlen) / double(zlen + 8) * pshare + (1.0 - pshare);
+        const double score = fill * halo;
+        if (score > best + 1e-9) {
+            best = score;
+            c.zchunks = zc;
+        }
+    }
+    return c;
+}
+
+PencilConfig choose(int kind, const GridDesc& g) {
+    {
+        std::lock_guard<std::mutex> lock(g_cfg_mu);
+        const Override& o = g_override[kind];
+        if (o.variant >= 0) {
+            PencilConfig c;
+            c.variant = o.variant;
+            c.zchunks = std::max(1, o.zchunks);
+            return c;
+        }
+    }
+    return heuristic(0, kind == SB200_KIND_HEAT_F32, g);
+}
+
+bool pencil_ok(const GridDesc& g, std::initializer_list<const void*> ptrs) {
+    if (g.nx % 4 != 0) return false;
+    for (const void* p : ptrs)
+        if (p && !aligned16(p)) return false;
+    return true;
+}
+
+int finish_launch(cudaError_t e, const char* where) {
+    if (e != cudaSuccess) return cuda_fail(e, where);
+    return SB200_OK;
+}
+
+int wave_step(const float* p, const float* p_prev, const float* vel2, float* p_next,
+              const sb200_grid* grid, int64_t src_index, float src_amp, void* stream,
+              bool allow_pencil, const char* where) {
+    GridDesc g;
+    if (int rc = to_desc(grid, &g)) return rc;
+    if (!p || !p_prev || !vel2 || !p_next)
+        return fail(SB200_ERR_INVALID, std::string(where) + ": NULL field pointer");
+    if (p_next == p)
+        return fail(SB200_ERR_INVALID, std::string(where) + ": p_next must not alias p_cur");
+    if (src_index >= g.size())
+        return fail(SB200_ERR_INVALID, std::string(where) + ": source index outside the grid");
+    if (!g.has_interior()) return SB200_OK;  // no interior point: nothing to update
+    auto st = static_cast<cudaStream_t>(stream);
+    if (allow_pencil && pencil_ok(g, {p, p_prev, vel2, p_next})) {
+        CUtensorMap map;
+        const PencilConfig cfg = choose(SB200_KIND_WAVE_F32, g);
+        int bx, by;
+        pencil_f32_box(cfg.variant, &bx, &by);
+        if (int rc = tensor_map_3d(&map, p, g.nx, g.ny, g.nz, 4, bx, by))
+            return fail(SB200_ERR_CUDA, std::string(where) + ": tensor map encode failed (" +
+                                            std::to_string(rc) + ")");
+        SourceDesc src;
+        src.idx = src_index;
+        src.w = src_amp;
+        return finish_launch(launch_wave_pencil_f32(&map, p_prev, vel2, p_next, g, src, cfg,
+                                                    device_error_ptr(), st),
+                             where);
+    }
+    return finish_launch(launch_wave_naive(p, p_prev, vel2, p_next, g, src_index, src_amp, st),
+                         where);
+}
+
+}  // namespace
+}  // namespace sb200
+
+using namespace sb200;
+
+extern "C" {
+
+int sb200_version(void) { return 100; }
+
+const char* sb200_last_error(void) { return t_last_error.c_str(); }
+
+int sb200_device_error(int clear) {
+    int* p = device_error_ptr();
+    if (!p) return fail(SB200_ERR_CUDA, "sb200_device_error: no usable CUDA device");
+    int v = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(&v, g_sb200_device_error, sizeof(int));
+    if (e != cudaSuccess) return cuda_fail(e, "sb200_device_error");
+    if (clear && v) {
+        const int zero = 0;
+        e = cudaMemcpyToSymbol(g_sb200_device_error, &zero, sizeof(int));
+        if (e != cudaSuccess) return cuda_fail(e, "sb200_device_error");
+    }
+    return v;
+}
+
+int sb200_upload_fd_coefficients(void) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaSetDevice(dev);  // initialises the primary context
+    if (e != cudaSuccess) return cuda_fail(e, "sb200_upload_fd_coefficients");
+    return SB200_OK;
+}
+
+int sb200_launch_naive(const float* p_cur, const float* p_prev, const float* vel2,
+                       float* p_next, const sb200_grid* grid, void* stream) {
+    return wave_step(p_cur, p_prev, vel2, p_next, grid, -1, 0.f, stream, false,
+                     "sb200_launch_naive");
+}
+
+int sb200_launch_tiled(const float* p_cur, const float* p_prev, const float* vel2,
+                       float* p_next, const sb200_grid* grid, void* stream) {
+    return wave_step(p_cur, p_prev, vel2, p_next, grid, -1, 0.f, stream, true,
+                     "sb200_launch_tiled");
+}
+
+int sb200_launch_slab(const float* p_cur, const float* p_prev, const float* vel2,
+                      float* p_next, const sb200_grid* grid, void* stream) {
+    return wave_step(p_cur, p_prev, vel2, p_next, grid, -1, 0.f, stream, true,
+                     "sb200_launch_slab");
+}
+
+int sb200_wave_step_f32(const float* p, const float* p_prev, const float* vel2, float* p_next,
+                        const sb200_grid* grid, int64_t src_index, float src_amp,
+                        void* stream) {
+    return wave_step(p, p_prev, vel2, p_next, grid, src_index, src_amp, stream, true,
+                     "sb200_wave_step_f32");
+}
+
+int sb200_wave_step_exact_f32(const float* p, const float* p_prev, const float* vel2,
+                              float* p_next, const sb200_grid* grid, int64_t src_index,
+                              float src_amp, void* stream) {
+    return wave_step(p, p_prev, vel2, p_next, grid, src_index, src_amp, stream, false,
+                     "sb200_wave_step_exact_f32");
+}
+
+int sb200_heat_step_f32(const float* u, float* u_next, const sb200_grid* grid, float alpha,
+                        void* stream) {
+    GridDesc g;
+    if (int rc = to_desc(grid, &g)) return rc;
+    if (!u || !u_next) return fail(SB200_ERR_INVALID, "sb200_heat_step_f32: NULL field pointer");
+    if (u == u_next)
+        return fail(SB200_ERR_INVALID, "sb200_heat_step_f32: u_next must not alias u");
+    if (!std::isfinite(alpha))
+        return fail(SB200_ERR_INVALID, "sb200_heat_step_f32: alpha must be finite");
+    if (!g.has_interior()) return SB200_OK;
+    const float alpha_dt = alpha * g.dt;
+    auto st = static_cast<cudaStream_t>(stream);
+    if (pencil_ok(g, {u, u_next})) {
+        CUtensorMap map;
+        const PencilConfig cfg = choose(SB200_KIND_HEAT_F32, g);
+        int bx, by;
+        pencil_f32_box(cfg.variant, &bx, &by);
+        if (int rc = tensor_map_3d(&map, u, g.nx, g.ny, g.nz, 4, bx, by))
+            return fail(SB200_ERR_CUDA, "sb200_heat_step_f32: tensor map encode failed (" +
+                                            std::to_string(rc) + ")");
+        return finish_launch(
+            launch_heat_pencil_f32(&map, u_next, g, alpha_dt, cfg, device_error_ptr(), st),
+            "sb200_heat_step_f32");
+    }
+    return finish_launch(launch_heat_naive(u, u_next, g, alpha_dt, st), "sb200_heat_step_f32");
+}
+
+int sb200_pencil_variant_count(int kind) {
+    if (kind != SB200_KIND_WAVE_F32 && kind != SB200_KIND_HEAT_F32)
+        return fail(SB200_ERR_INVALID, "unknown kernel kind");
+    return pencil_f32_variant_count();
+}
+
+const char* sb200_pencil_variant_name(int kind, int variant) {
+    if (kind != SB200_KIND_WAVE_F32 && kind != SB200_KIND_HEAT_F32) return nullptr;
+    return pencil_f32_variant_name(variant);
+}
+
+int sb200_set_pencil_override(int kind, int variant, int zchunks) {
+    if (kind != SB200_KIND_WAVE_F32 && kind != SB200_KIND_HEAT_F32)
+        return fail(SB200_ERR_INVALID, "unknown kernel kind");
+    if (variant >= pencil_f32_variant_count())
+        return fail(SB200_ERR_INVALID, "variant out of range");
+    if (zchunks < 1) return fail(SB200_ERR_INVALID, "zchunks must be >= 1");
+    std::lock_guard<std::mutex> lock(g_cfg_mu);
+    g_override[kind].variant = variant;
+    g_override[kind].zchunks = zchunks;
+    return SB200_OK;
+}
+
+int sb200_pencil_choice(int kind, const sb200_grid* grid, int* variant, int* zchunks) {
+    if (kind != SB200_KIND_WAVE_F32 && kind != SB200_KIND_HEAT_F32)
+        return fail(SB200_ERR_INVALID, "unknown kernel kind");
+    GridDesc g;
+    if (int rc = to_desc(grid, &g)) return rc;
+    if (!variant || !zchunks) return fail(SB200_ERR_INVALID, "NULL output pointer");
+    if (!g.has_interior()) return fail(SB200_ERR_INVALID, "grid has no interior");
+    const PencilConfig c = choose(kind, g);
+    *variant = c.variant;
+    *zchunks = c.zchunks;
+    return SB200_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,69 @@
+// Internal launcher interface between the C ABI (capi.cu) and the kernels.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sb200 {
+
+// Halo-inclusive grid, z slowest: idx = (z*ny + y)*nx + x.  Interior is [4, n-4)
+// on every axis (the reference's GridDims convention, include/stencil/types.hpp:115-140).
+struct GridDesc {
+    int64_t nx = 0, ny = 0, nz = 0;
+    float dx = 1.f, dy = 1.f, dz = 1.f, dt = 1.f;
+    bool has_interior() const { return nx > 8 && ny > 8 && nz > 8; }
+    int64_t size() const { return nx * ny * nz; }
+    int64_t interior() const {
+        return has_interior() ? (nx - 8) * (ny - 8) * (nz - 8) : 0;
+    }
+};
+
+// Tile configuration of a pencil launch (chosen by the tuner or a default).
+struct PencilConfig {
+    int variant = 0;  // index into the compiled tile table of the kernel family
+    int zchunks = 1;  // z splits of the interior (1 = march the whole column)
+};
+
+// Source injection for one step: p_next[idx] += (dt^2*vel2[idx]) * w.
+// When wavelet != nullptr the sample is read on the device as
+// wavelet[*step + step_offset], which lets a captured CUDA graph replay a chunk of
+// steps against a device-side step counter.
+struct SourceDesc {
+    int64_t idx = -1;
+    float w = 0.f;
+    const float* wavelet = nullptr;
+    const int* step = nullptr;
+    int step_offset = 0;
+};
+
+cudaError_t launch_wave_naive(const float* cur, const float* prev, const float* vel2,
+                              float* next, const GridDesc& g, int64_t src, float src_w,
+                              cudaStream_t stream);
+cudaError_t launch_heat_naive(const float* u, float* u_next, const GridDesc& g, float alpha_dt,
+                              cudaStream_t stream);
+
+// FP32 pencil kernels.  Preconditions (checked by the caller): nx % 4 == 0,
+// 16-byte aligned pointers, has_interior().  next may alias prev (in place).
+int pencil_f32_variant_count();
+const char* pencil_f32_variant_name(int v);
+cudaError_t launch_wave_pencil_f32(const CUtensorMap* pmap, const float* prev, const float* vel2,
+                                   float* next, const GridDesc& g, const SourceDesc& src,
+                                   const PencilConfig& cfg, int* err, cudaStream_t stream);
+cudaError_t launch_heat_pencil_f32(const CUtensorMap* umap, float* u_next, const GridDesc& g,
+                                   float alpha_dt, const PencilConfig& cfg, int* err,
+                                   cudaStream_t stream);
+// Box (x, y) extent of the tensor map a variant expects for p / u.
+void pencil_f32_box(int variant, int* bx, int* by);
+// Resident CTAs per SM of a variant (occupancy query; analytic if that fails).
+int pencil_f32_resident(int variant, bool heat);
+// Number of CTAs a launch uses (for occupancy/wave reasoning in the tuner).
+int64_t pencil_f32_ctas(int variant, const GridDesc& g, int zchunks);
+
+// Tensor maps (tmap.cpp).  Encodes (and caches) a 3-D tiled map over a
+// halo-inclusive field of element size esize bytes with the given box and copies
+// it to *out.  Returns 0 or a CUresult / -1 (driver entry point unavailable).
+int tensor_map_3d(CUtensorMap* out, const void* base, int64_t nx, int64_t ny, int64_t nz,
+                  int esize, int box_x, int box_y);
+
+}  // namespace sb200

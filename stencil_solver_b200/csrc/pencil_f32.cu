@@ -1,0 +1,493 @@
+// FP32 z-marching pencil kernels for sm_100a: acoustic leapfrog and explicit heat.
+//
+// Replaces the reference's kernel_tiled (src/kernels/stencil_tiled.cu:37-145) and
+// kernel_naive (src/kernels/stencil_naive.cu:49-89) behind launch_tiled / launch_naive.
+//
+// Work unit: one CTA owns a TX x TY tile of interior columns and marches z over
+// [zb, ze) (the whole interior unless the launch splits z into chunks).
+//   * x-y planes of p (with the 4-cell halo: (TX+8) x (TY+8) floats) are fetched by
+//     TMA into an S-stage shared-memory ring; each stage has an mbarrier that the
+//     copy completes (expect_tx / complete_tx).  Thread 0 refills a stage as soon as
+//     the CTA is past its last use, S-4 planes ahead of the first consumer.
+//   * Each thread owns a float4 of x (4 points) in RPT consecutive rows.  Its z
+//     neighbours (z-4..z+4) live in a 9-deep register queue; the loop is unrolled
+//     by 9 so queue slots are compile-time registers and nothing is shifted.
+//   * x and y neighbours come from the staged plane with 128-bit shared loads (a
+//     quarter-warp reads 128 contiguous bytes, so no bank conflicts).
+//   * p_prev and vel2 stream in with 128-bit loads (read once); p_next is written
+//     with 128-bit streaming stores and may alias p_prev (in-place leapfrog).
+// Algorithmic DRAM traffic: acoustic 16 B / interior point (read p, p_prev, vel2;
+// write p_next), heat 8 B (read u, write u_next).  Halo columns shared between
+// neighbouring tiles are re-read from L2, not DRAM.
+#include <algorithm>
+#include <mutex>
+
+#include "kernels.h"
+#include "sb200_common.cuh"
+
+namespace sb200 {
+
+namespace {
+
+struct PencilArgs {
+    const float* prev;  // acoustic: p at t-dt (may alias next); heat: unused
+    const float* vel2;  // acoustic: v^2; heat: unused
+    float* next;
+    int nx, ny, nz;
+    int64_t sy, sz;
+    int tiles_x, tiles_y, zlen;
+    Weights w;  // acoustic: weights * dt^2; heat: weights * alpha*dt
+    float dt2;  // acoustic: dt^2 (source term)
+    int src_x, src_y, src_z;  // -1 when there is no source
+    float src_w;
+    const float* src_wavelet;
+    const int* src_step;
+    int src_off;
+    int* err;
+};
+
+template <int TX, int TY, int RPT, int S>
+struct Shape {
+    static_assert(TX % 4 == 0, "TX must be a multiple of 4 (16-byte TMA origin)");
+    static_assert(TY % RPT == 0, "TY must be a multiple of RPT");
+    static_assert(S >= 8, "ring must hold the 8 planes the queue start-up reads");
+    static constexpr int SX = TX + 2 * R;
+    static constexpr int SY = TY + 2 * R;
+    static_assert(SX <= 256 && SY <= 256, "TMA box extent is at most 256");
+    static constexpr int TPR = TX / 4;
+    static constexpr int NT = TPR * (TY / RPT);
+    static constexpr uint32_t PLANE_BYTES = SX * SY * 4u;            // one TMA box
+    static constexpr int PLANE = int(((PLANE_BYTES + 127u) / 128u) * 32u);  // stage stride (floats), 128-B aligned
+    static constexpr size_t SMEM = size_t(S) * PLANE * 4 + 128;
+    static constexpr int MINB = (512 / NT) > 0 ? (512 / NT) : 1;  // caps registers at 128
+};
+
+// lap[j][i] += coefficient-weighted contributions of one loaded neighbour row k
+// (relative row index, outside the thread's own rows) in the y direction.
+template <int RPT>
+__device__ __forceinline__ void add_y_row(float (&lap)[RPT][4], const float4& v, int k,
+                                          const float (&ay)[R]) {
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+        const int d = k > j ? k - j : j - k;
+        if (d >= 1 && d <= R) {
+            lap[j][0] = fmaf(ay[d - 1], v.x, lap[j][0]);
+            lap[j][1] = fmaf(ay[d - 1], v.y, lap[j][1]);
+            lap[j][2] = fmaf(ay[d - 1], v.z, lap[j][2]);
+            lap[j][3] = fmaf(ay[d - 1], v.w, lap[j][3]);
+        }
+    }
+}
+
+template <int TX, int TY, int RPT, int S, bool HEAT, bool PF>
+__global__ void __launch_bounds__(Shape<TX, TY, RPT, S>::NT, Shape<TX, TY, RPT, S>::MINB)
+    pencil_f32_kernel(const __grid_constant__ CUtensorMap pmap, const PencilArgs a) {
+    using P = Shape<TX, TY, RPT, S>;
+    extern __shared__ unsigned char dsmem[];
+    __shared__ __align__(8) uint64_t full[S];
+    float* sm = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(dsmem) + 127) &
+                                         ~uintptr_t(127));
+
+    const int tid = threadIdx.x;
+    const int lx = tid % P::TPR;
+    const int ly = tid / P::TPR;
+    int b = blockIdx.x;
+    const int tx = b % a.tiles_x;
+    b /= a.tiles_x;
+    const int ty = b % a.tiles_y;
+    b /= a.tiles_y;
+    const int x0 = R + tx * TX;
+    const int y0 = R + ty * TY;
+    const int zb = R + b * a.zlen;
+    const int ze = min(zb + a.zlen, a.nz - R);
+    const int nint = ze - zb;       // interior planes this CTA computes (>= 1)
+    const int nplanes = nint + 2 * R;  // planes it reads (>= 9)
+
+    if (tid == 0) {
+        prefetch_tmap(&pmap);
+#pragma unroll
+        for (int s = 0; s < S; ++s) mbar_init(&full[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    int issued_hi = -1;  // thread 0: highest plane index handed to TMA
+    if (tid == 0) {
+        for (int s = 0; s < S && s < nplanes; ++s) {
+            mbar_arrive_expect_tx(&full[s], P::PLANE_BYTES);
+            tma_load_3d(sm + s * P::PLANE, &pmap, &full[s], x0 - R, y0 - R, zb - R + s);
+            issued_hi = s;
+        }
+    }
+
+    const int gx = x0 + 4 * lx;
+    const int gy = y0 + RPT * ly;
+    const bool xin = gx < a.nx - R;
+    bool rin[RPT];
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) rin[j] = xin && (gy + j < a.ny - R);
+    const int soff = (RPT * ly + R) * P::SX + 4 * lx + R;
+    int64_t goff = static_cast<int64_t>(zb) * a.sz + static_cast<int64_t>(gy) * a.sy + gx;
+
+    // Source ownership: which (row, lane element) of this thread, if any.
+    int src_j = -1, src_i = -1;
+    if (!HEAT && a.src_z >= 0 && a.src_x >= gx && a.src_x < gx + 4 && a.src_y >= gy &&
+        a.src_y < gy + RPT && xin) {
+        src_j = a.src_y - gy;
+        src_i = a.src_x - gx;
+    }
+
+    float ax[R], ay[R], az[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        ax[r] = a.w.ax[r];
+        ay[r] = a.w.ay[r];
+        az[r] = a.w.az[r];
+    }
+
+    float4 q[9][RPT];
+    bool bad = false;
+    // Start-up: planes 0..7 (z = zb-4 .. zb+3) fill queue slots 0..7.
+#pragma unroll
+    for (int jj = 0; jj < 8; ++jj) {
+        if (!mbar_wait(&full[jj % S], (jj / S) & 1)) bad = true;
+        const float* pl = sm + (jj % S) * P::PLANE + soff;
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) q[jj][j] = lds128(pl + j * P::SX);
+    }
+    bool abort_run = __syncthreads_or(bad) != 0;
+    if (!abort_run && tid == 0) {
+        // Planes 0..3 are only queue feed: their stages are free again.
+#pragma unroll
+        for (int jj = 0; jj < R; ++jj) {
+            const int jn = jj + S;
+            if (jn < nplanes) {
+                mbar_arrive_expect_tx(&full[jj], P::PLANE_BYTES);
+                tma_load_3d(sm + jj * P::PLANE, &pmap, &full[jj], x0 - R, y0 - R, zb - R + jn);
+                issued_hi = jn;
+            }
+        }
+    }
+
+    float4 pv_n[RPT], vv_n[RPT];  // next iteration's p_prev / vel2 (PF only)
+    if (PF && !HEAT) {
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) {
+            if (rin[j]) {
+                pv_n[j] = ldg_cs(a.prev + goff + j * a.sy);
+                vv_n[j] = ldg_stream(a.vel2 + goff + j * a.sy);
+            }
+        }
+    }
+
+    for (int i0 = 0; i0 < nint && !abort_run; i0 += 9) {
+#pragma unroll
+        for (int u = 0; u < 9; ++u) {
+            const int i = i0 + u;
+            if (i < nint && !abort_run) {
+                const int cs = (u + 4) % 9;  // centre slot (plane z)
+                // Streamed inputs of this plane.
+                float4 pv[RPT], vv[RPT];
+                if (!HEAT) {
+                    if (PF) {
+#pragma unroll
+                        for (int j = 0; j < RPT; ++j) {
+                            pv[j] = pv_n[j];
+                            vv[j] = vv_n[j];
+                        }
+                        if (i + 1 < nint) {
+#pragma unroll
+                            for (int j = 0; j < RPT; ++j) {
+                                if (rin[j]) {
+                                    pv_n[j] = ldg_cs(a.prev + goff + a.sz + j * a.sy);
+                                    vv_n[j] = ldg_stream(a.vel2 + goff + a.sz + j * a.sy);
+                                }
+                            }
+                        }
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < RPT; ++j) {
+                            if (rin[j]) {
+                                pv[j] = ldg_cs(a.prev + goff + j * a.sy);
+                                vv[j] = ldg_stream(a.vel2 + goff + j * a.sy);
+                            }
+                        }
+                    }
+                }
+                // Queue feed: plane z+4.
+                {
+                    const int jf = i + 8;
+                    if (!mbar_wait(&full[jf % S], (jf / S) & 1)) bad = true;
+                    const float* pf = sm + (jf % S) * P::PLANE + soff;
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) q[(u + 8) % 9][j] = lds128(pf + j * P::SX);
+                }
+                const float* pc = sm + ((i + 4) % S) * P::PLANE + soff;
+
+                float lap[RPT][4];
+#pragma unroll
+                for (int j = 0; j < RPT; ++j) {
+                    const float4 c = q[cs][j];
+                    lap[j][0] = a.w.a0 * c.x;
+                    lap[j][1] = a.w.a0 * c.y;
+                    lap[j][2] = a.w.a0 * c.z;
+                    lap[j][3] = a.w.a0 * c.w;
+                    // z neighbours from the register queue.
+#pragma unroll
+                    for (int r = 1; r <= R; ++r) {
+                        const float4 up = q[(u + 4 + r) % 9][j];
+                        const float4 dn = q[(u + 4 - r + 9) % 9][j];
+                        lap[j][0] = fmaf(az[r - 1], up.x + dn.x, lap[j][0]);
+                        lap[j][1] = fmaf(az[r - 1], up.y + dn.y, lap[j][1]);
+                        lap[j][2] = fmaf(az[r - 1], up.z + dn.z, lap[j][2]);
+                        lap[j][3] = fmaf(az[r - 1], up.w + dn.w, lap[j][3]);
+                    }
+                    // x neighbours: window [left | centre | right].
+                    const float4 lf = lds128(pc + j * P::SX - 4);
+                    const float4 rt = lds128(pc + j * P::SX + 4);
+                    const float win[12] = {lf.x, lf.y, lf.z, lf.w, c.x, c.y,
+                                           c.z,  c.w,  rt.x, rt.y, rt.z, rt.w};
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+#pragma unroll
+                        for (int r = 1; r <= R; ++r)
+                            lap[j][e] = fmaf(ax[r - 1], win[4 + e + r] + win[4 + e - r], lap[j][e]);
+                    }
+                }
+                // y neighbours: rows outside the own block from shared memory,
+                // own rows from the queue centre.
+#pragma unroll
+                for (int k = -R; k < RPT + R; ++k) {
+                    if (k >= 0 && k < RPT) {
+                        add_y_row<RPT>(lap, q[cs][k], k, ay);
+                    } else {
+                        add_y_row<RPT>(lap, lds128(pc + k * P::SX), k, ay);
+                    }
+                }
+                // Update and store.
+                const int z = zb + i;
+#pragma unroll
+                for (int j = 0; j < RPT; ++j) {
+                    const float4 c = q[cs][j];
+                    float4 o;
+                    if (HEAT) {
+                        o.x = c.x + lap[j][0];
+                        o.y = c.y + lap[j][1];
+                        o.z = c.z + lap[j][2];
+                        o.w = c.w + lap[j][3];
+                    } else {
+                        o.x = fmaf(vv[j].x, lap[j][0], fmaf(2.f, c.x, -pv[j].x));
+                        o.y = fmaf(vv[j].y, lap[j][1], fmaf(2.f, c.y, -pv[j].y));
+                        o.z = fmaf(vv[j].z, lap[j][2], fmaf(2.f, c.z, -pv[j].z));
+                        o.w = fmaf(vv[j].w, lap[j][3], fmaf(2.f, c.w, -pv[j].w));
+                        if (src_j == j && z == a.src_z) {
+                            const float wv = a.src_wavelet
+                                                 ? a.src_wavelet[*a.src_step + a.src_off]
+                                                 : a.src_w;
+                            const float kv = a.dt2 * f4get(vv[j], src_i);
+                            const float add = kv * wv;
+                            if (src_i == 0) o.x = o.x + add;
+                            if (src_i == 1) o.y = o.y + add;
+                            if (src_i == 2) o.z = o.z + add;
+                            if (src_i == 3) o.w = o.w + add;
+                        }
+                    }
+                    if (rin[j]) stg_stream(a.next + goff + j * a.sy, o);
+                }
+                goff += a.sz;
+                // The stage of plane z is now free: refill it S planes ahead.
+                abort_run = __syncthreads_or(bad) != 0;
+                if (!abort_run && tid == 0) {
+                    const int jr = i + 4;
+                    const int jn = jr + S;
+                    if (jn < nplanes) {
+                        mbar_arrive_expect_tx(&full[jr % S], P::PLANE_BYTES);
+                        tma_load_3d(sm + (jr % S) * P::PLANE, &pmap, &full[jr % S], x0 - R,
+                                    y0 - R, zb - R + jn);
+                        issued_hi = jn;
+                    }
+                }
+            }
+        }
+    }
+
+    if (abort_run && tid == 0) {
+        record_error(a.err, kDevWaitTimeout);
+        // Let every copy still in flight land before the CTA's shared memory is
+        // released (each stage has at most one outstanding fill).
+        for (int jj = max(0, issued_hi - S + 1); jj <= issued_hi; ++jj)
+            (void)mbar_wait(&full[jj % S], (jj / S) & 1);
+    }
+}
+
+// ── variant table ─────────────────────────────────────────────────────────────
+
+using LaunchFn = cudaError_t (*)(const CUtensorMap*, const PencilArgs&, unsigned, cudaStream_t);
+using ResidentFn = int (*)();
+
+template <int TX, int TY, int RPT, int S, bool HEAT, bool PF>
+cudaError_t launch_variant(const CUtensorMap* map, const PencilArgs& a, unsigned ctas,
+                           cudaStream_t stream) {
+    using P = Shape<TX, TY, RPT, S>;
+    auto kern = pencil_f32_kernel<TX, TY, RPT, S, HEAT, PF>;
+    // The attribute is per function and device; setting it is cheap and idempotent.
+    static std::once_flag once[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaError_t st = cudaSuccess;
+    std::call_once(once[dev & 63], [&] {
+        st = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(P::SMEM));
+    });
+    if (st != cudaSuccess) return st;
+    kern<<<ctas, P::NT, P::SMEM, stream>>>(*map, a);
+    return cudaGetLastError();
+}
+
+// CTAs of a variant that fit on one SM: the occupancy calculator when a device
+// is present, else the shared-memory / register limits computed here.
+template <int TX, int TY, int RPT, int S, bool HEAT, bool PF>
+int resident_variant() {
+    using P = Shape<TX, TY, RPT, S>;
+    static int cached[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cached[dev & 63] > 0) return cached[dev & 63];
+    auto kern = pencil_f32_kernel<TX, TY, RPT, S, HEAT, PF>;
+    int n = 0;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(P::SMEM)) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, P::NT, P::SMEM) == cudaSuccess &&
+        n > 0) {
+        cached[dev & 63] = n;
+        return n;
+    }
+    cudaGetLastError();
+    const int by_smem = int((228u * 1024u) / (P::SMEM + 1024u));
+    const int by_regs = 65536 / (P::NT * 128);
+    return std::max(1, std::min(by_smem, by_regs));
+}
+
+struct Variant {
+    int tx, ty, rpt, stages;
+    bool pf;
+    const char* name;
+    LaunchFn wave, heat;
+    ResidentFn wave_res, heat_res;
+};
+
+#define SB200_VARIANT(TX, TY, RPT, S, PF, NAME)                                              \
+    Variant {                                                                                \
+        TX, TY, RPT, S, PF, NAME, &launch_variant<TX, TY, RPT, S, false, PF>,               \
+            &launch_variant<TX, TY, RPT, S, true, PF>,                                      \
+            &resident_variant<TX, TY, RPT, S, false, PF>,                                   \
+            &resident_variant<TX, TY, RPT, S, true, PF>                                     \
+    }
+
+const Variant kVariants[] = {
+    SB200_VARIANT(32, 32, 2, 8, false, "t32x32_r2_s8"),
+    SB200_VARIANT(64, 16, 2, 8, false, "t64x16_r2_s8"),
+    SB200_VARIANT(32, 16, 1, 8, false, "t32x16_r1_s8"),
+    SB200_VARIANT(64, 32, 2, 8, false, "t64x32_r2_s8"),
+    SB200_VARIANT(32, 64, 2, 8, false, "t32x64_r2_s8"),
+};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+PencilArgs base_args(const GridDesc& g, const PencilConfig& cfg, int* err) {
+    const Variant& v = kVariants[cfg.variant];
+    PencilArgs a{};
+    a.nx = static_cast<int>(g.nx);
+    a.ny = static_cast<int>(g.ny);
+    a.nz = static_cast<int>(g.nz);
+    a.sy = g.nx;
+    a.sz = g.nx * g.ny;
+    a.tiles_x = static_cast<int>((g.nx - 2 * R + v.tx - 1) / v.tx);
+    a.tiles_y = static_cast<int>((g.ny - 2 * R + v.ty - 1) / v.ty);
+    const int inz = static_cast<int>(g.nz - 2 * R);
+    const int zc = std::max(1, std::min(cfg.zchunks, inz));
+    a.zlen = (inz + zc - 1) / zc;
+    a.src_x = a.src_y = a.src_z = -1;
+    a.err = err;
+    return a;
+}
+
+unsigned ctas_of(const PencilArgs& a, const GridDesc& g) {
+    const int inz = static_cast<int>(g.nz - 2 * R);
+    const int zc = (inz + a.zlen - 1) / a.zlen;
+    return static_cast<unsigned>(int64_t(a.tiles_x) * a.tiles_y * zc);
+}
+
+Weights fold_weights(const GridDesc& g, float scale) {
+    const float c[R] = {C1, C2, C3, C4};
+    const float ix2 = 1.0f / (g.dx * g.dx);
+    const float iy2 = 1.0f / (g.dy * g.dy);
+    const float iz2 = 1.0f / (g.dz * g.dz);
+    Weights w;
+    w.a0 = static_cast<float>(static_cast<double>(C0) * (double(ix2) + iy2 + iz2) * scale);
+    for (int r = 0; r < R; ++r) {
+        w.ax[r] = static_cast<float>(double(c[r]) * ix2 * scale);
+        w.ay[r] = static_cast<float>(double(c[r]) * iy2 * scale);
+        w.az[r] = static_cast<float>(double(c[r]) * iz2 * scale);
+    }
+    return w;
+}
+
+}  // namespace
+
+int pencil_f32_variant_count() { return kNumVariants; }
+
+const char* pencil_f32_variant_name(int v) {
+    return (v >= 0 && v < kNumVariants) ? kVariants[v].name : nullptr;
+}
+
+void pencil_f32_box(int variant, int* bx, int* by) {
+    const Variant& v = kVariants[variant];
+    *bx = v.tx + 2 * R;
+    *by = v.ty + 2 * R;
+}
+
+int pencil_f32_resident(int variant, bool heat) {
+    const Variant& v = kVariants[variant];
+    return heat ? v.heat_res() : v.wave_res();
+}
+
+int64_t pencil_f32_ctas(int variant, const GridDesc& g, int zchunks) {
+    PencilConfig c;
+    c.variant = variant;
+    c.zchunks = zchunks;
+    PencilArgs a = base_args(g, c, nullptr);
+    return ctas_of(a, g);
+}
+
+cudaError_t launch_wave_pencil_f32(const CUtensorMap* pmap, const float* prev, const float* vel2,
+                                   float* next, const GridDesc& g, const SourceDesc& src,
+                                   const PencilConfig& cfg, int* err, cudaStream_t stream) {
+    if (!g.has_interior()) return cudaSuccess;
+    PencilArgs a = base_args(g, cfg, err);
+    a.prev = prev;
+    a.vel2 = vel2;
+    a.next = next;
+    a.dt2 = g.dt * g.dt;
+    a.w = fold_weights(g, a.dt2);
+    if (src.idx >= 0) {
+        a.src_x = static_cast<int>(src.idx % g.nx);
+        a.src_y = static_cast<int>((src.idx / g.nx) % g.ny);
+        a.src_z = static_cast<int>(src.idx / (g.nx * g.ny));
+        a.src_w = src.w;
+        a.src_wavelet = src.wavelet;
+        a.src_step = src.step;
+        a.src_off = src.step_offset;
+    }
+    return kVariants[cfg.variant].wave(pmap, a, ctas_of(a, g), stream);
+}
+
+cudaError_t launch_heat_pencil_f32(const CUtensorMap* umap, float* u_next, const GridDesc& g,
+                                   float alpha_dt, const PencilConfig& cfg, int* err,
+                                   cudaStream_t stream) {
+    if (!g.has_interior()) return cudaSuccess;
+    PencilArgs a = base_args(g, cfg, err);
+    a.next = u_next;
+    a.w = fold_weights(g, alpha_dt);
+    return kVariants[cfg.variant].heat(umap, a, ctas_of(a, g), stream);
+}
+
+}  // namespace sb200
