@@ -129,7 +129,7 @@ def cpu_reference_sample(n: int, steps: int, warmup: int, seconds: float | None)
     kind = "reference" if variant else "port"
     sample = (f"{done} steps of a {n}x{n}x{nz} z-slab (interior {n-8}x{n-8}x{nz-8}) of the "
               f"same layered model and source, from rest; "
-              f"{'reference launch_naive CPU path (-O3 -march=x86-64-v3 -fopenmp)' if variant else 'oracle port'}")
+              f"{'reference launch_naive CPU path (-O3 -march=x86-64-v4 -fopenmp)' if variant else 'oracle port'}")
     return interior * done / el / 1e9, cores, sample, kind, done, el, dt, vmax
 
 

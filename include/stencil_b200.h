@@ -89,6 +89,18 @@ int sb200_wave_step_exact_f32(const float* p, const float* p_prev, const float* 
                               float* p_next, const sb200_grid* grid, int64_t src_index,
                               float src_amp, void* stream);
 
+/* sb200_wave_step_f32 with the source sample read on the device as
+ * wavelet[*step + step_offset] (wavelet and step are device pointers), so a
+ * captured CUDA graph of several steps can be replayed at any time offset.
+ * exact != 0 selects the reference-order kernel. */
+int sb200_wave_step_dev_f32(const float* p, const float* p_prev, const float* vel2,
+                            float* p_next, const sb200_grid* grid, int64_t src_index,
+                            const float* wavelet, const int* step, int step_offset, int exact,
+                            void* stream);
+
+/* Writes value to the device int *dst (one-thread kernel, stream-ordered). */
+int sb200_set_device_int(int* dst, int value, void* stream);
+
 /* One explicit heat step u_next = u + alpha*dt*lap(u) with a scalar diffusivity
  * (HeatDiffusionSolver::step_impl without its vel2 field and D2D copy: 8 B/point).
  * u_next must not alias u. */
@@ -112,6 +124,11 @@ int sb200_model_layered(float* vel2, int64_t nx, int64_t ny, int64_t nz, uint64_
 /* Ricker wavelet w(t_n) = (1 - 2 pi^2 f^2 tau^2) exp(-pi^2 f^2 tau^2),
  * tau = n*dt - t0, n = 0..n_steps-1, evaluated in double and rounded to float. */
 int sb200_ricker(double freq, double t0, double dt, int64_t n_steps, float* out);
+
+/* The heat step in the reference's operation order (no FMA contraction):
+ * u_next = u + (alpha*dt) * ((lap_x + lap_y) + lap_z). */
+int sb200_heat_step_exact_f32(const float* u, float* u_next, const sb200_grid* grid,
+                              float alpha, void* stream);
 
 /* ── pencil-kernel configuration (used by the tuner and the tests) ──────────── */
 #define SB200_KIND_WAVE_F32 0

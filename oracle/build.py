@@ -7,7 +7,7 @@ Produces
                                          from its sources where they lie (only
                                          when the reference checkout exists):
       f32_strict : -O3 -ffp-contract=off          (bit-exact pin of the oracle)
-      f32        : -O3 -march=x86-64-v3           (the reference's Release flags
+      f32        : -O3 -march=x86-64-v4           (the reference's Release flags
                                                    with a portable -march so the
                                                    library runs on any host of
                                                    the pool; timed CPU baseline)
@@ -39,7 +39,7 @@ REF_SOURCES = [
 
 REF_VARIANTS = {
     "f32_strict": ["-O3", "-ffp-contract=off"],
-    "f32": ["-O3", "-march=x86-64-v3"],
+    "f32": ["-O3", "-march=x86-64-v4"],
     "f64": ["-O3", "-ffp-contract=off", "-DSTENCIL_FP64"],
 }
 
@@ -93,9 +93,48 @@ def build_reference(force: bool = False) -> dict:
     return built
 
 
+# The reference's own test sources, compiled unchanged against the B200
+# library's drop-in headers (include/stencil/) and libstencil_b200.so, on the
+# GoogleTest-compatible shim in tests/cpp/gtest_shim.  CPU ones only need the
+# library to load; GPU ones exercise the kernels and solvers.
+REF_TESTS_CPU = ["tests/unit/test_fd_coeffs.cpp", "tests/unit/test_grid.cpp",
+                 "tests/unit/test_timer.cpp", "tests/unit/test_io.cpp",
+                 "tests/unit/test_solver_cpu.cpp"]
+REF_TESTS_GPU = ["tests/unit/test_kernels.cpp", "tests/unit/test_solver.cpp",
+                 "tests/integration/test_kernel_correctness.cpp",
+                 "tests/integration/test_wave_3d.cpp", "tests/integration/test_heat_3d.cpp"]
+
+
+def reference_test_binary(src: str) -> pathlib.Path:
+    return HERE / "_ref" / ("reftest_" + pathlib.Path(src).stem)
+
+
+def build_reference_tests(force: bool = False) -> list:
+    """Builds oracle/_ref/reftest_* (needs the reference checkout and the library)."""
+    repo = HERE.parent
+    lib = repo / "stencil_solver_b200" / "lib" / "libstencil_b200.so"
+    if not lib.exists() or not all((REF_ROOT / s).exists() for s in REF_TESTS_CPU + REF_TESTS_GPU):
+        return []
+    (HERE / "_ref").mkdir(exist_ok=True)
+    shim = repo / "tests" / "cpp" / "gtest_shim"
+    headers = list((repo / "include" / "stencil").glob("*")) + [shim / "gtest" / "gtest.h"]
+    out = []
+    for src in REF_TESTS_CPU + REF_TESTS_GPU:
+        exe = reference_test_binary(src)
+        deps = [REF_ROOT / src, shim / "gtest_main.cpp", lib, *headers]
+        if force or _newer(exe, deps):
+            _run(["nvcc", "-std=c++17", "-O2", "-w", "-I", str(repo / "include"), "-I", str(shim),
+                  str(REF_ROOT / src), str(shim / "gtest_main.cpp"), "-o", str(exe),
+                  "-L", str(lib.parent), "-lstencil_b200",
+                  "-Xlinker", "-rpath,$ORIGIN/../../stencil_solver_b200/lib"])
+        out.append(exe)
+    return out
+
+
 def build(force: bool = False) -> None:
     build_oracle(force)
     build_reference(force)
+    build_reference_tests(force)
 
 
 if __name__ == "__main__":

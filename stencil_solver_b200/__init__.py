@@ -88,6 +88,12 @@ _SIGNATURES = {
                                                 C.c_void_p], C.c_int),
     "sb200_wave_step_exact_f32": ([C.c_void_p] * 4 + [C.POINTER(sb200_grid), C.c_int64,
                                       C.c_float, C.c_void_p], C.c_int),
+    "sb200_wave_step_dev_f32": ([C.c_void_p] * 4 + [C.POINTER(sb200_grid), C.c_int64,
+                                    C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p],
+                                   C.c_int),
+    "sb200_set_device_int": ([C.c_void_p, C.c_int, C.c_void_p], C.c_int),
+    "sb200_heat_step_exact_f32": ([C.c_void_p, C.c_void_p, C.POINTER(sb200_grid), C.c_float,
+                                   C.c_void_p], C.c_int),
     "sb200_heat_step_f32": ([C.c_void_p, C.c_void_p, C.POINTER(sb200_grid), C.c_float,
                              C.c_void_p], C.c_int),
     "sb200_model_layered": ([C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_uint64, C.c_int,
@@ -213,6 +219,22 @@ def ricker(freq: float, t0: float, dt: float, n_steps: int):
     out = np.empty(n_steps, np.float32)
     _check(lib().sb200_ricker(freq, t0, dt, n_steps, out.ctypes.data))
     return out
+
+
+def heat_step_exact(u, u_next, grid: Grid, alpha: float, stream=None) -> None:
+    _check(lib().sb200_heat_step_exact_f32(_ptr(u), _ptr(u_next), _g(grid), alpha,
+                                           _stream(stream)))
+
+
+def wave_step_dev(p, p_prev, vel2, p_next, grid: Grid, src_index: int, wavelet, step,
+                  step_offset: int = 0, exact: bool = False, stream=None) -> None:
+    _check(lib().sb200_wave_step_dev_f32(_ptr(p), _ptr(p_prev), _ptr(vel2), _ptr(p_next),
+                                         _g(grid), src_index, _ptr(wavelet), _ptr(step),
+                                         step_offset, 1 if exact else 0, _stream(stream)))
+
+
+def set_device_int(dst, value: int, stream=None) -> None:
+    _check(lib().sb200_set_device_int(_ptr(dst), value, _stream(stream)))
 
 
 def device_error(clear: bool = True) -> int:

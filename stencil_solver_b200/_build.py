@@ -82,7 +82,9 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
     if _stale(LIB, objs):
         tmp = LIB.with_suffix(".so.tmp")
         cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-cudart", "static",
-               "-Xcompiler", "-fopenmp", "-lgomp", "-lpthread", "-ldl", "-lrt"]
+               "-Xcompiler", "-fopenmp", "-lgomp", "-lpthread", "-ldl", "-lrt",
+               # keep the static CUDA runtime private to the library
+               "-Xlinker", "--exclude-libs,ALL"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}{r.stderr}")

@@ -137,8 +137,9 @@ int finish_launch(cudaError_t e, const char* where) {
 }
 
 int wave_step(const float* p, const float* p_prev, const float* vel2, float* p_next,
-              const sb200_grid* grid, int64_t src_index, float src_amp, void* stream,
-              bool allow_pencil, const char* where) {
+              const sb200_grid* grid, const SourceDesc& src, void* stream, bool allow_pencil,
+              const char* where) {
+    const int64_t src_index = src.idx;
     GridDesc g;
     if (int rc = to_desc(grid, &g)) return rc;
     if (!p || !p_prev || !vel2 || !p_next)
@@ -157,15 +158,18 @@ int wave_step(const float* p, const float* p_prev, const float* vel2, float* p_n
         if (int rc = tensor_map_3d(&map, p, g.nx, g.ny, g.nz, 4, bx, by))
             return fail(SB200_ERR_CUDA, std::string(where) + ": tensor map encode failed (" +
                                             std::to_string(rc) + ")");
-        SourceDesc src;
-        src.idx = src_index;
-        src.w = src_amp;
         return finish_launch(launch_wave_pencil_f32(&map, p_prev, vel2, p_next, g, src, cfg,
                                                     device_error_ptr(), st),
                              where);
     }
-    return finish_launch(launch_wave_naive(p, p_prev, vel2, p_next, g, src_index, src_amp, st),
-                         where);
+    return finish_launch(launch_wave_naive(p, p_prev, vel2, p_next, g, src, st), where);
+}
+
+SourceDesc host_source(int64_t idx, float amp) {
+    SourceDesc s;
+    s.idx = idx;
+    s.w = amp;
+    return s;
 }
 
 }  // namespace
@@ -203,34 +207,71 @@ int sb200_upload_fd_coefficients(void) {
 
 int sb200_launch_naive(const float* p_cur, const float* p_prev, const float* vel2,
                        float* p_next, const sb200_grid* grid, void* stream) {
-    return wave_step(p_cur, p_prev, vel2, p_next, grid, -1, 0.f, stream, false,
+    return wave_step(p_cur, p_prev, vel2, p_next, grid, host_source(-1, 0.f), stream, false,
                      "sb200_launch_naive");
 }
 
 int sb200_launch_tiled(const float* p_cur, const float* p_prev, const float* vel2,
                        float* p_next, const sb200_grid* grid, void* stream) {
-    return wave_step(p_cur, p_prev, vel2, p_next, grid, -1, 0.f, stream, true,
+    return wave_step(p_cur, p_prev, vel2, p_next, grid, host_source(-1, 0.f), stream, true,
                      "sb200_launch_tiled");
 }
 
 int sb200_launch_slab(const float* p_cur, const float* p_prev, const float* vel2,
                       float* p_next, const sb200_grid* grid, void* stream) {
-    return wave_step(p_cur, p_prev, vel2, p_next, grid, -1, 0.f, stream, true,
+    return wave_step(p_cur, p_prev, vel2, p_next, grid, host_source(-1, 0.f), stream, true,
                      "sb200_launch_slab");
 }
 
 int sb200_wave_step_f32(const float* p, const float* p_prev, const float* vel2, float* p_next,
                         const sb200_grid* grid, int64_t src_index, float src_amp,
                         void* stream) {
-    return wave_step(p, p_prev, vel2, p_next, grid, src_index, src_amp, stream, true,
-                     "sb200_wave_step_f32");
+    return wave_step(p, p_prev, vel2, p_next, grid, host_source(src_index, src_amp), stream,
+                     true, "sb200_wave_step_f32");
 }
 
 int sb200_wave_step_exact_f32(const float* p, const float* p_prev, const float* vel2,
                               float* p_next, const sb200_grid* grid, int64_t src_index,
                               float src_amp, void* stream) {
-    return wave_step(p, p_prev, vel2, p_next, grid, src_index, src_amp, stream, false,
-                     "sb200_wave_step_exact_f32");
+    return wave_step(p, p_prev, vel2, p_next, grid, host_source(src_index, src_amp), stream,
+                     false, "sb200_wave_step_exact_f32");
+}
+
+int sb200_wave_step_dev_f32(const float* p, const float* p_prev, const float* vel2,
+                            float* p_next, const sb200_grid* grid, int64_t src_index,
+                            const float* wavelet, const int* step, int step_offset, int exact,
+                            void* stream) {
+    if (src_index >= 0 && (!wavelet || !step))
+        return fail(SB200_ERR_INVALID, "sb200_wave_step_dev_f32: NULL wavelet / step pointer");
+    SourceDesc s;
+    s.idx = src_index;
+    s.wavelet = wavelet;
+    s.step = step;
+    s.step_offset = step_offset;
+    return wave_step(p, p_prev, vel2, p_next, grid, s, stream, exact == 0,
+                     "sb200_wave_step_dev_f32");
+}
+
+int sb200_set_device_int(int* dst, int value, void* stream) {
+    if (!dst) return fail(SB200_ERR_INVALID, "sb200_set_device_int: NULL pointer");
+    return finish_launch(launch_set_int(dst, value, static_cast<cudaStream_t>(stream)),
+                         "sb200_set_device_int");
+}
+
+int sb200_heat_step_exact_f32(const float* u, float* u_next, const sb200_grid* grid,
+                              float alpha, void* stream) {
+    GridDesc g;
+    if (int rc = to_desc(grid, &g)) return rc;
+    if (!u || !u_next)
+        return fail(SB200_ERR_INVALID, "sb200_heat_step_exact_f32: NULL field pointer");
+    if (u == u_next)
+        return fail(SB200_ERR_INVALID, "sb200_heat_step_exact_f32: u_next must not alias u");
+    if (!std::isfinite(alpha))
+        return fail(SB200_ERR_INVALID, "sb200_heat_step_exact_f32: alpha must be finite");
+    if (!g.has_interior()) return SB200_OK;
+    return finish_launch(
+        launch_heat_naive(u, u_next, g, alpha * g.dt, static_cast<cudaStream_t>(stream)),
+        "sb200_heat_step_exact_f32");
 }
 
 int sb200_heat_step_f32(const float* u, float* u_next, const sb200_grid* grid, float alpha,

@@ -38,8 +38,9 @@ struct SourceDesc {
 };
 
 cudaError_t launch_wave_naive(const float* cur, const float* prev, const float* vel2,
-                              float* next, const GridDesc& g, int64_t src, float src_w,
+                              float* next, const GridDesc& g, const SourceDesc& src,
                               cudaStream_t stream);
+cudaError_t launch_set_int(int* dst, int value, cudaStream_t stream);
 cudaError_t launch_heat_naive(const float* u, float* u_next, const GridDesc& g, float alpha_dt,
                               cudaStream_t stream);
 

@@ -23,7 +23,10 @@ struct NaiveArgs {
     float inv_dx2, inv_dy2, inv_dz2;
     float k;  // wave: dt^2; heat: alpha*dt
     int64_t src;  // flat source index or -1
-    float src_w;  // wavelet sample for this step
+    float src_w;  // wavelet sample for this step (when wavelet == nullptr)
+    const float* wavelet;  // device samples: wavelet[*step + step_off]
+    const int* step;
+    int step_off;
 };
 
 template <bool kHeat>
@@ -59,14 +62,17 @@ __global__ void __launch_bounds__(256) naive_kernel(NaiveArgs a) {
     } else {
         const float kv = __fmul_rn(a.k, a.vel2[c]);
         out = __fadd_rn(__fsub_rn(__fmul_rn(2.0f, pc), a.prev[c]), __fmul_rn(kv, lap));
-        if (c == a.src) out = __fadd_rn(out, __fmul_rn(kv, a.src_w));
+        if (c == a.src) {
+            const float w = a.wavelet ? a.wavelet[*a.step + a.step_off] : a.src_w;
+            out = __fadd_rn(out, __fmul_rn(kv, w));
+        }
     }
     a.next[c] = out;
 }
 
 NaiveArgs make_args(const float* cur, const float* prev, const float* vel2, float* next,
                     const GridDesc& g, float k, int64_t src, float src_w) {
-    NaiveArgs a;
+    NaiveArgs a{};
     a.cur = cur;
     a.prev = prev;
     a.vel2 = vel2;
@@ -95,13 +101,25 @@ dim3 naive_grid(const GridDesc& g, dim3 block) {
 }  // namespace
 
 cudaError_t launch_wave_naive(const float* cur, const float* prev, const float* vel2,
-                              float* next, const GridDesc& g, int64_t src, float src_w,
+                              float* next, const GridDesc& g, const SourceDesc& src,
                               cudaStream_t stream) {
     if (!g.has_interior()) return cudaSuccess;
     const float dt2 = g.dt * g.dt;
     const dim3 block(32, 4, 2);
-    naive_kernel<false><<<naive_grid(g, block), block, 0, stream>>>(
-        make_args(cur, prev, vel2, next, g, dt2, src, src_w));
+    NaiveArgs a = make_args(cur, prev, vel2, next, g, dt2, src.idx, src.w);
+    a.wavelet = src.wavelet;
+    a.step = src.step;
+    a.step_off = src.step_offset;
+    naive_kernel<false><<<naive_grid(g, block), block, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+namespace {
+__global__ void set_int_kernel(int* dst, int value) { *dst = value; }
+}  // namespace
+
+cudaError_t launch_set_int(int* dst, int value, cudaStream_t stream) {
+    set_int_kernel<<<1, 1, 0, stream>>>(dst, value);
     return cudaGetLastError();
 }
 

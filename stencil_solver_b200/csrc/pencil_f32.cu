@@ -62,19 +62,19 @@ struct Shape {
     static constexpr int MINB = (512 / NT) > 0 ? (512 / NT) : 1;  // caps registers at 128
 };
 
-// lap[j][i] += coefficient-weighted contributions of one loaded neighbour row k
-// (relative row index, outside the thread's own rows) in the y direction.
+// ya[j][i] += weighted contributions of neighbour row k (row index relative to
+// the thread's first own row) to the y sums of the thread's own rows.
 template <int RPT>
-__device__ __forceinline__ void add_y_row(float (&lap)[RPT][4], const float4& v, int k,
+__device__ __forceinline__ void add_y_row(float (&ya)[RPT][4], const float4& v, int k,
                                           const float (&ay)[R]) {
 #pragma unroll
     for (int j = 0; j < RPT; ++j) {
         const int d = k > j ? k - j : j - k;
         if (d >= 1 && d <= R) {
-            lap[j][0] = fmaf(ay[d - 1], v.x, lap[j][0]);
-            lap[j][1] = fmaf(ay[d - 1], v.y, lap[j][1]);
-            lap[j][2] = fmaf(ay[d - 1], v.z, lap[j][2]);
-            lap[j][3] = fmaf(ay[d - 1], v.w, lap[j][3]);
+            ya[j][0] = fmaf(ay[d - 1], v.x, ya[j][0]);
+            ya[j][1] = fmaf(ay[d - 1], v.y, ya[j][1]);
+            ya[j][2] = fmaf(ay[d - 1], v.z, ya[j][2]);
+            ya[j][3] = fmaf(ay[d - 1], v.w, ya[j][3]);
         }
     }
 }
@@ -223,44 +223,42 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S>::NT, Shape<TX, TY, RPT, 
                 }
                 const float* pc = sm + ((i + 4) % S) * P::PLANE + soff;
 
+                // y: neighbour rows outside the own block from shared memory, own
+                // rows from the queue centre, accumulated from zero in row order
+                // (farthest rows, smallest weights, first).
+                float ya[RPT][4];
+#pragma unroll
+                for (int j = 0; j < RPT; ++j) ya[j][0] = ya[j][1] = ya[j][2] = ya[j][3] = 0.f;
+#pragma unroll
+                for (int k = -R; k < RPT + R; ++k) {
+                    if (k >= 0 && k < RPT) {
+                        add_y_row<RPT>(ya, q[cs][k], k, ay);
+                    } else {
+                        add_y_row<RPT>(ya, lds128(pc + k * P::SX), k, ay);
+                    }
+                }
                 float lap[RPT][4];
 #pragma unroll
                 for (int j = 0; j < RPT; ++j) {
                     const float4 c = q[cs][j];
-                    lap[j][0] = a.w.a0 * c.x;
-                    lap[j][1] = a.w.a0 * c.y;
-                    lap[j][2] = a.w.a0 * c.z;
-                    lap[j][3] = a.w.a0 * c.w;
-                    // z neighbours from the register queue.
-#pragma unroll
-                    for (int r = 1; r <= R; ++r) {
-                        const float4 up = q[(u + 4 + r) % 9][j];
-                        const float4 dn = q[(u + 4 - r + 9) % 9][j];
-                        lap[j][0] = fmaf(az[r - 1], up.x + dn.x, lap[j][0]);
-                        lap[j][1] = fmaf(az[r - 1], up.y + dn.y, lap[j][1]);
-                        lap[j][2] = fmaf(az[r - 1], up.z + dn.z, lap[j][2]);
-                        lap[j][3] = fmaf(az[r - 1], up.w + dn.w, lap[j][3]);
-                    }
-                    // x neighbours: window [left | centre | right].
                     const float4 lf = lds128(pc + j * P::SX - 4);
                     const float4 rt = lds128(pc + j * P::SX + 4);
                     const float win[12] = {lf.x, lf.y, lf.z, lf.w, c.x, c.y,
                                            c.z,  c.w,  rt.x, rt.y, rt.z, rt.w};
 #pragma unroll
                     for (int e = 0; e < 4; ++e) {
+                        const float ce = win[4 + e];
+                        float tz = a.w.cz * ce;
+                        float tx = a.w.cx * ce;
 #pragma unroll
-                        for (int r = 1; r <= R; ++r)
-                            lap[j][e] = fmaf(ax[r - 1], win[4 + e + r] + win[4 + e - r], lap[j][e]);
-                    }
-                }
-                // y neighbours: rows outside the own block from shared memory,
-                // own rows from the queue centre.
-#pragma unroll
-                for (int k = -R; k < RPT + R; ++k) {
-                    if (k >= 0 && k < RPT) {
-                        add_y_row<RPT>(lap, q[cs][k], k, ay);
-                    } else {
-                        add_y_row<RPT>(lap, lds128(pc + k * P::SX), k, ay);
+                        for (int r = 1; r <= R; ++r) {
+                            const float up = f4get(q[(u + 4 + r) % 9][j], e);
+                            const float dn = f4get(q[(u + 4 - r + 9) % 9][j], e);
+                            tz = fmaf(az[r - 1], up + dn, tz);
+                            tx = fmaf(ax[r - 1], win[4 + e + r] + win[4 + e - r], tx);
+                        }
+                        const float ty = fmaf(a.w.cy, ce, ya[j][e]);
+                        lap[j][e] = (tx + ty) + tz;
                     }
                 }
                 // Update and store.
@@ -422,7 +420,9 @@ Weights fold_weights(const GridDesc& g, float scale) {
     const float iy2 = 1.0f / (g.dy * g.dy);
     const float iz2 = 1.0f / (g.dz * g.dz);
     Weights w;
-    w.a0 = static_cast<float>(static_cast<double>(C0) * (double(ix2) + iy2 + iz2) * scale);
+    w.cx = static_cast<float>(double(C0) * ix2 * scale);
+    w.cy = static_cast<float>(double(C0) * iy2 * scale);
+    w.cz = static_cast<float>(double(C0) * iz2 * scale);
     for (int r = 0; r < R; ++r) {
         w.ax[r] = static_cast<float>(double(c[r]) * ix2 * scale);
         w.ay[r] = static_cast<float>(double(c[r]) * iy2 * scale);

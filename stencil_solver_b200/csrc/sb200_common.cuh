@@ -19,10 +19,13 @@ constexpr float C2 = static_cast<float>(-1.0 / 5.0);
 constexpr float C3 = static_cast<float>(8.0 / 315.0);
 constexpr float C4 = static_cast<float>(-1.0 / 560.0);
 
-// Laplacian weights with the grid spacing folded in (computed on the host once
-// per launch): lap = a0*p + sum_r ax[r]*(x-pair) + ay[r]*(y-pair) + az[r]*(z-pair).
+// Laplacian weights with the grid spacing (and the time-step factor) folded in,
+// computed on the host once per launch.  Per axis a:
+//   lap_a = ca*p + sum_r aa[r]*(p[+r] + p[-r]),   lap = (lap_x + lap_y) + lap_z,
+// evaluated so that each axis' large centre term cancels against its r = 1 pair
+// in one fused step, as the reference's per-axis sums do.
 struct Weights {
-    float a0;
+    float cx, cy, cz;
     float ax[R], ay[R], az[R];
 };
 

@@ -33,6 +33,7 @@ def _built():
         from stencil_solver_b200 import _build
 
         _build.build()
+    obuild.build_reference_tests()
     yield
 
 

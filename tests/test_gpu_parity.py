@@ -170,14 +170,12 @@ def test_acoustic_config_full_run(torch_cuda):
     p = dev(torch_cuda, np.zeros(shape, np.float32))
     q = dev(torch_cuda, np.zeros(shape, np.float32))
     v = dev(torch_cuda, np.full(shape, 2000.0 ** 2, np.float32))
-    trace = []
-    flat_q = None
+    trace = torch_cuda.empty(steps, dtype=torch_cuda.float32, device="cuda")
     for s in range(steps):
         sb.wave_step(p, q, v, q, g, src, float(np.float32(w[s])))
-        flat_q = q.view(-1)
-        trace.append(flat_q[src])
+        trace[s] = q.view(-1)[src]  # device-side copy of the sample
         p, q = q, p
-    tr = np.array([float(t) for t in trace], np.float32)
+    tr = host(trace)
     fin = host(p)
     assert rel(fin[n // 2], f["mid32"]) <= RUN_TOL
     assert rel(tr, f["trace32"]) <= RUN_TOL
