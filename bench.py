@@ -50,6 +50,9 @@ def args_():
     ap.add_argument("--e2e-steps", type=int, default=CONFIG_STEPS)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (heuristic tile)")
+    ap.add_argument("--variant", type=int, default=-1, help="force a pencil variant (profiling)")
+    ap.add_argument("--zchunks", type=int, default=1)
     return ap.parse_args()
 
 
@@ -257,6 +260,13 @@ def run_ours(a):
     q = torch.zeros_like(p)
     v = torch.from_numpy(vel2).cuda()
     step = 0
+    tuned = None
+    if a.variant >= 0:
+        sb.set_pencil_override(sb.KIND_WAVE_F32, a.variant, a.zchunks)
+    elif not a.no_tune:  # untimed: pick the tile shape / z split for this grid
+        scratch = torch.empty_like(p)
+        tuned = sb.tune(sb.KIND_WAVE_F32, g, p, q, v, scratch, reps=2)
+        del scratch
 
     def one():
         nonlocal p, q, step
@@ -276,8 +286,10 @@ def run_ours(a):
     e1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record(stream)
+    h0 = time.perf_counter()
     for _ in range(a.steps):
         one()
+    host_issue_ms = (time.perf_counter() - h0) * 1e3 / a.steps  # launch cost on the host
     e1.record(stream)
     torch.cuda.synchronize()
     if pg:
@@ -351,17 +363,19 @@ def run_ours(a):
         cv, cores, sample, kind, *_ = cpu_reference_sample(n, 1, 2, a.cpu_seconds)
         cpu = {"value": cv, "unit": "Gpts/s", "cores": cores, "kind": kind, "sample": sample}
 
-    vname = sb.variant_names()[sb.pencil_choice(sb.KIND_WAVE_F32, g)[0]]
+    choice = sb.pencil_choice(sb.KIND_WAVE_F32, g)
+    vname = sb.variant_names()[choice[0]]
     line = {
         "metric": "acoustic interior grid-point updates per second",
         "value": value, "unit": "Gpts/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_desc(n, g.dt, vmax) | {"parallelism": f"replicas{world}",
-                                               "tile": vname,
-                                               "zchunks": sb.pencil_choice(sb.KIND_WAVE_F32, g)[1]},
+                                               "tile": vname, "zchunks": choice[1],
+                                               "tuned": tuned is not None},
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
         "gpu_launches": a.steps,
+        "host_issue_ms_per_step": host_issue_ms,
     }
     if pg:
         pg.barrier()

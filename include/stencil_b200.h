@@ -141,6 +141,21 @@ int sb200_set_pencil_override(int kind, int variant, int zchunks);
 /* The (variant, zchunks) the next launch of `kind` on `grid` would use. */
 int sb200_pencil_choice(int kind, const sb200_grid* grid, int* variant, int* zchunks);
 
+/* ── autotuner ──────────────────────────────────────────────────────────────
+ * Times every compiled tile variant of `kind` at its three best-filling z splits
+ * on `grid` (reps launches each after one warm-up, CUDA events, legacy default
+ * stream, synchronous) and records the fastest for later launches of that kind
+ * on that grid and device.  The stencil reads field (and, for the acoustic kind,
+ * prev and vel2) and writes only `scratch`, a caller buffer of the grid's size
+ * that aliases none of them.  Outputs are optional. */
+int sb200_tune(int kind, const sb200_grid* grid, const void* field, const void* prev,
+               const void* vel2, void* scratch, int reps, int* variant, int* zchunks,
+               float* best_ms);
+/* Saves / loads the tuned table ("kind nx ny nz variant zchunks ms device" per
+ * line).  Load returns the number of entries read or a negative status. */
+int sb200_tune_save(const char* path);
+int sb200_tune_load(const char* path);
+
 #ifdef __cplusplus
 }
 #endif

@@ -100,6 +100,11 @@ _SIGNATURES = {
                              C.c_float, C.c_float, C.c_float, C.c_float,
                              C.POINTER(C.c_float)], C.c_int),
     "sb200_ricker": ([C.c_double, C.c_double, C.c_double, C.c_int64, C.c_void_p], C.c_int),
+    "sb200_tune": ([C.c_int, C.POINTER(sb200_grid)] + [C.c_void_p] * 4 +
+                   [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_float)],
+                   C.c_int),
+    "sb200_tune_save": ([C.c_char_p], C.c_int),
+    "sb200_tune_load": ([C.c_char_p], C.c_int),
     "sb200_pencil_variant_count": ([C.c_int], C.c_int),
     "sb200_pencil_variant_name": ([C.c_int, C.c_int], C.c_char_p),
     "sb200_set_pencil_override": ([C.c_int, C.c_int, C.c_int], C.c_int),
@@ -244,6 +249,22 @@ def device_error(clear: bool = True) -> int:
 def variant_names(kind: int = KIND_WAVE_F32):
     n = _check(lib().sb200_pencil_variant_count(kind))
     return [lib().sb200_pencil_variant_name(kind, i).decode() for i in range(n)]
+
+
+def tune(kind: int, grid: Grid, field, prev, vel2, scratch, reps: int = 3):
+    """Autotunes the pencil tile / z split for kind on grid; returns (variant, zchunks, ms)."""
+    v, z, ms = C.c_int(), C.c_int(), C.c_float()
+    _check(lib().sb200_tune(kind, _g(grid), _ptr(field), _ptr(prev), _ptr(vel2), _ptr(scratch),
+                            reps, C.byref(v), C.byref(z), C.byref(ms)))
+    return v.value, z.value, ms.value
+
+
+def tune_save(path: str) -> None:
+    _check(lib().sb200_tune_save(str(path).encode()))
+
+
+def tune_load(path: str) -> int:
+    return _check(lib().sb200_tune_load(str(path).encode()))
 
 
 def set_pencil_override(kind: int, variant: int, zchunks: int = 1) -> None:

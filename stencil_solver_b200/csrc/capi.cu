@@ -5,8 +5,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 
 #include "kernels.h"
 #include "stencil_b200.h"
@@ -83,33 +85,6 @@ int sm_count() {
     return n;
 }
 
-// Chooses zchunks so the CTA count fills whole waves (a wave = SMs x resident
-// CTAs), trading the tail of the last wave against the 8 extra halo planes each
-// chunk reads.
-PencilConfig heuristic(int variant, bool heat, const GridDesc& g) {
-    PencilConfig c;
-    c.variant = variant;
-    const int inz = static_cast<int>(g.nz - 8);
-    const double slots = double(sm_count()) * pencil_f32_resident(variant, heat);
-    double best = -1.0;
-    for (int zc = 1; zc <= 16 && zc <= inz; ++zc) {
-        const double ctas = double(pencil_f32_ctas(variant, g, zc));
-        const double waves = std::ceil(ctas / slots);
-        const double fill = ctas / (waves * slots);
-        const int zlen = (inz + zc - 1) / zc;
-        // Each chunk re-reads 8 halo planes of p; p is 1 of 4 streams (acoustic)
-        // or 1 of 2 (heat).
-        const double pshare = heat ? 0.5 : 0.25;
-        const double halo = double(zlen) / double(zlen + 8) * pshare + (1.0 - pshare);
-        const double score = fill * halo;
-        if (score > best + 1e-9) {
-            best = score;
-            c.zchunks = zc;
-        }
-    }
-    return c;
-}
-
 PencilConfig choose(int kind, const GridDesc& g) {
     {
         std::lock_guard<std::mutex> lock(g_cfg_mu);
@@ -121,7 +96,22 @@ PencilConfig choose(int kind, const GridDesc& g) {
             return c;
         }
     }
-    return heuristic(0, kind == SB200_KIND_HEAT_F32, g);
+    PencilConfig c;
+    if (tuned_choice(kind, g, &c)) return c;
+    // Heuristic pick, memoised per (kind, extents, device): launches stay cheap
+    // on the host.
+    static std::mutex memo_mu;
+    static std::map<std::tuple<int, int64_t, int64_t, int64_t, int>, PencilConfig> memo;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const auto key = std::make_tuple(kind, g.nx, g.ny, g.nz, dev);
+    std::lock_guard<std::mutex> lock(memo_mu);
+    auto it = memo.find(key);
+    if (it != memo.end()) return it->second;
+    c.variant = 0;
+    c.zchunks = zchunk_ranking(kind == SB200_KIND_HEAT_F32, 0, g, 1).front();
+    memo[key] = c;
+    return c;
 }
 
 bool pencil_ok(const GridDesc& g, std::initializer_list<const void*> ptrs) {
@@ -133,6 +123,25 @@ bool pencil_ok(const GridDesc& g, std::initializer_list<const void*> ptrs) {
 
 int finish_launch(cudaError_t e, const char* where) {
     if (e != cudaSuccess) return cuda_fail(e, where);
+    return SB200_OK;
+}
+
+// Encodes the tensor maps a pencil variant reads: the haloed box over the
+// stencil field and, where the variant stages them by TMA, the tile box over
+// p_prev and vel2.
+int pencil_maps(bool heat, int v, const GridDesc& g, const void* field, const void* prev,
+                const void* vel2, PencilMaps* m, const char* where) {
+    const PencilBoxes b = pencil_f32_boxes(heat, v);
+    int rc = tensor_map_3d(&m->p, field, g.nx, g.ny, g.nz, 4, b.halo_x, b.halo_y);
+    m->prev = m->p;
+    m->vel2 = m->p;
+    if (!rc && b.aux_tma) {
+        rc = tensor_map_3d(&m->prev, prev, g.nx, g.ny, g.nz, 4, b.tile_x, b.tile_y);
+        if (!rc) rc = tensor_map_3d(&m->vel2, vel2, g.nx, g.ny, g.nz, 4, b.tile_x, b.tile_y);
+    }
+    if (rc)
+        return fail(SB200_ERR_CUDA, std::string(where) + ": tensor map encode failed (" +
+                                        std::to_string(rc) + ")");
     return SB200_OK;
 }
 
@@ -151,14 +160,10 @@ int wave_step(const float* p, const float* p_prev, const float* vel2, float* p_n
     if (!g.has_interior()) return SB200_OK;  // no interior point: nothing to update
     auto st = static_cast<cudaStream_t>(stream);
     if (allow_pencil && pencil_ok(g, {p, p_prev, vel2, p_next})) {
-        CUtensorMap map;
         const PencilConfig cfg = choose(SB200_KIND_WAVE_F32, g);
-        int bx, by;
-        pencil_f32_box(cfg.variant, &bx, &by);
-        if (int rc = tensor_map_3d(&map, p, g.nx, g.ny, g.nz, 4, bx, by))
-            return fail(SB200_ERR_CUDA, std::string(where) + ": tensor map encode failed (" +
-                                            std::to_string(rc) + ")");
-        return finish_launch(launch_wave_pencil_f32(&map, p_prev, vel2, p_next, g, src, cfg,
+        PencilMaps maps;
+        if (int rc = pencil_maps(false, cfg.variant, g, p, p_prev, vel2, &maps, where)) return rc;
+        return finish_launch(launch_wave_pencil_f32(maps, p_prev, vel2, p_next, g, src, cfg,
                                                     device_error_ptr(), st),
                              where);
     }
@@ -173,6 +178,34 @@ SourceDesc host_source(int64_t idx, float amp) {
 }
 
 }  // namespace
+
+// A wave is SMs x resident CTAs; a split whose CTA count leaves the last wave
+// mostly empty wastes that fraction of the machine, and every extra split
+// re-reads 8 halo planes of p (p is 1 of 4 streams for the acoustic kernel,
+// 1 of 2 for heat).
+std::vector<int> zchunk_ranking(bool heat, int v, const GridDesc& g, int max_n) {
+    const int inz = static_cast<int>(g.nz - 8);
+    const double slots = double(sm_count()) * std::max(1, pencil_f32_resident(heat, v));
+    std::vector<std::pair<double, int>> scored;
+    for (int zc = 1; zc <= 16 && zc <= inz; ++zc) {
+        const double ctas = double(pencil_f32_ctas(heat, v, g, zc));
+        const double waves = std::ceil(ctas / slots);
+        const double fill = ctas / (waves * slots);
+        const int zlen = (inz + zc - 1) / zc;
+        const double pshare = heat ? 0.5 : 0.25;
+        const double halo = double(zlen) / double(zlen + 8) * pshare + (1.0 - pshare);
+        scored.emplace_back(-(fill * halo), zc);
+    }
+    std::stable_sort(scored.begin(), scored.end());
+    std::vector<int> out;
+    for (const auto& s : scored) {
+        if (static_cast<int>(out.size()) >= max_n) break;
+        out.push_back(s.second);
+    }
+    if (out.empty()) out.push_back(1);
+    return out;
+}
+
 }  // namespace sb200
 
 using namespace sb200;
@@ -287,15 +320,13 @@ int sb200_heat_step_f32(const float* u, float* u_next, const sb200_grid* grid, f
     const float alpha_dt = alpha * g.dt;
     auto st = static_cast<cudaStream_t>(stream);
     if (pencil_ok(g, {u, u_next})) {
-        CUtensorMap map;
         const PencilConfig cfg = choose(SB200_KIND_HEAT_F32, g);
-        int bx, by;
-        pencil_f32_box(cfg.variant, &bx, &by);
-        if (int rc = tensor_map_3d(&map, u, g.nx, g.ny, g.nz, 4, bx, by))
-            return fail(SB200_ERR_CUDA, "sb200_heat_step_f32: tensor map encode failed (" +
-                                            std::to_string(rc) + ")");
+        PencilMaps maps;
+        if (int rc = pencil_maps(true, cfg.variant, g, u, nullptr, nullptr, &maps,
+                                 "sb200_heat_step_f32"))
+            return rc;
         return finish_launch(
-            launch_heat_pencil_f32(&map, u_next, g, alpha_dt, cfg, device_error_ptr(), st),
+            launch_heat_pencil_f32(maps, u_next, g, alpha_dt, cfg, device_error_ptr(), st),
             "sb200_heat_step_f32");
     }
     return finish_launch(launch_heat_naive(u, u_next, g, alpha_dt, st), "sb200_heat_step_f32");
@@ -304,18 +335,18 @@ int sb200_heat_step_f32(const float* u, float* u_next, const sb200_grid* grid, f
 int sb200_pencil_variant_count(int kind) {
     if (kind != SB200_KIND_WAVE_F32 && kind != SB200_KIND_HEAT_F32)
         return fail(SB200_ERR_INVALID, "unknown kernel kind");
-    return pencil_f32_variant_count();
+    return pencil_f32_variant_count(kind == SB200_KIND_HEAT_F32);
 }
 
 const char* sb200_pencil_variant_name(int kind, int variant) {
     if (kind != SB200_KIND_WAVE_F32 && kind != SB200_KIND_HEAT_F32) return nullptr;
-    return pencil_f32_variant_name(variant);
+    return pencil_f32_variant_name(kind == SB200_KIND_HEAT_F32, variant);
 }
 
 int sb200_set_pencil_override(int kind, int variant, int zchunks) {
     if (kind != SB200_KIND_WAVE_F32 && kind != SB200_KIND_HEAT_F32)
         return fail(SB200_ERR_INVALID, "unknown kernel kind");
-    if (variant >= pencil_f32_variant_count())
+    if (variant >= pencil_f32_variant_count(kind == SB200_KIND_HEAT_F32))
         return fail(SB200_ERR_INVALID, "variant out of range");
     if (zchunks < 1) return fail(SB200_ERR_INVALID, "zchunks must be >= 1");
     std::lock_guard<std::mutex> lock(g_cfg_mu);

@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 namespace sb200 {
 
 // Halo-inclusive grid, z slowest: idx = (z*ny + y)*nx + x.  Interior is [4, n-4)
@@ -44,22 +46,44 @@ cudaError_t launch_set_int(int* dst, int value, cudaStream_t stream);
 cudaError_t launch_heat_naive(const float* u, float* u_next, const GridDesc& g, float alpha_dt,
                               cudaStream_t stream);
 
+// Tensor maps of one pencil launch: p (or u) with the halo box, and -- for the
+// acoustic variants that stage them through TMA -- p_prev and vel2 with the
+// interior tile box.  Unused maps may hold any valid map.
+struct PencilMaps {
+    CUtensorMap p, prev, vel2;
+};
+
+// TMA boxes a variant needs.
+struct PencilBoxes {
+    int halo_x = 0, halo_y = 0;  // p / u box: tile + 4-cell halo on each side
+    int tile_x = 0, tile_y = 0;  // p_prev / vel2 box
+    bool aux_tma = false;        // whether p_prev / vel2 go through TMA
+};
+
 // FP32 pencil kernels.  Preconditions (checked by the caller): nx % 4 == 0,
 // 16-byte aligned pointers, has_interior().  next may alias prev (in place).
-int pencil_f32_variant_count();
-const char* pencil_f32_variant_name(int v);
-cudaError_t launch_wave_pencil_f32(const CUtensorMap* pmap, const float* prev, const float* vel2,
+int pencil_f32_variant_count(bool heat);
+const char* pencil_f32_variant_name(bool heat, int v);
+PencilBoxes pencil_f32_boxes(bool heat, int v);
+cudaError_t launch_wave_pencil_f32(const PencilMaps& maps, const float* prev, const float* vel2,
                                    float* next, const GridDesc& g, const SourceDesc& src,
                                    const PencilConfig& cfg, int* err, cudaStream_t stream);
-cudaError_t launch_heat_pencil_f32(const CUtensorMap* umap, float* u_next, const GridDesc& g,
+cudaError_t launch_heat_pencil_f32(const PencilMaps& maps, float* u_next, const GridDesc& g,
                                    float alpha_dt, const PencilConfig& cfg, int* err,
                                    cudaStream_t stream);
-// Box (x, y) extent of the tensor map a variant expects for p / u.
-void pencil_f32_box(int variant, int* bx, int* by);
 // Resident CTAs per SM of a variant (occupancy query; analytic if that fails).
-int pencil_f32_resident(int variant, bool heat);
+int pencil_f32_resident(bool heat, int v);
 // Number of CTAs a launch uses (for occupancy/wave reasoning in the tuner).
-int64_t pencil_f32_ctas(int variant, const GridDesc& g, int zchunks);
+int64_t pencil_f32_ctas(bool heat, int v, const GridDesc& g, int zchunks);
+
+// z splits of variant v on grid g ranked by how well their CTA count fills whole
+// waves (SMs x resident CTAs), discounted by the 8 halo planes each extra split
+// re-reads; the first max_n (capi.cu).
+std::vector<int> zchunk_ranking(bool heat, int v, const GridDesc& g, int max_n);
+
+// Tuned (variant, zchunks) for kind on grid g on the current device, if the
+// tuner has one (tuner.cpp).
+bool tuned_choice(int kind, const GridDesc& g, PencilConfig* out);
 
 // Tensor maps (tmap.cpp).  Encodes (and caches) a 3-D tiled map over a
 // halo-inclusive field of element size esize bytes with the given box and copies

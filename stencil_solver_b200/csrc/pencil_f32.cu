@@ -9,16 +9,21 @@
 //     TMA into an S-stage shared-memory ring; each stage has an mbarrier that the
 //     copy completes (expect_tx / complete_tx).  Thread 0 refills a stage as soon as
 //     the CTA is past its last use, S-4 planes ahead of the first consumer.
+//   * Acoustic: the TX x TY tiles of p_prev and vel2 for plane z come by TMA into a
+//     second AUX-stage ring, AUX-1 planes ahead of their use (AUX = 0 instead loads
+//     them with 128-bit global loads at the start of the plane).
 //   * Each thread owns a float4 of x (4 points) in RPT consecutive rows.  Its z
 //     neighbours (z-4..z+4) live in a 9-deep register queue; the loop is unrolled
 //     by 9 so queue slots are compile-time registers and nothing is shifted.
 //   * x and y neighbours come from the staged plane with 128-bit shared loads (a
 //     quarter-warp reads 128 contiguous bytes, so no bank conflicts).
-//   * p_prev and vel2 stream in with 128-bit loads (read once); p_next is written
-//     with 128-bit streaming stores and may alias p_prev (in-place leapfrog).
+//   * p_next is written with 128-bit streaming stores and may alias p_prev (in-place
+//     leapfrog: each element of p_prev is read once, before its own update).
+// Arithmetic per point: each axis' centre term is cancelled against its r = 1 pair
+// in one FMA and the axes are combined as (x + y) + z, which keeps the rounding
+// close to the reference's per-axis evaluation.
 // Algorithmic DRAM traffic: acoustic 16 B / interior point (read p, p_prev, vel2;
-// write p_next), heat 8 B (read u, write u_next).  Halo columns shared between
-// neighbouring tiles are re-read from L2, not DRAM.
+// write p_next), heat 8 B (read u, write u_next).
 #include <algorithm>
 #include <mutex>
 
@@ -30,8 +35,8 @@ namespace sb200 {
 namespace {
 
 struct PencilArgs {
-    const float* prev;  // acoustic: p at t-dt (may alias next); heat: unused
-    const float* vel2;  // acoustic: v^2; heat: unused
+    const float* prev;  // acoustic, AUX = 0: p at t-dt (may alias next)
+    const float* vel2;  // acoustic, AUX = 0: v^2
     float* next;
     int nx, ny, nz;
     int64_t sy, sz;
@@ -46,7 +51,7 @@ struct PencilArgs {
     int* err;
 };
 
-template <int TX, int TY, int RPT, int S>
+template <int TX, int TY, int RPT, int S, int AUX>
 struct Shape {
     static_assert(TX % 4 == 0, "TX must be a multiple of 4 (16-byte TMA origin)");
     static_assert(TY % RPT == 0, "TY must be a multiple of RPT");
@@ -56,13 +61,15 @@ struct Shape {
     static_assert(SX <= 256 && SY <= 256, "TMA box extent is at most 256");
     static constexpr int TPR = TX / 4;
     static constexpr int NT = TPR * (TY / RPT);
-    static constexpr uint32_t PLANE_BYTES = SX * SY * 4u;            // one TMA box
-    static constexpr int PLANE = int(((PLANE_BYTES + 127u) / 128u) * 32u);  // stage stride (floats), 128-B aligned
-    static constexpr size_t SMEM = size_t(S) * PLANE * 4 + 128;
+    static constexpr uint32_t PLANE_BYTES = SX * SY * 4u;                  // one p box
+    static constexpr int PLANE = int(((PLANE_BYTES + 127u) / 128u) * 32u);  // stride (floats)
+    static constexpr uint32_t TILE_BYTES = TX * TY * 4u;                    // p_prev / vel2 box
+    static constexpr int TILE = int(((TILE_BYTES + 127u) / 128u) * 32u);
+    static constexpr size_t SMEM = size_t(S) * PLANE * 4 + size_t(AUX) * 2 * TILE * 4 + 128;
     static constexpr int MINB = (512 / NT) > 0 ? (512 / NT) : 1;  // caps registers at 128
 };
 
-// ya[j][i] += weighted contributions of neighbour row k (row index relative to
+// ya[j][e] += weighted contributions of neighbour row k (row index relative to
 // the thread's first own row) to the y sums of the thread's own rows.
 template <int RPT>
 __device__ __forceinline__ void add_y_row(float (&ya)[RPT][4], const float4& v, int k,
@@ -79,14 +86,20 @@ __device__ __forceinline__ void add_y_row(float (&ya)[RPT][4], const float4& v, 
     }
 }
 
-template <int TX, int TY, int RPT, int S, bool HEAT, bool PF>
-__global__ void __launch_bounds__(Shape<TX, TY, RPT, S>::NT, Shape<TX, TY, RPT, S>::MINB)
-    pencil_f32_kernel(const __grid_constant__ CUtensorMap pmap, const PencilArgs a) {
-    using P = Shape<TX, TY, RPT, S>;
+template <int TX, int TY, int RPT, int S, int AUX, bool HEAT>
+__global__ void __launch_bounds__(Shape<TX, TY, RPT, S, AUX>::NT, Shape<TX, TY, RPT, S, AUX>::MINB)
+    pencil_f32_kernel(const __grid_constant__ CUtensorMap pmap,
+                      const __grid_constant__ CUtensorMap qmap,
+                      const __grid_constant__ CUtensorMap vmap, const PencilArgs a) {
+    using P = Shape<TX, TY, RPT, S, AUX>;
+    constexpr bool kAuxTma = !HEAT && AUX > 0;
+    constexpr int NAUX = AUX > 0 ? AUX : 1;
     extern __shared__ unsigned char dsmem[];
     __shared__ __align__(8) uint64_t full[S];
+    __shared__ __align__(8) uint64_t auxf[NAUX];
     float* sm = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(dsmem) + 127) &
                                          ~uintptr_t(127));
+    float* aux = sm + S * P::PLANE;  // AUX stages of [p_prev tile | vel2 tile]
 
     const int tid = threadIdx.x;
     const int lx = tid % P::TPR;
@@ -100,23 +113,39 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S>::NT, Shape<TX, TY, RPT, 
     const int y0 = R + ty * TY;
     const int zb = R + b * a.zlen;
     const int ze = min(zb + a.zlen, a.nz - R);
-    const int nint = ze - zb;       // interior planes this CTA computes (>= 1)
-    const int nplanes = nint + 2 * R;  // planes it reads (>= 9)
+    const int nint = ze - zb;          // interior planes this CTA computes (>= 1)
+    const int nplanes = nint + 2 * R;  // planes of p it reads (>= 9)
 
     if (tid == 0) {
         prefetch_tmap(&pmap);
+        if (kAuxTma) {
+            prefetch_tmap(&qmap);
+            prefetch_tmap(&vmap);
+        }
 #pragma unroll
         for (int s = 0; s < S; ++s) mbar_init(&full[s], 1);
+#pragma unroll
+        for (int s = 0; s < NAUX; ++s) mbar_init(&auxf[s], 1);
         fence_barrier_init();
     }
     __syncthreads();
-    int issued_hi = -1;  // thread 0: highest plane index handed to TMA
+    int issued_hi = -1;      // thread 0: highest p plane handed to TMA
+    int aux_issued_hi = -1;  // thread 0: highest aux iteration handed to TMA
+    auto issue_aux = [&](int it) {  // thread 0 only
+        float* st = aux + (it % NAUX) * 2 * P::TILE;
+        mbar_arrive_expect_tx(&auxf[it % NAUX], 2 * P::TILE_BYTES);
+        tma_load_3d(st, &qmap, &auxf[it % NAUX], x0, y0, zb + it);
+        tma_load_3d(st + P::TILE, &vmap, &auxf[it % NAUX], x0, y0, zb + it);
+        aux_issued_hi = it;
+    };
     if (tid == 0) {
         for (int s = 0; s < S && s < nplanes; ++s) {
             mbar_arrive_expect_tx(&full[s], P::PLANE_BYTES);
             tma_load_3d(sm + s * P::PLANE, &pmap, &full[s], x0 - R, y0 - R, zb - R + s);
             issued_hi = s;
         }
+        if (kAuxTma)
+            for (int it = 0; it < NAUX && it < nint; ++it) issue_aux(it);
     }
 
     const int gx = x0 + 4 * lx;
@@ -126,6 +155,7 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S>::NT, Shape<TX, TY, RPT, 
 #pragma unroll
     for (int j = 0; j < RPT; ++j) rin[j] = xin && (gy + j < a.ny - R);
     const int soff = (RPT * ly + R) * P::SX + 4 * lx + R;
+    const int aoff = RPT * ly * TX + 4 * lx;  // this thread's first point in an aux tile
     int64_t goff = static_cast<int64_t>(zb) * a.sz + static_cast<int64_t>(gy) * a.sy + gx;
 
     // Source ownership: which (row, lane element) of this thread, if any.
@@ -168,48 +198,20 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S>::NT, Shape<TX, TY, RPT, 
         }
     }
 
-    float4 pv_n[RPT], vv_n[RPT];  // next iteration's p_prev / vel2 (PF only)
-    if (PF && !HEAT) {
-#pragma unroll
-        for (int j = 0; j < RPT; ++j) {
-            if (rin[j]) {
-                pv_n[j] = ldg_cs(a.prev + goff + j * a.sy);
-                vv_n[j] = ldg_stream(a.vel2 + goff + j * a.sy);
-            }
-        }
-    }
-
     for (int i0 = 0; i0 < nint && !abort_run; i0 += 9) {
 #pragma unroll
         for (int u = 0; u < 9; ++u) {
             const int i = i0 + u;
             if (i < nint && !abort_run) {
                 const int cs = (u + 4) % 9;  // centre slot (plane z)
-                // Streamed inputs of this plane.
+                // p_prev / vel2 of this plane (global-load variant).
                 float4 pv[RPT], vv[RPT];
-                if (!HEAT) {
-                    if (PF) {
+                if (!HEAT && !kAuxTma) {
 #pragma unroll
-                        for (int j = 0; j < RPT; ++j) {
-                            pv[j] = pv_n[j];
-                            vv[j] = vv_n[j];
-                        }
-                        if (i + 1 < nint) {
-#pragma unroll
-                            for (int j = 0; j < RPT; ++j) {
-                                if (rin[j]) {
-                                    pv_n[j] = ldg_cs(a.prev + goff + a.sz + j * a.sy);
-                                    vv_n[j] = ldg_stream(a.vel2 + goff + a.sz + j * a.sy);
-                                }
-                            }
-                        }
-                    } else {
-#pragma unroll
-                        for (int j = 0; j < RPT; ++j) {
-                            if (rin[j]) {
-                                pv[j] = ldg_cs(a.prev + goff + j * a.sy);
-                                vv[j] = ldg_stream(a.vel2 + goff + j * a.sy);
-                            }
+                    for (int j = 0; j < RPT; ++j) {
+                        if (rin[j]) {
+                            pv[j] = ldg_cs(a.prev + goff + j * a.sy);
+                            vv[j] = ldg_stream(a.vel2 + goff + j * a.sy);
                         }
                     }
                 }
@@ -261,6 +263,15 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S>::NT, Shape<TX, TY, RPT, 
                         lap[j][e] = (tx + ty) + tz;
                     }
                 }
+                if (kAuxTma) {
+                    if (!mbar_wait(&auxf[i % NAUX], (i / NAUX) & 1)) bad = true;
+                    const float* st = aux + (i % NAUX) * 2 * P::TILE + aoff;
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) {
+                        pv[j] = lds128(st + j * TX);
+                        vv[j] = lds128(st + P::TILE + j * TX);
+                    }
+                }
                 // Update and store.
                 const int z = zb + i;
 #pragma unroll
@@ -292,7 +303,8 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S>::NT, Shape<TX, TY, RPT, 
                     if (rin[j]) stg_stream(a.next + goff + j * a.sy, o);
                 }
                 goff += a.sz;
-                // The stage of plane z is now free: refill it S planes ahead.
+                // The stages of plane z (p) and of iteration i (aux) are free now:
+                // refill them S planes / AUX iterations ahead.
                 abort_run = __syncthreads_or(bad) != 0;
                 if (!abort_run && tid == 0) {
                     const int jr = i + 4;
@@ -303,6 +315,7 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S>::NT, Shape<TX, TY, RPT, 
                                     y0 - R, zb - R + jn);
                         issued_hi = jn;
                     }
+                    if (kAuxTma && i + NAUX < nint) issue_aux(i + NAUX);
                 }
             }
         }
@@ -314,20 +327,23 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S>::NT, Shape<TX, TY, RPT, 
         // released (each stage has at most one outstanding fill).
         for (int jj = max(0, issued_hi - S + 1); jj <= issued_hi; ++jj)
             (void)mbar_wait(&full[jj % S], (jj / S) & 1);
+        if (kAuxTma)
+            for (int it = max(0, aux_issued_hi - NAUX + 1); it <= aux_issued_hi; ++it)
+                (void)mbar_wait(&auxf[it % NAUX], (it / NAUX) & 1);
     }
 }
 
-// ── variant table ─────────────────────────────────────────────────────────────
+// ── variant tables ────────────────────────────────────────────────────────────
 
-using LaunchFn = cudaError_t (*)(const CUtensorMap*, const PencilArgs&, unsigned, cudaStream_t);
+using LaunchFn = cudaError_t (*)(const PencilMaps&, const PencilArgs&, unsigned, cudaStream_t);
 using ResidentFn = int (*)();
 
-template <int TX, int TY, int RPT, int S, bool HEAT, bool PF>
-cudaError_t launch_variant(const CUtensorMap* map, const PencilArgs& a, unsigned ctas,
+template <int TX, int TY, int RPT, int S, int AUX, bool HEAT>
+cudaError_t launch_variant(const PencilMaps& m, const PencilArgs& a, unsigned ctas,
                            cudaStream_t stream) {
-    using P = Shape<TX, TY, RPT, S>;
-    auto kern = pencil_f32_kernel<TX, TY, RPT, S, HEAT, PF>;
-    // The attribute is per function and device; setting it is cheap and idempotent.
+    using P = Shape<TX, TY, RPT, S, AUX>;
+    auto kern = pencil_f32_kernel<TX, TY, RPT, S, AUX, HEAT>;
+    // The attribute is per function and device; set once per device.
     static std::once_flag once[64];
     int dev = 0;
     cudaGetDevice(&dev);
@@ -337,20 +353,20 @@ cudaError_t launch_variant(const CUtensorMap* map, const PencilArgs& a, unsigned
                                   static_cast<int>(P::SMEM));
     });
     if (st != cudaSuccess) return st;
-    kern<<<ctas, P::NT, P::SMEM, stream>>>(*map, a);
+    kern<<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev, m.vel2, a);
     return cudaGetLastError();
 }
 
 // CTAs of a variant that fit on one SM: the occupancy calculator when a device
 // is present, else the shared-memory / register limits computed here.
-template <int TX, int TY, int RPT, int S, bool HEAT, bool PF>
+template <int TX, int TY, int RPT, int S, int AUX, bool HEAT>
 int resident_variant() {
-    using P = Shape<TX, TY, RPT, S>;
+    using P = Shape<TX, TY, RPT, S, AUX>;
     static int cached[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (cached[dev & 63] > 0) return cached[dev & 63];
-    auto kern = pencil_f32_kernel<TX, TY, RPT, S, HEAT, PF>;
+    auto kern = pencil_f32_kernel<TX, TY, RPT, S, AUX, HEAT>;
     int n = 0;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(P::SMEM)) == cudaSuccess &&
@@ -366,32 +382,41 @@ int resident_variant() {
 }
 
 struct Variant {
-    int tx, ty, rpt, stages;
-    bool pf;
+    int tx, ty, rpt, stages, aux;
     const char* name;
-    LaunchFn wave, heat;
-    ResidentFn wave_res, heat_res;
+    LaunchFn launch;
+    ResidentFn resident;
 };
 
-#define SB200_VARIANT(TX, TY, RPT, S, PF, NAME)                                              \
-    Variant {                                                                                \
-        TX, TY, RPT, S, PF, NAME, &launch_variant<TX, TY, RPT, S, false, PF>,               \
-            &launch_variant<TX, TY, RPT, S, true, PF>,                                      \
-            &resident_variant<TX, TY, RPT, S, false, PF>,                                   \
-            &resident_variant<TX, TY, RPT, S, true, PF>                                     \
+#define SB200_VARIANT(TX, TY, RPT, S, AUX, HEAT, NAME)                              \
+    Variant {                                                                       \
+        TX, TY, RPT, S, AUX, NAME, &launch_variant<TX, TY, RPT, S, AUX, HEAT>,     \
+            &resident_variant<TX, TY, RPT, S, AUX, HEAT>                           \
     }
 
-const Variant kVariants[] = {
-    SB200_VARIANT(32, 32, 2, 8, false, "t32x32_r2_s8"),
-    SB200_VARIANT(64, 16, 2, 8, false, "t64x16_r2_s8"),
-    SB200_VARIANT(32, 16, 1, 8, false, "t32x16_r1_s8"),
-    SB200_VARIANT(64, 32, 2, 8, false, "t64x32_r2_s8"),
-    SB200_VARIANT(32, 64, 2, 8, false, "t32x64_r2_s8"),
+// Index 0 of each table is the default when no tuned choice exists.
+const Variant kWave[] = {
+    SB200_VARIANT(32, 32, 2, 8, 4, false, "t32x32_r2_s8_a4"),
+    SB200_VARIANT(32, 32, 2, 8, 2, false, "t32x32_r2_s8_a2"),
+    SB200_VARIANT(32, 32, 2, 8, 0, false, "t32x32_r2_s8_ldg"),
+    SB200_VARIANT(64, 16, 2, 8, 3, false, "t64x16_r2_s8_a3"),
+    SB200_VARIANT(32, 16, 1, 8, 4, false, "t32x16_r1_s8_a4"),
+    SB200_VARIANT(64, 32, 2, 8, 3, false, "t64x32_r2_s8_a3"),
+    SB200_VARIANT(32, 64, 2, 8, 3, false, "t32x64_r2_s8_a3"),
 };
-constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+const Variant kHeat[] = {
+    SB200_VARIANT(32, 32, 2, 8, 0, true, "t32x32_r2_s8"),
+    SB200_VARIANT(64, 16, 2, 8, 0, true, "t64x16_r2_s8"),
+    SB200_VARIANT(32, 16, 1, 8, 0, true, "t32x16_r1_s8"),
+    SB200_VARIANT(64, 32, 2, 8, 0, true, "t64x32_r2_s8"),
+    SB200_VARIANT(32, 64, 2, 8, 0, true, "t32x64_r2_s8"),
+};
+constexpr int kNumWave = sizeof(kWave) / sizeof(kWave[0]);
+constexpr int kNumHeat = sizeof(kHeat) / sizeof(kHeat[0]);
 
-PencilArgs base_args(const GridDesc& g, const PencilConfig& cfg, int* err) {
-    const Variant& v = kVariants[cfg.variant];
+const Variant& variant_of(bool heat, int v) { return heat ? kHeat[v] : kWave[v]; }
+
+PencilArgs base_args(const Variant& v, const GridDesc& g, int zchunks, int* err) {
     PencilArgs a{};
     a.nx = static_cast<int>(g.nx);
     a.ny = static_cast<int>(g.ny);
@@ -401,7 +426,7 @@ PencilArgs base_args(const GridDesc& g, const PencilConfig& cfg, int* err) {
     a.tiles_x = static_cast<int>((g.nx - 2 * R + v.tx - 1) / v.tx);
     a.tiles_y = static_cast<int>((g.ny - 2 * R + v.ty - 1) / v.ty);
     const int inz = static_cast<int>(g.nz - 2 * R);
-    const int zc = std::max(1, std::min(cfg.zchunks, inz));
+    const int zc = std::max(1, std::min(zchunks, inz));
     a.zlen = (inz + zc - 1) / zc;
     a.src_x = a.src_y = a.src_z = -1;
     a.err = err;
@@ -433,36 +458,35 @@ Weights fold_weights(const GridDesc& g, float scale) {
 
 }  // namespace
 
-int pencil_f32_variant_count() { return kNumVariants; }
+int pencil_f32_variant_count(bool heat) { return heat ? kNumHeat : kNumWave; }
 
-const char* pencil_f32_variant_name(int v) {
-    return (v >= 0 && v < kNumVariants) ? kVariants[v].name : nullptr;
+const char* pencil_f32_variant_name(bool heat, int v) {
+    return (v >= 0 && v < pencil_f32_variant_count(heat)) ? variant_of(heat, v).name : nullptr;
 }
 
-void pencil_f32_box(int variant, int* bx, int* by) {
-    const Variant& v = kVariants[variant];
-    *bx = v.tx + 2 * R;
-    *by = v.ty + 2 * R;
+PencilBoxes pencil_f32_boxes(bool heat, int v) {
+    const Variant& x = variant_of(heat, v);
+    PencilBoxes b;
+    b.halo_x = x.tx + 2 * R;
+    b.halo_y = x.ty + 2 * R;
+    b.tile_x = x.tx;
+    b.tile_y = x.ty;
+    b.aux_tma = !heat && x.aux > 0;
+    return b;
 }
 
-int pencil_f32_resident(int variant, bool heat) {
-    const Variant& v = kVariants[variant];
-    return heat ? v.heat_res() : v.wave_res();
+int pencil_f32_resident(bool heat, int v) { return variant_of(heat, v).resident(); }
+
+int64_t pencil_f32_ctas(bool heat, int v, const GridDesc& g, int zchunks) {
+    return ctas_of(base_args(variant_of(heat, v), g, zchunks, nullptr), g);
 }
 
-int64_t pencil_f32_ctas(int variant, const GridDesc& g, int zchunks) {
-    PencilConfig c;
-    c.variant = variant;
-    c.zchunks = zchunks;
-    PencilArgs a = base_args(g, c, nullptr);
-    return ctas_of(a, g);
-}
-
-cudaError_t launch_wave_pencil_f32(const CUtensorMap* pmap, const float* prev, const float* vel2,
+cudaError_t launch_wave_pencil_f32(const PencilMaps& maps, const float* prev, const float* vel2,
                                    float* next, const GridDesc& g, const SourceDesc& src,
                                    const PencilConfig& cfg, int* err, cudaStream_t stream) {
     if (!g.has_interior()) return cudaSuccess;
-    PencilArgs a = base_args(g, cfg, err);
+    const Variant& v = kWave[cfg.variant];
+    PencilArgs a = base_args(v, g, cfg.zchunks, err);
     a.prev = prev;
     a.vel2 = vel2;
     a.next = next;
@@ -477,17 +501,18 @@ cudaError_t launch_wave_pencil_f32(const CUtensorMap* pmap, const float* prev, c
         a.src_step = src.step;
         a.src_off = src.step_offset;
     }
-    return kVariants[cfg.variant].wave(pmap, a, ctas_of(a, g), stream);
+    return v.launch(maps, a, ctas_of(a, g), stream);
 }
 
-cudaError_t launch_heat_pencil_f32(const CUtensorMap* umap, float* u_next, const GridDesc& g,
+cudaError_t launch_heat_pencil_f32(const PencilMaps& maps, float* u_next, const GridDesc& g,
                                    float alpha_dt, const PencilConfig& cfg, int* err,
                                    cudaStream_t stream) {
     if (!g.has_interior()) return cudaSuccess;
-    PencilArgs a = base_args(g, cfg, err);
+    const Variant& v = kHeat[cfg.variant];
+    PencilArgs a = base_args(v, g, cfg.zchunks, err);
     a.next = u_next;
     a.w = fold_weights(g, alpha_dt);
-    return kVariants[cfg.variant].heat(umap, a, ctas_of(a, g), stream);
+    return v.launch(maps, a, ctas_of(a, g), stream);
 }
 
 }  // namespace sb200

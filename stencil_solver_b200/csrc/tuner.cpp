@@ -1,0 +1,188 @@
+// Autotuner for the pencil kernels: per (kernel kind, grid extents, device), time
+// every compiled tile variant at a few z splits and keep the fastest.
+//
+// Choices live in a process-wide table consulted by every launch of that kind
+// on that grid; they can be saved to and loaded from a plain-text cache file
+// (one "kind nx ny nz variant zchunks ms device" line per entry), so a tuned
+// configuration survives across runs on the same GPU model.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "kernels.h"
+#include "stencil_b200.h"
+
+namespace sb200 {
+
+namespace {
+
+using Key = std::tuple<int, int64_t, int64_t, int64_t, std::string>;
+
+struct Choice {
+    int variant = 0;
+    int zchunks = 1;
+    float ms = 0.f;
+};
+
+std::mutex g_mu;
+std::map<Key, Choice>* g_table = nullptr;
+
+// Device model name, looked up once per device: cudaGetDeviceProperties costs
+// milliseconds, far too much for the per-launch path that consults the table.
+std::string device_name() {
+    static std::mutex mu;
+    static std::string names[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return "unknown";
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (names[dev].empty()) {
+        cudaDeviceProp p{};
+        std::string s = "unknown";
+        if (cudaGetDeviceProperties(&p, dev) == cudaSuccess) s = p.name;
+        cudaGetLastError();
+        std::replace(s.begin(), s.end(), ' ', '_');
+        names[dev] = s;
+    }
+    return names[dev];
+}
+
+std::map<Key, Choice>& table() {
+    if (!g_table) g_table = new std::map<Key, Choice>();
+    return *g_table;
+}
+
+}  // namespace
+
+bool tuned_choice(int kind, const GridDesc& g, PencilConfig* out) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (!g_table) return false;
+    auto it = g_table->find(Key{kind, g.nx, g.ny, g.nz, device_name()});
+    if (it == g_table->end()) return false;
+    out->variant = it->second.variant;
+    out->zchunks = it->second.zchunks;
+    return true;
+}
+
+}  // namespace sb200
+
+using namespace sb200;
+
+extern "C" {
+
+int sb200_tune(int kind, const sb200_grid* grid, const void* field, const void* prev,
+               const void* vel2, void* scratch, int reps, int* variant, int* zchunks,
+               float* best_ms) {
+    if (kind != SB200_KIND_WAVE_F32 && kind != SB200_KIND_HEAT_F32) return SB200_ERR_INVALID;
+    if (!grid || !field || !scratch || (kind == SB200_KIND_WAVE_F32 && (!prev || !vel2)))
+        return SB200_ERR_INVALID;
+    if (scratch == field || scratch == prev || scratch == vel2) return SB200_ERR_INVALID;
+    const bool heat = kind == SB200_KIND_HEAT_F32;
+    const int nvar = sb200_pencil_variant_count(kind);
+    const int inz = static_cast<int>(grid->nz - 8);
+    if (nvar <= 0 || inz < 1 || grid->nx % 4 != 0) return SB200_ERR_UNSUPPORTED;
+    reps = std::max(1, reps);
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+        return SB200_ERR_CUDA;
+    Choice best;
+    best.ms = 1e30f;
+    GridDesc gd;
+    gd.nx = grid->nx;
+    gd.ny = grid->ny;
+    gd.nz = grid->nz;
+    for (int v = 0; v < nvar; ++v) {
+        // The three best-filling z splits of this tile shape (see zchunk_ranking).
+        for (int zc : zchunk_ranking(heat, v, gd, 3)) {
+            sb200_set_pencil_override(kind, v, zc);
+            auto launch = [&]() {
+                return heat ? sb200_heat_step_f32(static_cast<const float*>(field),
+                                                  static_cast<float*>(scratch), grid, 1.0f, nullptr)
+                            : sb200_launch_tiled(static_cast<const float*>(field),
+                                                 static_cast<const float*>(prev),
+                                                 static_cast<const float*>(vel2),
+                                                 static_cast<float*>(scratch), grid, nullptr);
+            };
+            if (launch() != SB200_OK) continue;  // warm-up (sets attributes, encodes maps)
+            cudaEventRecord(e0, nullptr);
+            for (int r = 0; r < reps; ++r) launch();
+            cudaEventRecord(e1, nullptr);
+            if (cudaEventSynchronize(e1) != cudaSuccess) break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms /= reps;
+            if (ms < best.ms) {
+                best.ms = ms;
+                best.variant = v;
+                best.zchunks = zc;
+            }
+        }
+    }
+    sb200_set_pencil_override(kind, -1, 1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (cudaGetLastError() != cudaSuccess || best.ms >= 1e29f) return SB200_ERR_CUDA;
+    {
+        std::lock_guard<std::mutex> lock(g_mu);
+        table()[Key{kind, grid->nx, grid->ny, grid->nz, device_name()}] = best;
+    }
+    if (variant) *variant = best.variant;
+    if (zchunks) *zchunks = best.zchunks;
+    if (best_ms) *best_ms = best.ms;
+    return SB200_OK;
+}
+
+int sb200_tune_save(const char* path) {
+    if (!path) return SB200_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(g_mu);
+    std::ofstream f(path);
+    if (!f) return SB200_ERR_INVALID;
+    if (g_table)
+        for (const auto& kv : *g_table)
+            f << std::get<0>(kv.first) << ' ' << std::get<1>(kv.first) << ' '
+              << std::get<2>(kv.first) << ' ' << std::get<3>(kv.first) << ' ' << kv.second.variant
+              << ' ' << kv.second.zchunks << ' ' << kv.second.ms << ' ' << std::get<4>(kv.first)
+              << '\n';
+    return SB200_OK;
+}
+
+int sb200_tune_load(const char* path) {
+    if (!path) return SB200_ERR_INVALID;
+    std::ifstream f(path);
+    if (!f) return SB200_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(g_mu);
+    std::string line;
+    int n = 0;
+    while (std::getline(f, line)) {
+        std::istringstream s(line);
+        int kind = 0, v = 0, zc = 1;
+        int64_t nx = 0, ny = 0, nz = 0;
+        float ms = 0.f;
+        std::string dev;
+        if (!(s >> kind >> nx >> ny >> nz >> v >> zc >> ms >> dev)) continue;
+        const bool heat = kind == SB200_KIND_HEAT_F32;
+        if ((kind != SB200_KIND_WAVE_F32 && !heat) || v < 0 ||
+            v >= pencil_f32_variant_count(heat) || zc < 1)
+            continue;  // stale entry from another build
+        Choice c;
+        c.variant = v;
+        c.zchunks = zc;
+        c.ms = ms;
+        table()[Key{kind, nx, ny, nz, dev}] = c;
+        ++n;
+    }
+    return n;
+}
+
+}  // extern "C"

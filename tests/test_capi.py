@@ -98,3 +98,17 @@ def test_override_validation():
 def test_grid_struct_layout():
     # int64 x3 then float x4, naturally aligned: 40 bytes.
     assert C.sizeof(sb.sb200_grid) == 40
+
+
+def test_tune_cache_load_skips_bad_lines(tmp_path):
+    f = tmp_path / "tune.txt"
+    f.write_text("0 1024 1024 1024 1 4 2.5 NVIDIA_B200\n"
+                 "garbage line\n"
+                 "0 64 64 64 999 1 1.0 NVIDIA_B200\n"   # variant out of range
+                 "1 512 512 512 0 2 0.7 NVIDIA_B200\n")
+    assert sb.tune_load(str(f)) == 2
+    out = tmp_path / "out.txt"
+    sb.tune_save(str(out))
+    lines = out.read_text().split("\n")
+    assert any(l.startswith("0 1024 1024 1024 1 4") for l in lines)
+    assert any(l.startswith("1 512 512 512 0 2") for l in lines)

@@ -117,7 +117,7 @@ def test_tiled_odd_extents_falls_back_bitexact(torch_cuda):
 # ── pencil kernel: tolerance against the oracle ───────────────────────────────
 
 @pytest.mark.parametrize("zchunks", [1, 3])
-@pytest.mark.parametrize("variant", range(5))
+@pytest.mark.parametrize("variant", range(8))
 def test_tiled_variants_one_step(torch_cuda, variant, zchunks):
     if variant >= len(sb.variant_names()):
         pytest.skip("variant not compiled")
@@ -181,6 +181,22 @@ def test_acoustic_config_full_run(torch_cuda):
     assert rel(tr, f["trace32"]) <= RUN_TOL
     # and against the FP64 oracle (reported bar: same order as the reference's own FP32)
     assert rel(fin[n // 2], f["mid64"]) <= 5e-5
+
+
+def test_tuner_choice_is_applied_and_correct(torch_cuda):
+    shape = (72, 68, 80)
+    cur, prev, vel2 = random_case(shape, 21)
+    g = sb.Grid(80, 68, 72, 10, 10, 10, 1e-3)
+    d = [dev(torch_cuda, a) for a in (cur, prev, vel2)]
+    scratch = dev(torch_cuda, np.zeros(shape, np.float32))
+    v, z, ms = sb.tune(sb.KIND_WAVE_F32, g, d[0], d[1], d[2], scratch, reps=2)
+    assert ms > 0 and 0 <= v < len(sb.variant_names()) and z >= 1
+    assert sb.pencil_choice(sb.KIND_WAVE_F32, g) == (v, z)
+    # the tuner wrote only the scratch buffer
+    assert np.array_equal(host(d[1]), prev) and np.array_equal(host(d[0]), cur)
+    out = dev(torch_cuda, np.zeros(shape, np.float32))
+    sb.launch_tiled(d[0], d[1], d[2], out, g)
+    assert rel(host(out), oracle.wave_step(cur, prev, vel2, 10, 10, 10, 1e-3)) <= STEP_TOL
 
 
 # ── heat ──────────────────────────────────────────────────────────────────────
