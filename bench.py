@@ -265,7 +265,7 @@ def run_ours(a):
         sb.set_pencil_override(sb.KIND_WAVE_F32, a.variant, a.zchunks)
     elif not a.no_tune:  # untimed: pick the tile shape / z split for this grid
         scratch = torch.empty_like(p)
-        tuned = sb.tune(sb.KIND_WAVE_F32, g, p, q, v, scratch, reps=2)
+        tuned = sb.tune(sb.KIND_WAVE_F32, g, p, q, v, scratch, reps=5)
         del scratch
 
     def one():
