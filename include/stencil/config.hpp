@@ -38,6 +38,11 @@ enum class VelocityModel {
     Layered,   ///< seeded layered model, see sb200_model_layered()
 };
 
+enum class Precision {
+    FP32,  ///< FP32 fields (reference)
+    FP16,  ///< acoustic only: FP16 p / p_prev with a power-of-two scale, BF16 vel2 dt^2/dx^2
+};
+
 enum class InitialCondition {
     Gaussian,       ///< interior Gaussian pulse for p and p_prev (reference)
     Rest,           ///< p = p_prev = 0 (source-driven runs)
@@ -90,6 +95,9 @@ struct Config {
     InitialCondition initial = InitialCondition::Gaussian;
     bool use_graphs = true;  ///< run() replays captured CUDA graphs of graph_chunk steps
     int graph_chunk = 100;
+    Precision precision = Precision::FP32;
+    int renorm_every = 50;   ///< FP16: steps between scale renormalisations
+    int monitor_every = 0;   ///< FP32: steps between stability-monitor checks (0: chunk ends)
 
     /// Grid descriptor: extents and spacing from the config; dt = dt_override
     /// when set, else CFL_LIMIT * min(dx, dy, dz) / velocity.
@@ -117,7 +125,7 @@ struct Config {
  *   --physics wave|heat --kernel naive|tiled|multigpu --device --output --verbose
  * (--ny/--nz must equal --nx when given: the reference CLI is cubic-only).
  * Added: --dt F, --source X,Y,Z, --freq F, --model constant|layered, --seed N,
- *        --ic gaussian|rest|uniform.
+ *        --ic gaussian|rest|uniform, --precision fp32|fp16.
  * Throws std::runtime_error on unknown flags, values or missing arguments.
  */
 inline Config parse_args(int argc, char** argv) {
@@ -199,6 +207,14 @@ inline Config parse_args(int argc, char** argv) {
                 throw std::runtime_error("unknown model: " + v);
         } else if (flag == "--seed") {
             cfg.seed = static_cast<std::uint64_t>(std::stoull(value()));
+        } else if (flag == "--precision") {
+            const std::string v = value();
+            if (v == "fp32")
+                cfg.precision = Precision::FP32;
+            else if (v == "fp16")
+                cfg.precision = Precision::FP16;
+            else
+                throw std::runtime_error("unknown precision: " + v);
         } else if (flag == "--ic") {
             const std::string v = value();
             if (v == "gaussian")

@@ -130,9 +130,54 @@ int sb200_ricker(double freq, double t0, double dt, int64_t n_steps, float* out)
 int sb200_heat_step_exact_f32(const float* u, float* u_next, const sb200_grid* grid,
                               float alpha, void* stream);
 
+/* ── FP16-storage acoustic path (no reference counterpart: the north-star
+ *    precision variant).  p and p_prev are FP16 holding a * p for a power-of-two
+ *    scale a kept in device memory (sb200_f16_scale); K = vel2 dt^2 / dx^2 is
+ *    BF16; arithmetic is FP32.  8 B per interior point and step. ─────────────── */
+typedef struct sb200_f16_scale {
+    float a; /* current storage scale (fields hold a * p) */
+    float r; /* a_new / a_old of the last renormalisation */
+} sb200_f16_scale;
+
+/* dst[i] = fp16(src[i] * scale) / src[i] = float(dst[i]) / scale over n elements. */
+int sb200_f16_pack(const float* src, uint16_t* dst, int64_t n, float scale, void* stream);
+int sb200_f16_unpack(const uint16_t* src, float* dst, int64_t n, float scale, void* stream);
+/* K[i] = bf16(vel2[i] * dt^2 / dx^2) over the whole grid. */
+int sb200_k_field_bf16(const float* vel2, uint16_t* k, const sb200_grid* grid, void* stream);
+/* One FP16-storage step, p_next written in place over p_prev.  phase 0 = plain,
+ * 1 = the renormalisation step (output scaled by scale->r), 2 = the step after
+ * it (p_prev scaled by scale->r).  The source adds a * dt^2 vel2[src] * w with
+ * w = wavelet[*step + step_offset] (device) or src_amp when wavelet is NULL.
+ * Needs nx % 8 == 0 and 16-byte aligned fields (SB200_ERR_UNSUPPORTED
+ * otherwise). */
+int sb200_wave_step_f16(const uint16_t* p, uint16_t* p_prev_next, const uint16_t* k,
+                        const sb200_grid* grid, int64_t src_index, float src_amp,
+                        const float* wavelet, const int* step, int step_offset,
+                        const sb200_f16_scale* scale, int phase, void* stream);
+/* Renormalisation (one device thread): with m = stats3[1] / a (stats of the
+ * stored field) and b = bound[*step] (or bound_host when bound is NULL),
+ * a_new = 2^floor(log2(target / (m + b))), r = a_new / a, a = a_new. */
+int sb200_f16_renorm(const double* stats3, sb200_f16_scale* scale, const float* bound,
+                     const int* step, float bound_host, float target, void* stream);
+
+/* ── FP64 field statistics (stability monitor, FP16 scale renormalisation) ──
+ * out3 (device, 3 doubles) receives, over the interior of the field:
+ *   out3[0] = sum of (f/scale)^2, out3[1] = max |f/scale|, out3[2] = number of
+ *   non-finite values,
+ * accumulated in double with a fixed reduction order (bit-reproducible).
+ * scratch (device) must hold at least sb200_field_stats_scratch_len(grid)
+ * doubles; it is overwritten.  Asynchronous on `stream`. */
+int64_t sb200_field_stats_scratch_len(const sb200_grid* grid);
+int sb200_field_stats_f32(const float* field, const sb200_grid* grid, double* out3,
+                          double* scratch, int64_t scratch_len, void* stream);
+/* The same over an FP16 field stored scaled by `scale` (a value v is v/scale). */
+int sb200_field_stats_f16(const uint16_t* field, const sb200_grid* grid, float scale,
+                          double* out3, double* scratch, int64_t scratch_len, void* stream);
+
 /* ── pencil-kernel configuration (used by the tuner and the tests) ──────────── */
 #define SB200_KIND_WAVE_F32 0
 #define SB200_KIND_HEAT_F32 1
+#define SB200_KIND_WAVE_F16 2
 int sb200_pencil_variant_count(int kind);
 const char* sb200_pencil_variant_name(int kind, int variant);
 /* Forces (variant, zchunks) for every later launch of `kind` on this process;
@@ -140,6 +185,58 @@ const char* sb200_pencil_variant_name(int kind, int variant);
 int sb200_set_pencil_override(int kind, int variant, int zchunks);
 /* The (variant, zchunks) the next launch of `kind` on `grid` would use. */
 int sb200_pencil_choice(int kind, const sb200_grid* grid, int* variant, int* zchunks);
+
+/* ── run handle: a whole simulation behind one object ─────────────────────────
+ * Replaces the reference's ISolver / SolverBase (include/stencil/solver.hpp:13-24,
+ * src/solver/solver_base.cpp:28-116) for C callers: the handle owns the device
+ * state (it is the one part of this ABI that allocates), takes the initial
+ * fields from host memory, steps on its own stream (CUDA-graph chunks), records
+ * the source trace, runs the FP64 stability monitor and hands results back to
+ * host memory. */
+#define SB200_PHYSICS_WAVE 0
+#define SB200_PHYSICS_HEAT 1
+#define SB200_PRECISION_F32 0
+#define SB200_PRECISION_F16 1 /* acoustic only: FP16 p/p_prev, BF16 vel2 dt^2/dx^2 */
+
+typedef struct sb200_run_config {
+    sb200_grid grid;
+    int physics;          /* SB200_PHYSICS_* */
+    int precision;        /* SB200_PRECISION_* */
+    int exact;            /* FP32 only: 1 = reference-order kernels (bit-exact path) */
+    float diffusivity;    /* heat: alpha (the step is u += alpha*dt*lap u) */
+    int64_t src_index;    /* acoustic point source cell; < 0: no source */
+    float src_freq;       /* Ricker peak frequency [Hz]; <= 0: set the wavelet explicitly */
+    float src_t0;         /* Ricker delay [s]; < 0: 1/src_freq */
+    int graph_chunk;      /* steps per captured CUDA graph (rounded down to even); 0: none */
+    int renorm_every;     /* FP16: steps between renormalisations (even, >= 2; 0: 50) */
+    int monitor_every;    /* FP32: steps between monitor checks (0: only at sync points) */
+    float monitor_limit;  /* largest |p| the monitor accepts (<= 0: 1e30) */
+    float f16_target;     /* FP16: renormalise so that max|p| * a <= target (<= 0: 4096) */
+} sb200_run_config;
+
+/* Fills cfg with defaults for a grid (wave, FP32, no source, graphs of 100). */
+void sb200_run_config_init(sb200_run_config* cfg, const sb200_grid* grid);
+int sb200_run_create(const sb200_run_config* cfg, void** handle);
+int sb200_run_destroy(void* handle);
+/* Initial fields from host memory (nx*ny*nz floats each): p, p_prev (NULL: =
+ * p), vel2 (acoustic; ignored for heat).  Resets the step count.  Synchronous. */
+int sb200_run_set_fields(void* handle, const float* p, const float* p_prev, const float* vel2);
+/* Replaces the source wavelet with n host samples (one per step). */
+int sb200_run_set_wavelet(void* handle, const float* w, int64_t n);
+/* Enqueues n steps on the handle's stream (asynchronous). */
+int sb200_run_steps(void* handle, int64_t n);
+/* Waits for the enqueued steps; returns SB200_ERR_MONITOR if the monitor saw a
+ * non-finite value or |p| above the limit, SB200_ERR_DEVICE on a device error. */
+int sb200_run_synchronize(void* handle);
+/* Current field in physical units into host memory (synchronous). */
+int sb200_run_get_field(void* handle, float* p);
+/* First n source-trace samples (p at the source after each step) to host memory. */
+int sb200_run_get_trace(void* handle, float* trace, int64_t n);
+/* FP64 statistics {sum p^2, max |p|, non-finite count} of the current field. */
+int sb200_run_stats(void* handle, double* out3);
+int64_t sb200_run_steps_done(void* handle);
+/* The handle's cudaStream_t. */
+void* sb200_run_stream(void* handle);
 
 /* ── autotuner ──────────────────────────────────────────────────────────────
  * Times every compiled tile variant of `kind` at its three best-filling z splits

@@ -48,6 +48,19 @@ def lib() -> C.CDLL:
         L.oracle_ricker.restype = None
         L.oracle_fd_coefficients.argtypes = [_f64p]
         L.oracle_fd_coefficients.restype = None
+        _u16p = np.ctypeslib.ndpointer(dtype=np.uint16, flags="C_CONTIGUOUS")
+        L.oracle_wave_step_f16.argtypes = [_u16p, _u16p, _u16p, _u16p, _i64, _i64, _i64, C.c_float,
+                                           C.c_float, C.c_float, C.c_float, C.c_float, _i64,
+                                           C.c_float, C.c_float]
+        L.oracle_wave_step_f16.restype = None
+        L.oracle_f32_to_f16.argtypes = [C.c_float]
+        L.oracle_f32_to_f16.restype = C.c_uint16
+        L.oracle_f16_to_f32.argtypes = [C.c_uint16]
+        L.oracle_f16_to_f32.restype = C.c_float
+        L.oracle_f32_to_bf16.argtypes = [C.c_float]
+        L.oracle_f32_to_bf16.restype = C.c_uint16
+        L.oracle_bf16_to_f32.argtypes = [C.c_uint16]
+        L.oracle_bf16_to_f32.restype = C.c_float
         L.oracle_rms_diff_f32.argtypes = [_f32p, _f32p, _i64]
         L.oracle_rms_diff_f32.restype = C.c_double
         L.oracle_max_abs_diff_f32.argtypes = [_f32p, _f32p, _i64]
@@ -105,6 +118,26 @@ def wave_run(cur, prev, vel2, dx, dy, dz, dt, n_steps, src=-1, wavelet=None, tra
         wl.ctypes.data if wl is not None else None,
         tr.ctypes.data if tr is not None else None)
     return cur, prev, tr
+
+
+def wave_step_f16(P, Q, K, dx, dy, dz, m_out=1.0, m_q=1.0, src=-1, w=0.0, a=1.0, out=None):
+    """One FP16-storage step (uint16 fields holding fp16 / bf16 bit patterns)."""
+    nz, ny, nx = P.shape
+    if out is None:
+        out = Q.copy()
+    lib().oracle_wave_step_f16(P, Q, K, out, nx, ny, nz, dx, dy, dz, m_out, m_q, src, w, a)
+    return out
+
+
+def to_f16(a, scale=1.0) -> np.ndarray:
+    """fp16 bit patterns of float32(a) * scale (round to nearest even)."""
+    return (np.asarray(a, np.float32) * np.float32(scale)).astype(np.float16).view(np.uint16)
+
+
+def to_bf16(a) -> np.ndarray:
+    """bf16 bit patterns of float32 values (round to nearest even)."""
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    return ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
 
 
 def ricker(f, t0, dt, n_steps) -> np.ndarray:

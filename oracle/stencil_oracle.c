@@ -190,3 +190,84 @@ double oracle_max_abs_diff_f32(const float* a, const float* b, int64_t n) {
     }
     return m;
 }
+
+/* ── FP16-storage scheme (the B200 precision variant; no reference counterpart) ──
+ * Conversions follow the IEEE 754 binary16 / bfloat16 definitions with round to
+ * nearest even.  The step evaluates, in FP32 and the reference's per-axis order,
+ *   out = m_out * (2 p - m_q q + K * L'(p)),  L' = sum_a (dx/d_a)^2 (c0 p + sum_r c_r (p+r + p-r)),
+ * with p, q decoded from FP16 and K from BF16, then rounds out to FP16; the
+ * source adds ((K[src] * dx^2) * w) * a before the rounding. */
+static uint32_t f32_bits(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
+static float bits_f32(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
+
+float oracle_f16_to_f32(uint16_t h) {
+    const uint32_t sign = (uint32_t)(h & 0x8000u) << 16;
+    const uint32_t e = (h >> 10) & 0x1fu, m = h & 0x3ffu;
+    if (e == 0) { /* zero / subnormal: m * 2^-24 */
+        const float v = (float)m * 5.9604644775390625e-8f;
+        return sign ? -v : v;
+    }
+    if (e == 31) return bits_f32(sign | 0x7f800000u | (m << 13));
+    return bits_f32(sign | ((e + 112u) << 23) | (m << 13));
+}
+
+uint16_t oracle_f32_to_f16(float f) {
+    const uint32_t u = f32_bits(f);
+    const uint16_t sign = (uint16_t)((u >> 16) & 0x8000u);
+    const uint32_t a = u & 0x7fffffffu;
+    if (a >= 0x7f800000u) return sign | (a > 0x7f800000u ? 0x7e00u : 0x7c00u);
+    const float af = bits_f32(a);
+    if (af >= 65520.0f) return sign | 0x7c00u; /* rounds to infinity */
+    if (af < 6.103515625e-05f) { /* subnormal result: quantum 2^-24, exact scaling */
+        const float q = af * 16777216.0f; /* af / 2^-24 */
+        const float r = nearbyintf(q);    /* round half to even (default mode) */
+        return sign | (uint16_t)r;
+    }
+    /* normal: keep 10 mantissa bits, round to nearest even on the 13 dropped */
+    uint32_t e = (a >> 23) - 112u, m = a & 0x7fffffu;
+    uint32_t hm = m >> 13, rest = m & 0x1fffu;
+    if (rest > 0x1000u || (rest == 0x1000u && (hm & 1u))) {
+        if (++hm == 0x400u) { hm = 0; ++e; }
+    }
+    return sign | (uint16_t)((e << 10) | hm);
+}
+
+float oracle_bf16_to_f32(uint16_t b) { return bits_f32((uint32_t)b << 16); }
+
+uint16_t oracle_f32_to_bf16(float f) {
+    const uint32_t u = f32_bits(f);
+    if ((u & 0x7f800000u) == 0x7f800000u && (u & 0x7fffffu)) return (uint16_t)((u >> 16) | 0x40u);
+    return (uint16_t)((u + 0x7fffu + ((u >> 16) & 1u)) >> 16);
+}
+
+void oracle_wave_step_f16(const uint16_t* P, const uint16_t* Q, const uint16_t* K, uint16_t* out,
+                          int64_t nx, int64_t ny, int64_t nz, float dx, float dy, float dz,
+                          float m_out, float m_q, int64_t src, float w, float a) {
+    const float ry = (float)((double)dx * dx / ((double)dy * dy));
+    const float rz = (float)((double)dx * dx / ((double)dz * dz));
+    const float c0 = (float)C0_D;
+    float c[R];
+    for (int r = 0; r < R; ++r) c[r] = (float)C_D[r];
+    const int64_t sy = nx, sz = nx * ny;
+    const float dx2 = dx * dx;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int64_t iz = R; iz < nz - R; ++iz)
+        for (int64_t iy = R; iy < ny - R; ++iy)
+            for (int64_t ix = R; ix < nx - R; ++ix) {
+                const int64_t ci = iz * sz + iy * sy + ix;
+                const float p = oracle_f16_to_f32(P[ci]);
+                float lx = c0 * p, ly = c0 * p * ry, lz = c0 * p * rz;
+                for (int r = 1; r <= R; ++r) {
+                    lx += c[r - 1] * (oracle_f16_to_f32(P[ci + r]) + oracle_f16_to_f32(P[ci - r]));
+                    ly += c[r - 1] * (oracle_f16_to_f32(P[ci + r * sy]) +
+                                      oracle_f16_to_f32(P[ci - r * sy])) * ry;
+                    lz += c[r - 1] * (oracle_f16_to_f32(P[ci + r * sz]) +
+                                      oracle_f16_to_f32(P[ci - r * sz])) * rz;
+                }
+                const float kk = oracle_bf16_to_f32(K[ci]);
+                float o = m_out * ((2.0f * p - m_q * oracle_f16_to_f32(Q[ci])) +
+                                   kk * ((lx + ly) + lz));
+                if (ci == src) o = o + ((kk * dx2) * w) * a;
+                out[ci] = oracle_f32_to_f16(o);
+            }
+}

@@ -74,6 +74,22 @@ class Grid:
         return sb200_grid(self.nx, self.ny, self.nz, self.dx, self.dy, self.dz, self.dt)
 
 
+class sb200_run_config(C.Structure):
+    _fields_ = [("grid", sb200_grid), ("physics", C.c_int), ("precision", C.c_int),
+                ("exact", C.c_int), ("diffusivity", C.c_float), ("src_index", C.c_int64),
+                ("src_freq", C.c_float), ("src_t0", C.c_float), ("graph_chunk", C.c_int),
+                ("renorm_every", C.c_int), ("monitor_every", C.c_int),
+                ("monitor_limit", C.c_float), ("f16_target", C.c_float)]
+
+
+class sb200_f16_scale(C.Structure):
+    _fields_ = [("a", C.c_float), ("r", C.c_float)]
+
+
+PHYSICS_WAVE, PHYSICS_HEAT = 0, 1
+PRECISION_F32, PRECISION_F16 = 0, 1
+KIND_WAVE_F16 = 2
+
 _lib: C.CDLL | None = None
 
 _SIGNATURES = {
@@ -105,6 +121,31 @@ _SIGNATURES = {
                    C.c_int),
     "sb200_tune_save": ([C.c_char_p], C.c_int),
     "sb200_tune_load": ([C.c_char_p], C.c_int),
+    "sb200_field_stats_scratch_len": ([C.POINTER(sb200_grid)], C.c_int64),
+    "sb200_field_stats_f32": ([C.c_void_p, C.POINTER(sb200_grid), C.c_void_p, C.c_void_p,
+                               C.c_int64, C.c_void_p], C.c_int),
+    "sb200_field_stats_f16": ([C.c_void_p, C.POINTER(sb200_grid), C.c_float, C.c_void_p,
+                               C.c_void_p, C.c_int64, C.c_void_p], C.c_int),
+    "sb200_f16_pack": ([C.c_void_p, C.c_void_p, C.c_int64, C.c_float, C.c_void_p], C.c_int),
+    "sb200_f16_unpack": ([C.c_void_p, C.c_void_p, C.c_int64, C.c_float, C.c_void_p], C.c_int),
+    "sb200_k_field_bf16": ([C.c_void_p, C.c_void_p, C.POINTER(sb200_grid), C.c_void_p], C.c_int),
+    "sb200_wave_step_f16": ([C.c_void_p] * 3 + [C.POINTER(sb200_grid), C.c_int64, C.c_float,
+                            C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p],
+                           C.c_int),
+    "sb200_f16_renorm": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_float,
+                          C.c_void_p], C.c_int),
+    "sb200_run_config_init": ([C.POINTER(sb200_run_config), C.POINTER(sb200_grid)], None),
+    "sb200_run_create": ([C.POINTER(sb200_run_config), C.POINTER(C.c_void_p)], C.c_int),
+    "sb200_run_destroy": ([C.c_void_p], C.c_int),
+    "sb200_run_set_fields": ([C.c_void_p] * 4, C.c_int),
+    "sb200_run_set_wavelet": ([C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
+    "sb200_run_steps": ([C.c_void_p, C.c_int64], C.c_int),
+    "sb200_run_synchronize": ([C.c_void_p], C.c_int),
+    "sb200_run_get_field": ([C.c_void_p, C.c_void_p], C.c_int),
+    "sb200_run_get_trace": ([C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
+    "sb200_run_stats": ([C.c_void_p, C.c_void_p], C.c_int),
+    "sb200_run_steps_done": ([C.c_void_p], C.c_int64),
+    "sb200_run_stream": ([C.c_void_p], C.c_void_p),
     "sb200_pencil_variant_count": ([C.c_int], C.c_int),
     "sb200_pencil_variant_name": ([C.c_int, C.c_int], C.c_char_p),
     "sb200_set_pencil_override": ([C.c_int, C.c_int, C.c_int], C.c_int),
@@ -240,6 +281,148 @@ def wave_step_dev(p, p_prev, vel2, p_next, grid: Grid, src_index: int, wavelet, 
 
 def set_device_int(dst, value: int, stream=None) -> None:
     _check(lib().sb200_set_device_int(_ptr(dst), value, _stream(stream)))
+
+
+def field_stats_scratch_len(grid: Grid) -> int:
+    return _check(lib().sb200_field_stats_scratch_len(_g(grid)))
+
+
+def field_stats(field, grid: Grid, out3, scratch, scale: float = 1.0, stream=None) -> None:
+    """Enqueues the FP64 interior statistics {sum f^2, max|f|, non-finite count} of an
+    FP32 or FP16 (by dtype; values stored times `scale`) field into the 3-double out3.
+    scratch is a float64 device tensor of at least field_stats_scratch_len(grid)."""
+    n = scratch.numel()
+    if str(field.dtype).endswith("float16"):
+        _check(lib().sb200_field_stats_f16(_ptr(field), _g(grid), scale, _ptr(out3),
+                                           _ptr(scratch), n, _stream(stream)))
+    else:
+        _check(lib().sb200_field_stats_f32(_ptr(field), _g(grid), _ptr(out3), _ptr(scratch), n,
+                                           _stream(stream)))
+
+
+def f16_pack(src, dst, n: int, scale: float, stream=None) -> None:
+    _check(lib().sb200_f16_pack(_ptr(src), _ptr(dst), n, scale, _stream(stream)))
+
+
+def f16_unpack(src, dst, n: int, scale: float, stream=None) -> None:
+    _check(lib().sb200_f16_unpack(_ptr(src), _ptr(dst), n, scale, _stream(stream)))
+
+
+def k_field_bf16(vel2, k, grid: Grid, stream=None) -> None:
+    _check(lib().sb200_k_field_bf16(_ptr(vel2), _ptr(k), _g(grid), _stream(stream)))
+
+
+def wave_step_f16(p, p_prev_next, k, grid: Grid, scale, phase: int = 0, src_index: int = -1,
+                  src_amp: float = 0.0, wavelet=None, step=None, step_offset: int = 0,
+                  stream=None) -> None:
+    _check(lib().sb200_wave_step_f16(_ptr(p), _ptr(p_prev_next), _ptr(k), _g(grid), src_index,
+                                     src_amp, _ptr(wavelet), _ptr(step), step_offset, _ptr(scale),
+                                     phase, _stream(stream)))
+
+
+def f16_renorm(stats3, scale, bound_host: float, target: float = 4096.0, bound=None, step=None,
+               stream=None) -> None:
+    _check(lib().sb200_f16_renorm(_ptr(stats3), _ptr(scale), _ptr(bound), _ptr(step), bound_host,
+                                  target, _stream(stream)))
+
+
+class Run:
+    """A whole simulation behind the C-ABI run handle (sb200_run_*): fields in from
+    host memory, steps on the device (CUDA-graph chunks), results back to host memory.
+
+    Keyword options map onto sb200_run_config (physics, precision, exact, diffusivity,
+    src_index, src_freq, src_t0, graph_chunk, renorm_every, monitor_every,
+    monitor_limit, f16_target)."""
+
+    def __init__(self, grid: Grid, **opts):
+        cfg = sb200_run_config()
+        lib().sb200_run_config_init(C.byref(cfg), _g(grid))
+        for k, v in opts.items():
+            if not hasattr(cfg, k):
+                raise TypeError(f"unknown run option {k!r}")
+            setattr(cfg, k, v)
+        h = C.c_void_p()
+        _check(lib().sb200_run_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self.grid = grid
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().sb200_run_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @staticmethod
+    def _host(a):
+        import numpy as np
+
+        if a is None:
+            return None
+        if hasattr(a, "data_ptr"):  # a host tensor (pinned or not)
+            return a.data_ptr()
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        return a.ctypes.data, a
+
+    def set_fields(self, p, p_prev=None, vel2=None) -> None:
+        keep = []
+        ptrs = []
+        for x in (p, p_prev, vel2):
+            h = self._host(x)
+            if isinstance(h, tuple):
+                keep.append(h[1])
+                h = h[0]
+            ptrs.append(h)
+        _check(lib().sb200_run_set_fields(self._h, *ptrs))
+
+    def set_wavelet(self, w) -> None:
+        import numpy as np
+
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        _check(lib().sb200_run_set_wavelet(self._h, w.ctypes.data, w.size))
+
+    def steps(self, n: int) -> None:
+        _check(lib().sb200_run_steps(self._h, n))
+
+    def synchronize(self) -> None:
+        _check(lib().sb200_run_synchronize(self._h))
+
+    def field(self, out=None):
+        import numpy as np
+
+        if out is None:
+            out = np.empty(self.grid.shape, np.float32)
+        ptr = out.data_ptr() if hasattr(out, "data_ptr") else out.ctypes.data
+        _check(lib().sb200_run_get_field(self._h, ptr))
+        return out
+
+    def trace(self, n: int):
+        import numpy as np
+
+        out = np.empty(n, np.float32)
+        _check(lib().sb200_run_get_trace(self._h, out.ctypes.data, n))
+        return out
+
+    def stats(self):
+        import numpy as np
+
+        out = np.zeros(3, np.float64)
+        _check(lib().sb200_run_stats(self._h, out.ctypes.data))
+        return out
+
+    @property
+    def steps_done(self) -> int:
+        return lib().sb200_run_steps_done(self._h)
+
+    @property
+    def stream(self) -> int:
+        return lib().sb200_run_stream(self._h) or 0
 
 
 def device_error(clear: bool = True) -> int:

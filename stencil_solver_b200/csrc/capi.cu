@@ -76,13 +76,33 @@ struct Override {
     int zchunks = 1;
 };
 std::mutex g_cfg_mu;
-Override g_override[2];
+Override g_override[3];
+
+bool valid_kind(int kind) {
+    return kind == SB200_KIND_WAVE_F32 || kind == SB200_KIND_HEAT_F32 ||
+           kind == SB200_KIND_WAVE_F16;
+}
+
+int variant_count(int kind) {
+    return kind == SB200_KIND_WAVE_F16 ? pencil_f16_variant_count()
+                                       : pencil_f32_variant_count(kind == SB200_KIND_HEAT_F32);
+}
 
 int sm_count() {
     int dev = 0, n = 148;
     if (cudaGetDevice(&dev) == cudaSuccess)
         cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
     return n;
+}
+
+// z split for the FP16 kernel's default tile: the smallest split reaching at
+// least 6 waves (the FP32 measurements favour several waves over one long march).
+int f16_zchunks(const GridDesc& g) {
+    const double slots = double(sm_count()) * std::max(1, pencil_f16_resident(0));
+    const int inz = static_cast<int>(g.nz - 8);
+    for (int zc = 1; zc <= 16 && zc <= inz; ++zc)
+        if (double(pencil_f16_ctas(0, g, zc)) / slots >= 6.0) return zc;
+    return std::max(1, std::min(16, inz));
 }
 
 PencilConfig choose(int kind, const GridDesc& g) {
@@ -109,7 +129,8 @@ PencilConfig choose(int kind, const GridDesc& g) {
     auto it = memo.find(key);
     if (it != memo.end()) return it->second;
     c.variant = 0;
-    c.zchunks = zchunk_ranking(kind == SB200_KIND_HEAT_F32, 0, g, 1).front();
+    c.zchunks = kind == SB200_KIND_WAVE_F16 ? f16_zchunks(g)
+                                            : zchunk_ranking(kind == SB200_KIND_HEAT_F32, 0, g, 1).front();
     memo[key] = c;
     return c;
 }
@@ -177,7 +198,57 @@ SourceDesc host_source(int64_t idx, float amp) {
     return s;
 }
 
+int wave_step_f16(const uint16_t* p, uint16_t* p_prev_next, const uint16_t* k,
+                  const sb200_grid* grid, const SourceDesc& src, const sb200_f16_scale* scale,
+                  int phase, void* stream) {
+    const char* where = "sb200_wave_step_f16";
+    GridDesc g;
+    if (int rc = to_desc(grid, &g)) return rc;
+    if (!p || !p_prev_next || !k || !scale)
+        return fail(SB200_ERR_INVALID, std::string(where) + ": NULL pointer");
+    if (p == p_prev_next)
+        return fail(SB200_ERR_INVALID, std::string(where) + ": p_next must not alias p");
+    if (phase < 0 || phase > 2) return fail(SB200_ERR_INVALID, std::string(where) + ": bad phase");
+    if (src.idx >= g.size())
+        return fail(SB200_ERR_INVALID, std::string(where) + ": source index outside the grid");
+    if (src.idx >= 0 && src.wavelet && !src.step)
+        return fail(SB200_ERR_INVALID, std::string(where) + ": wavelet without step pointer");
+    if (!g.has_interior()) return SB200_OK;
+    if (g.nx % 8 != 0 || !aligned16(p) || !aligned16(p_prev_next) || !aligned16(k))
+        return fail(SB200_ERR_UNSUPPORTED,
+                    std::string(where) + ": needs nx % 8 == 0 and 16-byte aligned fields");
+    const PencilConfig cfg = choose(SB200_KIND_WAVE_F16, g);
+    const PencilBoxes b = pencil_f16_boxes(cfg.variant);
+    PencilMaps maps;
+    int rc = tensor_map_3d(&maps.p, p, g.nx, g.ny, g.nz, 2, b.halo_x, b.halo_y);
+    if (!rc) rc = tensor_map_3d(&maps.prev, p_prev_next, g.nx, g.ny, g.nz, 2, b.tile_x, b.tile_y);
+    if (!rc) rc = tensor_map_3d(&maps.vel2, k, g.nx, g.ny, g.nz, 2, b.tile_x, b.tile_y);
+    if (rc)
+        return fail(SB200_ERR_CUDA, std::string(where) + ": tensor map encode failed (" +
+                                        std::to_string(rc) + ")");
+    return finish_launch(
+        launch_wave_pencil_f16(maps, p_prev_next, g, src, reinterpret_cast<const F16Scale*>(scale),
+                               phase, cfg, device_error_ptr(), static_cast<cudaStream_t>(stream)),
+        where);
+}
+
 }  // namespace
+
+// Step dispatch with a full source descriptor (trace included), for the run
+// engine; the public entry points wrap these.
+int dispatch_wave_f32(const float* p, const float* p_prev, const float* vel2, float* p_next,
+                      const sb200_grid* grid, const SourceDesc& src, void* stream, bool exact) {
+    return wave_step(p, p_prev, vel2, p_next, grid, src, stream, !exact,
+                     exact ? "sb200_wave_step_exact_f32" : "sb200_wave_step_f32");
+}
+
+int dispatch_wave_f16(const uint16_t* p, uint16_t* p_prev_next, const uint16_t* k,
+                      const sb200_grid* grid, const SourceDesc& src, const sb200_f16_scale* scale,
+                      int phase, void* stream) {
+    return wave_step_f16(p, p_prev_next, k, grid, src, scale, phase, stream);
+}
+
+int set_error(int code, const std::string& msg) { return fail(code, msg); }
 
 // A wave is SMs x resident CTAs; a split whose CTA count leaves the last wave
 // mostly empty wastes that fraction of the machine, and every extra split
@@ -332,21 +403,113 @@ int sb200_heat_step_f32(const float* u, float* u_next, const sb200_grid* grid, f
     return finish_launch(launch_heat_naive(u, u_next, g, alpha_dt, st), "sb200_heat_step_f32");
 }
 
+int sb200_f16_pack(const float* src, uint16_t* dst, int64_t n, float scale, void* stream) {
+    if (!src || !dst || n < 0) return fail(SB200_ERR_INVALID, "sb200_f16_pack: bad arguments");
+    if (!(scale > 0.f) || !std::isfinite(scale))
+        return fail(SB200_ERR_INVALID, "sb200_f16_pack: scale must be positive");
+    if (n == 0) return SB200_OK;
+    return finish_launch(launch_f16_pack(src, dst, n, scale, static_cast<cudaStream_t>(stream)),
+                         "sb200_f16_pack");
+}
+
+int sb200_f16_unpack(const uint16_t* src, float* dst, int64_t n, float scale, void* stream) {
+    if (!src || !dst || n < 0)
+        return fail(SB200_ERR_INVALID, "sb200_f16_unpack: bad arguments");
+    if (!(scale > 0.f) || !std::isfinite(scale))
+        return fail(SB200_ERR_INVALID, "sb200_f16_unpack: scale must be positive");
+    if (n == 0) return SB200_OK;
+    return finish_launch(launch_f16_unpack(src, dst, n, scale, static_cast<cudaStream_t>(stream)),
+                         "sb200_f16_unpack");
+}
+
+int sb200_k_field_bf16(const float* vel2, uint16_t* k, const sb200_grid* grid, void* stream) {
+    GridDesc g;
+    if (int rc = to_desc(grid, &g)) return rc;
+    if (!vel2 || !k) return fail(SB200_ERR_INVALID, "sb200_k_field_bf16: NULL pointer");
+    if (!(g.dt > 0.f)) return fail(SB200_ERR_INVALID, "sb200_k_field_bf16: dt must be positive");
+    if (g.size() == 0) return SB200_OK;
+    const float f = static_cast<float>(double(g.dt) * g.dt / (double(g.dx) * g.dx));
+    return finish_launch(launch_k_bf16(vel2, k, g.size(), f, static_cast<cudaStream_t>(stream)),
+                         "sb200_k_field_bf16");
+}
+
+int sb200_wave_step_f16(const uint16_t* p, uint16_t* p_prev_next, const uint16_t* k,
+                        const sb200_grid* grid, int64_t src_index, float src_amp,
+                        const float* wavelet, const int* step, int step_offset,
+                        const sb200_f16_scale* scale, int phase, void* stream) {
+    SourceDesc src;
+    src.idx = src_index;
+    src.w = src_amp;
+    src.wavelet = wavelet;
+    src.step = step;
+    src.step_offset = step_offset;
+    return wave_step_f16(p, p_prev_next, k, grid, src, scale, phase, stream);
+}
+
+int sb200_f16_renorm(const double* stats3, sb200_f16_scale* scale, const float* bound,
+                     const int* step, float bound_host, float target, void* stream) {
+    if (!stats3 || !scale || (bound && !step))
+        return fail(SB200_ERR_INVALID, "sb200_f16_renorm: NULL pointer");
+    if (!(target > 0.f) || !(bound_host >= 0.f))
+        return fail(SB200_ERR_INVALID, "sb200_f16_renorm: bad target / bound");
+    return finish_launch(launch_f16_renorm(stats3, reinterpret_cast<F16Scale*>(scale), bound,
+                                           step, bound_host, target,
+                                           static_cast<cudaStream_t>(stream)),
+                         "sb200_f16_renorm");
+}
+
+int64_t sb200_field_stats_scratch_len(const sb200_grid* grid) {
+    GridDesc g;
+    if (int rc = to_desc(grid, &g)) return rc;
+    if (!g.has_interior()) return fail(SB200_ERR_INVALID, "grid has no interior");
+    return 3 * static_cast<int64_t>(stats_blocks(g));
+}
+
+namespace {
+int field_stats(const void* field, bool half, const sb200_grid* grid, float scale, double* out3,
+                double* scratch, int64_t scratch_len, void* stream, const char* where) {
+    GridDesc g;
+    if (int rc = to_desc(grid, &g)) return rc;
+    if (!field || !out3 || !scratch)
+        return fail(SB200_ERR_INVALID, std::string(where) + ": NULL pointer");
+    if (!g.has_interior()) return fail(SB200_ERR_INVALID, std::string(where) + ": no interior");
+    if (!(scale > 0.f) || !std::isfinite(scale))
+        return fail(SB200_ERR_INVALID, std::string(where) + ": scale must be positive");
+    if (scratch_len < 3 * static_cast<int64_t>(stats_blocks(g)))
+        return fail(SB200_ERR_INVALID, std::string(where) + ": scratch too small (need " +
+                                           std::to_string(3 * stats_blocks(g)) + " doubles)");
+    return finish_launch(launch_field_stats(field, half, g, scale, out3, scratch,
+                                            static_cast<cudaStream_t>(stream)),
+                         where);
+}
+}  // namespace
+
+int sb200_field_stats_f32(const float* field, const sb200_grid* grid, double* out3,
+                          double* scratch, int64_t scratch_len, void* stream) {
+    return field_stats(field, false, grid, 1.0f, out3, scratch, scratch_len, stream,
+                       "sb200_field_stats_f32");
+}
+
+int sb200_field_stats_f16(const uint16_t* field, const sb200_grid* grid, float scale,
+                          double* out3, double* scratch, int64_t scratch_len, void* stream) {
+    return field_stats(field, true, grid, scale, out3, scratch, scratch_len, stream,
+                       "sb200_field_stats_f16");
+}
+
 int sb200_pencil_variant_count(int kind) {
-    if (kind != SB200_KIND_WAVE_F32 && kind != SB200_KIND_HEAT_F32)
-        return fail(SB200_ERR_INVALID, "unknown kernel kind");
-    return pencil_f32_variant_count(kind == SB200_KIND_HEAT_F32);
+    if (!valid_kind(kind)) return fail(SB200_ERR_INVALID, "unknown kernel kind");
+    return variant_count(kind);
 }
 
 const char* sb200_pencil_variant_name(int kind, int variant) {
-    if (kind != SB200_KIND_WAVE_F32 && kind != SB200_KIND_HEAT_F32) return nullptr;
+    if (!valid_kind(kind)) return nullptr;
+    if (kind == SB200_KIND_WAVE_F16) return pencil_f16_variant_name(variant);
     return pencil_f32_variant_name(kind == SB200_KIND_HEAT_F32, variant);
 }
 
 int sb200_set_pencil_override(int kind, int variant, int zchunks) {
-    if (kind != SB200_KIND_WAVE_F32 && kind != SB200_KIND_HEAT_F32)
-        return fail(SB200_ERR_INVALID, "unknown kernel kind");
-    if (variant >= pencil_f32_variant_count(kind == SB200_KIND_HEAT_F32))
+    if (!valid_kind(kind)) return fail(SB200_ERR_INVALID, "unknown kernel kind");
+    if (variant >= variant_count(kind))
         return fail(SB200_ERR_INVALID, "variant out of range");
     if (zchunks < 1) return fail(SB200_ERR_INVALID, "zchunks must be >= 1");
     std::lock_guard<std::mutex> lock(g_cfg_mu);
@@ -356,8 +519,7 @@ int sb200_set_pencil_override(int kind, int variant, int zchunks) {
 }
 
 int sb200_pencil_choice(int kind, const sb200_grid* grid, int* variant, int* zchunks) {
-    if (kind != SB200_KIND_WAVE_F32 && kind != SB200_KIND_HEAT_F32)
-        return fail(SB200_ERR_INVALID, "unknown kernel kind");
+    if (!valid_kind(kind)) return fail(SB200_ERR_INVALID, "unknown kernel kind");
     GridDesc g;
     if (int rc = to_desc(grid, &g)) return rc;
     if (!variant || !zchunks) return fail(SB200_ERR_INVALID, "NULL output pointer");

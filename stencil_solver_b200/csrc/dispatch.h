@@ -1,0 +1,21 @@
+// Internal step dispatch shared by the C ABI (capi.cu) and the run engine
+// (run.cu): argument checks, kernel choice and tensor maps, with the full
+// source descriptor (wavelet, device step counter, trace).
+#pragma once
+
+#include <string>
+
+#include "kernels.h"
+#include "stencil_b200.h"
+
+namespace sb200 {
+
+int dispatch_wave_f32(const float* p, const float* p_prev, const float* vel2, float* p_next,
+                      const sb200_grid* grid, const SourceDesc& src, void* stream, bool exact);
+int dispatch_wave_f16(const uint16_t* p, uint16_t* p_prev_next, const uint16_t* k,
+                      const sb200_grid* grid, const SourceDesc& src, const sb200_f16_scale* scale,
+                      int phase, void* stream);
+// Records msg as the calling thread's last error and returns code.
+int set_error(int code, const std::string& msg);
+
+}  // namespace sb200

@@ -30,13 +30,16 @@ struct PencilConfig {
 // Source injection for one step: p_next[idx] += (dt^2*vel2[idx]) * w.
 // When wavelet != nullptr the sample is read on the device as
 // wavelet[*step + step_offset], which lets a captured CUDA graph replay a chunk of
-// steps against a device-side step counter.
+// steps against a device-side step counter.  When trace != nullptr the thread
+// that injects also records the new value at the source (physical units) in
+// trace[(step ? *step : 0) + step_offset].
 struct SourceDesc {
     int64_t idx = -1;
     float w = 0.f;
     const float* wavelet = nullptr;
     const int* step = nullptr;
     int step_offset = 0;
+    float* trace = nullptr;
 };
 
 cudaError_t launch_wave_naive(const float* cur, const float* prev, const float* vel2,
@@ -72,7 +75,12 @@ cudaError_t launch_heat_pencil_f32(const PencilMaps& maps, float* u_next, const 
                                    float alpha_dt, const PencilConfig& cfg, int* err,
                                    cudaStream_t stream);
 // Resident CTAs per SM of a variant (occupancy query; analytic if that fails).
+// The first call per device also sets the variant's shared-memory attribute.
 int pencil_f32_resident(bool heat, int v);
+// Sets up every variant on the current device (before a stream capture, whose
+// launches must not be the first ones).
+void pencil_f32_prepare();
+void pencil_f16_prepare();
 // Number of CTAs a launch uses (for occupancy/wave reasoning in the tuner).
 int64_t pencil_f32_ctas(bool heat, int v, const GridDesc& g, int zchunks);
 
@@ -84,6 +92,41 @@ std::vector<int> zchunk_ranking(bool heat, int v, const GridDesc& g, int max_n);
 // Tuned (variant, zchunks) for kind on grid g on the current device, if the
 // tuner has one (tuner.cpp).
 bool tuned_choice(int kind, const GridDesc& g, PencilConfig* out);
+
+// Storage scale of the FP16 path, in device memory: fields hold a * p; a
+// renormalisation sets a to a_new and r = a_new / a_old (powers of two).
+struct F16Scale {
+    float a;
+    float r;
+};
+
+// FP16-storage acoustic pencil kernel (pencil_f16.cu).  phase 0: plain step;
+// 1: output scaled by r (renormalisation step); 2: p_prev scaled by r.
+// Preconditions: nx % 8 == 0, 16-byte aligned pointers.
+int pencil_f16_variant_count();
+const char* pencil_f16_variant_name(int v);
+PencilBoxes pencil_f16_boxes(int v);
+int pencil_f16_resident(int v);
+int64_t pencil_f16_ctas(int v, const GridDesc& g, int zchunks);
+cudaError_t launch_wave_pencil_f16(const PencilMaps& maps, uint16_t* next, const GridDesc& g,
+                                   const SourceDesc& src, const F16Scale* scale, int phase,
+                                   const PencilConfig& cfg, int* err, cudaStream_t stream);
+
+cudaError_t launch_f16_pack(const float* f, uint16_t* h, int64_t n, float scale, cudaStream_t st);
+cudaError_t launch_f16_unpack(const uint16_t* h, float* f, int64_t n, float scale,
+                              cudaStream_t st);
+cudaError_t launch_k_bf16(const float* vel2, uint16_t* k, int64_t n, float dt2_over_dx2,
+                          cudaStream_t st);
+cudaError_t launch_f16_renorm(const double* stats3, F16Scale* scale, const float* bound,
+                              const int* step, float bound_host, float target, cudaStream_t st);
+
+// FP64 interior statistics (reduce.cu): out3 = {sum of (f/scale)^2, max |f/scale|,
+// count of non-finite values}.  scratch holds 3 doubles per pass-1 block
+// (stats_blocks(g) blocks, at most kMaxStatsBlocks).
+constexpr int kMaxStatsBlocks = 1184;  // 148 SMs x 8
+int stats_blocks(const GridDesc& g);
+cudaError_t launch_field_stats(const void* field, bool half, const GridDesc& g, float scale,
+                               double* out3, double* scratch, cudaStream_t stream);
 
 // Tensor maps (tmap.cpp).  Encodes (and caches) a 3-D tiled map over a
 // halo-inclusive field of element size esize bytes with the given box and copies

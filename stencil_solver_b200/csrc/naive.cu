@@ -27,6 +27,7 @@ struct NaiveArgs {
     const float* wavelet;  // device samples: wavelet[*step + step_off]
     const int* step;
     int step_off;
+    float* trace;  // value at the source after the step, at [(*step or 0) + step_off]
 };
 
 template <bool kHeat>
@@ -65,6 +66,7 @@ __global__ void __launch_bounds__(256) naive_kernel(NaiveArgs a) {
         if (c == a.src) {
             const float w = a.wavelet ? a.wavelet[*a.step + a.step_off] : a.src_w;
             out = __fadd_rn(out, __fmul_rn(kv, w));
+            if (a.trace) a.trace[(a.step ? *a.step : 0) + a.step_off] = out;
         }
     }
     a.next[c] = out;
@@ -110,6 +112,7 @@ cudaError_t launch_wave_naive(const float* cur, const float* prev, const float* 
     a.wavelet = src.wavelet;
     a.step = src.step;
     a.step_off = src.step_offset;
+    a.trace = src.trace;
     naive_kernel<false><<<naive_grid(g, block), block, 0, stream>>>(a);
     return cudaGetLastError();
 }

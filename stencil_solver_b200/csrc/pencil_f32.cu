@@ -48,6 +48,7 @@ struct PencilArgs {
     const float* src_wavelet;
     const int* src_step;
     int src_off;
+    float* trace;
     int* err;
 };
 
@@ -298,6 +299,9 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S, AUX>::NT, Shape<TX, TY, 
                             if (src_i == 1) o.y = o.y + add;
                             if (src_i == 2) o.z = o.z + add;
                             if (src_i == 3) o.w = o.w + add;
+                            if (a.trace)
+                                a.trace[(a.src_step ? *a.src_step : 0) + a.src_off] =
+                                    f4get(o, src_i);
                         }
                     }
                     if (rin[j]) stg_stream(a.next + goff + j * a.sy, o);
@@ -338,25 +342,6 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S, AUX>::NT, Shape<TX, TY, 
 using LaunchFn = cudaError_t (*)(const PencilMaps&, const PencilArgs&, unsigned, cudaStream_t);
 using ResidentFn = int (*)();
 
-template <int TX, int TY, int RPT, int S, int AUX, bool HEAT>
-cudaError_t launch_variant(const PencilMaps& m, const PencilArgs& a, unsigned ctas,
-                           cudaStream_t stream) {
-    using P = Shape<TX, TY, RPT, S, AUX>;
-    auto kern = pencil_f32_kernel<TX, TY, RPT, S, AUX, HEAT>;
-    // The attribute is per function and device; set once per device.
-    static std::once_flag once[64];
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaError_t st = cudaSuccess;
-    std::call_once(once[dev & 63], [&] {
-        st = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>(P::SMEM));
-    });
-    if (st != cudaSuccess) return st;
-    kern<<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev, m.vel2, a);
-    return cudaGetLastError();
-}
-
 // CTAs of a variant that fit on one SM: the occupancy calculator when a device
 // is present, else the shared-memory / register limits computed here.
 template <int TX, int TY, int RPT, int S, int AUX, bool HEAT>
@@ -379,6 +364,17 @@ int resident_variant() {
     const int by_smem = int((228u * 1024u) / (P::SMEM + 1024u));
     const int by_regs = 65536 / (P::NT * 128);
     return std::max(1, std::min(by_smem, by_regs));
+}
+
+template <int TX, int TY, int RPT, int S, int AUX, bool HEAT>
+cudaError_t launch_variant(const PencilMaps& m, const PencilArgs& a, unsigned ctas,
+                           cudaStream_t stream) {
+    using P = Shape<TX, TY, RPT, S, AUX>;
+    // Sets the shared-memory attribute on the first call per device (cached).
+    resident_variant<TX, TY, RPT, S, AUX, HEAT>();
+    pencil_f32_kernel<TX, TY, RPT, S, AUX, HEAT><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
+                                                                                 m.vel2, a);
+    return cudaGetLastError();
 }
 
 struct Variant {
@@ -477,6 +473,11 @@ PencilBoxes pencil_f32_boxes(bool heat, int v) {
 
 int pencil_f32_resident(bool heat, int v) { return variant_of(heat, v).resident(); }
 
+void pencil_f32_prepare() {
+    for (int v = 0; v < kNumWave; ++v) kWave[v].resident();
+    for (int v = 0; v < kNumHeat; ++v) kHeat[v].resident();
+}
+
 int64_t pencil_f32_ctas(bool heat, int v, const GridDesc& g, int zchunks) {
     return ctas_of(base_args(variant_of(heat, v), g, zchunks, nullptr), g);
 }
@@ -500,6 +501,7 @@ cudaError_t launch_wave_pencil_f32(const PencilMaps& maps, const float* prev, co
         a.src_wavelet = src.wavelet;
         a.src_step = src.step;
         a.src_off = src.step_offset;
+        a.trace = src.trace;
     }
     return v.launch(maps, a, ctas_of(a, g), stream);
 }
