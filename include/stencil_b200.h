@@ -173,6 +173,19 @@ int sb200_field_stats_f32(const float* field, const sb200_grid* grid, double* ou
 /* The same over an FP16 field stored scaled by `scale` (a value v is v/scale). */
 int sb200_field_stats_f16(const uint16_t* field, const sb200_grid* grid, float scale,
                           double* out3, double* scratch, int64_t scratch_len, void* stream);
+/* No reference counterpart.  sb200_field_stats_f32 without a scratch argument,
+ * for callers that cannot allocate device memory (for example a monitor
+ * running while another thread captures a CUDA graph in global capture mode,
+ * where cudaMalloc is refused).  It allocates nothing: the per-block partials
+ * go to a static device array of 3 * 1184 doubles (28,416 bytes) in the
+ * library, which no grid outgrows (a larger need would be rejected with
+ * SB200_ERR_INVALID).  Same kernels and block count as sb200_field_stats_f32,
+ * so the same bits.  Nothing in the array must start at zero.  The array is
+ * shared per device: calls that overlap on the device (unordered streams) race.
+ * The first call per device looks up the array's address
+ * (cudaGetSymbolAddress); make it before any stream capture starts. */
+int sb200_field_stats_f32_noalloc(const float* field, const sb200_grid* grid, double* out3,
+                                  void* stream);
 
 /* ── pencil-kernel configuration (used by the tuner and the tests) ──────────── */
 #define SB200_KIND_WAVE_F32 0

@@ -126,6 +126,8 @@ _SIGNATURES = {
                                C.c_int64, C.c_void_p], C.c_int),
     "sb200_field_stats_f16": ([C.c_void_p, C.POINTER(sb200_grid), C.c_float, C.c_void_p,
                                C.c_void_p, C.c_int64, C.c_void_p], C.c_int),
+    "sb200_field_stats_f32_noalloc": ([C.c_void_p, C.POINTER(sb200_grid), C.c_void_p, C.c_void_p],
+                                      C.c_int),
     "sb200_f16_pack": ([C.c_void_p, C.c_void_p, C.c_int64, C.c_float, C.c_void_p], C.c_int),
     "sb200_f16_unpack": ([C.c_void_p, C.c_void_p, C.c_int64, C.c_float, C.c_void_p], C.c_int),
     "sb200_k_field_bf16": ([C.c_void_p, C.c_void_p, C.POINTER(sb200_grid), C.c_void_p], C.c_int),
@@ -298,6 +300,13 @@ def field_stats(field, grid: Grid, out3, scratch, scale: float = 1.0, stream=Non
     else:
         _check(lib().sb200_field_stats_f32(_ptr(field), _g(grid), _ptr(out3), _ptr(scratch), n,
                                            _stream(stream)))
+
+
+def field_stats_noalloc(field, grid: Grid, out3, stream=None) -> None:
+    """field_stats of an FP32 field with the library's static device scratch:
+    allocates nothing.  Calls that overlap on the device share that scratch."""
+    _check(lib().sb200_field_stats_f32_noalloc(_ptr(field), _g(grid), _ptr(out3),
+                                               _stream(stream)))
 
 
 def f16_pack(src, dst, n: int, scale: float, stream=None) -> None:
