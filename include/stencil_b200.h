@@ -266,6 +266,51 @@ int sb200_tune(int kind, const sb200_grid* grid, const void* field, const void* 
 int sb200_tune_save(const char* path);
 int sb200_tune_load(const char* path);
 
+/* ── batched shots ─────────────────────────────────────────────────────────
+ * No reference counterpart (the reference runs one grid per solver).  Many
+ * independent acoustic shots of uneven sizes advance together: each step is one
+ * persistent launch whose CTAs pull (shot, tile, z chunk) items from a device
+ * work queue; chunks of graph_chunk steps replay from captured CUDA graphs.
+ * Every shot uses the same arithmetic as sb200_wave_step_f32 (in-place leapfrog,
+ * source rule p[src] += dt^2 vel2[src] w[n] after the update, trace = p[src]
+ * after each step).  Shots need nx % 4 == 0 and a source (if any) in the
+ * interior.  The handle owns its device memory and a non-blocking stream. */
+typedef struct {
+    sb200_grid grid;
+    int64_t src_index; /* flat source cell, or -1 */
+} sb200_shot;
+
+typedef struct {
+    int precision;     /* SB200_PRECISION_F32 */
+    int graph_chunk;   /* steps per captured graph; 0 = one launch per step */
+    int64_t max_steps; /* capacity of the per-shot wavelet and trace tables */
+} sb200_batch_config;
+
+void sb200_batch_config_init(sb200_batch_config* cfg);
+int sb200_batch_create(const sb200_shot* shots, int n_shots, const sb200_batch_config* cfg,
+                       void** handle);
+int sb200_batch_destroy(void* handle);
+/* Host fields of one shot (halo-inclusive, z-major); p_prev NULL means p. */
+int sb200_batch_set_fields(void* handle, int shot, const float* p, const float* p_prev,
+                           const float* vel2);
+/* Source samples w[0..n) of one shot (n <= max_steps; the rest stay zero). */
+int sb200_batch_set_wavelet(void* handle, int shot, const float* w, int64_t n);
+/* Enqueues n steps of every shot; the run may not pass max_steps in total. */
+int sb200_batch_steps(void* handle, int64_t n);
+int sb200_batch_synchronize(void* handle);
+int sb200_batch_get_field(void* handle, int shot, float* p);
+int sb200_batch_get_trace(void* handle, int shot, float* trace, int64_t n);
+/* Times every (tile variant, z-chunk length) on the batch's own buffers and
+ * keeps the fastest (cached per process by the shots' extents).  Call it before
+ * sb200_batch_set_fields: it leaves fields, traces and the step count zeroed. */
+int sb200_batch_tune(void* handle, int reps);
+int sb200_batch_set_choice(void* handle, int variant, int zlen);
+int sb200_batch_choice(void* handle, int* variant, int* zlen, int* n_items, int* ctas);
+int64_t sb200_batch_steps_done(void* handle);
+void* sb200_batch_stream(void* handle);
+int sb200_batch_variant_count(void);
+const char* sb200_batch_variant_name(int variant);
+
 #ifdef __cplusplus
 }
 #endif

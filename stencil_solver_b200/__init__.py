@@ -82,6 +82,14 @@ class sb200_run_config(C.Structure):
                 ("monitor_limit", C.c_float), ("f16_target", C.c_float)]
 
 
+class sb200_shot(C.Structure):
+    _fields_ = [("grid", sb200_grid), ("src_index", C.c_int64)]
+
+
+class sb200_batch_config(C.Structure):
+    _fields_ = [("precision", C.c_int), ("graph_chunk", C.c_int), ("max_steps", C.c_int64)]
+
+
 class sb200_f16_scale(C.Structure):
     _fields_ = [("a", C.c_float), ("r", C.c_float)]
 
@@ -148,6 +156,23 @@ _SIGNATURES = {
     "sb200_run_stats": ([C.c_void_p, C.c_void_p], C.c_int),
     "sb200_run_steps_done": ([C.c_void_p], C.c_int64),
     "sb200_run_stream": ([C.c_void_p], C.c_void_p),
+    "sb200_batch_config_init": ([C.POINTER(sb200_batch_config)], None),
+    "sb200_batch_create": ([C.POINTER(sb200_shot), C.c_int, C.POINTER(sb200_batch_config),
+                            C.POINTER(C.c_void_p)], C.c_int),
+    "sb200_batch_destroy": ([C.c_void_p], C.c_int),
+    "sb200_batch_set_fields": ([C.c_void_p, C.c_int] + [C.c_void_p] * 3, C.c_int),
+    "sb200_batch_set_wavelet": ([C.c_void_p, C.c_int, C.c_void_p, C.c_int64], C.c_int),
+    "sb200_batch_steps": ([C.c_void_p, C.c_int64], C.c_int),
+    "sb200_batch_synchronize": ([C.c_void_p], C.c_int),
+    "sb200_batch_get_field": ([C.c_void_p, C.c_int, C.c_void_p], C.c_int),
+    "sb200_batch_get_trace": ([C.c_void_p, C.c_int, C.c_void_p, C.c_int64], C.c_int),
+    "sb200_batch_tune": ([C.c_void_p, C.c_int], C.c_int),
+    "sb200_batch_set_choice": ([C.c_void_p, C.c_int, C.c_int], C.c_int),
+    "sb200_batch_choice": ([C.c_void_p] + [C.POINTER(C.c_int)] * 4, C.c_int),
+    "sb200_batch_steps_done": ([C.c_void_p], C.c_int64),
+    "sb200_batch_stream": ([C.c_void_p], C.c_void_p),
+    "sb200_batch_variant_count": ([], C.c_int),
+    "sb200_batch_variant_name": ([C.c_int], C.c_char_p),
     "sb200_pencil_variant_count": ([C.c_int], C.c_int),
     "sb200_pencil_variant_name": ([C.c_int, C.c_int], C.c_char_p),
     "sb200_set_pencil_override": ([C.c_int, C.c_int, C.c_int], C.c_int),
@@ -353,11 +378,12 @@ class Run:
         h = C.c_void_p()
         _check(lib().sb200_run_create(C.byref(cfg), C.byref(h)))
         self._h = h
+        self._destroy = lib().sb200_run_destroy  # still callable at interpreter exit
         self.grid = grid
 
     def close(self):
         if getattr(self, "_h", None):
-            lib().sb200_run_destroy(self._h)
+            self._destroy(self._h)
             self._h = None
 
     __del__ = close
@@ -467,3 +493,91 @@ def pencil_choice(kind: int, grid: Grid):
     v, z = C.c_int(), C.c_int()
     _check(lib().sb200_pencil_choice(kind, _g(grid), C.byref(v), C.byref(z)))
     return v.value, z.value
+
+
+class Batch:
+    """Independent acoustic shots of uneven sizes advanced together by one
+    persistent launch per step (C-ABI handle sb200_batch_*).  shots is a list of
+    (Grid, src_index) pairs; max_steps bounds the run (source and trace tables)."""
+
+    def __init__(self, shots, max_steps: int, graph_chunk: int = 100):
+        arr = (sb200_shot * len(shots))()
+        for i, (g, src) in enumerate(shots):
+            arr[i].grid = g.c()
+            arr[i].src_index = -1 if src is None else int(src)
+        cfg = sb200_batch_config()
+        lib().sb200_batch_config_init(C.byref(cfg))
+        cfg.graph_chunk = graph_chunk
+        cfg.max_steps = max_steps
+        h = C.c_void_p()
+        _check(lib().sb200_batch_create(arr, len(shots), C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._destroy = lib().sb200_batch_destroy  # still callable at interpreter exit
+        self.grids = [g for g, _ in shots]
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_fields(self, shot: int, p, p_prev=None, vel2=None) -> None:
+        import numpy as np
+
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+                for a in (p, p_prev, vel2)]
+        ptrs = [None if a is None else a.ctypes.data for a in arrs]
+        _check(lib().sb200_batch_set_fields(self._h, shot, *ptrs))
+
+    def set_wavelet(self, shot: int, w) -> None:
+        import numpy as np
+
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        _check(lib().sb200_batch_set_wavelet(self._h, shot, w.ctypes.data, w.size))
+
+    def steps(self, n: int) -> None:
+        _check(lib().sb200_batch_steps(self._h, n))
+
+    def synchronize(self) -> None:
+        _check(lib().sb200_batch_synchronize(self._h))
+
+    def field(self, shot: int):
+        import numpy as np
+
+        out = np.empty(self.grids[shot].shape, np.float32)
+        _check(lib().sb200_batch_get_field(self._h, shot, out.ctypes.data))
+        return out
+
+    def trace(self, shot: int, n: int):
+        import numpy as np
+
+        out = np.empty(n, np.float32)
+        _check(lib().sb200_batch_get_trace(self._h, shot, out.ctypes.data, n))
+        return out
+
+    def tune(self, reps: int = 3) -> None:
+        _check(lib().sb200_batch_tune(self._h, reps))
+
+    def set_choice(self, variant: int, zlen: int) -> None:
+        _check(lib().sb200_batch_set_choice(self._h, variant, zlen))
+
+    def choice(self) -> dict:
+        v, z, n, c = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        _check(lib().sb200_batch_choice(self._h, C.byref(v), C.byref(z), C.byref(n), C.byref(c)))
+        return {"variant": v.value, "zlen": z.value, "items": n.value, "ctas": c.value,
+                "name": lib().sb200_batch_variant_name(v.value).decode()}
+
+    @property
+    def steps_done(self) -> int:
+        return _check(lib().sb200_batch_steps_done(self._h))
+
+    @property
+    def stream(self) -> int:
+        return lib().sb200_batch_stream(self._h)

@@ -250,6 +250,8 @@ int dispatch_wave_f16(const uint16_t* p, uint16_t* p_prev_next, const uint16_t* 
 
 int set_error(int code, const std::string& msg) { return fail(code, msg); }
 
+int* device_error_word() { return device_error_ptr(); }
+
 // A wave is SMs x resident CTAs; a split whose CTA count leaves the last wave
 // mostly empty wastes that fraction of the machine, and every extra split
 // re-reads 8 halo planes of p (p is 1 of 4 streams for the acoustic kernel,

@@ -17,5 +17,8 @@ int dispatch_wave_f16(const uint16_t* p, uint16_t* p_prev_next, const uint16_t* 
                       int phase, void* stream);
 // Records msg as the calling thread's last error and returns code.
 int set_error(int code, const std::string& msg);
+// Address of the library's device error word on the current device (the word
+// kernels record bounded-wait failures in), or nullptr if it cannot be looked up.
+int* device_error_word();
 
 }  // namespace sb200

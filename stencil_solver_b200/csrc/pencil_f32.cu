@@ -27,30 +27,13 @@
 #include <algorithm>
 #include <mutex>
 
+#include "batch.h"
 #include "kernels.h"
 #include "sb200_common.cuh"
 
 namespace sb200 {
 
 namespace {
-
-struct PencilArgs {
-    const float* prev;  // acoustic, AUX = 0: p at t-dt (may alias next)
-    const float* vel2;  // acoustic, AUX = 0: v^2
-    float* next;
-    int nx, ny, nz;
-    int64_t sy, sz;
-    int tiles_x, tiles_y, zlen;
-    Weights w;  // acoustic: weights * dt^2; heat: weights * alpha*dt
-    float dt2;  // acoustic: dt^2 (source term)
-    int src_x, src_y, src_z;  // -1 when there is no source
-    float src_w;
-    const float* src_wavelet;
-    const int* src_step;
-    int src_off;
-    float* trace;
-    int* err;
-};
 
 template <int TX, int TY, int RPT, int S, int AUX>
 struct Shape {
@@ -87,64 +70,72 @@ __device__ __forceinline__ void add_y_row(float (&ya)[RPT][4], const float4& v, 
     }
 }
 
+// Ring position a CTA carries from one tile to the next: the sequence numbers of
+// the next p plane and the next aux iteration.  Stage = seq % ring size, phase
+// parity = (seq / ring size) & 1, so the mbarriers are initialised once per CTA
+// and their phases simply continue across the tiles a persistent CTA processes.
+struct Ring {
+    uint32_t p = 0;
+    uint32_t aux = 0;
+};
+
+// One tile: columns [x0, x0+TX) x [y0, y0+TY) of the interior, marched over the
+// z chunk zc.  All threads of the CTA call it; `sm`, `full` and `auxf` are the
+// CTA's rings, initialised by the caller.  Returns false when a bounded wait gave
+// up: the error is recorded and every copy in flight has landed.
 template <int TX, int TY, int RPT, int S, int AUX, bool HEAT>
-__global__ void __launch_bounds__(Shape<TX, TY, RPT, S, AUX>::NT, Shape<TX, TY, RPT, S, AUX>::MINB)
-    pencil_f32_kernel(const __grid_constant__ CUtensorMap pmap,
-                      const __grid_constant__ CUtensorMap qmap,
-                      const __grid_constant__ CUtensorMap vmap, const PencilArgs a) {
+__device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUtensorMap* qmap,
+                                            const CUtensorMap* vmap, const PencilArgs& a,
+                                            int tile_x, int tile_y, int zc, float* sm,
+                                            uint64_t* full, uint64_t* auxf, Ring& ring) {
     using P = Shape<TX, TY, RPT, S, AUX>;
     constexpr bool kAuxTma = !HEAT && AUX > 0;
     constexpr int NAUX = AUX > 0 ? AUX : 1;
-    extern __shared__ unsigned char dsmem[];
-    __shared__ __align__(8) uint64_t full[S];
-    __shared__ __align__(8) uint64_t auxf[NAUX];
-    float* sm = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(dsmem) + 127) &
-                                         ~uintptr_t(127));
     float* aux = sm + S * P::PLANE;  // AUX stages of [p_prev tile | vel2 tile]
 
     const int tid = threadIdx.x;
     const int lx = tid % P::TPR;
     const int ly = tid / P::TPR;
-    int b = blockIdx.x;
-    const int tx = b % a.tiles_x;
-    b /= a.tiles_x;
-    const int ty = b % a.tiles_y;
-    b /= a.tiles_y;
-    const int x0 = R + tx * TX;
-    const int y0 = R + ty * TY;
-    const int zb = R + b * a.zlen;
+    const int x0 = R + tile_x * TX;
+    const int y0 = R + tile_y * TY;
+    const int zb = R + zc * a.zlen;
     const int ze = min(zb + a.zlen, a.nz - R);
-    const int nint = ze - zb;          // interior planes this CTA computes (>= 1)
+    const int nint = ze - zb;          // interior planes this tile computes (>= 1)
     const int nplanes = nint + 2 * R;  // planes of p it reads (>= 9)
+    const uint32_t pb = ring.p;        // sequence number of plane 0
+    const uint32_t ab = ring.aux;      // sequence number of aux iteration 0
 
-    if (tid == 0) {
-        prefetch_tmap(&pmap);
-        if (kAuxTma) {
-            prefetch_tmap(&qmap);
-            prefetch_tmap(&vmap);
-        }
-#pragma unroll
-        for (int s = 0; s < S; ++s) mbar_init(&full[s], 1);
-#pragma unroll
-        for (int s = 0; s < NAUX; ++s) mbar_init(&auxf[s], 1);
-        fence_barrier_init();
-    }
-    __syncthreads();
     int issued_hi = -1;      // thread 0: highest p plane handed to TMA
     int aux_issued_hi = -1;  // thread 0: highest aux iteration handed to TMA
+    auto issue_plane = [&](int j) {  // thread 0 only
+        const uint32_t s = (pb + j) % S;
+        mbar_arrive_expect_tx(&full[s], P::PLANE_BYTES);
+        tma_load_3d(sm + s * P::PLANE, pmap, &full[s], x0 - R, y0 - R, zb - R + j);
+        issued_hi = j;
+    };
     auto issue_aux = [&](int it) {  // thread 0 only
-        float* st = aux + (it % NAUX) * 2 * P::TILE;
-        mbar_arrive_expect_tx(&auxf[it % NAUX], 2 * P::TILE_BYTES);
-        tma_load_3d(st, &qmap, &auxf[it % NAUX], x0, y0, zb + it);
-        tma_load_3d(st + P::TILE, &vmap, &auxf[it % NAUX], x0, y0, zb + it);
+        const uint32_t s = (ab + it) % NAUX;
+        float* st = aux + s * 2 * P::TILE;
+        mbar_arrive_expect_tx(&auxf[s], 2 * P::TILE_BYTES);
+        tma_load_3d(st, qmap, &auxf[s], x0, y0, zb + it);
+        tma_load_3d(st + P::TILE, vmap, &auxf[s], x0, y0, zb + it);
         aux_issued_hi = it;
     };
+    auto wait_plane = [&](int j) {
+        return mbar_wait(&full[(pb + j) % S], ((pb + j) / S) & 1);
+    };
+    auto wait_aux = [&](int it) {
+        return mbar_wait(&auxf[(ab + it) % NAUX], ((ab + it) / NAUX) & 1);
+    };
+    auto plane = [&](int j) -> const float* { return sm + ((pb + j) % S) * P::PLANE; };
+
     if (tid == 0) {
-        for (int s = 0; s < S && s < nplanes; ++s) {
-            mbar_arrive_expect_tx(&full[s], P::PLANE_BYTES);
-            tma_load_3d(sm + s * P::PLANE, &pmap, &full[s], x0 - R, y0 - R, zb - R + s);
-            issued_hi = s;
+        prefetch_tmap(pmap);
+        if (kAuxTma) {
+            prefetch_tmap(qmap);
+            prefetch_tmap(vmap);
         }
+        for (int s = 0; s < S && s < nplanes; ++s) issue_plane(s);
         if (kAuxTma)
             for (int it = 0; it < NAUX && it < nint; ++it) issue_aux(it);
     }
@@ -180,8 +171,8 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S, AUX>::NT, Shape<TX, TY, 
     // Start-up: planes 0..7 (z = zb-4 .. zb+3) fill queue slots 0..7.
 #pragma unroll
     for (int jj = 0; jj < 8; ++jj) {
-        if (!mbar_wait(&full[jj % S], (jj / S) & 1)) bad = true;
-        const float* pl = sm + (jj % S) * P::PLANE + soff;
+        if (!wait_plane(jj)) bad = true;
+        const float* pl = plane(jj) + soff;
 #pragma unroll
         for (int j = 0; j < RPT; ++j) q[jj][j] = lds128(pl + j * P::SX);
     }
@@ -189,14 +180,8 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S, AUX>::NT, Shape<TX, TY, 
     if (!abort_run && tid == 0) {
         // Planes 0..3 are only queue feed: their stages are free again.
 #pragma unroll
-        for (int jj = 0; jj < R; ++jj) {
-            const int jn = jj + S;
-            if (jn < nplanes) {
-                mbar_arrive_expect_tx(&full[jj], P::PLANE_BYTES);
-                tma_load_3d(sm + jj * P::PLANE, &pmap, &full[jj], x0 - R, y0 - R, zb - R + jn);
-                issued_hi = jn;
-            }
-        }
+        for (int jj = 0; jj < R; ++jj)
+            if (jj + S < nplanes) issue_plane(jj + S);
     }
 
     for (int i0 = 0; i0 < nint && !abort_run; i0 += 9) {
@@ -219,12 +204,12 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S, AUX>::NT, Shape<TX, TY, 
                 // Queue feed: plane z+4.
                 {
                     const int jf = i + 8;
-                    if (!mbar_wait(&full[jf % S], (jf / S) & 1)) bad = true;
-                    const float* pf = sm + (jf % S) * P::PLANE + soff;
+                    if (!wait_plane(jf)) bad = true;
+                    const float* pf = plane(jf) + soff;
 #pragma unroll
                     for (int j = 0; j < RPT; ++j) q[(u + 8) % 9][j] = lds128(pf + j * P::SX);
                 }
-                const float* pc = sm + ((i + 4) % S) * P::PLANE + soff;
+                const float* pc = plane(i + 4) + soff;
 
                 // y: neighbour rows outside the own block from shared memory, own
                 // rows from the queue centre, accumulated from zero in row order
@@ -265,8 +250,8 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S, AUX>::NT, Shape<TX, TY, 
                     }
                 }
                 if (kAuxTma) {
-                    if (!mbar_wait(&auxf[i % NAUX], (i / NAUX) & 1)) bad = true;
-                    const float* st = aux + (i % NAUX) * 2 * P::TILE + aoff;
+                    if (!wait_aux(i)) bad = true;
+                    const float* st = aux + ((ab + i) % NAUX) * 2 * P::TILE + aoff;
 #pragma unroll
                     for (int j = 0; j < RPT; ++j) {
                         pv[j] = lds128(st + j * TX);
@@ -311,29 +296,106 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S, AUX>::NT, Shape<TX, TY, 
                 // refill them S planes / AUX iterations ahead.
                 abort_run = __syncthreads_or(bad) != 0;
                 if (!abort_run && tid == 0) {
-                    const int jr = i + 4;
-                    const int jn = jr + S;
-                    if (jn < nplanes) {
-                        mbar_arrive_expect_tx(&full[jr % S], P::PLANE_BYTES);
-                        tma_load_3d(sm + (jr % S) * P::PLANE, &pmap, &full[jr % S], x0 - R,
-                                    y0 - R, zb - R + jn);
-                        issued_hi = jn;
-                    }
+                    if (i + 4 + S < nplanes) issue_plane(i + 4 + S);
                     if (kAuxTma && i + NAUX < nint) issue_aux(i + NAUX);
                 }
             }
         }
     }
 
-    if (abort_run && tid == 0) {
-        record_error(a.err, kDevWaitTimeout);
-        // Let every copy still in flight land before the CTA's shared memory is
-        // released (each stage has at most one outstanding fill).
-        for (int jj = max(0, issued_hi - S + 1); jj <= issued_hi; ++jj)
-            (void)mbar_wait(&full[jj % S], (jj / S) & 1);
-        if (kAuxTma)
-            for (int it = max(0, aux_issued_hi - NAUX + 1); it <= aux_issued_hi; ++it)
-                (void)mbar_wait(&auxf[it % NAUX], (it / NAUX) & 1);
+    if (abort_run) {
+        if (tid == 0) {
+            record_error(a.err, kDevWaitTimeout);
+            // Let every copy still in flight land before the CTA's shared memory
+            // is released or reused (each stage has at most one outstanding fill).
+            for (int jj = max(0, issued_hi - S + 1); jj <= issued_hi; ++jj) (void)wait_plane(jj);
+            if (kAuxTma)
+                for (int it = max(0, aux_issued_hi - NAUX + 1); it <= aux_issued_hi; ++it)
+                    (void)wait_aux(it);
+        }
+        return false;
+    }
+    ring.p = pb + nplanes;
+    if (kAuxTma) ring.aux = ab + nint;
+    return true;
+}
+
+// Shared-memory rings of a CTA: S planes of p, AUX stages of [p_prev | vel2]
+// tiles, and their mbarriers (initialised here by thread 0).
+template <int TX, int TY, int RPT, int S, int AUX>
+__device__ __forceinline__ float* setup_rings(unsigned char* dsmem, uint64_t* full,
+                                              uint64_t* auxf) {
+    constexpr int NAUX = AUX > 0 ? AUX : 1;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int s = 0; s < S; ++s) mbar_init(&full[s], 1);
+#pragma unroll
+        for (int s = 0; s < NAUX; ++s) mbar_init(&auxf[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    return reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(dsmem) + 127) & ~uintptr_t(127));
+}
+
+// One grid: CTA b owns tile (b % tiles_x, (b / tiles_x) % tiles_y) and z chunk
+// b / (tiles_x * tiles_y).
+template <int TX, int TY, int RPT, int S, int AUX, bool HEAT>
+__global__ void __launch_bounds__(Shape<TX, TY, RPT, S, AUX>::NT, Shape<TX, TY, RPT, S, AUX>::MINB)
+    pencil_f32_kernel(const __grid_constant__ CUtensorMap pmap,
+                      const __grid_constant__ CUtensorMap qmap,
+                      const __grid_constant__ CUtensorMap vmap, const PencilArgs a) {
+    constexpr int NAUX = AUX > 0 ? AUX : 1;
+    extern __shared__ unsigned char dsmem[];
+    __shared__ __align__(8) uint64_t full[S];
+    __shared__ __align__(8) uint64_t auxf[NAUX];
+    float* sm = setup_rings<TX, TY, RPT, S, AUX>(dsmem, full, auxf);
+    int b = blockIdx.x;
+    const int tx = b % a.tiles_x;
+    b /= a.tiles_x;
+    const int ty = b % a.tiles_y;
+    b /= a.tiles_y;
+    Ring ring;
+    (void)pencil_tile<TX, TY, RPT, S, AUX, HEAT>(&pmap, &qmap, &vmap, a, tx, ty, b, sm, full,
+                                                 auxf, ring);
+}
+
+// Many grids (shots) in one persistent launch.  Each CTA takes work items --
+// (shot, tile x, tile y, z chunk) -- from a device queue with an atomic counter
+// until the queue is empty; the last CTA to finish resets the queue and advances
+// the step counter the sources read, so the next launch (eager or in a CUDA
+// graph) starts clean without a host-side reset.
+template <int TX, int TY, int RPT, int S, int AUX>
+__global__ void __launch_bounds__(Shape<TX, TY, RPT, S, AUX>::NT, Shape<TX, TY, RPT, S, AUX>::MINB)
+    batch_f32_kernel(const ShotF32* __restrict__ shots, const int4* __restrict__ items,
+                     int n_items, BatchQueue* queue) {
+    constexpr int NAUX = AUX > 0 ? AUX : 1;
+    extern __shared__ unsigned char dsmem[];
+    __shared__ __align__(8) uint64_t full[S];
+    __shared__ __align__(8) uint64_t auxf[NAUX];
+    __shared__ int s_item;
+    float* sm = setup_rings<TX, TY, RPT, S, AUX>(dsmem, full, auxf);
+    Ring ring;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(&queue->next, 1);
+        __syncthreads();
+        const int it = s_item;
+        __syncthreads();  // every thread has read s_item before it is replaced
+        if (it >= n_items) break;
+        const int4 w = items[it];
+        const ShotF32* sh = shots + w.x;
+        const PencilArgs a = sh->args;
+        if (!pencil_tile<TX, TY, RPT, S, AUX, false>(&sh->p, &sh->prev, &sh->vel2, a, w.y, w.z,
+                                                     w.w, sm, full, auxf, ring))
+            break;
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&queue->done, 1) == static_cast<int>(gridDim.x) - 1) {
+            queue->next = 0;
+            queue->done = 0;
+            queue->step += 1;
+            __threadfence();
+        }
     }
 }
 
@@ -412,15 +474,15 @@ constexpr int kNumHeat = sizeof(kHeat) / sizeof(kHeat[0]);
 
 const Variant& variant_of(bool heat, int v) { return heat ? kHeat[v] : kWave[v]; }
 
-PencilArgs base_args(const Variant& v, const GridDesc& g, int zchunks, int* err) {
+PencilArgs base_args(int tile_x, int tile_y, const GridDesc& g, int zchunks, int* err) {
     PencilArgs a{};
     a.nx = static_cast<int>(g.nx);
     a.ny = static_cast<int>(g.ny);
     a.nz = static_cast<int>(g.nz);
     a.sy = g.nx;
     a.sz = g.nx * g.ny;
-    a.tiles_x = static_cast<int>((g.nx - 2 * R + v.tx - 1) / v.tx);
-    a.tiles_y = static_cast<int>((g.ny - 2 * R + v.ty - 1) / v.ty);
+    a.tiles_x = static_cast<int>((g.nx - 2 * R + tile_x - 1) / tile_x);
+    a.tiles_y = static_cast<int>((g.ny - 2 * R + tile_y - 1) / tile_y);
     const int inz = static_cast<int>(g.nz - 2 * R);
     const int zc = std::max(1, std::min(zchunks, inz));
     a.zlen = (inz + zc - 1) / zc;
@@ -479,7 +541,7 @@ void pencil_f32_prepare() {
 }
 
 int64_t pencil_f32_ctas(bool heat, int v, const GridDesc& g, int zchunks) {
-    return ctas_of(base_args(variant_of(heat, v), g, zchunks, nullptr), g);
+    return ctas_of(base_args(variant_of(heat, v).tx, variant_of(heat, v).ty, g, zchunks, nullptr), g);
 }
 
 cudaError_t launch_wave_pencil_f32(const PencilMaps& maps, const float* prev, const float* vel2,
@@ -487,7 +549,7 @@ cudaError_t launch_wave_pencil_f32(const PencilMaps& maps, const float* prev, co
                                    const PencilConfig& cfg, int* err, cudaStream_t stream) {
     if (!g.has_interior()) return cudaSuccess;
     const Variant& v = kWave[cfg.variant];
-    PencilArgs a = base_args(v, g, cfg.zchunks, err);
+    PencilArgs a = base_args(v.tx, v.ty, g, cfg.zchunks, err);
     a.prev = prev;
     a.vel2 = vel2;
     a.next = next;
@@ -511,10 +573,113 @@ cudaError_t launch_heat_pencil_f32(const PencilMaps& maps, float* u_next, const 
                                    cudaStream_t stream) {
     if (!g.has_interior()) return cudaSuccess;
     const Variant& v = kHeat[cfg.variant];
-    PencilArgs a = base_args(v, g, cfg.zchunks, err);
+    PencilArgs a = base_args(v.tx, v.ty, g, cfg.zchunks, err);
     a.next = u_next;
     a.w = fold_weights(g, alpha_dt);
     return v.launch(maps, a, ctas_of(a, g), stream);
+}
+
+// ── batched shots ─────────────────────────────────────────────────────────────
+
+namespace {
+
+template <int TX, int TY, int RPT, int S, int AUX>
+int resident_batch() {
+    using P = Shape<TX, TY, RPT, S, AUX>;
+    static int cached[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cached[dev & 63] > 0) return cached[dev & 63];
+    auto kern = batch_f32_kernel<TX, TY, RPT, S, AUX>;
+    int n = 0;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(P::SMEM)) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, P::NT, P::SMEM) == cudaSuccess &&
+        n > 0) {
+        cached[dev & 63] = n;
+        return n;
+    }
+    cudaGetLastError();
+    const int by_smem = int((228u * 1024u) / (P::SMEM + 1024u));
+    const int by_regs = 65536 / (P::NT * 128);
+    return std::max(1, std::min(by_smem, by_regs));
+}
+
+template <int TX, int TY, int RPT, int S, int AUX>
+cudaError_t launch_batch(const ShotF32* shots, const int4* items, int n_items, BatchQueue* q,
+                         unsigned ctas, cudaStream_t stream) {
+    using P = Shape<TX, TY, RPT, S, AUX>;
+    resident_batch<TX, TY, RPT, S, AUX>();
+    batch_f32_kernel<TX, TY, RPT, S, AUX><<<ctas, P::NT, P::SMEM, stream>>>(shots, items, n_items,
+                                                                           q);
+    return cudaGetLastError();
+}
+
+struct BatchVariant {
+    int tx, ty;
+    const char* name;
+    cudaError_t (*launch)(const ShotF32*, const int4*, int, BatchQueue*, unsigned, cudaStream_t);
+    int (*resident)();
+};
+
+#define SB200_BATCH_VARIANT(TX, TY, RPT, S, AUX, NAME) \
+    BatchVariant { TX, TY, NAME, &launch_batch<TX, TY, RPT, S, AUX>, &resident_batch<TX, TY, RPT, S, AUX> }
+
+const BatchVariant kBatch[] = {
+    SB200_BATCH_VARIANT(32, 32, 2, 8, 4, "b32x32_r2_s8_a4"),
+    SB200_BATCH_VARIANT(64, 16, 2, 8, 3, "b64x16_r2_s8_a3"),
+    SB200_BATCH_VARIANT(32, 16, 1, 8, 4, "b32x16_r1_s8_a4"),
+    SB200_BATCH_VARIANT(64, 32, 2, 8, 3, "b64x32_r2_s8_a3"),
+};
+constexpr int kNumBatch = sizeof(kBatch) / sizeof(kBatch[0]);
+
+}  // namespace
+
+int batch_f32_variant_count() { return kNumBatch; }
+
+const char* batch_f32_variant_name(int v) {
+    return (v >= 0 && v < kNumBatch) ? kBatch[v].name : nullptr;
+}
+
+PencilBoxes batch_f32_boxes(int v) {
+    PencilBoxes b;
+    b.halo_x = kBatch[v].tx + 2 * R;
+    b.halo_y = kBatch[v].ty + 2 * R;
+    b.tile_x = kBatch[v].tx;
+    b.tile_y = kBatch[v].ty;
+    b.aux_tma = true;
+    return b;
+}
+
+int batch_f32_resident(int v) { return kBatch[v].resident(); }
+
+void batch_f32_prepare() {
+    for (int v = 0; v < kNumBatch; ++v) kBatch[v].resident();
+}
+
+PencilArgs batch_f32_shot_args(int v, const GridDesc& g, int zchunks, float* next,
+                               const SourceDesc& src, int* err) {
+    PencilArgs a = base_args(kBatch[v].tx, kBatch[v].ty, g, zchunks, err);
+    a.prev = next;
+    a.next = next;
+    a.dt2 = g.dt * g.dt;
+    a.w = fold_weights(g, a.dt2);
+    if (src.idx >= 0) {
+        a.src_x = static_cast<int>(src.idx % g.nx);
+        a.src_y = static_cast<int>((src.idx / g.nx) % g.ny);
+        a.src_z = static_cast<int>(src.idx / (g.nx * g.ny));
+        a.src_w = src.w;
+        a.src_wavelet = src.wavelet;
+        a.src_step = src.step;
+        a.src_off = src.step_offset;
+        a.trace = src.trace;
+    }
+    return a;
+}
+
+cudaError_t launch_batch_f32(int v, const ShotF32* shots, const int4* items, int n_items,
+                             BatchQueue* queue, unsigned ctas, cudaStream_t stream) {
+    return kBatch[v].launch(shots, items, n_items, queue, ctas, stream);
 }
 
 }  // namespace sb200

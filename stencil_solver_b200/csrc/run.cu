@@ -100,8 +100,7 @@ public:
             const double t0 = c_.src_t0 >= 0.f ? c_.src_t0 : 1.0 / c_.src_freq;
             std::vector<float> w(4096);
             sb200_ricker(c_.src_freq, t0, c_.grid.dt, static_cast<int64_t>(w.size()), w.data());
-            ricker_ = true;
-            if (int rc = set_wavelet(w.data(), static_cast<int64_t>(w.size()))) return rc;
+            if (int rc = set_wavelet(w.data(), static_cast<int64_t>(w.size()), true)) return rc;
         }
         return cuda(cudaStreamSynchronize(st_));
     }
@@ -158,10 +157,13 @@ public:
         return cuda(cudaStreamSynchronize(st_));
     }
 
-    int set_wavelet(const float* w, int64_t n) {
+    // generated: the samples are the run's own Ricker, which steps() extends on
+    // demand; caller samples are used as given and bound the run's length.
+    int set_wavelet(const float* w, int64_t n, bool generated = false) {
         if (!w || n <= 0) return set_error(SB200_ERR_INVALID, "sb200_run_set_wavelet: bad samples");
         if (heat_ || c_.src_index < 0)
             return set_error(SB200_ERR_INVALID, "sb200_run_set_wavelet: the run has no source");
+        ricker_ = generated;
         wavelet_host_.assign(w, w + n);
         if (int rc = upload_tables(std::max<int64_t>(n, cap_))) return rc;
         rebuild_bound();

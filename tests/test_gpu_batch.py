@@ -1,0 +1,118 @@
+"""Batched shots (sb200_batch_*): uneven grids advanced by one persistent launch
+per step.  Each shot must match the single-grid run engine bit for bit (same
+per-point arithmetic) and the FP32 oracle within the full-run bound, for every
+tile variant and z-chunk length, eager and through CUDA graphs."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+import stencil_solver_b200 as sb
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 60
+
+
+@pytest.fixture(autouse=True)
+def _clean(torch_cuda):
+    yield
+    assert sb.device_error() == 0
+
+
+def make_shots(seed=7, dims=((40, 48, 36), (64, 40, 56), (32, 32, 32), (56, 24, 44), (48, 64, 40))):
+    rng = np.random.default_rng(seed)
+    shots = []
+    for nx, ny, nz in dims:
+        g = sb.Grid(nx, ny, nz, 10.0, 10.0, 10.0, 1e-3)
+        vel2 = (rng.uniform(1500.0, 3000.0, g.shape) ** 2).astype(np.float32)
+        src = g.index(int(rng.integers(4, nx - 4)), int(rng.integers(4, ny - 4)),
+                      int(rng.integers(4, nz - 4)))
+        f = float(rng.uniform(10.0, 25.0))
+        w = oracle.ricker(f, 1.0 / f, 1e-3, STEPS).astype(np.float32)
+        shots.append((g, src, vel2, w))
+    return shots
+
+
+def run_batch(shots, steps=STEPS, chunk=20, choice=None, split=(7, 53)):
+    with sb.Batch([(g, s) for g, s, _, _ in shots], max_steps=steps, graph_chunk=chunk) as b:
+        if choice is not None:
+            b.set_choice(*choice)
+        for i, (g, _, v, w) in enumerate(shots):
+            z = np.zeros(g.shape, np.float32)
+            b.set_fields(i, z, z, v)
+            b.set_wavelet(i, w)
+        for k in split:
+            b.steps(k)
+        b.synchronize()
+        return [(b.field(i), b.trace(i, steps)) for i in range(len(shots))]
+
+
+def test_batch_matches_single_grid_runs_bitwise():
+    shots = make_shots()
+    got = run_batch(shots)
+    for (g, src, v, w), (p, tr) in zip(shots, got):
+        z = np.zeros(g.shape, np.float32)
+        with sb.Run(g, src_index=src, graph_chunk=0) as r:
+            r.set_fields(z, z, v)
+            r.set_wavelet(w)
+            r.steps(STEPS)
+            ref_p, ref_tr = r.field(), r.trace(STEPS)
+        assert np.array_equal(p, ref_p)
+        assert np.array_equal(tr, ref_tr)
+
+
+def test_batch_matches_oracle():
+    shots = make_shots(seed=11)
+    got = run_batch(shots)
+    for (g, src, v, w), (p, tr) in zip(shots, got):
+        z = np.zeros(g.shape, np.float32)
+        cur, _, otr = oracle.wave_run(z.copy(), z.copy(), v, 10.0, 10.0, 10.0, 1e-3, STEPS,
+                                      src=src, wavelet=w.astype(np.float64), trace=True)
+        assert oracle.rel_l2(p, cur) <= 1e-5
+        assert oracle.rel_l2(tr, otr) <= 1e-5
+
+
+@pytest.mark.parametrize("zlen", [0, 16])
+def test_batch_every_variant_agrees(zlen):
+    shots = make_shots(seed=3)
+    base = run_batch(shots, choice=(0, 64))
+    for v in range(sb.lib().sb200_batch_variant_count()):
+        got = run_batch(shots, choice=(v, zlen), chunk=0, split=(STEPS,))
+        for (p0, t0), (p, t) in zip(base, got):
+            assert np.array_equal(p, p0) and np.array_equal(t, t0)
+
+
+def test_batch_tune_then_run():
+    shots = make_shots(seed=5, dims=((64, 64, 64), (40, 72, 48)))
+    with sb.Batch([(g, s) for g, s, _, _ in shots], max_steps=STEPS, graph_chunk=20) as b:
+        b.tune(reps=2)
+        assert b.steps_done == 0
+        c = b.choice()
+        assert 0 <= c["variant"] < sb.lib().sb200_batch_variant_count() and c["items"] > 0
+        assert np.count_nonzero(b.field(0)) == 0
+        for i, (g, _, v, w) in enumerate(shots):
+            z = np.zeros(g.shape, np.float32)
+            b.set_fields(i, z, z, v)
+            b.set_wavelet(i, w)
+        b.steps(STEPS)
+        p = b.field(1)
+    ref = run_batch(shots)
+    assert np.array_equal(p, ref[1][0])
+
+
+def test_batch_rejects_bad_shots():
+    g = sb.Grid(42, 40, 40)  # nx % 4 != 0
+    with pytest.raises(sb.StencilError) as e:
+        sb.Batch([(g, None)], max_steps=10)
+    assert e.value.status == sb.SB200_ERR_UNSUPPORTED
+    g = sb.Grid(40, 40, 40)
+    with pytest.raises(sb.StencilError) as e:
+        sb.Batch([(g, g.index(2, 20, 20))], max_steps=10)  # source in the halo
+    assert e.value.status == sb.SB200_ERR_INVALID
+    with sb.Batch([(g, g.index(20, 20, 20))], max_steps=10, graph_chunk=0) as b:
+        b.steps(10)
+        with pytest.raises(sb.StencilError) as e:
+            b.steps(1)
+        assert e.value.status == sb.SB200_ERR_INVALID

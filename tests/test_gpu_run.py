@@ -46,6 +46,10 @@ def test_run_fp32_graphs_match_reference():
 def test_run_exact_mode_is_bit_identical_to_reference():
     f, run = acoustic128(graph_chunk=100, exact=1)
     with run:
+        # The golden samples were taken at t = n * 1e-3 in double; the run's own
+        # Ricker uses the grid's FP32 dt, a few ulps away.  Bit equality is about
+        # the stepping, so both sides get the same samples.
+        run.set_wavelet(f["wavelet"])
         run.steps(300)
         p, tr = run.field(), run.trace(300)
     assert np.array_equal(tr, f["trace32"])
@@ -115,3 +119,22 @@ def test_stats_of_run():
         s = r.stats()
     i = p0[4:-4, 4:-4, 4:-4].astype(np.float64)
     assert s[0] == pytest.approx(np.sum(i * i), rel=1e-12) and s[1] == np.abs(i).max()
+
+
+def test_caller_wavelet_is_kept_and_bounds_the_run():
+    n = 24
+    g = sb.Grid(n, n, n, 10.0, 10.0, 10.0, 1e-3)
+    z = np.zeros(g.shape, np.float32)
+    v = np.full(g.shape, 2000.0 ** 2, np.float32)
+    w = np.linspace(1.0, 2.0, 12).astype(np.float32)
+    with sb.Run(g, src_index=g.index(12, 12, 12), src_freq=15.0, graph_chunk=0) as r:
+        r.set_fields(z, z, v)
+        r.set_wavelet(w)
+        r.steps(12)
+        tr = r.trace(12)
+        with pytest.raises(sb.StencilError) as e:
+            r.steps(1)
+        assert e.value.status == sb.SB200_ERR_INVALID
+    # first step from rest: p = dt^2 vel2 w[0] at the source
+    k = np.float32(np.float32(1e-3) * np.float32(1e-3)) * np.float32(2000.0 ** 2)
+    assert tr[0] == np.float32(k * w[0])
