@@ -3,9 +3,10 @@
  *
  * Plain pointers and sizes only.  Device pointers are CUDA device memory owned by
  * the caller; `stream` is a cudaStream_t (NULL = legacy default stream).  Every
- * call is asynchronous on that stream unless stated otherwise, returns an int
- * status (SB200_OK or a negative SB200_ERR_* code) and never allocates device
- * memory.  sb200_last_error() describes the last failure on the calling thread.
+ * call is asynchronous on that stream unless stated otherwise and returns an int
+ * status (SB200_OK or a negative SB200_ERR_* code).  The kernel entry points
+ * never allocate device memory; the run and batch handles own theirs, and the
+ * tuner allocates only a few bytes.  sb200_last_error() describes the last failure on the calling thread.
  *
  * Field layout (the reference's GridDims, include/stencil/types.hpp:103-140):
  * extents include a 4-cell halo on every face, z is slowest,
@@ -130,8 +131,8 @@ int sb200_ricker(double freq, double t0, double dt, int64_t n_steps, float* out)
 int sb200_heat_step_exact_f32(const float* u, float* u_next, const sb200_grid* grid,
                               float alpha, void* stream);
 
-/* ── FP16-storage acoustic path (no reference counterpart: the north-star
- *    precision variant).  p and p_prev are FP16 holding a * p for a power-of-two
+/* ── FP16-storage acoustic path (no reference counterpart: a reduced-storage
+ *    precision variant of the acoustic step).  p and p_prev are FP16 holding a * p for a power-of-two
  *    scale a kept in device memory (sb200_f16_scale); K = vel2 dt^2 / dx^2 is
  *    BF16; arithmetic is FP32.  8 B per interior point and step. ─────────────── */
 typedef struct sb200_f16_scale {
@@ -257,7 +258,10 @@ void* sb200_run_stream(void* handle);
  * stream, synchronous) and records the fastest for later launches of that kind
  * on that grid and device.  The stencil reads field (and, for the acoustic kind,
  * prev and vel2) and writes only `scratch`, a caller buffer of the grid's size
- * that aliases none of them.  Outputs are optional. */
+ * that aliases none of them.  For SB200_KIND_WAVE_F16, field is p (FP16), vel2
+ * is K (BF16), prev is only checked for NULL, and scratch is the in-place
+ * p_prev / p_next buffer (FP16; its contents are overwritten).  Outputs are
+ * optional. */
 int sb200_tune(int kind, const sb200_grid* grid, const void* field, const void* prev,
                const void* vel2, void* scratch, int reps, int* variant, int* zchunks,
                float* best_ms);

@@ -9,8 +9,8 @@ Produces
       f32_strict : -O3 -ffp-contract=off          (bit-exact pin of the oracle)
       f32        : -O3 -march=x86-64-v4           (the reference's Release flags
                                                    with a portable -march so the
-                                                   library runs on any host of
-                                                   the pool; timed CPU baseline)
+                                                   library runs on any AVX-512
+                                                   host; timed CPU baseline)
       f64        : -O3 -ffp-contract=off -DSTENCIL_FP64   (FP64 CPU oracle)
 The reference sources are never copied into this repository; oracle/_ref/ is
 git-ignored.

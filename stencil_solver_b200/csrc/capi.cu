@@ -95,16 +95,6 @@ int sm_count() {
     return n;
 }
 
-// z split for the FP16 kernel's default tile: the smallest split reaching at
-// least 6 waves (the FP32 measurements favour several waves over one long march).
-int f16_zchunks(const GridDesc& g) {
-    const double slots = double(sm_count()) * std::max(1, pencil_f16_resident(0));
-    const int inz = static_cast<int>(g.nz - 8);
-    for (int zc = 1; zc <= 16 && zc <= inz; ++zc)
-        if (double(pencil_f16_ctas(0, g, zc)) / slots >= 6.0) return zc;
-    return std::max(1, std::min(16, inz));
-}
-
 PencilConfig choose(int kind, const GridDesc& g) {
     {
         std::lock_guard<std::mutex> lock(g_cfg_mu);
@@ -129,8 +119,7 @@ PencilConfig choose(int kind, const GridDesc& g) {
     auto it = memo.find(key);
     if (it != memo.end()) return it->second;
     c.variant = 0;
-    c.zchunks = kind == SB200_KIND_WAVE_F16 ? f16_zchunks(g)
-                                            : zchunk_ranking(kind == SB200_KIND_HEAT_F32, 0, g, 1).front();
+    c.zchunks = zchunk_ranking(kind, 0, g, 1).front();
     memo[key] = c;
     return c;
 }
@@ -254,14 +243,17 @@ int* device_error_word() { return device_error_ptr(); }
 
 // A wave is SMs x resident CTAs; a split whose CTA count leaves the last wave
 // mostly empty wastes that fraction of the machine, and every extra split
-// re-reads 8 halo planes of p (p is 1 of 4 streams for the acoustic kernel,
+// re-reads 8 halo planes of p (p is 1 of 4 streams for the acoustic kernels,
 // 1 of 2 for heat).
-std::vector<int> zchunk_ranking(bool heat, int v, const GridDesc& g, int max_n) {
+std::vector<int> zchunk_ranking(int kind, int v, const GridDesc& g, int max_n) {
+    const bool f16 = kind == SB200_KIND_WAVE_F16;
+    const bool heat = kind == SB200_KIND_HEAT_F32;
     const int inz = static_cast<int>(g.nz - 8);
-    const double slots = double(sm_count()) * std::max(1, pencil_f32_resident(heat, v));
+    const int resident = f16 ? pencil_f16_resident(v) : pencil_f32_resident(heat, v);
+    const double slots = double(sm_count()) * std::max(1, resident);
     std::vector<std::pair<double, int>> scored;
     for (int zc = 1; zc <= 16 && zc <= inz; ++zc) {
-        const double ctas = double(pencil_f32_ctas(heat, v, g, zc));
+        const double ctas = double(f16 ? pencil_f16_ctas(v, g, zc) : pencil_f32_ctas(heat, v, g, zc));
         const double waves = std::ceil(ctas / slots);
         const double fill = ctas / (waves * slots);
         const int zlen = (inz + zc - 1) / zc;

@@ -87,7 +87,7 @@ int64_t pencil_f32_ctas(bool heat, int v, const GridDesc& g, int zchunks);
 // z splits of variant v on grid g ranked by how well their CTA count fills whole
 // waves (SMs x resident CTAs), discounted by the 8 halo planes each extra split
 // re-reads; the first max_n (capi.cu).
-std::vector<int> zchunk_ranking(bool heat, int v, const GridDesc& g, int max_n);
+std::vector<int> zchunk_ranking(int kind, int v, const GridDesc& g, int max_n);
 
 // Tuned (variant, zchunks) for kind on grid g on the current device, if the
 // tuner has one (tuner.cpp).

@@ -84,18 +84,32 @@ extern "C" {
 int sb200_tune(int kind, const sb200_grid* grid, const void* field, const void* prev,
                const void* vel2, void* scratch, int reps, int* variant, int* zchunks,
                float* best_ms) {
-    if (kind != SB200_KIND_WAVE_F32 && kind != SB200_KIND_HEAT_F32) return SB200_ERR_INVALID;
-    if (!grid || !field || !scratch || (kind == SB200_KIND_WAVE_F32 && (!prev || !vel2)))
+    if (kind != SB200_KIND_WAVE_F32 && kind != SB200_KIND_HEAT_F32 && kind != SB200_KIND_WAVE_F16)
         return SB200_ERR_INVALID;
-    if (scratch == field || scratch == prev || scratch == vel2) return SB200_ERR_INVALID;
     const bool heat = kind == SB200_KIND_HEAT_F32;
+    const bool f16 = kind == SB200_KIND_WAVE_F16;
+    if (!grid || !field || !scratch || (!heat && (!prev || !vel2))) return SB200_ERR_INVALID;
+    if (scratch == field || scratch == prev || scratch == vel2) return SB200_ERR_INVALID;
     const int nvar = sb200_pencil_variant_count(kind);
     const int inz = static_cast<int>(grid->nz - 8);
-    if (nvar <= 0 || inz < 1 || grid->nx % 4 != 0) return SB200_ERR_UNSUPPORTED;
+    if (nvar <= 0 || inz < 1 || grid->nx % (f16 ? 8 : 4) != 0) return SB200_ERR_UNSUPPORTED;
     reps = std::max(1, reps);
+    // FP16 trials run plain steps (no source, no rescale), which never read the
+    // scale; the kernel still takes a valid device pointer.
+    sb200_f16_scale* unit = nullptr;
+    if (f16) {
+        const sb200_f16_scale one{1.f, 1.f};
+        if (cudaMalloc(reinterpret_cast<void**>(&unit), sizeof(one)) != cudaSuccess ||
+            cudaMemcpy(unit, &one, sizeof(one), cudaMemcpyHostToDevice) != cudaSuccess) {
+            if (unit) cudaFree(unit);
+            return SB200_ERR_CUDA;
+        }
+    }
     cudaEvent_t e0, e1;
-    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        if (unit) cudaFree(unit);
         return SB200_ERR_CUDA;
+    }
     Choice best;
     best.ms = 1e30f;
     GridDesc gd;
@@ -104,9 +118,14 @@ int sb200_tune(int kind, const sb200_grid* grid, const void* field, const void* 
     gd.nz = grid->nz;
     for (int v = 0; v < nvar; ++v) {
         // The three best-filling z splits of this tile shape (see zchunk_ranking).
-        for (int zc : zchunk_ranking(heat, v, gd, 3)) {
+        for (int zc : zchunk_ranking(kind, v, gd, 3)) {
             sb200_set_pencil_override(kind, v, zc);
             auto launch = [&]() {
+                if (f16)
+                    return sb200_wave_step_f16(static_cast<const uint16_t*>(field),
+                                               static_cast<uint16_t*>(scratch),
+                                               static_cast<const uint16_t*>(vel2), grid, -1, 0.f,
+                                               nullptr, nullptr, 0, unit, 0, nullptr);
                 return heat ? sb200_heat_step_f32(static_cast<const float*>(field),
                                                   static_cast<float*>(scratch), grid, 1.0f, nullptr)
                             : sb200_launch_tiled(static_cast<const float*>(field),
@@ -132,6 +151,7 @@ int sb200_tune(int kind, const sb200_grid* grid, const void* field, const void* 
     sb200_set_pencil_override(kind, -1, 1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if (unit) cudaFree(unit);
     if (cudaGetLastError() != cudaSuccess || best.ms >= 1e29f) return SB200_ERR_CUDA;
     {
         std::lock_guard<std::mutex> lock(g_mu);

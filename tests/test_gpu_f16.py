@@ -124,6 +124,43 @@ def test_f16_step_matches_oracle(torch_cuda, phase, r, variant):
         sb.set_pencil_override(sb.KIND_WAVE_F16, -1, 1)
 
 
+def test_f16_variants_agree_bitwise(torch_cuda):
+    """The per-point arithmetic does not depend on the tile shape or z split."""
+    shape = (45, 52, 80)
+    P, Q, K = f16_case(shape, 21)
+    g = sb.Grid(80, 52, 45, 10.0, 12.0, 9.0, 1e-3)
+    n = sb.lib().sb200_pencil_variant_count(sb.KIND_WAVE_F16)
+    outs = {}
+    try:
+        for v in range(n):
+            for phase in (0, 1, 2):
+                sb.set_pencil_override(sb.KIND_WAVE_F16, v, 1 + v % 3)
+                out = dev(torch_cuda, Q.view(np.int16))
+                sb.wave_step_f16(dev(torch_cuda, P.view(np.int16)), out,
+                                 dev(torch_cuda, K.view(np.int16)), g,
+                                 scale_state(torch_cuda, 1024.0, 0.5), phase)
+                outs[(v, phase)] = host(out)
+    finally:
+        sb.set_pencil_override(sb.KIND_WAVE_F16, -1, 1)
+    for (v, phase), o in outs.items():
+        assert np.array_equal(o, outs[(0, phase)]), (v, phase)
+
+
+def test_f16_tuner_picks_a_variant(torch_cuda):
+    import ctypes as C
+
+    g = sb.Grid(96, 80, 72, 10.0, 10.0, 10.0, 1e-3)
+    P, Q, K = f16_case(g.shape, 4)
+    p, q, k = (dev(torch_cuda, x.view(np.int16)) for x in (P, Q, K))
+    scratch = q.clone()
+    v, zc, ms = C.c_int(-1), C.c_int(-1), C.c_float(0)
+    rc = sb.lib().sb200_tune(sb.KIND_WAVE_F16, sb._g(g), p.data_ptr(), q.data_ptr(), k.data_ptr(),
+                             scratch.data_ptr(), 2, C.byref(v), C.byref(zc), C.byref(ms))
+    assert rc == 0, sb.last_error()
+    assert 0 <= v.value < sb.lib().sb200_pencil_variant_count(sb.KIND_WAVE_F16)
+    assert zc.value >= 1 and ms.value > 0
+
+
 def test_f16_source_injection(torch_cuda):
     shape = (24, 24, 32)
     P, Q, K = f16_case(shape, 9, scale=64.0)

@@ -1,6 +1,6 @@
 """GPU parity of the FP32 kernels against the oracle, through the C ABI.
 
-Tolerances (BASELINE acoustic bar, FP32 vs the reference CPU path on identical
+Tolerances (the acoustic parity bar, FP32 vs the reference CPU path on identical
 inputs): relative L2 <= 1e-6 after one step and <= 1e-5 after a full run.  The
 reference-order kernels (launch_naive, wave_step_exact) are held to bit
 equality with the oracle / golden fixtures.
