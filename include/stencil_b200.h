@@ -5,8 +5,9 @@
  * the caller; `stream` is a cudaStream_t (NULL = legacy default stream).  Every
  * call is asynchronous on that stream unless stated otherwise and returns an int
  * status (SB200_OK or a negative SB200_ERR_* code).  The kernel entry points
- * never allocate device memory; the run and batch handles own theirs, and the
- * tuner allocates only a few bytes.  sb200_last_error() describes the last failure on the calling thread.
+ * never allocate device memory; the run, batch and MLP handles own theirs, and
+ * the tuner allocates only a few bytes.  sb200_last_error() describes the last
+ * failure on the calling thread.
  *
  * Field layout (the reference's GridDims, include/stencil/types.hpp:103-140):
  * extents include a 4-cell halo on every face, z is slowest,
@@ -131,10 +132,11 @@ int sb200_ricker(double freq, double t0, double dt, int64_t n_steps, float* out)
 int sb200_heat_step_exact_f32(const float* u, float* u_next, const sb200_grid* grid,
                               float alpha, void* stream);
 
-/* ── FP16-storage acoustic path (no reference counterpart: a reduced-storage
- *    precision variant of the acoustic step).  p and p_prev are FP16 holding a * p for a power-of-two
- *    scale a kept in device memory (sb200_f16_scale); K = vel2 dt^2 / dx^2 is
- *    BF16; arithmetic is FP32.  8 B per interior point and step. ─────────────── */
+/* ── FP16-storage acoustic path ─────────────────────────────────────────────
+ * No reference counterpart: a reduced-storage precision variant of the
+ * acoustic step.  p and p_prev are FP16 holding a * p for a power-of-two scale
+ * a kept in device memory (sb200_f16_scale); K = vel2 dt^2 / dx^2 is BF16;
+ * arithmetic is FP32.  8 B per interior point and step. */
 typedef struct sb200_f16_scale {
     float a; /* current storage scale (fields hold a * p) */
     float r; /* a_new / a_old of the last renormalisation */
@@ -314,6 +316,57 @@ int64_t sb200_batch_steps_done(void* handle);
 void* sb200_batch_stream(void* handle);
 int sb200_batch_variant_count(void);
 const char* sb200_batch_variant_name(int variant);
+
+/* ── learned coarse correction ─────────────────────────────────────────────
+ * No reference counterpart.  A per-point MLP 26 -> 32 -> 32 -> 1 (ReLU), BF16
+ * tensor-core mma with FP32 accumulation, corrects a 2x-coarser grid stepped
+ * with 2x dt:  p_next[i] += s_i * c * MLP(f_i).  f_i is the 25-point star of p
+ * at i in a difference basis, divided by s_i (the star's largest magnitude):
+ * [p_c, (p_+r - p_-r) for axis x, y, z and r = 1..4, (p_+r + p_-r - 2 p_c)
+ * likewise], evaluated in FP32; then the Courant number sqrt(vel2) dt / dx;
+ * zero-padded to 32 BF16 features per row.  c is the handle's output scale.
+ * Parameters (FP32, SB200_MLP_NPARAM): W1[32][32] (out x in; inputs 26..31
+ * unused), b1[32], W2[32][32], b2[32], w3[32], b3. */
+#define SB200_MLP_NPARAM 2145
+#define SB200_MLP_FEATURES 32
+
+/* Handle with the parameters on the current device, He-initialised from seed. */
+int sb200_mlp_create(uint64_t seed, void** handle);
+int sb200_mlp_destroy(void* handle);
+/* Host copies of the FP32 parameters (synchronous); set also resets Adam. */
+int sb200_mlp_get_params(void* handle, float* params);
+int sb200_mlp_set_params(void* handle, const float* params);
+/* Output scale c of the correction (default 1; training divides the targets by
+ * it).  Get returns 0 for a NULL handle. */
+int sb200_mlp_set_output_scale(void* handle, float scale);
+float sb200_mlp_output_scale(void* handle);
+/* y[r] = MLP(X[r]) for n rows of 32 BF16 features (device pointers). */
+int sb200_mlp_forward(void* handle, const uint16_t* X, float* y, int64_t n, void* stream);
+/* Gradient of mean_r (MLP(X[r]) - t[r])^2 into grad[0..NPARAM) (device FP32,
+ * overwritten) and the loss into grad[NPARAM]. */
+int sb200_mlp_gradients(void* handle, const uint16_t* X, const float* t, int64_t n, float* grad,
+                        void* stream);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) on the batch; *loss (device,
+ * optional) receives the batch loss before the step. */
+int sb200_mlp_train_step(void* handle, const uint16_t* X, const float* t, int64_t n, float lr,
+                         float* loss, void* stream);
+/* p_next += s * c * MLP(features of p) on the interior (p, vel2, p_next device
+ * FP32; p_next must not alias p). */
+int sb200_mlp_correct(void* handle, const float* p, const float* vel2, float* p_next,
+                      const sb200_grid* grid, void* stream);
+/* Training rows at n cells (device int64 flat indices, interior only):
+ * X[r] = features of p at cells[r], t[r] = (p_true - p_plain)[cell] / s. */
+int sb200_mlp_samples(const float* p, const float* vel2, const float* p_true, const float* p_plain,
+                      const sb200_grid* grid, const int64_t* cells, int64_t n, uint16_t* X,
+                      float* t, void* stream);
+/* field[x0+i, y0+j, z0+k] += scale * pattern[(k*by + j)*bx + i] for the box's
+ * interior cells (pattern device FP32): a spatially extended source term. */
+int sb200_add_box(float* field, const sb200_grid* grid, int x0, int y0, int z0, int bx, int by,
+                  int bz, const float* pattern, float scale, void* stream);
+/* coarse[x,y,z] = fine[2x+offset, 2y+offset, 2z+offset] on the coarse interior
+ * (zero on its halo and where the fine index falls outside the fine grid). */
+int sb200_restrict2(const float* fine, const sb200_grid* fine_grid, float* coarse,
+                    const sb200_grid* coarse_grid, int offset, void* stream);
 
 #ifdef __cplusplus
 }

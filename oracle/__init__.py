@@ -61,6 +61,13 @@ def lib() -> C.CDLL:
         L.oracle_f32_to_bf16.restype = C.c_uint16
         L.oracle_bf16_to_f32.argtypes = [C.c_uint16]
         L.oracle_bf16_to_f32.restype = C.c_float
+        L.oracle_mlp_nparam.restype = C.c_int
+        L.oracle_mlp_features.argtypes = [_f32p, _f32p, _i64, _i64, _i64, C.c_float, _u16p]
+        L.oracle_mlp_features.restype = C.c_float
+        L.oracle_mlp_forward.argtypes = [_f32p, _u16p, _i64, C.c_int, _f64p]
+        L.oracle_mlp_forward.restype = None
+        L.oracle_mlp_grad.argtypes = [_f32p, _u16p, _f32p, _i64, C.c_int, _f64p]
+        L.oracle_mlp_grad.restype = C.c_double
         L.oracle_rms_diff_f32.argtypes = [_f32p, _f32p, _i64]
         L.oracle_rms_diff_f32.restype = C.c_double
         L.oracle_max_abs_diff_f32.argtypes = [_f32p, _f32p, _i64]
@@ -127,6 +134,34 @@ def wave_step_f16(P, Q, K, dx, dy, dz, m_out=1.0, m_q=1.0, src=-1, w=0.0, a=1.0,
         out = Q.copy()
     lib().oracle_wave_step_f16(P, Q, K, out, nx, ny, nz, dx, dy, dz, m_out, m_q, src, w, a)
     return out
+
+
+def mlp_features(p, vel2, cell, dt_over_dx):
+    """(row of 32 BF16 bit patterns, scale s) of the star at flat index cell."""
+    nz, ny, nx = p.shape
+    row = np.zeros(32, np.uint16)
+    s = lib().oracle_mlp_features(np.ascontiguousarray(p, np.float32),
+                                  np.ascontiguousarray(vel2, np.float32), nx, ny, int(cell),
+                                  dt_over_dx, row)
+    return row, s
+
+
+def mlp_forward(params, X, round_bf16=True):
+    X = np.ascontiguousarray(X, np.uint16)
+    y = np.zeros(X.shape[0], np.float64)
+    lib().oracle_mlp_forward(np.ascontiguousarray(params, np.float32), X, X.shape[0],
+                             int(round_bf16), y)
+    return y
+
+
+def mlp_grad(params, X, t, round_bf16=True):
+    """(loss, gradient) of mean (MLP(X) - t)^2 in double."""
+    X = np.ascontiguousarray(X, np.uint16)
+    g = np.zeros(lib().oracle_mlp_nparam(), np.float64)
+    loss = lib().oracle_mlp_grad(np.ascontiguousarray(params, np.float32), X,
+                                 np.ascontiguousarray(t, np.float32), X.shape[0],
+                                 int(round_bf16), g)
+    return loss, g
 
 
 def to_f16(a, scale=1.0) -> np.ndarray:

@@ -271,3 +271,123 @@ void oracle_wave_step_f16(const uint16_t* P, const uint16_t* Q, const uint16_t* 
                 out[ci] = oracle_f32_to_f16(o);
             }
 }
+
+/* ── learned coarse correction (no reference counterpart) ──────────────────────
+ * Restates the library's MLP path (stencil_solver_b200/csrc/mlp.cu) for the
+ * gradient check: features of a 25-point star, the 26 -> 32 -> 32 -> 1 ReLU
+ * network and the gradient of mean (y - t)^2.  Parameters in the library's
+ * layout: W1[32][32] (out x in), b1[32], W2[32][32], b2[32], w3[32], b3.
+ * With round_bf16 != 0 the operands are rounded to BF16 where the GPU's mma
+ * reads them (W1, W2, x, h1 for layer 2, dh2 and dh1 for the weight-gradient
+ * products, W2 for dh1); every sum is in double.  With round_bf16 == 0 all of
+ * it is exact FP64 arithmetic (for finite-difference checks). */
+#define MLP_H 32
+#define MLP_F 32
+#define MLP_OFF_B1 (MLP_H * MLP_F)
+#define MLP_OFF_W2 (MLP_OFF_B1 + MLP_H)
+#define MLP_OFF_B2 (MLP_OFF_W2 + MLP_H * MLP_H)
+#define MLP_OFF_W3 (MLP_OFF_B2 + MLP_H)
+#define MLP_OFF_B3 (MLP_OFF_W3 + MLP_H)
+#define MLP_NPARAM (MLP_OFF_B3 + 1)
+
+int oracle_mlp_nparam(void) { return MLP_NPARAM; }
+
+static double mlp_rnd(double v, int on) {
+    return on ? (double)oracle_bf16_to_f32(oracle_f32_to_bf16((float)v)) : v;
+}
+
+/* Feature row (32 BF16) and scale of the star at flat cell c, as the library
+ * builds it: the difference basis / s in FP32, then BF16; feature 25 =
+ * sqrtf(vel2) * dt_over_dx. */
+float oracle_mlp_features(const float* p, const float* vel2, int64_t nx, int64_t ny, int64_t c,
+                          float dt_over_dx, uint16_t* row) {
+    float v[25];
+    int k = 1;
+    const int64_t sy = nx, sz = nx * ny;
+    v[0] = p[c];
+    for (int r = -4; r <= 4; ++r)
+        if (r) v[k++] = p[c + r];
+    for (int r = -4; r <= 4; ++r)
+        if (r) v[k++] = p[c + r * sy];
+    for (int r = -4; r <= 4; ++r)
+        if (r) v[k++] = p[c + r * sz];
+    float s = 0.f;
+    for (int j = 0; j < 25; ++j) s = fabsf(v[j]) > s ? fabsf(v[j]) : s;
+    const float inv = s > 0.f ? 1.f / s : 0.f;
+    /* difference basis: p_c, then (p_+r - p_-r) and (p_+r + p_-r - 2 p_c) per axis
+     * and radius, all / s; v[1 + 8a + k] holds axis a's offset k - 4 (k < 4) or
+     * k - 3 (k >= 4) */
+    row[0] = oracle_f32_to_bf16(v[0] * inv);
+    for (int a = 0; a < 3; ++a)
+        for (int r = 1; r <= 4; ++r) {
+            const float up = v[1 + 8 * a + 3 + r], dn = v[1 + 8 * a + 4 - r];
+            row[1 + 4 * a + r - 1] = oracle_f32_to_bf16((up - dn) * inv);
+            row[13 + 4 * a + r - 1] = oracle_f32_to_bf16(((up + dn) - 2.f * v[0]) * inv);
+        }
+    row[25] = oracle_f32_to_bf16(sqrtf(vel2[c]) * dt_over_dx);
+    for (int j = 26; j < 32; ++j) row[j] = 0;
+    return s;
+}
+
+/* Forward of one row; h1, h2 (optional) receive the activations. */
+static double mlp_row(const float* prm, const uint16_t* x, int rb, double* h1, double* h2) {
+    double a1[MLP_H], a2[MLP_H];
+    for (int o = 0; o < MLP_H; ++o) {
+        double acc = prm[MLP_OFF_B1 + o];
+        for (int i = 0; i < MLP_F; ++i)
+            acc += mlp_rnd(prm[o * MLP_F + i], rb) * (double)oracle_bf16_to_f32(x[i]);
+        a1[o] = acc > 0.0 ? acc : 0.0;
+    }
+    double y = prm[MLP_OFF_B3];
+    for (int o = 0; o < MLP_H; ++o) {
+        double acc = prm[MLP_OFF_B2 + o];
+        for (int i = 0; i < MLP_H; ++i)
+            acc += mlp_rnd(prm[MLP_OFF_W2 + o * MLP_H + i], rb) * mlp_rnd(a1[i], rb);
+        a2[o] = acc > 0.0 ? acc : 0.0;
+        y += (double)prm[MLP_OFF_W3 + o] * a2[o];
+    }
+    if (h1) memcpy(h1, a1, sizeof(a1));
+    if (h2) memcpy(h2, a2, sizeof(a2));
+    return y;
+}
+
+void oracle_mlp_forward(const float* prm, const uint16_t* X, int64_t n, int round_bf16,
+                        double* y) {
+    for (int64_t r = 0; r < n; ++r) y[r] = mlp_row(prm, X + r * MLP_F, round_bf16, NULL, NULL);
+}
+
+/* grad[0..NPARAM) = d/dparam of mean_r (y_r - t_r)^2; returns the loss. */
+double oracle_mlp_grad(const float* prm, const uint16_t* X, const float* t, int64_t n,
+                       int round_bf16, double* grad) {
+    const int rb = round_bf16;
+    double loss = 0.0;
+    memset(grad, 0, sizeof(double) * MLP_NPARAM);
+    for (int64_t r = 0; r < n; ++r) {
+        const uint16_t* x = X + r * MLP_F;
+        double h1[MLP_H], h2[MLP_H], dh2[MLP_H], dh1[MLP_H];
+        const double y = mlp_row(prm, x, rb, h1, h2);
+        const double e = y - (double)t[r];
+        loss += e * e / (double)n;
+        const double dy = 2.0 * e / (double)n;
+        grad[MLP_OFF_B3] += dy;
+        for (int o = 0; o < MLP_H; ++o) {
+            grad[MLP_OFF_W3 + o] += dy * h2[o];
+            dh2[o] = h2[o] > 0.0 ? dy * (double)prm[MLP_OFF_W3 + o] : 0.0;
+            grad[MLP_OFF_B2 + o] += dh2[o];
+        }
+        for (int o = 0; o < MLP_H; ++o)
+            for (int i = 0; i < MLP_H; ++i)
+                grad[MLP_OFF_W2 + o * MLP_H + i] += mlp_rnd(dh2[o], rb) * mlp_rnd(h1[i], rb);
+        for (int i = 0; i < MLP_H; ++i) {
+            double acc = 0.0;
+            for (int o = 0; o < MLP_H; ++o)
+                acc += mlp_rnd(dh2[o], rb) * mlp_rnd(prm[MLP_OFF_W2 + o * MLP_H + i], rb);
+            dh1[i] = h1[i] > 0.0 ? acc : 0.0;
+            grad[MLP_OFF_B1 + i] += dh1[i];
+        }
+        for (int o = 0; o < MLP_H; ++o)
+            for (int i = 0; i < MLP_F; ++i)
+                grad[o * MLP_F + i] += mlp_rnd(dh1[o], rb) * (double)oracle_bf16_to_f32(x[i]);
+    }
+    return loss;
+}

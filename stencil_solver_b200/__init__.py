@@ -173,6 +173,23 @@ _SIGNATURES = {
     "sb200_batch_stream": ([C.c_void_p], C.c_void_p),
     "sb200_batch_variant_count": ([], C.c_int),
     "sb200_batch_variant_name": ([C.c_int], C.c_char_p),
+    "sb200_mlp_create": ([C.c_uint64, C.POINTER(C.c_void_p)], C.c_int),
+    "sb200_mlp_destroy": ([C.c_void_p], C.c_int),
+    "sb200_mlp_get_params": ([C.c_void_p, C.c_void_p], C.c_int),
+    "sb200_mlp_set_params": ([C.c_void_p, C.c_void_p], C.c_int),
+    "sb200_mlp_set_output_scale": ([C.c_void_p, C.c_float], C.c_int),
+    "sb200_mlp_output_scale": ([C.c_void_p], C.c_float),
+    "sb200_mlp_forward": ([C.c_void_p] * 3 + [C.c_int64, C.c_void_p], C.c_int),
+    "sb200_mlp_gradients": ([C.c_void_p] * 3 + [C.c_int64, C.c_void_p, C.c_void_p], C.c_int),
+    "sb200_mlp_train_step": ([C.c_void_p] * 3 + [C.c_int64, C.c_float, C.c_void_p, C.c_void_p],
+                             C.c_int),
+    "sb200_mlp_correct": ([C.c_void_p] * 4 + [C.POINTER(sb200_grid), C.c_void_p], C.c_int),
+    "sb200_mlp_samples": ([C.c_void_p] * 4 + [C.POINTER(sb200_grid), C.c_void_p, C.c_int64,
+                                               C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "sb200_add_box": ([C.c_void_p, C.POINTER(sb200_grid)] + [C.c_int] * 6 +
+                      [C.c_void_p, C.c_float, C.c_void_p], C.c_int),
+    "sb200_restrict2": ([C.c_void_p, C.POINTER(sb200_grid), C.c_void_p, C.POINTER(sb200_grid),
+                         C.c_int, C.c_void_p], C.c_int),
     "sb200_pencil_variant_count": ([C.c_int], C.c_int),
     "sb200_pencil_variant_name": ([C.c_int, C.c_int], C.c_char_p),
     "sb200_set_pencil_override": ([C.c_int, C.c_int, C.c_int], C.c_int),
@@ -581,3 +598,95 @@ class Batch:
     @property
     def stream(self) -> int:
         return lib().sb200_batch_stream(self._h)
+
+
+MLP_NPARAM = 2145
+MLP_FEATURES = 32
+
+
+class Mlp:
+    """The learned-correction network (sb200_mlp_*): FP32 parameters on the device,
+    BF16 tensor-core forward / backward, Adam.  Feature rows are int16 / uint16
+    CUDA tensors of shape (n, 32) holding BF16 bit patterns."""
+
+    def __init__(self, seed: int = 0):
+        h = C.c_void_p()
+        _check(lib().sb200_mlp_create(seed, C.byref(h)))
+        self._h = h
+        self._destroy = lib().sb200_mlp_destroy  # still callable at interpreter exit
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def params(self):
+        import numpy as np
+
+        out = np.empty(MLP_NPARAM, np.float32)
+        _check(lib().sb200_mlp_get_params(self._h, out.ctypes.data))
+        return out
+
+    def set_params(self, w) -> None:
+        import numpy as np
+
+        w = np.ascontiguousarray(w, np.float32)
+        if w.size != MLP_NPARAM:
+            raise ValueError(f"expected {MLP_NPARAM} parameters")
+        _check(lib().sb200_mlp_set_params(self._h, w.ctypes.data))
+
+    @property
+    def output_scale(self) -> float:
+        return float(lib().sb200_mlp_output_scale(self._h))
+
+    @output_scale.setter
+    def output_scale(self, c: float) -> None:
+        _check(lib().sb200_mlp_set_output_scale(self._h, c))
+
+    def forward(self, X, y, n=None, stream=None) -> None:
+        n = X.shape[0] if n is None else n
+        _check(lib().sb200_mlp_forward(self._h, _ptr(X), _ptr(y), n, _stream(stream)))
+
+    def gradients(self, X, t, grad, n=None, stream=None) -> None:
+        n = X.shape[0] if n is None else n
+        _check(lib().sb200_mlp_gradients(self._h, _ptr(X), _ptr(t), n, _ptr(grad),
+                                          _stream(stream)))
+
+    def train_step(self, X, t, lr: float, loss=None, n=None, stream=None) -> None:
+        n = X.shape[0] if n is None else n
+        _check(lib().sb200_mlp_train_step(self._h, _ptr(X), _ptr(t), n, lr, _ptr(loss),
+                                           _stream(stream)))
+
+    def correct(self, p, vel2, p_next, grid: Grid, stream=None) -> None:
+        _check(lib().sb200_mlp_correct(self._h, _ptr(p), _ptr(vel2), _ptr(p_next), _g(grid),
+                                        _stream(stream)))
+
+
+def mlp_samples(p, vel2, p_true, p_plain, grid: Grid, cells, X, t, stream=None) -> None:
+    _check(lib().sb200_mlp_samples(_ptr(p), _ptr(vel2), _ptr(p_true), _ptr(p_plain), _g(grid),
+                                   _ptr(cells), cells.numel(), _ptr(X), _ptr(t),
+                                   _stream(stream)))
+
+
+def restrict2(fine, fine_grid: Grid, coarse, coarse_grid: Grid, offset: int = -4,
+              stream=None) -> None:
+    _check(lib().sb200_restrict2(_ptr(fine), _g(fine_grid), _ptr(coarse), _g(coarse_grid),
+                                 offset, _stream(stream)))
+
+
+def add_box(field, grid: Grid, origin, dims, pattern, scale: float, stream=None) -> None:
+    """field[box] += scale * pattern, box at origin (x, y, z) of dims (bx, by, bz)."""
+    _check(lib().sb200_add_box(_ptr(field), _g(grid), *origin, *dims, _ptr(pattern), scale,
+                               _stream(stream)))

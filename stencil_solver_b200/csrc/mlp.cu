@@ -1,0 +1,787 @@
+// Learned coarse correction: a per-point MLP 26 -> 32 -> 32 -> 1 (ReLU) on BF16
+// tensor-core mma with FP32 accumulation, and the kernels that train it.
+//
+// No reference counterpart.  A coarse grid (2x the spacing, 2x the time step)
+// advanced by the plain acoustic step is corrected after every step by
+//   p_next[i] += s_i * c * MLP(f_i),   c a fixed output scale (the training
+// targets' RMS, so the network itself works on O(1) values),
+// where f_i is the 25-point star of p around i (in a difference basis, see
+// feature_row) divided by its largest magnitude s_i, plus the local Courant
+// number sqrt(vel2) dt / dx, padded to 32 features.  The correction is
+// positively homogeneous in p (scaling the field scales the correction).
+//
+// Parameters: FP32 masters [W1 (32x32, out x in; input columns 26..31 stay 0),
+// b1, W2 (32x32), b2, w3 (32), b3] and BF16 copies of W1, W2 and W2^T that the
+// mma kernels read.  Forward: x (BF16) -> h1 = relu(W1 x + b1) (FP32, rounded
+// to BF16 as the next A operand) -> h2 = relu(W2 h1 + b2) (FP32) ->
+// y = w3 . h2 + b3 (FP32).  Backward of mean((y - t)^2) with the same BF16
+// operands: dW2 = dh2^T h1, dh1 = dh2 W2, dW1 = dh1^T x as mma over the batch;
+// dW3, biases and the loss in FP32.  Adam keeps FP32 moments.
+//
+// Tensor-core fragments (mma.sync.m16n8k16, row.col, bf16 -> f32): a warp owns
+// 16 rows (samples).  The accumulator fragment of one layer (rows g, g+8; cols
+// 8t + 2q, +1 for n-tile t, g = lane / 4, q = lane % 4) is exactly the A
+// fragment of the next layer's k-step t / 2, so activations never leave the
+// registers in the forward pass.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "dispatch.h"
+#include "kernels.h"
+#include "stencil_b200.h"
+
+namespace sb200 {
+namespace {
+
+constexpr int H = 32;    // hidden width
+constexpr int F = 32;    // padded input width
+constexpr int NIN = 26;  // real inputs
+constexpr int OFF_W1 = 0;
+constexpr int OFF_B1 = OFF_W1 + H * F;
+constexpr int OFF_W2 = OFF_B1 + H;
+constexpr int OFF_B2 = OFF_W2 + H * H;
+constexpr int OFF_W3 = OFF_B2 + H;
+constexpr int OFF_B3 = OFF_W3 + H;
+constexpr int NPARAM = OFF_B3 + 1;  // 2145
+constexpr int NSLOT = NPARAM + 1;   // + loss
+static_assert(NPARAM == SB200_MLP_NPARAM, "parameter count");
+
+__device__ __forceinline__ uint32_t pack_bf2(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+__device__ __forceinline__ uint16_t bf16_bits(float x) {
+    return static_cast<uint16_t>(pack_bf2(x, 0.f) & 0xffffu);
+}
+
+__device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4],
+                                         const uint32_t (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+        "{%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// Per-warp copy of the network: B fragments of W1 and W2 for every (n-tile,
+// k-step), and this lane's bias / w3 columns.
+struct NetFrag {
+    uint32_t w1[4][2][2];
+    uint32_t w2[4][2][2];
+    float b1[4][2], b2[4][2], w3[4][2];
+    float b3;
+};
+
+__device__ __forceinline__ void load_net(NetFrag& n, const float* __restrict__ prm,
+                                         const uint32_t* __restrict__ w1b,
+                                         const uint32_t* __restrict__ w2b) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+#pragma unroll
+        for (int ks = 0; ks < 2; ++ks) {
+            // B(k, n) = W(n, k): row n = 8t + g of W, k = 16 ks + 2q (+8)
+            const int w = (8 * t + g) * (F / 2) + 8 * ks + q;
+            n.w1[t][ks][0] = w1b[w];
+            n.w1[t][ks][1] = w1b[w + 4];
+            n.w2[t][ks][0] = w2b[w];
+            n.w2[t][ks][1] = w2b[w + 4];
+        }
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int c = 8 * t + 2 * q + e;
+            n.b1[t][e] = prm[OFF_B1 + c];
+            n.b2[t][e] = prm[OFF_B2 + c];
+            n.w3[t][e] = prm[OFF_W3 + c];
+        }
+    }
+    n.b3 = prm[OFF_B3];
+}
+
+// Activations of one 16-row tile, kept for the backward pass.
+struct Acts {
+    float h1[4][4];     // relu(W1 x + b1), accumulator layout
+    uint32_t a2[2][4];  // h1 as BF16 A fragments of layer 2
+    float h2[4][4];     // relu(W2 h1 + b2)
+    float y[2];         // outputs of rows g and g + 8
+};
+
+// x: A fragments of the tile's features (2 k-steps).
+__device__ __forceinline__ void forward_tile(const NetFrag& n, const uint32_t (&x)[2][4], Acts& s) {
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        float d[4] = {n.b1[t][0], n.b1[t][1], n.b1[t][0], n.b1[t][1]};
+        mma16816(d, x[0], n.w1[t][0]);
+        mma16816(d, x[1], n.w1[t][1]);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) s.h1[t][e] = fmaxf(d[e], 0.f);
+    }
+#pragma unroll
+    for (int kk = 0; kk < 2; ++kk) {
+        s.a2[kk][0] = pack_bf2(s.h1[2 * kk][0], s.h1[2 * kk][1]);
+        s.a2[kk][1] = pack_bf2(s.h1[2 * kk][2], s.h1[2 * kk][3]);
+        s.a2[kk][2] = pack_bf2(s.h1[2 * kk + 1][0], s.h1[2 * kk + 1][1]);
+        s.a2[kk][3] = pack_bf2(s.h1[2 * kk + 1][2], s.h1[2 * kk + 1][3]);
+    }
+    float y0 = 0.f, y1 = 0.f;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        float d[4] = {n.b2[t][0], n.b2[t][1], n.b2[t][0], n.b2[t][1]};
+        mma16816(d, s.a2[0], n.w2[t][0]);
+        mma16816(d, s.a2[1], n.w2[t][1]);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) s.h2[t][e] = fmaxf(d[e], 0.f);
+        y0 = fmaf(n.w3[t][0], s.h2[t][0], fmaf(n.w3[t][1], s.h2[t][1], y0));
+        y1 = fmaf(n.w3[t][0], s.h2[t][2], fmaf(n.w3[t][1], s.h2[t][3], y1));
+    }
+    y0 += __shfl_xor_sync(0xffffffffu, y0, 1);
+    y0 += __shfl_xor_sync(0xffffffffu, y0, 2);
+    y1 += __shfl_xor_sync(0xffffffffu, y1, 1);
+    y1 += __shfl_xor_sync(0xffffffffu, y1, 2);
+    s.y[0] = y0 + n.b3;
+    s.y[1] = y1 + n.b3;
+}
+
+// A fragments of rows [r0, r0+16) of a row-major BF16 feature matrix (32 per
+// row); rows at or beyond n read as zero.
+__device__ __forceinline__ void load_x(uint32_t (&x)[2][4], const uint32_t* __restrict__ X,
+                                       int64_t r0, int64_t n) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+    const int64_t ra = r0 + g, rb = r0 + g + 8;
+#pragma unroll
+    for (int ks = 0; ks < 2; ++ks) {
+        x[ks][0] = ra < n ? X[ra * 16 + 8 * ks + q] : 0u;
+        x[ks][1] = rb < n ? X[rb * 16 + 8 * ks + q] : 0u;
+        x[ks][2] = ra < n ? X[ra * 16 + 8 * ks + 4 + q] : 0u;
+        x[ks][3] = rb < n ? X[rb * 16 + 8 * ks + 4 + q] : 0u;
+    }
+}
+
+constexpr int kWarps = 4;  // warps per block of the training kernels
+
+__global__ void __launch_bounds__(32 * kWarps)
+    mlp_forward_kernel(const float* __restrict__ prm, const uint32_t* __restrict__ w1b,
+                       const uint32_t* __restrict__ w2b, const uint32_t* __restrict__ X,
+                       float* __restrict__ y, int64_t n) {
+    NetFrag net;
+    load_net(net, prm, w1b, w2b);
+    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+    const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t r0 = warp * 16; r0 < n; r0 += nw * 16) {
+        uint32_t x[2][4];
+        load_x(x, X, r0, n);
+        Acts s;
+        forward_tile(net, x, s);
+        if (q == 0) {
+            if (r0 + g < n) y[r0 + g] = s.y[0];
+            if (r0 + g + 8 < n) y[r0 + g + 8] = s.y[1];
+        }
+    }
+}
+
+// Per-warp scratch for the transposes the weight-gradient mma need: rows of
+// 16 samples, padded to 24 halves (48 bytes) so fragment loads hit distinct banks.
+constexpr int TP = 24;
+struct WarpT {
+    uint16_t dh2[H][TP];  // dh2^T: [output unit][sample]
+    uint16_t h1[H][TP];   // h1^T
+    uint16_t dh1[H][TP];  // dh1^T
+    uint16_t x[F][TP];    // x^T
+};
+
+__device__ __forceinline__ uint32_t ld_pair(const uint16_t* p) {
+    return *reinterpret_cast<const uint32_t*>(p);
+}
+
+// Gradient of sum over rows of (y - t)^2 * inv_n (the caller passes 1 / n_total),
+// accumulated into grad[NPARAM] (and the loss into grad[NPARAM]).
+__global__ void __launch_bounds__(32 * kWarps)
+    mlp_grad_kernel(const float* __restrict__ prm, const uint32_t* __restrict__ w1b,
+                    const uint32_t* __restrict__ w2b, const uint32_t* __restrict__ w2tb,
+                    const uint32_t* __restrict__ X, const float* __restrict__ tgt, int64_t n,
+                    float inv_n, float* __restrict__ grad) {
+    __shared__ WarpT wt[kWarps];
+    __shared__ float red[NSLOT];
+    for (int i = threadIdx.x; i < NSLOT; i += blockDim.x) red[i] = 0.f;
+
+    NetFrag net;
+    load_net(net, prm, w1b, w2b);
+    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3, wi = threadIdx.x >> 5;
+    WarpT& T = wt[wi];
+    // W2^T as B fragments of dh1 = dh2 W2 (k = output unit o, n = input unit i).
+    uint32_t w2t[4][2][2];
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+#pragma unroll
+        for (int ks = 0; ks < 2; ++ks) {
+            const int w = (8 * t + g) * (H / 2) + 8 * ks + q;
+            w2t[t][ks][0] = w2tb[w];
+            w2t[t][ks][1] = w2tb[w + 4];
+        }
+
+    float gw1[2][4][4], gw2[2][4][4];  // [m-tile of out units][n-tile][frag]
+#pragma unroll
+    for (int m = 0; m < 2; ++m)
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) gw1[m][t][e] = gw2[m][t][e] = 0.f;
+    float gb1[4][2] = {}, gb2[4][2] = {}, gw3[4][2] = {};
+    float gb3 = 0.f, loss = 0.f;
+
+    const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t r0 = warp * 16; r0 < n; r0 += nw * 16) {
+        uint32_t x[2][4];
+        load_x(x, X, r0, n);
+        Acts s;
+        forward_tile(net, x, s);
+        float dy[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int64_t r = r0 + g + 8 * h;
+            const float e = r < n ? s.y[h] - tgt[r] : 0.f;
+            dy[h] = 2.f * e * inv_n;
+            if (q == 0) {
+                loss = fmaf(e * inv_n, e, loss);
+                gb3 += dy[h];
+            }
+        }
+        // dh2 = dy w3 [h2 > 0]; dW3, db2 rows partial sums.
+        float dh2[4][4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int h = e >> 1, c = e & 1;
+                gw3[t][c] = fmaf(dy[h], s.h2[t][e], gw3[t][c]);
+                dh2[t][e] = s.h2[t][e] > 0.f ? dy[h] * net.w3[t][c] : 0.f;
+                gb2[t][c] += dh2[t][e];
+            }
+        // Transposes for the weight-gradient mma: dh2^T, h1^T (BF16 as used), x^T.
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int row = g + 8 * (e >> 1), col = 8 * t + 2 * q + (e & 1);
+                T.dh2[col][row] = bf16_bits(dh2[t][e]);
+            }
+#pragma unroll
+        for (int kk = 0; kk < 2; ++kk)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                // a2[kk][r]: rows g (+8 for r odd), cols 16 kk + 2q (+8 for r >= 2)
+                const int row = g + 8 * (r & 1), col = 16 * kk + 2 * q + 8 * (r >> 1);
+                T.h1[col][row] = static_cast<uint16_t>(s.a2[kk][r] & 0xffffu);
+                T.h1[col + 1][row] = static_cast<uint16_t>(s.a2[kk][r] >> 16);
+                T.x[col][row] = static_cast<uint16_t>(x[kk][r] & 0xffffu);
+                T.x[col + 1][row] = static_cast<uint16_t>(x[kk][r] >> 16);
+            }
+        __syncwarp();
+        // dW2[o][i] += sum_r dh2[r][o] h1[r][i]: A = dh2^T (o x r), B = h1 (r x i).
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+            uint32_t a[4];
+            a[0] = ld_pair(&T.dh2[16 * m + g][2 * q]);
+            a[1] = ld_pair(&T.dh2[16 * m + g + 8][2 * q]);
+            a[2] = ld_pair(&T.dh2[16 * m + g][2 * q + 8]);
+            a[3] = ld_pair(&T.dh2[16 * m + g + 8][2 * q + 8]);
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const uint32_t b[2] = {ld_pair(&T.h1[8 * t + g][2 * q]),
+                                       ld_pair(&T.h1[8 * t + g][2 * q + 8])};
+                mma16816(gw2[m][t], a, b);
+            }
+        }
+        // dh1 = (dh2 W2) [h1 > 0]: A = dh2 (accumulator layout -> A), B = W2^T frags.
+        uint32_t ad[2][4];
+#pragma unroll
+        for (int kk = 0; kk < 2; ++kk) {
+            ad[kk][0] = pack_bf2(dh2[2 * kk][0], dh2[2 * kk][1]);
+            ad[kk][1] = pack_bf2(dh2[2 * kk][2], dh2[2 * kk][3]);
+            ad[kk][2] = pack_bf2(dh2[2 * kk + 1][0], dh2[2 * kk + 1][1]);
+            ad[kk][3] = pack_bf2(dh2[2 * kk + 1][2], dh2[2 * kk + 1][3]);
+        }
+        float dh1[4][4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            float d[4] = {0.f, 0.f, 0.f, 0.f};
+            mma16816(d, ad[0], w2t[t][0]);
+            mma16816(d, ad[1], w2t[t][1]);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                dh1[t][e] = s.h1[t][e] > 0.f ? d[e] : 0.f;
+                gb1[t][e & 1] += dh1[t][e];
+                const int row = g + 8 * (e >> 1), col = 8 * t + 2 * q + (e & 1);
+                T.dh1[col][row] = bf16_bits(dh1[t][e]);
+            }
+        }
+        __syncwarp();
+        // dW1[o][f] += sum_r dh1[r][o] x[r][f].
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+            uint32_t a[4];
+            a[0] = ld_pair(&T.dh1[16 * m + g][2 * q]);
+            a[1] = ld_pair(&T.dh1[16 * m + g + 8][2 * q]);
+            a[2] = ld_pair(&T.dh1[16 * m + g][2 * q + 8]);
+            a[3] = ld_pair(&T.dh1[16 * m + g + 8][2 * q + 8]);
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const uint32_t b[2] = {ld_pair(&T.x[8 * t + g][2 * q]),
+                                       ld_pair(&T.x[8 * t + g][2 * q + 8])};
+                mma16816(gw1[m][t], a, b);
+            }
+        }
+        __syncwarp();  // the transposes are rewritten by the next tile
+    }
+
+    // Block reduction in shared memory, then one global add per parameter.
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < 2; ++m)
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int o = 16 * m + g + 8 * (e >> 1), i = 8 * t + 2 * q + (e & 1);
+                atomicAdd(&red[OFF_W1 + o * F + i], gw1[m][t][e]);
+                atomicAdd(&red[OFF_W2 + o * H + i], gw2[m][t][e]);
+            }
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const int col = 8 * t + 2 * q + c;
+            atomicAdd(&red[OFF_B1 + col], gb1[t][c]);
+            atomicAdd(&red[OFF_B2 + col], gb2[t][c]);
+            atomicAdd(&red[OFF_W3 + col], gw3[t][c]);
+        }
+    if (q == 0) {
+        atomicAdd(&red[OFF_B3], gb3);
+        atomicAdd(&red[NPARAM], loss);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < NSLOT; i += blockDim.x)
+        if (red[i] != 0.f) atomicAdd(&grad[i], red[i]);
+}
+
+// Adam on the FP32 masters (one thread per parameter; input columns 26..31 of
+// W1 never move).
+__global__ void mlp_adam_kernel(float* __restrict__ prm, float* __restrict__ m1,
+                                float* __restrict__ m2, const float* __restrict__ grad, float lr,
+                                float b1, float b2, float eps, float c1, float c2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= NPARAM) return;
+    if (i < OFF_B1 && (i % F) >= NIN) return;
+    const float gr = grad[i];
+    const float a = b1 * m1[i] + (1.f - b1) * gr;
+    const float v = b2 * m2[i] + (1.f - b2) * gr * gr;
+    m1[i] = a;
+    m2[i] = v;
+    prm[i] -= lr * (a / c1) / (sqrtf(v / c2) + eps);
+}
+
+// BF16 copies of W1, W2 and W2^T read by the mma kernels.
+__global__ void mlp_bf16_kernel(const float* __restrict__ prm, uint16_t* __restrict__ w1b,
+                                uint16_t* __restrict__ w2b, uint16_t* __restrict__ w2tb) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= H * F) return;
+    w1b[i] = bf16_bits(prm[OFF_W1 + i]);
+    const uint16_t v = bf16_bits(prm[OFF_W2 + i]);
+    w2b[i] = v;
+    w2tb[(i % H) * H + i / H] = v;
+}
+
+// ── features ──────────────────────────────────────────────────────────────────
+
+// The 25-point star of p around c (centre, then x-4..x-1, x+1..x+4, then y and
+// z likewise) and its largest magnitude.
+struct Star {
+    float v[25];
+    float s;
+};
+
+__device__ __forceinline__ void gather_star(Star& st, const float* __restrict__ p, int64_t c,
+                                            int64_t sy, int64_t sz) {
+    st.v[0] = p[c];
+    int k = 1;
+#pragma unroll
+    for (int r = -4; r <= 4; ++r)
+        if (r) st.v[k++] = p[c + r];
+#pragma unroll
+    for (int r = -4; r <= 4; ++r)
+        if (r) st.v[k++] = p[c + r * sy];
+#pragma unroll
+    for (int r = -4; r <= 4; ++r)
+        if (r) st.v[k++] = p[c + r * sz];
+    float m = 0.f;
+#pragma unroll
+    for (int j = 0; j < 25; ++j) m = fmaxf(m, fabsf(st.v[j]));
+    st.s = m;
+}
+
+// Feature row (32 BF16) of a star, in a difference basis computed in FP32
+// before the rounding: [p_c, (p_+r - p_-r) for axis x, y, z and r = 1..4,
+// (p_+r + p_-r - 2 p_c) likewise] / s, then the Courant number, then zeros.
+// The same information as the 25 values, but the small differences that the
+// scheme's error is made of survive the BF16 rounding.
+__device__ __forceinline__ void feature_row(uint32_t* row, const Star& st, float courant) {
+    const float inv = st.s > 0.f ? 1.f / st.s : 0.f;
+    const float c = st.v[0];
+    float f[26];
+    f[0] = c * inv;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int r = 1; r <= 4; ++r) {
+            const float up = st.v[1 + 8 * a + 3 + r];  // +r: slot 4 + r - 1 of the axis' 8
+            const float dn = st.v[1 + 8 * a + 4 - r];  // -r: slot 4 - r
+            f[1 + 4 * a + (r - 1)] = (up - dn) * inv;
+            f[13 + 4 * a + (r - 1)] = ((up + dn) - 2.f * c) * inv;
+        }
+    f[25] = courant;
+#pragma unroll
+    for (int j = 0; j < 13; ++j) row[j] = pack_bf2(f[2 * j], f[2 * j + 1]);
+#pragma unroll
+    for (int j = 13; j < 16; ++j) row[j] = 0u;
+}
+
+__global__ void mlp_samples_kernel(const float* __restrict__ p, const float* __restrict__ vel2,
+                                   const float* __restrict__ p_true,
+                                   const float* __restrict__ p_plain, int64_t nx, int64_t ny,
+                                   float dt_over_dx, const int64_t* __restrict__ cells, int64_t n,
+                                   uint32_t* __restrict__ X, float* __restrict__ t) {
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t c = cells[i];
+    Star st;
+    gather_star(st, p, c, nx, nx * ny);
+    feature_row(X + i * 16, st, sqrtf(vel2[c]) * dt_over_dx);
+    t[i] = st.s > 0.f ? (p_true[c] - p_plain[c]) / st.s : 0.f;
+}
+
+__global__ void restrict2_kernel(const float* __restrict__ fine, int64_t fnx, int64_t fny,
+                                 int64_t fnz, float* __restrict__ coarse, int64_t nx, int64_t ny,
+                                 int64_t nz, int off) {
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nx * ny * nz) return;
+    const int64_t x = i % nx, y = (i / nx) % ny, z = i / (nx * ny);
+    float v = 0.f;
+    if (x >= 4 && y >= 4 && z >= 4 && x < nx - 4 && y < ny - 4 && z < nz - 4) {
+        const int64_t fx = 2 * x + off, fy = 2 * y + off, fz = 2 * z + off;
+        if (fx >= 0 && fy >= 0 && fz >= 0 && fx < fnx && fy < fny && fz < fnz)
+            v = fine[(fz * fny + fy) * fnx + fx];
+    }
+    coarse[i] = v;
+}
+
+// field[box] += scale * pattern over a bx x by x bz box at (x0, y0, z0) (a
+// spatially extended source); cells outside the grid's interior are skipped.
+__global__ void add_box_kernel(float* __restrict__ f, int64_t nx, int64_t ny, int64_t nz, int x0,
+                               int y0, int z0, int bx, int by, int bz,
+                               const float* __restrict__ pattern, float scale) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= bx * by * bz) return;
+    const int64_t x = x0 + i % bx, y = y0 + (i / bx) % by, z = z0 + i / (bx * by);
+    if (x < 4 || y < 4 || z < 4 || x >= nx - 4 || y >= ny - 4 || z >= nz - 4) return;
+    f[(z * ny + y) * nx + x] += scale * pattern[i];
+}
+
+// Fused correction: each warp takes 32 consecutive interior points of a row,
+// lanes build their feature rows in shared memory, two 16-row mma tiles run
+// the network, and p_next += s * c * y.
+constexpr int CP = 40;  // feature row stride in shared memory (halves): conflict-free A loads
+constexpr int kCorrWarps = 8;
+
+__global__ void __launch_bounds__(32 * kCorrWarps)
+    mlp_correct_kernel(const float* __restrict__ prm, const uint32_t* __restrict__ w1b,
+                       const uint32_t* __restrict__ w2b, const float* __restrict__ p,
+                       const float* __restrict__ vel2, float* __restrict__ p_next, int64_t nx,
+                       int64_t ny, int64_t nz, float dt_over_dx, float out_scale) {
+    __shared__ __align__(16) uint16_t feat[kCorrWarps][32][CP];
+    __shared__ float scale[kCorrWarps][32];
+    NetFrag net;
+    load_net(net, prm, w1b, w2b);
+    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3, wi = threadIdx.x >> 5;
+    const int64_t ix = nx - 8, segs = (ix + 31) / 32;
+    const int64_t items = segs * (ny - 8) * (nz - 8);
+    const int64_t warp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    const int64_t sy = nx, sz = nx * ny;
+    for (int64_t it = warp; it < items; it += nw) {
+        const int64_t seg = it % segs, row = it / segs;
+        const int64_t y = 4 + row % (ny - 8), z = 4 + row / (ny - 8);
+        const int64_t x = 4 + seg * 32 + lane;
+        const bool live = x < nx - 4;
+        const int64_t c = (z * ny + y) * nx + x;
+        uint32_t* fr = reinterpret_cast<uint32_t*>(&feat[wi][lane][0]);
+        float s = 0.f;
+        if (live) {
+            Star st;
+            gather_star(st, p, c, sy, sz);
+            feature_row(fr, st, sqrtf(vel2[c]) * dt_over_dx);
+            s = st.s;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) fr[j] = 0u;
+        }
+        scale[wi][lane] = s * out_scale;
+        __syncwarp();
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+            uint32_t xa[2][4];
+#pragma unroll
+            for (int ks = 0; ks < 2; ++ks) {
+                xa[ks][0] = ld_pair(&feat[wi][16 * m + g][16 * ks + 2 * q]);
+                xa[ks][1] = ld_pair(&feat[wi][16 * m + g + 8][16 * ks + 2 * q]);
+                xa[ks][2] = ld_pair(&feat[wi][16 * m + g][16 * ks + 8 + 2 * q]);
+                xa[ks][3] = ld_pair(&feat[wi][16 * m + g + 8][16 * ks + 8 + 2 * q]);
+            }
+            Acts a;
+            forward_tile(net, xa, a);
+            if (q < 2) {  // lane q = 0 writes row g, q = 1 row g + 8
+                const int r = 16 * m + g + 8 * q;
+                const int64_t xr = 4 + seg * 32 + r;
+                const float sr = scale[wi][r];
+                if (xr < nx - 4 && sr > 0.f) {
+                    const int64_t cr = (z * ny + y) * nx + xr;
+                    p_next[cr] = fmaf(sr, q == 0 ? a.y[0] : a.y[1], p_next[cr]);
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ── host side ────────────────────────────────────────────────────────────────
+
+struct Mlp {
+    float* prm = nullptr;  // NPARAM FP32 masters
+    float* m1 = nullptr;
+    float* m2 = nullptr;
+    float* grad = nullptr;  // NSLOT (gradients + loss)
+    uint16_t* w1b = nullptr;
+    uint16_t* w2b = nullptr;
+    uint16_t* w2tb = nullptr;
+    int64_t adam_t = 0;
+    int sms = 148;
+    float out_scale = 1.f;  // the correction is s * out_scale * y
+};
+
+int cuda_err(cudaError_t e, const char* where) {
+    if (e == cudaSuccess) return SB200_OK;
+    return set_error(SB200_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+void init_params(std::vector<float>& w, uint64_t seed) {
+    std::mt19937_64 rng(seed);
+    std::normal_distribution<double> nd(0.0, 1.0);
+    w.assign(NPARAM, 0.f);
+    for (int o = 0; o < H; ++o)
+        for (int i = 0; i < NIN; ++i)
+            w[OFF_W1 + o * F + i] = static_cast<float>(nd(rng) * std::sqrt(2.0 / NIN));
+    for (int o = 0; o < H; ++o)
+        for (int i = 0; i < H; ++i)
+            w[OFF_W2 + o * H + i] = static_cast<float>(nd(rng) * std::sqrt(2.0 / H));
+    for (int i = 0; i < H; ++i) w[OFF_W3 + i] = static_cast<float>(nd(rng) * 0.1 / std::sqrt(H));
+}
+
+int grid_blocks(const Mlp& m, int64_t work_units_per_block, int64_t units) {
+    const int64_t want = (units + work_units_per_block - 1) / work_units_per_block;
+    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(want, int64_t(m.sms) * 8)));
+}
+
+}  // namespace
+}  // namespace sb200
+
+using namespace sb200;
+
+extern "C" {
+
+int sb200_mlp_create(uint64_t seed, void** handle) {
+    if (!handle) return set_error(SB200_ERR_INVALID, "sb200_mlp_create: NULL handle");
+    *handle = nullptr;
+    Mlp* m = new Mlp();
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+        cudaDeviceGetAttribute(&m->sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaGetLastError();
+    int rc = cuda_err(cudaMalloc(&m->prm, NPARAM * 4), "sb200_mlp_create");
+    if (!rc) rc = cuda_err(cudaMalloc(&m->m1, NPARAM * 4), "sb200_mlp_create");
+    if (!rc) rc = cuda_err(cudaMalloc(&m->m2, NPARAM * 4), "sb200_mlp_create");
+    if (!rc) rc = cuda_err(cudaMalloc(&m->grad, NSLOT * 4), "sb200_mlp_create");
+    if (!rc) rc = cuda_err(cudaMalloc(&m->w1b, H * F * 2), "sb200_mlp_create");
+    if (!rc) rc = cuda_err(cudaMalloc(&m->w2b, H * H * 2), "sb200_mlp_create");
+    if (!rc) rc = cuda_err(cudaMalloc(&m->w2tb, H * H * 2), "sb200_mlp_create");
+    if (rc) {
+        sb200_mlp_destroy(m);
+        return rc;
+    }
+    *handle = m;
+    std::vector<float> w;
+    init_params(w, seed);
+    return sb200_mlp_set_params(m, w.data());
+}
+
+int sb200_mlp_destroy(void* h) {
+    Mlp* m = static_cast<Mlp*>(h);
+    if (!m) return SB200_OK;
+    for (void* p : {static_cast<void*>(m->prm), static_cast<void*>(m->m1),
+                    static_cast<void*>(m->m2), static_cast<void*>(m->grad),
+                    static_cast<void*>(m->w1b), static_cast<void*>(m->w2b),
+                    static_cast<void*>(m->w2tb)})
+        if (p) cudaFree(p);
+    delete m;
+    return SB200_OK;
+}
+
+int sb200_mlp_set_params(void* h, const float* params) {
+    Mlp* m = static_cast<Mlp*>(h);
+    if (!m || !params) return set_error(SB200_ERR_INVALID, "sb200_mlp_set_params: NULL argument");
+    std::vector<float> w(params, params + NPARAM);
+    for (int o = 0; o < H; ++o)
+        for (int i = NIN; i < F; ++i) w[OFF_W1 + o * F + i] = 0.f;  // padding inputs
+    int rc = cuda_err(cudaMemcpy(m->prm, w.data(), NPARAM * 4, cudaMemcpyHostToDevice),
+                      "sb200_mlp_set_params");
+    if (!rc) rc = cuda_err(cudaMemset(m->m1, 0, NPARAM * 4), "sb200_mlp_set_params");
+    if (!rc) rc = cuda_err(cudaMemset(m->m2, 0, NPARAM * 4), "sb200_mlp_set_params");
+    if (rc) return rc;
+    m->adam_t = 0;
+    mlp_bf16_kernel<<<(H * F + 255) / 256, 256>>>(m->prm, m->w1b, m->w2b, m->w2tb);
+    rc = cuda_err(cudaGetLastError(), "sb200_mlp_set_params");
+    if (!rc) rc = cuda_err(cudaDeviceSynchronize(), "sb200_mlp_set_params");
+    return rc;
+}
+
+int sb200_mlp_get_params(void* h, float* params) {
+    Mlp* m = static_cast<Mlp*>(h);
+    if (!m || !params) return set_error(SB200_ERR_INVALID, "sb200_mlp_get_params: NULL argument");
+    return cuda_err(cudaMemcpy(params, m->prm, NPARAM * 4, cudaMemcpyDeviceToHost),
+                    "sb200_mlp_get_params");
+}
+
+int sb200_mlp_set_output_scale(void* h, float scale) {
+    Mlp* m = static_cast<Mlp*>(h);
+    if (!m || !(scale > 0.f) || !std::isfinite(scale))
+        return set_error(SB200_ERR_INVALID, "sb200_mlp_set_output_scale: bad arguments");
+    m->out_scale = scale;
+    return SB200_OK;
+}
+
+float sb200_mlp_output_scale(void* h) {
+    Mlp* m = static_cast<Mlp*>(h);
+    return m ? m->out_scale : 0.f;
+}
+
+int sb200_mlp_forward(void* h, const uint16_t* X, float* y, int64_t n, void* stream) {
+    Mlp* m = static_cast<Mlp*>(h);
+    if (!m || !X || !y || n < 0) return set_error(SB200_ERR_INVALID, "sb200_mlp_forward: bad arguments");
+    if (n == 0) return SB200_OK;
+    const int blocks = grid_blocks(*m, 16 * kWarps, n);
+    mlp_forward_kernel<<<blocks, 32 * kWarps, 0, static_cast<cudaStream_t>(stream)>>>(
+        m->prm, reinterpret_cast<const uint32_t*>(m->w1b), reinterpret_cast<const uint32_t*>(m->w2b),
+        reinterpret_cast<const uint32_t*>(X), y, n);
+    return cuda_err(cudaGetLastError(), "sb200_mlp_forward");
+}
+
+int sb200_mlp_gradients(void* h, const uint16_t* X, const float* t, int64_t n, float* grad,
+                        void* stream) {
+    Mlp* m = static_cast<Mlp*>(h);
+    if (!m || !X || !t || !grad || n <= 0)
+        return set_error(SB200_ERR_INVALID, "sb200_mlp_gradients: bad arguments");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int rc = cuda_err(cudaMemsetAsync(grad, 0, NSLOT * 4, st), "sb200_mlp_gradients");
+    if (rc) return rc;
+    const int blocks = grid_blocks(*m, 16 * kWarps * 4, n);
+    mlp_grad_kernel<<<blocks, 32 * kWarps, 0, st>>>(
+        m->prm, reinterpret_cast<const uint32_t*>(m->w1b), reinterpret_cast<const uint32_t*>(m->w2b),
+        reinterpret_cast<const uint32_t*>(m->w2tb), reinterpret_cast<const uint32_t*>(X), t, n,
+        1.f / static_cast<float>(n), grad);
+    return cuda_err(cudaGetLastError(), "sb200_mlp_gradients");
+}
+
+int sb200_mlp_train_step(void* h, const uint16_t* X, const float* t, int64_t n, float lr,
+                         float* loss, void* stream) {
+    Mlp* m = static_cast<Mlp*>(h);
+    if (!m) return set_error(SB200_ERR_INVALID, "sb200_mlp_train_step: NULL handle");
+    if (!(lr > 0.f)) return set_error(SB200_ERR_INVALID, "sb200_mlp_train_step: lr must be positive");
+    if (int rc = sb200_mlp_gradients(h, X, t, n, m->grad, stream)) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    m->adam_t += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - std::pow(b1, float(m->adam_t)), c2 = 1.f - std::pow(b2, float(m->adam_t));
+    mlp_adam_kernel<<<(NPARAM + 255) / 256, 256, 0, st>>>(m->prm, m->m1, m->m2, m->grad, lr, b1, b2,
+                                                          1e-8f, c1, c2);
+    int rc = cuda_err(cudaGetLastError(), "sb200_mlp_train_step");
+    if (rc) return rc;
+    mlp_bf16_kernel<<<(H * F + 255) / 256, 256, 0, st>>>(m->prm, m->w1b, m->w2b, m->w2tb);
+    rc = cuda_err(cudaGetLastError(), "sb200_mlp_train_step");
+    if (!rc && loss)
+        rc = cuda_err(cudaMemcpyAsync(loss, m->grad + NPARAM, 4, cudaMemcpyDeviceToDevice, st),
+                      "sb200_mlp_train_step");
+    return rc;
+}
+
+int sb200_mlp_correct(void* h, const float* p, const float* vel2, float* p_next,
+                      const sb200_grid* grid, void* stream) {
+    Mlp* m = static_cast<Mlp*>(h);
+    if (!m || !p || !vel2 || !p_next || !grid)
+        return set_error(SB200_ERR_INVALID, "sb200_mlp_correct: NULL argument");
+    if (p == p_next) return set_error(SB200_ERR_INVALID, "sb200_mlp_correct: p_next must not alias p");
+    if (grid->nx <= 8 || grid->ny <= 8 || grid->nz <= 8) return SB200_OK;
+    const float dx = std::min(grid->dx, std::min(grid->dy, grid->dz));
+    const int64_t items = ((grid->nx - 8 + 31) / 32) * (grid->ny - 8) * (grid->nz - 8);
+    const int blocks = grid_blocks(*m, kCorrWarps * 4, items);
+    mlp_correct_kernel<<<blocks, 32 * kCorrWarps, 0, static_cast<cudaStream_t>(stream)>>>(
+        m->prm, reinterpret_cast<const uint32_t*>(m->w1b), reinterpret_cast<const uint32_t*>(m->w2b),
+        p, vel2, p_next, grid->nx, grid->ny, grid->nz, grid->dt / dx, m->out_scale);
+    return cuda_err(cudaGetLastError(), "sb200_mlp_correct");
+}
+
+int sb200_mlp_samples(const float* p, const float* vel2, const float* p_true, const float* p_plain,
+                      const sb200_grid* grid, const int64_t* cells, int64_t n, uint16_t* X,
+                      float* t, void* stream) {
+    if (!p || !vel2 || !p_true || !p_plain || !grid || !cells || !X || !t || n < 0)
+        return set_error(SB200_ERR_INVALID, "sb200_mlp_samples: bad arguments");
+    if (n == 0) return SB200_OK;
+    const float dx = std::min(grid->dx, std::min(grid->dy, grid->dz));
+    mlp_samples_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0,
+                         static_cast<cudaStream_t>(stream)>>>(
+        p, vel2, p_true, p_plain, grid->nx, grid->ny, grid->dt / dx, cells, n,
+        reinterpret_cast<uint32_t*>(X), t);
+    return cuda_err(cudaGetLastError(), "sb200_mlp_samples");
+}
+
+int sb200_add_box(float* field, const sb200_grid* grid, int x0, int y0, int z0, int bx, int by,
+                  int bz, const float* pattern, float scale, void* stream) {
+    if (!field || !grid || !pattern || bx < 0 || by < 0 || bz < 0)
+        return set_error(SB200_ERR_INVALID, "sb200_add_box: bad arguments");
+    const int n = bx * by * bz;
+    if (n == 0) return SB200_OK;
+    add_box_kernel<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        field, grid->nx, grid->ny, grid->nz, x0, y0, z0, bx, by, bz, pattern, scale);
+    return cuda_err(cudaGetLastError(), "sb200_add_box");
+}
+
+int sb200_restrict2(const float* fine, const sb200_grid* fine_grid, float* coarse,
+                    const sb200_grid* coarse_grid, int offset, void* stream) {
+    if (!fine || !fine_grid || !coarse || !coarse_grid)
+        return set_error(SB200_ERR_INVALID, "sb200_restrict2: NULL argument");
+    const int64_t n = coarse_grid->nx * coarse_grid->ny * coarse_grid->nz;
+    if (n <= 0) return SB200_OK;
+    restrict2_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0,
+                       static_cast<cudaStream_t>(stream)>>>(
+        fine, fine_grid->nx, fine_grid->ny, fine_grid->nz, coarse, coarse_grid->nx,
+        coarse_grid->ny, coarse_grid->nz, offset);
+    return cuda_err(cudaGetLastError(), "sb200_restrict2");
+}
+
+}  // extern "C"

@@ -1,0 +1,337 @@
+"""Learned 2x-coarse stepping: training pairs from the plain fine solver, training
+of the correction network on the GPU, and the coarse run it corrects.
+
+No reference counterpart (the reference solves on one grid only).  Geometry:
+a coarse grid of nc points per axis at spacing h and time step dt pairs with a
+fine grid of 2 nc - 8 points at h / 2 and dt / 2, aligned so that coarse cell i
+sits on fine cell 2 i - 4.  Both grids then have their interior start and their
+far wall at the same physical positions (the near wall differs by half a coarse
+cell).
+
+Source: both grids discretise the same continuum term S(x, t) = A v^2 w(t) g(x),
+w a Ricker wavelet and g a Gaussian of width sigma (2 coarse cells by default)
+around the source point: each step adds dt^2 S(x_j, t_n) on a box of cells.  A
+point source (the reference's rule, one cell) puts energy above the coarse
+grid's Nyquist wavenumber, which no coarse state can represent; the Gaussian
+keeps the field band-limited, so the coarse-grid error is the scheme's
+dispersion error, a function of the local state.
+
+Velocity: the coarse grid samples the fine model.  A sharply layered model is a
+different medium on the two grids (an interface moves by up to half a coarse
+cell), so `smooth_cells` > 0 first smooths the fine model with a Gaussian of
+that width (in coarse cells): the medium both grids resolve.
+
+Training pairs (coarse state at t, fine state at t + dt restricted): with C_m
+the restriction of the fine field after 2m fine steps, the plain coarse step
+from (C_{m-1}, C_{m-2}) gives P_m; the network learns (C_m - P_m) / s from the
+features of C_{m-1} (see stencil_b200.h, sb200_mlp_*).
+
+The host loop here only orders C-ABI calls on device buffers (torch allocates
+them); every operation on field data is a kernel of the library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import Grid, Mlp, _check, add_box, lib, mlp_samples, restrict2, wave_step
+
+OFFSET = -4  # coarse cell i <-> fine cell 2 i + OFFSET
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def fine_extent(nc: int) -> int:
+    return 2 * nc - 8
+
+
+@dataclass
+class Problem:
+    """One velocity model on the coarse / fine pair of grids."""
+    nc: int
+    h: float            # coarse spacing [m]
+    dt: float           # coarse time step [s]
+    seed: int
+    freq: float = 25.0
+    src_c: tuple = None  # source point in coarse cells (x, y, z); default: the centre
+    sigma_cells: float = 2.0  # source width in coarse cells
+    model: str = "layered"    # "layered" or "constant"
+    smooth_cells: float = 0.0  # Gaussian smoothing of the fine model, in coarse cells
+    layers: int = 8
+    v_top: float = 1500.0
+    v_bottom: float = 4500.0
+    perturbation: float = 0.05
+    corr_cells: float = 20.0
+
+    def __post_init__(self):
+        if self.src_c is None:
+            c = self.nc // 2
+            self.src_c = (c, c, c)
+        self._vf = None
+
+    @property
+    def coarse(self) -> Grid:
+        return Grid(self.nc, self.nc, self.nc, self.h, self.h, self.h, self.dt)
+
+    @property
+    def fine(self) -> Grid:
+        nf = fine_extent(self.nc)
+        return Grid(nf, nf, nf, self.h / 2, self.h / 2, self.h / 2, self.dt / 2)
+
+    def wavelet(self, fine: bool, n: int) -> np.ndarray:
+        """w(t_k), k < n, at the grid's own time step."""
+        g = self.fine if fine else self.coarse
+        w = np.empty(n, np.float32)
+        _check(lib().sb200_ricker(self.freq, 1.0 / self.freq, g.dt, n, w.ctypes.data))
+        return w
+
+    def vel2_fine_host(self) -> np.ndarray:
+        """The fine model: seeded layered (host generator of the library) or
+        constant (a seeded speed in [v_top, v_bottom]), optionally smoothed."""
+        if self._vf is None:
+            g = self.fine
+            if self.model == "constant":
+                v = np.random.default_rng(self.seed).uniform(self.v_top, self.v_bottom)
+                v2 = np.full(g.shape, v * v, np.float32)
+            else:
+                v2 = np.empty(g.shape, np.float32)
+                vmax = C.c_float()
+                _check(lib().sb200_model_layered(v2.ctypes.data, g.nx, g.ny, g.nz, self.seed,
+                                                 self.layers, self.v_top, self.v_bottom,
+                                                 self.perturbation, self.corr_cells,
+                                                 C.byref(vmax)))
+            if self.smooth_cells > 0:
+                from scipy.ndimage import gaussian_filter
+
+                vel = gaussian_filter(np.sqrt(v2.astype(np.float64)), 2.0 * self.smooth_cells,
+                                      mode="nearest")
+                v2 = (vel * vel).astype(np.float32)
+            self._vf = v2
+        return self._vf
+
+    def vel2_coarse_host(self) -> np.ndarray:
+        """The fine model sampled at the coarse cells (as sb200_restrict2 does)."""
+        vf = self.vel2_fine_host()
+        nc = self.nc
+        vc = np.zeros((nc, nc, nc), np.float32)
+        i = np.arange(4, nc - 4)
+        vc[4:-4, 4:-4, 4:-4] = vf[np.ix_(2 * i + OFFSET, 2 * i + OFFSET, 2 * i + OFFSET)]
+        return vc
+
+    def device_models(self):
+        """(vel2 fine, vel2 coarse) on the device; the coarse one is restricted."""
+        torch = _torch()
+        vf = torch.from_numpy(self.vel2_fine_host()).cuda()
+        vc = torch.empty(self.coarse.shape, device="cuda")
+        restrict2(vf, self.fine, vc, self.coarse, OFFSET)
+        return vf, vc
+
+    def source(self, fine: bool):
+        """(origin, dims, pattern on the device, amplitude A): pattern_j = vel2_j g(x_j)
+        on the box of cells within 3.5 sigma of the source point."""
+        torch = _torch()
+        sig = self.sigma_cells  # in coarse cells
+        rad_c = int(math.ceil(3.5 * sig))
+        if fine:
+            v = self.vel2_fine_host()
+            centre = [2 * c + OFFSET for c in self.src_c]
+            rad, unit = 2 * rad_c + 1, 0.5  # a fine cell is half a coarse cell
+        else:
+            v = self.vel2_coarse_host()
+            centre = list(self.src_c)
+            rad, unit = rad_c, 1.0
+        origin = [c - rad for c in centre]
+        n = 2 * rad + 1
+        off = (np.arange(n) - rad) * unit
+        r2 = off[None, None, :] ** 2 + off[None, :, None] ** 2 + off[:, None, None] ** 2
+        gx = np.exp(-r2 / (2 * sig * sig))
+        zs, ys, xs = [slice(o, o + n) for o in origin[::-1]]
+        pat = (v[zs, ys, xs] * gx).astype(np.float32)
+        amp = 1.0 / (self.dt * self.dt * 3000.0 * 3000.0)  # O(1) fields
+        return tuple(origin), (n, n, n), torch.from_numpy(np.ascontiguousarray(pat)).cuda(), amp
+
+
+def _inject(pb: Problem, fine: bool, fld, src, w, k) -> None:
+    origin, dims, pat, amp = src
+    g = pb.fine if fine else pb.coarse
+    add_box(fld, g, origin, dims, pat, float(g.dt * g.dt * amp * w[k]))
+
+
+def fine_solve(pb: Problem, vf, steps: int, on_even=None):
+    """Plain fine solve from rest for `steps` fine steps.  on_even(m, field) is
+    called after every even number 2m of steps (m >= 0) with the device field."""
+    torch = _torch()
+    g = pb.fine
+    p = torch.zeros(g.shape, device="cuda")
+    q = torch.zeros(g.shape, device="cuda")
+    w = pb.wavelet(True, steps)
+    src = pb.source(True)
+    if on_even:
+        on_even(0, p)
+    for n in range(steps):
+        wave_step(p, q, vf, q, g)
+        _inject(pb, True, q, src, w, n)
+        p, q = q, p
+        if on_even and (n + 1) % 2 == 0:
+            on_even((n + 1) // 2, p)
+    return p
+
+
+def coarse_step(pb: Problem, vc, p, q, src, w, m, mlp: Mlp | None = None) -> None:
+    """One coarse step from level m (p) over level m-1 (q, overwritten with m+1)."""
+    g = pb.coarse
+    wave_step(p, q, vc, q, g)
+    _inject(pb, False, q, src, w, m)
+    if mlp is not None:
+        mlp.correct(p, vc, q, g)
+
+
+def coarse_solve(pb: Problem, vc, steps: int, mlp: Mlp | None = None):
+    """Plain (mlp None) or corrected coarse solve from rest for `steps` coarse steps."""
+    torch = _torch()
+    g = pb.coarse
+    p = torch.zeros(g.shape, device="cuda")
+    q = torch.zeros(g.shape, device="cuda")
+    w = pb.wavelet(False, steps)
+    src = pb.source(False)
+    for m in range(steps):
+        coarse_step(pb, vc, p, q, src, w, m, mlp)
+        p, q = q, p
+    return p
+
+
+@dataclass
+class Dataset:
+    X: object  # (n, 32) int16 BF16 bit patterns, device
+    t: object  # (n,) float32, device
+    per_model: list = field(default_factory=list)
+
+    @property
+    def n(self) -> int:
+        return int(self.t.numel())
+
+
+def make_pairs(problems, fine_steps: int, samples_per_pair: int = 4096, every: int = 4,
+               first: int = 8, wall: int = 12, amp_floor: float = 0.05, src_clear: float = 3.5,
+               seed: int = 0) -> Dataset:
+    """Training rows from the plain fine solver on each problem: every `every`
+    coarse steps from `first` on, samples_per_pair random coarse cells at least
+    `wall` cells from the walls and src_clear source widths from the source point,
+    whose local field exceeds amp_floor x the field's largest magnitude.  (Inside
+    the source the two grids' time sampling of the wavelet differs, and where the
+    field is small its round-off dominates the normalised residual: neither is a
+    function of the local state.)"""
+    torch = _torch()
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    Xs, ts, counts = [], [], []
+    for pb in problems:
+        vf, vc = pb.device_models()
+        gc = pb.coarse
+        w_c = pb.wavelet(False, fine_steps // 2 + 2)
+        src_c = pb.source(False)
+        ring = {}
+        plain = torch.empty(gc.shape, device="cuda")
+        nz, ny, nx = gc.shape
+        box = torch.zeros(gc.shape, dtype=torch.bool, device="cuda")
+        box[wall:nz - wall, wall:ny - wall, wall:nx - wall] = True
+        zz, yy, xx = torch.meshgrid(*(torch.arange(k, device="cuda") for k in (nz, ny, nx)),
+                                    indexing="ij")
+        sx, sy, sz = pb.src_c
+        d2 = (xx - sx) ** 2 + (yy - sy) ** 2 + (zz - sz) ** 2
+        box &= d2 > (src_clear * pb.sigma_cells) ** 2
+        del zz, yy, xx, d2
+        before = sum(x.shape[0] for x in Xs)
+
+        def on_even(m, f):
+            c = torch.empty(gc.shape, device="cuda")
+            restrict2(f, pb.fine, c, gc, OFFSET)
+            ring[m] = c
+            ring.pop(m - 3, None)
+            if m >= max(first, 2) and (m - first) % every == 0:
+                cm2, cm1, cm = ring[m - 2], ring[m - 1], ring[m]
+                plain.copy_(cm2)  # in-place leapfrog writes over the older level
+                coarse_step(pb, vc, cm1, plain, src_c, w_c, m - 1)
+                mag = cm1.abs()
+                ok = box & (mag > amp_floor * float(mag.max()))
+                cand = torch.nonzero(ok.view(-1)).view(-1)
+                if cand.numel() == 0:
+                    return
+                pick = cand[torch.randint(0, cand.numel(), (min(samples_per_pair, cand.numel()),),
+                                          generator=gen, device="cuda")]
+                X = torch.empty((pick.numel(), 32), dtype=torch.int16, device="cuda")
+                t = torch.empty(pick.numel(), dtype=torch.float32, device="cuda")
+                mlp_samples(cm1, vc, cm, plain, gc, pick.to(torch.int64), X, t)
+                Xs.append(X)
+                ts.append(t)
+
+        fine_solve(pb, vf, fine_steps, on_even)
+        counts.append(sum(x.shape[0] for x in Xs) - before)
+        del vf, vc
+    return Dataset(torch.cat(Xs), torch.cat(ts), counts)
+
+
+def train(ds: Dataset, mlp: Mlp, epochs: int = 4, batch: int = 8192, lr: float = 2e-3,
+          lr_final: float = 1e-4, seed: int = 0, log=None) -> list:
+    """Adam over shuffled mini-batches with a cosine learning-rate decay.  The
+    targets are divided by their RMS, which becomes the network's output scale.
+    Returns the mean batch loss (in units of that RMS squared) of every epoch."""
+    torch = _torch()
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    n = ds.n
+    rms = float(ds.t.double().pow(2).mean().sqrt())
+    mlp.output_scale = rms if rms > 0 else 1.0
+    tn = ds.t / mlp.output_scale
+    steps_per_epoch = max(1, n // batch)
+    total = epochs * steps_per_epoch
+    loss = torch.zeros(1, device="cuda")
+    acc = torch.zeros(1, device="cuda")
+    history = []
+    k = 0
+    for ep in range(epochs):
+        perm = torch.randperm(n, generator=gen, device="cuda")
+        acc.zero_()
+        for b in range(steps_per_epoch):
+            idx = perm[b * batch:(b + 1) * batch]
+            X = ds.X.index_select(0, idx)
+            t = tn.index_select(0, idx)
+            cur = lr_final + 0.5 * (lr - lr_final) * (1 + math.cos(math.pi * k / max(1, total - 1)))
+            mlp.train_step(X, t, cur, loss)
+            acc += loss
+            k += 1
+        history.append(float(acc.item()) / steps_per_epoch)
+        if log:
+            log(f"epoch {ep}: loss {history[-1]:.4e}")
+    return history
+
+
+def rel_l2(a, b) -> float:
+    """||a - b|| / ||b|| over the interior, in double."""
+    torch = _torch()
+    a = a[4:-4, 4:-4, 4:-4].double()
+    b = b[4:-4, 4:-4, 4:-4].double()
+    nb = torch.linalg.vector_norm(b)
+    return float(torch.linalg.vector_norm(a - b) / nb) if float(nb) > 0 else float("nan")
+
+
+def evaluate(pb: Problem, coarse_steps: int, mlp: Mlp | None):
+    """Errors of the plain and the corrected coarse solves against the restricted
+    plain fine solve (the judge) after coarse_steps steps: {"plain": e0, "learned": e1}."""
+    torch = _torch()
+    vf, vc = pb.device_models()
+    judge_f = fine_solve(pb, vf, 2 * coarse_steps)
+    judge = torch.empty(pb.coarse.shape, device="cuda")
+    restrict2(judge_f, pb.fine, judge, pb.coarse, OFFSET)
+    del judge_f, vf
+    out = {"plain": rel_l2(coarse_solve(pb, vc, coarse_steps), judge)}
+    if mlp is not None:
+        out["learned"] = rel_l2(coarse_solve(pb, vc, coarse_steps, mlp), judge)
+    return out

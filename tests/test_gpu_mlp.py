@@ -1,0 +1,191 @@
+"""The learned-correction kernels against the oracle: feature rows (bit-exact),
+forward and gradients of the BF16 mma network (tolerances in the tests), the
+fused correction kernel, restriction, box injection, and that Adam training
+lowers the loss."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+import stencil_solver_b200 as sb
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(autouse=True)
+def _clean(torch_cuda):
+    yield
+    torch_cuda.cuda.synchronize()
+    assert sb.device_error() == 0
+
+
+def dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def net_and_rows(seed, n):
+    rng = np.random.default_rng(seed)
+    w = (rng.standard_normal(sb.MLP_NPARAM) * 0.3).astype(np.float32)
+    w[:1024].reshape(32, 32)[:, 26:] = 0
+    X = oracle.to_bf16(rng.uniform(-1, 1, (n, 32)).astype(np.float32))
+    X[:, 26:] = 0
+    t = rng.standard_normal(n).astype(np.float32)
+    return w, X, t
+
+
+def field_case(seed, shape=(40, 36, 44)):
+    rng = np.random.default_rng(seed)
+    p = rng.standard_normal(shape).astype(np.float32)
+    v2 = rng.uniform(1500, 4500, shape).astype(np.float32) ** 2
+    m = np.ones(shape, bool)
+    m[4:-4, 4:-4, 4:-4] = False
+    p[m] = 0
+    return p, v2
+
+
+def interior_cells(shape):
+    nz, ny, nx = shape
+    z, y, x = np.meshgrid(np.arange(4, nz - 4), np.arange(4, ny - 4), np.arange(4, nx - 4),
+                          indexing="ij")
+    return ((z * ny + y) * nx + x).ravel().astype(np.int64)
+
+
+def test_samples_are_bit_exact(torch_cuda):
+    torch = torch_cuda
+    p, v2 = field_case(1)
+    nz, ny, nx = p.shape
+    g = sb.Grid(nx, ny, nz, 10.0, 10.0, 10.0, 8e-4)
+    rng = np.random.default_rng(2)
+    pt = (p + 0.01 * rng.standard_normal(p.shape)).astype(np.float32)
+    pp = (p + 0.01 * rng.standard_normal(p.shape)).astype(np.float32)
+    cells = rng.choice(interior_cells(p.shape), 500, replace=False)
+    X = torch.empty((500, 32), dtype=torch.int16, device="cuda")
+    t = torch.empty(500, dtype=torch.float32, device="cuda")
+    sb.mlp_samples(dev(torch, p), dev(torch, v2), dev(torch, pt), dev(torch, pp), g,
+                   dev(torch, cells), X, t)
+    torch.cuda.synchronize()
+    Xh, th = X.cpu().numpy().view(np.uint16), t.cpu().numpy()
+    dtdx = np.float32(np.float32(8e-4) / np.float32(10.0))
+    for r, c in enumerate(cells):
+        row, s = oracle.mlp_features(p, v2, c, dtdx)
+        assert np.array_equal(Xh[r], row)
+        assert th[r] == (np.float32(pt.flat[c] - pp.flat[c]) / np.float32(s))
+
+
+def test_forward_matches_oracle(torch_cuda):
+    torch = torch_cuda
+    w, X, _ = net_and_rows(3, 1000)
+    with sb.Mlp() as m:
+        m.set_params(w)
+        y = torch.empty(1000, dtype=torch.float32, device="cuda")
+        m.forward(dev(torch, X.view(np.int16)), y)
+        yg = y.cpu().numpy()
+    ref = oracle.mlp_forward(w, X, round_bf16=True)
+    # FP32 accumulation vs double; h1 rounds to BF16 on both sides, so an
+    # FP32-level difference can move one h1 by a BF16 ulp: bounded by 2e-2 of the scale.
+    assert np.max(np.abs(yg - ref)) <= 2e-2 * (1 + np.max(np.abs(ref)))
+    assert np.median(np.abs(yg - ref)) <= 1e-5 * (1 + np.max(np.abs(ref)))
+
+
+def test_gradients_match_oracle(torch_cuda):
+    torch = torch_cuda
+    w, X, t = net_and_rows(4, 4096)
+    with sb.Mlp() as m:
+        m.set_params(w)
+        grad = torch.empty(sb.MLP_NPARAM + 1, dtype=torch.float32, device="cuda")
+        m.gradients(dev(torch, X.view(np.int16)), dev(torch, t), grad)
+        gg = grad.cpu().numpy().astype(np.float64)
+    loss, ref = oracle.mlp_grad(w, X, t, round_bf16=True)
+    assert abs(gg[-1] - loss) <= 1e-4 * loss
+    # per parameter block: relative L2 of the difference
+    blocks = {"W1": slice(0, 1024), "b1": slice(1024, 1056), "W2": slice(1056, 2080),
+              "b2": slice(2080, 2112), "w3": slice(2112, 2144), "b3": slice(2144, 2145)}
+    for name, sl in blocks.items():
+        d = np.linalg.norm(gg[sl] - ref[sl]) / max(np.linalg.norm(ref[sl]), 1e-12)
+        assert d <= 5e-3, (name, d)
+
+
+def test_training_lowers_the_loss(torch_cuda):
+    torch = torch_cuda
+    rng = np.random.default_rng(5)
+    n = 1 << 15
+    F = rng.uniform(-1, 1, (n, 26)).astype(np.float32)
+    target = (0.5 * F[:, 0] - 0.25 * F[:, 1:9].sum(1) + 0.1 * np.maximum(F[:, 9], 0)).astype(np.float32)
+    X = np.zeros((n, 32), np.uint16)
+    X[:, :26] = oracle.to_bf16(F)
+    Xd, td = dev(torch, X.view(np.int16)), dev(torch, target)
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    with sb.Mlp(seed=11) as m:
+        losses = []
+        for step in range(300):
+            sl = slice((step * 4096) % n, (step * 4096) % n + 4096)
+            m.train_step(Xd[sl], td[sl], 3e-3, loss)
+            if step % 50 == 0 or step == 299:
+                losses.append(float(loss.item()))
+    assert losses[-1] < 0.1 * losses[0], losses
+
+
+def test_correct_kernel_adds_scaled_mlp(torch_cuda):
+    torch = torch_cuda
+    p, v2 = field_case(6, (24, 20, 40))
+    nz, ny, nx = p.shape
+    g = sb.Grid(nx, ny, nz, 10.0, 10.0, 10.0, 8e-4)
+    w, _, _ = net_and_rows(7, 1)
+    base = np.random.default_rng(8).standard_normal(p.shape).astype(np.float32)
+    with sb.Mlp() as m:
+        m.set_params(w)
+        m.output_scale = 0.5
+        out = dev(torch, base)
+        m.correct(dev(torch, p), dev(torch, v2), out, g)
+        got = out.cpu().numpy()
+    dtdx = np.float32(np.float32(8e-4) / np.float32(10.0))
+    cells = interior_cells(p.shape)
+    rows = np.zeros((cells.size, 32), np.uint16)
+    s = np.zeros(cells.size, np.float64)
+    for r, c in enumerate(cells):
+        rows[r], s[r] = oracle.mlp_features(p, v2, c, dtdx)
+    ref = base.ravel().astype(np.float64).copy()
+    ref[cells] += 0.5 * s * oracle.mlp_forward(w, rows, True)
+    err = np.abs(got.ravel() - ref)
+    assert np.max(err[cells]) <= 2e-2 * (1 + np.max(np.abs(s)))
+    halo = np.ones(p.size, bool)
+    halo[cells] = False
+    assert np.array_equal(got.ravel()[halo], base.ravel()[halo])
+
+
+def test_restrict2(torch_cuda):
+    torch = torch_cuda
+    rng = np.random.default_rng(9)
+    fine = rng.standard_normal((56, 48, 40)).astype(np.float32)
+    fg = sb.Grid(40, 48, 56, 5.0, 5.0, 5.0, 4e-4)
+    cg = sb.Grid(24, 28, 32, 10.0, 10.0, 10.0, 8e-4)
+    out = torch.full(cg.shape, 7.0, device="cuda")
+    sb.restrict2(dev(torch, fine), fg, out, cg, -4)
+    got = out.cpu().numpy()
+    ref = np.zeros(cg.shape, np.float32)
+    for z in range(4, 28):
+        for y in range(4, 24):
+            for x in range(4, 20):
+                fz, fy, fx = 2 * z - 4, 2 * y - 4, 2 * x - 4
+                if fz < 56 and fy < 48 and fx < 40:
+                    ref[z, y, x] = fine[fz, fy, fx]
+    assert np.array_equal(got, ref)
+
+
+def test_add_box_skips_the_halo(torch_cuda):
+    torch = torch_cuda
+    g = sb.Grid(24, 20, 16)
+    f = torch.zeros(g.shape, device="cuda")
+    pat = torch.arange(1, 7 * 7 * 7 + 1, dtype=torch.float32, device="cuda")
+    sb.add_box(f, g, (1, 2, 3), (7, 7, 7), pat, 0.5)
+    got = f.cpu().numpy()
+    ref = np.zeros(g.shape, np.float32)
+    pv = pat.cpu().numpy().reshape(7, 7, 7)
+    for k in range(7):
+        for j in range(7):
+            for i in range(7):
+                x, y, z = 1 + i, 2 + j, 3 + k
+                if 4 <= x < 20 and 4 <= y < 16 and 4 <= z < 12:
+                    ref[z, y, x] += 0.5 * pv[k, j, i]
+    assert np.array_equal(got, ref)
