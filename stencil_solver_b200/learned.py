@@ -10,7 +10,9 @@ cell).
 
 Source: both grids discretise the same continuum term S(x, t) = A v^2 w(t) g(x),
 w a Ricker wavelet and g a Gaussian of width sigma (2 coarse cells by default)
-around the source point: each step adds dt^2 S(x_j, t_n) on a box of cells.  A
+around the source point: each step adds dt^2 S(x_j, t_n) on a box of cells
+(the coarse grid's w samples are the [1, 2, 1] / 4 average of the fine ones,
+see Problem.wavelet).  A
 point source (the reference's rule, one cell) puts energy above the coarse
 grid's Nyquist wavenumber, which no coarse state can represent; the Gaussian
 keeps the field band-limited, so the coarse-grid error is the scheme's
@@ -86,11 +88,21 @@ class Problem:
         return Grid(nf, nf, nf, self.h / 2, self.h / 2, self.h / 2, self.dt / 2)
 
     def wavelet(self, fine: bool, n: int) -> np.ndarray:
-        """w(t_k), k < n, at the grid's own time step."""
-        g = self.fine if fine else self.coarse
-        w = np.empty(n, np.float32)
-        _check(lib().sb200_ricker(self.freq, 1.0 / self.freq, g.dt, n, w.ctypes.data))
-        return w
+        """Source samples of the first n steps.  Fine: w(k dt_f).  Coarse:
+        (w(t - dt_f) + 2 w(t) + w(t + dt_f)) / 4 at t = m dt_c -- two fine
+        leapfrog steps add up to one coarse step whose source term is exactly
+        that [1, 2, 1] / 4 average of the fine samples, so the coarse grid
+        injects what the fine grid does, to the scheme's order."""
+        dtf = self.fine.dt
+        if fine:
+            w = np.empty(n, np.float32)
+            _check(lib().sb200_ricker(self.freq, 1.0 / self.freq, dtf, n, w.ctypes.data))
+            return w
+        s = np.empty(2 * n + 2, np.float32)  # s[k] = w((k - 1) dt_f)
+        _check(lib().sb200_ricker(self.freq, 1.0 / self.freq + dtf, dtf, 2 * n + 2,
+                                  s.ctypes.data))
+        s = s.astype(np.float64)
+        return ((s[0:2 * n:2] + 2 * s[1:2 * n + 1:2] + s[2:2 * n + 2:2]) / 4).astype(np.float32)
 
     def vel2_fine_host(self) -> np.ndarray:
         """The fine model: seeded layered (host generator of the library) or
