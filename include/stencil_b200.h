@@ -351,9 +351,12 @@ int sb200_mlp_gradients(void* handle, const uint16_t* X, const float* t, int64_t
 int sb200_mlp_train_step(void* handle, const uint16_t* X, const float* t, int64_t n, float lr,
                          float* loss, void* stream);
 /* p_next += s * c * MLP(features of p) on the interior (p, vel2, p_next device
- * FP32; p_next must not alias p). */
+ * FP32; p_next must not alias p).  Runs on tcgen05 (TMEM accumulators) unless
+ * sb200_mlp_set_kernel selected the mma.sync kernel. */
 int sb200_mlp_correct(void* handle, const float* p, const float* vel2, float* p_next,
                       const sb200_grid* grid, void* stream);
+/* Correction kernel of the handle: 0 = tcgen05 (default), 1 = mma.sync. */
+int sb200_mlp_set_kernel(void* handle, int kernel);
 /* Training rows at n cells (device int64 flat indices, interior only):
  * X[r] = features of p at cells[r], t[r] = (p_true - p_plain)[cell] / s. */
 int sb200_mlp_samples(const float* p, const float* vel2, const float* p_true, const float* p_plain,

@@ -178,6 +178,7 @@ _SIGNATURES = {
     "sb200_mlp_get_params": ([C.c_void_p, C.c_void_p], C.c_int),
     "sb200_mlp_set_params": ([C.c_void_p, C.c_void_p], C.c_int),
     "sb200_mlp_set_output_scale": ([C.c_void_p, C.c_float], C.c_int),
+    "sb200_mlp_set_kernel": ([C.c_void_p, C.c_int], C.c_int),
     "sb200_mlp_output_scale": ([C.c_void_p], C.c_float),
     "sb200_mlp_forward": ([C.c_void_p] * 3 + [C.c_int64, C.c_void_p], C.c_int),
     "sb200_mlp_gradients": ([C.c_void_p] * 3 + [C.c_int64, C.c_void_p, C.c_void_p], C.c_int),
@@ -654,6 +655,10 @@ class Mlp:
     @output_scale.setter
     def output_scale(self, c: float) -> None:
         _check(lib().sb200_mlp_set_output_scale(self._h, c))
+
+    def set_kernel(self, kernel: str) -> None:
+        """Correction kernel: "tcgen05" (default) or "mma"."""
+        _check(lib().sb200_mlp_set_kernel(self._h, {"tcgen05": 0, "mma": 1}[kernel]))
 
     def forward(self, X, y, n=None, stream=None) -> None:
         n = X.shape[0] if n is None else n

@@ -34,6 +34,7 @@
 
 #include "dispatch.h"
 #include "kernels.h"
+#include "sb200_common.cuh"
 #include "stencil_b200.h"
 
 namespace sb200 {
@@ -561,6 +562,278 @@ __global__ void __launch_bounds__(32 * kCorrWarps)
     }
 }
 
+// ── tcgen05 correction ───────────────────────────────────────────────────────
+// The same correction on the 5th-generation tensor cores: a CTA of 128 threads
+// takes tiles of 128 points (4 row segments of 32), writes their feature rows
+// to shared memory, and one thread issues tcgen05.mma (M = 128, N = 32,
+// K = 16, BF16 operands from shared memory, FP32 accumulator in TMEM): two per
+// layer.  Each thread then owns one point (one TMEM lane): tcgen05.ld of its 32
+// accumulator columns, bias + ReLU + BF16 for layer 2's A operand, and the
+// final 32-term dot product with w3 in FP32.
+constexpr int kTcThreads = 128;
+constexpr uint32_t kTcCols = 64;  // TMEM columns: layer 1 in 0..31, layer 2 in 32..63
+// Dynamic shared memory requested per CTA (20.5 KB of tiles + alignment): at
+// most 8 CTAs then fit on one SM, 8 x 64 = 512 TMEM columns, so tcgen05.alloc
+// never waits for another CTA.
+constexpr int kTcSmem = 26 * 1024;
+constexpr uint32_t kTcIdesc = (1u << 4)                   // D: FP32
+                              | (1u << 7) | (1u << 10)   // A, B: BF16 (both K-major)
+                              | (uint32_t(32 >> 3) << 17)  // N = 32
+                              | (uint32_t(128 >> 4) << 24);  // M = 128
+
+// Byte offset of element (row, k) of a K-major BF16 operand in the no-swizzle
+// canonical layout: 8-row x 16-byte core matrices, the 4 K-chunks of a row
+// group 128 B apart (leading byte offset), row groups 512 B apart (stride byte
+// offset).  A K = 16 step starts 256 B further.
+__device__ __forceinline__ uint32_t core_off(int row, int k) {
+    return uint32_t((row >> 3) * 512 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+    return uint64_t((saddr >> 4) & 0x3FFFu)  // start address
+           | (uint64_t(128 >> 4) << 16)      // leading byte offset
+           | (uint64_t(512 >> 4) << 32)      // stride byte offset
+           | (uint64_t(1) << 46);            // descriptor version; no swizzle
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t accumulate) {
+    const uint32_t mask = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
+        :
+        : "r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate), "r"(mask)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+// 32 consecutive FP32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+        "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
+        "%28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+          "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+          "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ uint32_t relu_bf2(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+
+// One feature / activation row (16 words = 32 BF16) into a K-major operand tile.
+__device__ __forceinline__ void store_row(unsigned char* tile, int row, const uint32_t (&w)[16]) {
+#pragma unroll
+    for (int kc = 0; kc < 4; ++kc)
+        *reinterpret_cast<uint4*>(tile + core_off(row, 8 * kc)) =
+            make_uint4(w[4 * kc], w[4 * kc + 1], w[4 * kc + 2], w[4 * kc + 3]);
+}
+
+// Packed FP32 pairs (sm_100 f32x2): each lane rounds as the scalar op would.
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mov.b64 rc, {%6, %7};\n\tfma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return d;
+}
+
+__global__ void __launch_bounds__(kTcThreads)
+    mlp_correct_tc_kernel(const float* __restrict__ prm, const uint16_t* __restrict__ w1b,
+                          const uint16_t* __restrict__ w2b, const float* __restrict__ p,
+                          const float* __restrict__ vel2, float* __restrict__ p_next, int nx,
+                          int ny, int nz, float dt_over_dx, float out_scale, int* err) {
+    extern __shared__ unsigned char dyn[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_flag;  // 1: the last MMA wait gave up
+    __shared__ __align__(16) float sb1[H], sb2[H], sw3[H];
+    unsigned char* base = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(dyn) + 1023) & ~uintptr_t(1023));
+    unsigned char* sA = base;            // 128 x 32 BF16 features
+    unsigned char* sA2 = base + 8192;    // 128 x 32 BF16 h1
+    unsigned char* sW1 = base + 16384;   // 32 x 32 BF16
+    unsigned char* sW2 = base + 18432;   // 32 x 32 BF16
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    for (int i = tid; i < H * F; i += kTcThreads) {
+        *reinterpret_cast<uint16_t*>(sW1 + core_off(i / F, i % F)) = w1b[i];
+        *reinterpret_cast<uint16_t*>(sW2 + core_off(i / H, i % H)) = w2b[i];
+    }
+    if (tid < H) {
+        sb1[tid] = prm[OFF_B1 + tid];
+        sb2[tid] = prm[OFF_B2 + tid];
+        sw3[tid] = prm[OFF_W3 + tid];
+    }
+    const float b3 = prm[OFF_B3];
+    if (tid == 0) {
+        mbar_init(&mbar, 1);
+        fence_barrier_init();
+        s_flag = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&s_tmem)),
+                     "r"(kTcCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const uint32_t lane_base = tmem + (uint32_t(32 * warp) << 16);
+    const uint32_t aA = smem_u32(sA), aA2 = smem_u32(sA2), aW1 = smem_u32(sW1),
+                   aW2 = smem_u32(sW2);
+
+    // Work: 32-point segments of interior rows, 4 per tile (one per warp).
+    const unsigned segs = unsigned(nx - 8 + 31) / 32u, rows_y = unsigned(ny - 8);
+    const unsigned items = segs * rows_y * unsigned(nz - 8);
+    const unsigned tiles = (items + 3u) / 4u;
+    const int64_t sy = nx, sz = int64_t(nx) * ny;
+    int issued = 0, completed = 0;  // thread 0: commits issued / seen complete
+    bool abort_run = false;
+    // One thread waits for the MMAs; the others meet it at the barrier that
+    // follows (no spinning warps).
+    auto wait_mma = [&](uint32_t parity) {
+        if (tid == 0) {
+            if (mbar_wait(&mbar, parity))
+                completed = issued;
+            else
+                s_flag = 1;
+        }
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        return s_flag == 0;
+    };
+    for (unsigned tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const unsigned item = tile * 4u + unsigned(warp);
+        int64_t c = 0;
+        float sc = 0.f;
+        uint32_t fr[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) fr[j] = 0u;
+        if (item < items) {
+            const unsigned seg = item % segs, row = item / segs;
+            const int y = 4 + int(row % rows_y), z = 4 + int(row / rows_y);
+            const int x = 4 + int(seg) * 32 + lane;
+            if (x < nx - 4) {
+                c = (int64_t(z) * ny + y) * nx + x;
+                Star st;
+                gather_star(st, p, c, sy, sz);
+                feature_row(fr, st, sqrtf(vel2[c]) * dt_over_dx);
+                sc = st.s * out_scale;
+            }
+        }
+        store_row(sA, tid, fr);
+        fence_async_smem();
+        // A tile whose points are all exactly zero has a zero correction: skip it.
+        if (__syncthreads_or(sc > 0.f) == 0) continue;
+        if (tid == 0) {
+            tc_fence_after();
+            tc_mma(tmem, umma_desc(aA), umma_desc(aW1), 0u);
+            tc_mma(tmem, umma_desc(aA + 256), umma_desc(aW1 + 256), 1u);
+            tc_commit(&mbar);
+            ++issued;
+        }
+        if (!wait_mma(0)) {
+            abort_run = true;
+            break;
+        }
+        float d[32];
+        tc_ld32(lane_base, d);
+        uint32_t h[16];
+#pragma unroll
+        for (int q4 = 0; q4 < 8; ++q4) {
+            const float4 bb = *reinterpret_cast<const float4*>(&sb1[4 * q4]);
+            const float2 u = add2(make_float2(d[4 * q4], d[4 * q4 + 1]), make_float2(bb.x, bb.y));
+            const float2 v = add2(make_float2(d[4 * q4 + 2], d[4 * q4 + 3]), make_float2(bb.z, bb.w));
+            h[2 * q4] = relu_bf2(u.x, u.y);
+            h[2 * q4 + 1] = relu_bf2(v.x, v.y);
+        }
+        store_row(sA2, tid, h);
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            tc_mma(tmem + 32, umma_desc(aA2), umma_desc(aW2), 0u);
+            tc_mma(tmem + 32, umma_desc(aA2 + 256), umma_desc(aW2 + 256), 1u);
+            tc_commit(&mbar);
+            ++issued;
+        }
+        if (!wait_mma(1)) {
+            abort_run = true;
+            break;
+        }
+        tc_ld32(lane_base + 32, d);
+        float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int q4 = 0; q4 < 8; ++q4) {
+            const float4 bb = *reinterpret_cast<const float4*>(&sb2[4 * q4]);
+            const float4 ww = *reinterpret_cast<const float4*>(&sw3[4 * q4]);
+            const float2 u = add2(make_float2(d[4 * q4], d[4 * q4 + 1]), make_float2(bb.x, bb.y));
+            const float2 v = add2(make_float2(d[4 * q4 + 2], d[4 * q4 + 3]), make_float2(bb.z, bb.w));
+            acc = fma2(make_float2(ww.x, ww.y), make_float2(fmaxf(u.x, 0.f), fmaxf(u.y, 0.f)), acc);
+            acc = fma2(make_float2(ww.z, ww.w), make_float2(fmaxf(v.x, 0.f), fmaxf(v.y, 0.f)), acc);
+        }
+        const float yv = (acc.x + acc.y) + b3;
+        if (sc > 0.f) p_next[c] = fmaf(sc, yv, p_next[c]);
+        tc_fence_before();
+    }
+    if (abort_run && tid == 0) {
+        record_error(err, kDevWaitTimeout);
+        // Let the MMAs still in flight finish (bounded) before TMEM is released.
+        for (int k = completed; k < issued; ++k) (void)mbar_wait(&mbar, k & 1);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(kTcCols)
+                     : "memory");
+}
+
 // ── host side ────────────────────────────────────────────────────────────────
 
 struct Mlp {
@@ -574,6 +847,7 @@ struct Mlp {
     int64_t adam_t = 0;
     int sms = 148;
     float out_scale = 1.f;  // the correction is s * out_scale * y
+    int kernel = 0;         // correction kernel: 0 = tcgen05, 1 = mma.sync
 };
 
 int cuda_err(cudaError_t e, const char* where) {
@@ -739,11 +1013,44 @@ int sb200_mlp_correct(void* h, const float* p, const float* vel2, float* p_next,
     if (grid->nx <= 8 || grid->ny <= 8 || grid->nz <= 8) return SB200_OK;
     const float dx = std::min(grid->dx, std::min(grid->dy, grid->dz));
     const int64_t items = ((grid->nx - 8 + 31) / 32) * (grid->ny - 8) * (grid->nz - 8);
-    const int blocks = grid_blocks(*m, kCorrWarps * 4, items);
-    mlp_correct_kernel<<<blocks, 32 * kCorrWarps, 0, static_cast<cudaStream_t>(stream)>>>(
-        m->prm, reinterpret_cast<const uint32_t*>(m->w1b), reinterpret_cast<const uint32_t*>(m->w2b),
-        p, vel2, p_next, grid->nx, grid->ny, grid->nz, grid->dt / dx, m->out_scale);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (m->kernel == 1) {
+        const int blocks = grid_blocks(*m, kCorrWarps * 4, items);
+        mlp_correct_kernel<<<blocks, 32 * kCorrWarps, 0, st>>>(
+            m->prm, reinterpret_cast<const uint32_t*>(m->w1b),
+            reinterpret_cast<const uint32_t*>(m->w2b), p, vel2, p_next, grid->nx, grid->ny,
+            grid->nz, grid->dt / dx, m->out_scale);
+        return cuda_err(cudaGetLastError(), "sb200_mlp_correct");
+    }
+    int* err = device_error_word();
+    if (!err) return set_error(SB200_ERR_CUDA, "sb200_mlp_correct: device error word unavailable");
+    static bool attr[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!attr[dev & 63]) {
+        if (int rc = cuda_err(cudaFuncSetAttribute(mlp_correct_tc_kernel,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   kTcSmem),
+                              "sb200_mlp_correct"))
+            return rc;
+        attr[dev & 63] = true;
+    }
+    if (items >= (int64_t(1) << 31) || grid->nx > (1 << 20) || grid->ny > (1 << 20))
+        return set_error(SB200_ERR_UNSUPPORTED, "sb200_mlp_correct: grid too large");
+    const int64_t tiles = (items + 3) / 4;
+    const int blocks = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(tiles, int64_t(m->sms) * 8)));
+    mlp_correct_tc_kernel<<<blocks, kTcThreads, kTcSmem, st>>>(
+        m->prm, m->w1b, m->w2b, p, vel2, p_next, static_cast<int>(grid->nx),
+        static_cast<int>(grid->ny), static_cast<int>(grid->nz), grid->dt / dx, m->out_scale, err);
     return cuda_err(cudaGetLastError(), "sb200_mlp_correct");
+}
+
+int sb200_mlp_set_kernel(void* h, int kernel) {
+    Mlp* m = static_cast<Mlp*>(h);
+    if (!m || kernel < 0 || kernel > 1)
+        return set_error(SB200_ERR_INVALID, "sb200_mlp_set_kernel: bad arguments");
+    m->kernel = kernel;
+    return SB200_OK;
 }
 
 int sb200_mlp_samples(const float* p, const float* vel2, const float* p_true, const float* p_plain,

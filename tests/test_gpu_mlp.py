@@ -189,3 +189,29 @@ def test_add_box_skips_the_halo(torch_cuda):
                 if 4 <= x < 20 and 4 <= y < 16 and 4 <= z < 12:
                     ref[z, y, x] += 0.5 * pv[k, j, i]
     assert np.array_equal(got, ref)
+
+
+def test_tcgen05_and_mma_correction_agree(torch_cuda):
+    """The tcgen05 (TMEM) correction and the mma.sync one: same BF16 operands, FP32
+    accumulation in a different order, so equal up to FP32 rounding and the odd
+    BF16 flip of a hidden activation."""
+    torch = torch_cuda
+    p, v2 = field_case(10, (40, 36, 72))
+    nz, ny, nx = p.shape
+    g = sb.Grid(nx, ny, nz, 10.0, 10.0, 10.0, 8e-4)
+    w, _, _ = net_and_rows(12, 1)
+    outs = {}
+    with sb.Mlp() as m:
+        m.set_params(w)
+        m.output_scale = 0.25
+        for kern in ("mma", "tcgen05", "tcgen05"):
+            out = torch.zeros(g.shape, device="cuda")
+            m.set_kernel(kern)
+            m.correct(dev(torch, p), dev(torch, v2), out, g)
+            outs.setdefault(kern, []).append(out.cpu().numpy())
+    a, b = outs["mma"][0], outs["tcgen05"][0]
+    scale = np.max(np.abs(a))
+    assert scale > 0
+    assert np.max(np.abs(a - b)) <= 2e-2 * scale
+    assert np.median(np.abs(a - b)) <= 1e-5 * scale
+    assert np.array_equal(outs["tcgen05"][0], outs["tcgen05"][1])  # deterministic
