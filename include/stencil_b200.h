@@ -366,6 +366,12 @@ int sb200_mlp_samples(const float* p, const float* vel2, const float* p_true, co
  * interior cells (pattern device FP32): a spatially extended source term. */
 int sb200_add_box(float* field, const sb200_grid* grid, int x0, int y0, int z0, int bx, int by,
                   int bz, const float* pattern, float scale, void* stream);
+/* In-place Gaussian smoothing (separable, clamp-to-edge, width sigma_cells <= 16,
+ * radius 3 sigma) of a whole halo-inclusive field; tmp is a device buffer of
+ * the same size.  Used to give a velocity model the resolution both grids of
+ * the learned path share.  Synchronous on `stream`. */
+int sb200_smooth3(float* field, float* tmp, const sb200_grid* grid, float sigma_cells,
+                  void* stream);
 /* coarse[x,y,z] = fine[2x+offset, 2y+offset, 2z+offset] on the coarse interior
  * (zero on its halo and where the fine index falls outside the fine grid). */
 int sb200_restrict2(const float* fine, const sb200_grid* fine_grid, float* coarse,

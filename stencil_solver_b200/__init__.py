@@ -189,6 +189,8 @@ _SIGNATURES = {
                                                C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "sb200_add_box": ([C.c_void_p, C.POINTER(sb200_grid)] + [C.c_int] * 6 +
                       [C.c_void_p, C.c_float, C.c_void_p], C.c_int),
+    "sb200_smooth3": ([C.c_void_p, C.c_void_p, C.POINTER(sb200_grid), C.c_float, C.c_void_p],
+                      C.c_int),
     "sb200_restrict2": ([C.c_void_p, C.POINTER(sb200_grid), C.c_void_p, C.POINTER(sb200_grid),
                          C.c_int, C.c_void_p], C.c_int),
     "sb200_pencil_variant_count": ([C.c_int], C.c_int),
@@ -695,3 +697,8 @@ def add_box(field, grid: Grid, origin, dims, pattern, scale: float, stream=None)
     """field[box] += scale * pattern, box at origin (x, y, z) of dims (bx, by, bz)."""
     _check(lib().sb200_add_box(_ptr(field), _g(grid), *origin, *dims, _ptr(pattern), scale,
                                _stream(stream)))
+
+
+def smooth3(field, tmp, grid: Grid, sigma_cells: float, stream=None) -> None:
+    """In-place separable Gaussian smoothing of a device field (tmp: same size)."""
+    _check(lib().sb200_smooth3(_ptr(field), _ptr(tmp), _g(grid), sigma_cells, _stream(stream)))

@@ -834,6 +834,29 @@ __global__ void __launch_bounds__(kTcThreads)
                      : "memory");
 }
 
+// One axis of a separable Gaussian blur (clamp-to-edge): out = sum_k w[k] in[i + k - r]
+// along `axis` (0 = x, 1 = y, 2 = z).
+constexpr int kBlurMaxR = 48;
+struct BlurWeights {
+    float w[2 * kBlurMaxR + 1];
+};
+
+__global__ void blur_axis_kernel(const float* __restrict__ in, float* __restrict__ out, int64_t nx,
+                                 int64_t ny, int64_t nz, int axis, const BlurWeights bw, int r) {
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nx * ny * nz) return;
+    const int64_t x = i % nx, y = (i / nx) % ny, z = i / (nx * ny);
+    const int64_t n = axis == 0 ? nx : (axis == 1 ? ny : nz);
+    const int64_t pos = axis == 0 ? x : (axis == 1 ? y : z);
+    const int64_t stride = axis == 0 ? 1 : (axis == 1 ? nx : nx * ny);
+    float acc = 0.f;
+    for (int k = -r; k <= r; ++k) {
+        const int64_t j = min(max(pos + k, int64_t(0)), n - 1);
+        acc = fmaf(bw.w[k + r], in[i + (j - pos) * stride], acc);
+    }
+    out[i] = acc;
+}
+
 // ── host side ────────────────────────────────────────────────────────────────
 
 struct Mlp {
@@ -1076,6 +1099,34 @@ int sb200_add_box(float* field, const sb200_grid* grid, int x0, int y0, int z0, 
     add_box_kernel<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
         field, grid->nx, grid->ny, grid->nz, x0, y0, z0, bx, by, bz, pattern, scale);
     return cuda_err(cudaGetLastError(), "sb200_add_box");
+}
+
+int sb200_smooth3(float* field, float* tmp, const sb200_grid* grid, float sigma_cells,
+                  void* stream) {
+    if (!field || !tmp || !grid || !(sigma_cells > 0.f) || sigma_cells > 16.f)
+        return set_error(SB200_ERR_INVALID, "sb200_smooth3: need 0 < sigma_cells <= 16");
+    const int r = std::max(1, std::min(kBlurMaxR, static_cast<int>(std::ceil(3.0f * sigma_cells))));
+    BlurWeights bw{};
+    double sum = 0.0;
+    const double s2 = double(sigma_cells) * sigma_cells;
+    for (int k = -r; k <= r; ++k) sum += std::exp(-0.5 * double(k) * k / s2);
+    for (int k = -r; k <= r; ++k) bw.w[k + r] = static_cast<float>(std::exp(-0.5 * double(k) * k / s2) / sum);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t n = grid->nx * grid->ny * grid->nz;
+    const unsigned blocks = static_cast<unsigned>((n + 255) / 256);
+    float* src = field;
+    float* dst = tmp;
+    int rc = SB200_OK;
+    for (int axis = 0; axis < 3 && !rc; ++axis) {
+        blur_axis_kernel<<<blocks, 256, 0, st>>>(src, dst, grid->nx, grid->ny, grid->nz, axis, bw, r);
+        rc = cuda_err(cudaGetLastError(), "sb200_smooth3");
+        std::swap(src, dst);
+    }
+    // three passes leave the result in tmp: copy it back
+    if (!rc)
+        rc = cuda_err(cudaMemcpyAsync(field, src, n * 4, cudaMemcpyDeviceToDevice, st), "sb200_smooth3");
+    if (!rc) rc = cuda_err(cudaStreamSynchronize(st), "sb200_smooth3");
+    return rc;
 }
 
 int sb200_restrict2(const float* fine, const sb200_grid* fine_grid, float* coarse,

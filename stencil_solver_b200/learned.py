@@ -21,7 +21,8 @@ dispersion error, a function of the local state.
 Velocity: the coarse grid samples the fine model.  A sharply layered model is a
 different medium on the two grids (an interface moves by up to half a coarse
 cell), so `smooth_cells` > 0 first smooths the fine model with a Gaussian of
-that width (in coarse cells): the medium both grids resolve.
+that width (in coarse cells; sb200_smooth3 on the device): the medium both
+grids resolve.
 
 Training pairs (coarse state at t, fine state at t + dt restricted): with C_m
 the restriction of the fine field after 2m fine steps, the plain coarse step
@@ -39,7 +40,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import Grid, Mlp, _check, add_box, lib, mlp_samples, restrict2, wave_step
+from . import Grid, Mlp, _check, add_box, lib, mlp_samples, restrict2, smooth3, wave_step
 
 OFFSET = -4  # coarse cell i <-> fine cell 2 i + OFFSET
 
@@ -71,12 +72,13 @@ class Problem:
     v_bottom: float = 4500.0
     perturbation: float = 0.05
     corr_cells: float = 20.0
+    vel2_window: object = None  # device fine model to use instead of generating one
 
     def __post_init__(self):
         if self.src_c is None:
             c = self.nc // 2
             self.src_c = (c, c, c)
-        self._vf = None
+        self._vf = self._vc = None
 
     @property
     def coarse(self) -> Grid:
@@ -105,58 +107,55 @@ class Problem:
         return ((s[0:2 * n:2] + 2 * s[1:2 * n + 1:2] + s[2:2 * n + 2:2]) / 4).astype(np.float32)
 
     def vel2_fine_host(self) -> np.ndarray:
-        """The fine model: seeded layered (host generator of the library) or
-        constant (a seeded speed in [v_top, v_bottom]), optionally smoothed."""
-        if self._vf is None:
-            g = self.fine
-            if self.model == "constant":
-                v = np.random.default_rng(self.seed).uniform(self.v_top, self.v_bottom)
-                v2 = np.full(g.shape, v * v, np.float32)
-            else:
-                v2 = np.empty(g.shape, np.float32)
-                vmax = C.c_float()
-                _check(lib().sb200_model_layered(v2.ctypes.data, g.nx, g.ny, g.nz, self.seed,
-                                                 self.layers, self.v_top, self.v_bottom,
-                                                 self.perturbation, self.corr_cells,
-                                                 C.byref(vmax)))
-            if self.smooth_cells > 0:
-                from scipy.ndimage import gaussian_filter
-
-                vel = gaussian_filter(np.sqrt(v2.astype(np.float64)), 2.0 * self.smooth_cells,
-                                      mode="nearest")
-                v2 = (vel * vel).astype(np.float32)
-            self._vf = v2
-        return self._vf
-
-    def vel2_coarse_host(self) -> np.ndarray:
-        """The fine model sampled at the coarse cells (as sb200_restrict2 does)."""
-        vf = self.vel2_fine_host()
-        nc = self.nc
-        vc = np.zeros((nc, nc, nc), np.float32)
-        i = np.arange(4, nc - 4)
-        vc[4:-4, 4:-4, 4:-4] = vf[np.ix_(2 * i + OFFSET, 2 * i + OFFSET, 2 * i + OFFSET)]
-        return vc
+        """The unsmoothed fine model: seeded layered (host generator of the
+        library) or constant (a seeded speed in [v_top, v_bottom])."""
+        g = self.fine
+        if self.model == "constant":
+            v = np.random.default_rng(self.seed).uniform(self.v_top, self.v_bottom)
+            return np.full(g.shape, v * v, np.float32)
+        v2 = np.empty(g.shape, np.float32)
+        vmax = C.c_float()
+        _check(lib().sb200_model_layered(v2.ctypes.data, g.nx, g.ny, g.nz, self.seed, self.layers,
+                                         self.v_top, self.v_bottom, self.perturbation,
+                                         self.corr_cells, C.byref(vmax)))
+        return v2
 
     def device_models(self):
-        """(vel2 fine, vel2 coarse) on the device; the coarse one is restricted."""
-        torch = _torch()
-        vf = torch.from_numpy(self.vel2_fine_host()).cuda()
-        vc = torch.empty(self.coarse.shape, device="cuda")
-        restrict2(vf, self.fine, vc, self.coarse, OFFSET)
-        return vf, vc
+        """(vel2 fine, vel2 coarse) on the device, built once: the fine model,
+        smoothed by smooth_cells coarse cells (sb200_smooth3), and its
+        restriction to the coarse grid."""
+        if self._vf is None:
+            torch = _torch()
+            if self.vel2_window is not None:
+                vf = self.vel2_window
+            else:
+                vf = torch.from_numpy(self.vel2_fine_host()).cuda()
+            if self.smooth_cells > 0 and self.vel2_window is None:
+                tmp = torch.empty_like(vf)
+                smooth3(vf, tmp, self.fine, 2.0 * self.smooth_cells)
+                del tmp
+            vc = torch.empty(self.coarse.shape, device="cuda")
+            restrict2(vf, self.fine, vc, self.coarse, OFFSET)
+            self._vf, self._vc = vf, vc
+        return self._vf, self._vc
+
+    def release(self) -> None:
+        """Drops the cached device models."""
+        self._vf = self._vc = None
 
     def source(self, fine: bool):
         """(origin, dims, pattern on the device, amplitude A): pattern_j = vel2_j g(x_j)
         on the box of cells within 3.5 sigma of the source point."""
         torch = _torch()
+        vf, vc = self.device_models()
         sig = self.sigma_cells  # in coarse cells
         rad_c = int(math.ceil(3.5 * sig))
         if fine:
-            v = self.vel2_fine_host()
+            v = vf
             centre = [2 * c + OFFSET for c in self.src_c]
             rad, unit = 2 * rad_c + 1, 0.5  # a fine cell is half a coarse cell
         else:
-            v = self.vel2_coarse_host()
+            v = vc
             centre = list(self.src_c)
             rad, unit = rad_c, 1.0
         origin = [c - rad for c in centre]
@@ -165,7 +164,8 @@ class Problem:
         r2 = off[None, None, :] ** 2 + off[None, :, None] ** 2 + off[:, None, None] ** 2
         gx = np.exp(-r2 / (2 * sig * sig))
         zs, ys, xs = [slice(o, o + n) for o in origin[::-1]]
-        pat = (v[zs, ys, xs] * gx).astype(np.float32)
+        box = v[zs, ys, xs].cpu().numpy().astype(np.float64)
+        pat = (box * gx).astype(np.float32)
         amp = 1.0 / (self.dt * self.dt * 3000.0 * 3000.0)  # O(1) fields
         return tuple(origin), (n, n, n), torch.from_numpy(np.ascontiguousarray(pat)).cuda(), amp
 
@@ -287,6 +287,7 @@ def make_pairs(problems, fine_steps: int, samples_per_pair: int = 4096, every: i
         fine_solve(pb, vf, fine_steps, on_even)
         counts.append(sum(x.shape[0] for x in Xs) - before)
         del vf, vc
+        pb.release()
     return Dataset(torch.cat(Xs), torch.cat(ts), counts)
 
 
@@ -347,3 +348,103 @@ def evaluate(pb: Problem, coarse_steps: int, mlp: Mlp | None):
     if mlp is not None:
         out["learned"] = rel_l2(coarse_solve(pb, vc, coarse_steps, mlp), judge)
     return out
+
+
+def proxy_of(pb: Problem, nc_proxy: int = 64) -> Problem:
+    """A small pair of grids cut from pb's (smoothed) fine model around its
+    source, with the source at its centre: the judge's test problem."""
+    torch = _torch()
+    vf, _ = pb.device_models()
+    nfp = fine_extent(nc_proxy)
+    cp = nc_proxy // 2
+    starts = []
+    for s_ax, n_f in zip(pb.src_c[::-1], pb.fine.shape):  # z, y, x
+        w0 = 2 * (s_ax - cp)  # even: coarse cells of the window line up with pb's
+        w0 = max(0, min(w0 - w0 % 2, (n_f - nfp) - (n_f - nfp) % 2))
+        starts.append(w0)
+    z0, y0, x0 = starts
+    win = vf[z0:z0 + nfp, y0:y0 + nfp, x0:x0 + nfp].contiguous()
+    src = (pb.src_c[0] - x0 // 2, pb.src_c[1] - y0 // 2, pb.src_c[2] - z0 // 2)
+    return Problem(nc_proxy, pb.h, pb.dt, pb.seed, freq=pb.freq, src_c=src,
+                   sigma_cells=pb.sigma_cells, vel2_window=win)
+
+
+@dataclass
+class SolveReport:
+    steps: int                # coarse steps asked for
+    fallback_at: object       # coarse step at which the judge tripped, or None
+    checks: list              # (coarse step, the proxy's relative L2 error)
+    ms: float                 # device time of the whole solve
+    field: object             # result on the coarse grid (restricted fine solve after a fallback)
+
+
+def learned_solve(pb: Problem, coarse_steps: int, mlp: Mlp, bound: float = 1e-3,
+                  check_every: int = 20, nc_proxy: int = 64) -> SolveReport:
+    """Corrected coarse solve with the plain fine solver as judge and fallback.
+
+    A proxy pair (proxy_of) is advanced alongside the main coarse solve: its
+    plain fine solve (2 steps per coarse step) and its corrected coarse solve.
+    Every check_every coarse steps the proxy's corrected field is compared with
+    its restricted fine field; when the relative L2 error exceeds `bound` the
+    corrected solve is abandoned and the plain fine solve computes the answer.
+    Device time (CUDA events) covers everything, fallback included."""
+    torch = _torch()
+    vf, vc = pb.device_models()
+    px = proxy_of(pb, nc_proxy)
+    pvf, pvc = px.device_models()
+    e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+    torch.cuda.synchronize()
+    e0.record()
+    g, gp, gpf = pb.coarse, px.coarse, px.fine
+    p = torch.zeros(g.shape, device="cuda")
+    q = torch.zeros(g.shape, device="cuda")
+    pp = torch.zeros(gp.shape, device="cuda")
+    pq = torch.zeros(gp.shape, device="cuda")
+    fp = torch.zeros(gpf.shape, device="cuda")
+    fq = torch.zeros(gpf.shape, device="cuda")
+    judge = torch.empty(gp.shape, device="cuda")
+    w = pb.wavelet(False, coarse_steps)
+    wp = px.wavelet(False, coarse_steps)
+    wf = px.wavelet(True, 2 * coarse_steps)
+    src, psrc, pfsrc = pb.source(False), px.source(False), px.source(True)
+    checks, fallback = [], None
+    for m in range(coarse_steps):
+        coarse_step(pb, vc, p, q, src, w, m, mlp)
+        p, q = q, p
+        coarse_step(px, pvc, pp, pq, psrc, wp, m, mlp)
+        pp, pq = pq, pp
+        for k in (2 * m, 2 * m + 1):
+            wave_step(fp, fq, pvf, fq, gpf)
+            _inject(px, True, fq, pfsrc, wf, k)
+            fp, fq = fq, fp
+        if (m + 1) % check_every == 0 or m + 1 == coarse_steps:
+            restrict2(fp, gpf, judge, gp, OFFSET)
+            err = rel_l2(pp, judge)
+            checks.append((m + 1, err))
+            if err > bound:
+                fallback = m + 1
+                break
+    if fallback is not None:
+        del p, q
+        ff = fine_solve(pb, vf, 2 * coarse_steps)
+        p = torch.empty(g.shape, device="cuda")
+        restrict2(ff, pb.fine, p, g, OFFSET)
+        del ff
+    e1.record()
+    torch.cuda.synchronize()
+    return SolveReport(coarse_steps, fallback, checks, e0.elapsed_time(e1), p)
+
+
+def time_fine_solve(pb: Problem, fine_steps: int):
+    """(device ms, restricted result) of the plain fine solve."""
+    torch = _torch()
+    vf, _ = pb.device_models()
+    e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
+    torch.cuda.synchronize()
+    e0.record()
+    f = fine_solve(pb, vf, fine_steps)
+    e1.record()
+    torch.cuda.synchronize()
+    out = torch.empty(pb.coarse.shape, device="cuda")
+    restrict2(f, pb.fine, out, pb.coarse, OFFSET)
+    return e0.elapsed_time(e1), out

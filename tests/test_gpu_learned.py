@@ -47,16 +47,49 @@ def test_geometry_and_source_agree_between_grids(torch_cuda):
     assert hits >= dc[0] - 1
 
 
-def test_learned_correction_beats_plain_coarse(torch_cuda):
-    nc, c = 80, 40
-    mk = lambda s, **kw: learned.Problem(nc, H, DT, seed=s, smooth_cells=1.5, **kw)  # noqa: E731
-    train_pbs = [mk(s, src_c=(c - 4 + s % 8, c - 2 + s % 5, c - 3 + s % 7)) for s in range(1, 11)]
-    ds = learned.make_pairs(train_pbs, fine_steps=320, samples_per_pair=4096, every=4)
+NC80, C80 = 80, 40
+
+
+def mk80(s, **kw):
+    return learned.Problem(NC80, H, DT, seed=s, smooth_cells=1.5, **kw)
+
+
+@pytest.fixture(scope="module")
+def trained(torch_cuda):
+    """A network trained on 10 smoothed layered models (80^3 coarse / 152^3 fine)."""
+    pbs = [mk80(s, src_c=(C80 - 4 + s % 8, C80 - 2 + s % 5, C80 - 3 + s % 7)) for s in range(1, 11)]
+    ds = learned.make_pairs(pbs, fine_steps=320, samples_per_pair=4096, every=4)
     assert ds.n > 500_000
-    with sb.Mlp(seed=3) as mlp:
-        hist = learned.train(ds, mlp, epochs=10, batch=8192, lr=2e-3)
-        assert hist[-1] < 0.2 * hist[0]
-        errs = {k: learned.evaluate(mk(99), k, mlp) for k in (40, 120)}
+    mlp = sb.Mlp(seed=3)
+    hist = learned.train(ds, mlp, epochs=10, batch=8192, lr=2e-3)
+    del ds
+    yield mlp, hist
+    mlp.close()
+
+
+def test_learned_correction_beats_plain_coarse(trained):
+    mlp, hist = trained
+    assert hist[-1] < 0.2 * hist[0]
+    errs = {k: learned.evaluate(mk80(99), k, mlp) for k in (40, 120)}
     print("ablation", errs, "loss", hist[0], hist[-1])
     for k, e in errs.items():
         assert e["learned"] < 0.8 * e["plain"], (k, e)
+
+
+def test_judged_solve_without_fallback_is_the_corrected_solve(trained):
+    mlp, _ = trained
+    pb = mk80(77)
+    rep = learned.learned_solve(pb, 60, mlp, bound=1.0, check_every=20)
+    assert rep.fallback_at is None and [c[0] for c in rep.checks] == [20, 40, 60]
+    _, vc = pb.device_models()
+    ref = learned.coarse_solve(pb, vc, 60, mlp)
+    assert bool((rep.field == ref).all())
+
+
+def test_judged_solve_falls_back_to_the_fine_solve(trained):
+    mlp, _ = trained
+    pb = mk80(78)
+    rep = learned.learned_solve(pb, 40, mlp, bound=1e-12, check_every=10)
+    assert rep.fallback_at == 10 and len(rep.checks) == 1 and rep.checks[0][1] > 1e-12
+    _, ref = learned.time_fine_solve(pb, 80)
+    assert bool((rep.field == ref).all())
