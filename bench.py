@@ -53,6 +53,8 @@ def args_():
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (heuristic tile)")
     ap.add_argument("--variant", type=int, default=-1, help="force a pencil variant (profiling)")
     ap.add_argument("--zchunks", type=int, default=1)
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the heat / FP16 / batch / learned measurements")
     return ap.parse_args()
 
 
@@ -231,6 +233,236 @@ def profiled_traffic_per_point():
     return float(m.group(1)) if m else None
 
 
+# ── secondary measurements (rank 0, one GPU): the other configurations ─────────
+
+def _events():
+    import torch
+
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def secondary_heat(n: int = 512, steps: int = 40):
+    """Heat 512^3, alpha dt / dx^2 = 0.05, seeded U[0,1) interior, zero walls:
+    sb200_heat_step_f32 (8 B / interior point), tuned."""
+    import torch
+
+    import stencil_solver_b200 as sb
+
+    g = sb.Grid(n, n, n, 10.0, 10.0, 10.0, 1.0)
+    alpha = 0.05 * 100.0  # alpha dt / dx^2 = 0.05
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(SEED)
+    u = torch.zeros(g.shape, device="cuda")
+    u[4:-4, 4:-4, 4:-4] = torch.rand((n - 8,) * 3, generator=gen, device="cuda")
+    un = u.clone()
+    sb.tune(sb.KIND_HEAT_F32, g, u, u, u, un, reps=3)
+    for _ in range(3):
+        sb.heat_step(u, un, g, alpha)
+        u, un = un, u
+    e0, e1 = _events()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        sb.heat_step(u, un, g, alpha)
+        u, un = un, u
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    peak, _ = measured_peak()
+    gbs = 8 * g.interior / (ms * 1e-3) / 1e9
+    ch = sb.pencil_choice(sb.KIND_HEAT_F32, g)
+    return {"workload": f"heat_fp32_{n}^3", "ms_per_step": ms,
+            "gpts_per_s": g.interior / (ms * 1e-3) / 1e9, "achieved_gbs": gbs,
+            "frac_of_measured_hbm": gbs / peak, "bytes_per_point": 8,
+            "tile": sb.variant_names(sb.KIND_HEAT_F32)[ch[0]], "zchunks": ch[1]}
+
+
+def secondary_fp16(n: int, fp32_ms: float, steps: int = 30):
+    """FP16-storage acoustic (p / p_prev FP16 with a power-of-two scale, K in
+    BF16, FP32 arithmetic) at n^3, tuned; and its accuracy against the FP32 path
+    on a 256^3 instance of the layered model over 500 steps (FP32 itself is
+    within 1e-5 of the FP64 oracle there: tests/test_gpu_parity.py)."""
+    import torch
+
+    import stencil_solver_b200 as sb
+
+    g, vel2, vmax, src = workload(n)
+    v = torch.from_numpy(vel2).cuda()
+    K = torch.empty(g.shape, dtype=torch.int16, device="cuda")
+    sb.k_field_bf16(v, K, g)
+    del v
+    P = torch.zeros(g.shape, dtype=torch.int16, device="cuda")
+    Q = torch.zeros_like(P)
+    scale = torch.tensor([1024.0, 1.0], device="cuda")
+    sb.tune(sb.KIND_WAVE_F16, g, P, Q, K, Q.clone(), reps=3)
+    for _ in range(3):
+        sb.wave_step_f16(P, Q, K, g, scale, 0)
+        P, Q = Q, P
+    e0, e1 = _events()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        sb.wave_step_f16(P, Q, K, g, scale, 0)
+        P, Q = Q, P
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    del P, Q, K
+    torch.cuda.empty_cache()
+    peak, _ = measured_peak()
+    gbs = 8 * g.interior / (ms * 1e-3) / 1e9
+    ch = sb.pencil_choice(sb.KIND_WAVE_F16, g)
+    out = {"workload": f"acoustic_fp16_storage_{n}^3_layered", "ms_per_step": ms,
+           "gpts_per_s": g.interior / (ms * 1e-3) / 1e9, "speedup_vs_fp32": fp32_ms / ms,
+           "achieved_gbs": gbs, "frac_of_measured_hbm": gbs / peak, "bytes_per_point": 8,
+           "tile": sb.variant_names(sb.KIND_WAVE_F16)[ch[0]], "zchunks": ch[1]}
+    # accuracy: 256^3 instance, 500 steps, source at the centre
+    m = 256
+    vel2s, vmaxs = sb.model_layered(m, m, m, SEED)
+    dts = float(np.float32(0.4 * DX / vmaxs))
+    gs = sb.Grid(m, m, m, DX, DX, DX, dts)
+    srcs = gs.index(m // 2, m // 2, m // 2)
+    z = np.zeros(gs.shape, np.float32)
+    res = {}
+    for prec in (sb.PRECISION_F32, sb.PRECISION_F16):
+        with sb.Run(gs, precision=prec, src_index=srcs, src_freq=FREQ) as r:
+            r.set_fields(z, z, vel2s)
+            r.steps(500)
+            res[prec] = (r.field().astype(np.float64), r.trace(500).astype(np.float64))
+    (p32, t32), (p16, t16) = res[sb.PRECISION_F32], res[sb.PRECISION_F16]
+    out["accuracy_256^3_500_steps"] = {
+        "field_rel_l2_vs_fp32": float(np.linalg.norm(p16 - p32) / np.linalg.norm(p32)),
+        "trace_rel_l2_vs_fp32": float(np.linalg.norm(t16 - t32) / np.linalg.norm(t32)),
+        "renorm_every": 50}
+    return out
+
+
+def secondary_batch(n_shots: int = 48, steps: int = 400):
+    """48 independent acoustic shots, extents U{96..320 step 8} per axis, each its
+    own seeded layered model, a Ricker (U[10, 25] Hz) at a random interior cell,
+    400 steps in 100-step CUDA-graph chunks, tuned: one persistent launch per
+    step, against the same shots as separate runs (one graph chain each)."""
+    import torch
+
+    import stencil_solver_b200 as sb
+
+    rng = np.random.default_rng(SEED)
+    shots, fields = [], []
+    for s in range(n_shots):
+        nx, ny, nz = (int(rng.choice(np.arange(96, 321, 8))) for _ in range(3))
+        vel2, vmax = sb.model_layered(nx, ny, nz, SEED + 100 + s)
+        dt = float(np.float32(0.4 * DX / vmax))
+        g = sb.Grid(nx, ny, nz, DX, DX, DX, dt)
+        src = g.index(int(rng.integers(4, nx - 4)), int(rng.integers(4, ny - 4)),
+                      int(rng.integers(4, nz - 4)))
+        f = float(rng.uniform(10.0, 25.0))
+        shots.append((g, src))
+        fields.append((vel2, sb.ricker(f, 1.0 / f, dt, steps)))
+    pts = sum(g.interior for g, _ in shots)
+    out = {"workload": f"batch_{n_shots}_shots_fp32", "shots": n_shots, "steps": steps,
+           "interior_points": pts}
+    with sb.Batch(shots, max_steps=steps, graph_chunk=100) as b:
+        b.tune(reps=3)
+        for i, ((g, _), (vel2, w)) in enumerate(zip(shots, fields)):
+            z = np.zeros(g.shape, np.float32)
+            b.set_fields(i, z, z, vel2)
+            b.set_wavelet(i, w)
+        st = torch.cuda.ExternalStream(b.stream)
+        e0, e1 = _events()
+        torch.cuda.synchronize()
+        e0.record(st)
+        b.steps(steps)
+        e1.record(st)
+        b.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        out["batched"] = {"ms_per_step": ms, "gpts_per_s": pts / (ms * 1e-3) / 1e9,
+                          "achieved_gbs": 16 * pts / (ms * 1e-3) / 1e9, **b.choice()}
+    runs = []
+    for (g, src), (vel2, w) in zip(shots, fields):
+        r = sb.Run(g, src_index=src, graph_chunk=100)
+        z = np.zeros(g.shape, np.float32)
+        r.set_fields(z, z, vel2)
+        r.set_wavelet(w)
+        runs.append(r)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for r in runs:
+        r.steps(steps)
+    for r in runs:
+        r.synchronize()
+    wall = (time.perf_counter() - t0) * 1e3 / steps
+    for r in runs:
+        r.close()
+    out["separate_runs"] = {"ms_per_step_wall": wall, "gpts_per_s": pts / (wall * 1e-3) / 1e9}
+    out["speedup_batched_vs_separate"] = wall / ms
+    return out
+
+
+def secondary_learned(train_models: int = 16, nc_eval: int = 516, coarse_steps: int = 200):
+    """Learned 2x-coarse stepping: the network is trained (hand-written forward /
+    backward / Adam kernels) on pairs from the plain fine solver over
+    train_models seeded 256^3 fine / 132^3 coarse models (600 fine steps each),
+    then evaluated on an unseen model: 1024^3 fine (dx 5 m) vs 516^3 coarse
+    (dx 10 m, 2x dt), 25 Hz Ricker, Gaussian-smoothed layered velocity.  Errors are
+    relative L2 against the restricted plain fine solve (FP32; the judge)."""
+    import torch
+
+    import stencil_solver_b200 as sb
+    from stencil_solver_b200 import learned
+
+    h, dt = 10.0, 0.4 * 10.0 / 4700.0
+    nct = 132
+    rng = np.random.default_rng(SEED)
+    c = nct // 2
+    pbs = [learned.Problem(nct, h, dt, seed=SEED + 1000 + k, smooth_cells=1.5,
+                           src_c=tuple(int(v) for v in rng.integers(c - 20, c + 20, 3)))
+           for k in range(train_models)]
+    t0 = time.perf_counter()
+    ds = learned.make_pairs(pbs, fine_steps=600, samples_per_pair=4096, every=6)
+    mlp = sb.Mlp(seed=3)
+    hist = learned.train(ds, mlp, epochs=8, batch=16384, lr=2e-3)
+    t_train = time.perf_counter() - t0
+    rows = ds.n
+    del ds
+    pb = learned.Problem(nc_eval, h, dt, seed=SEED + 99999, smooth_cells=1.5)
+    pb.device_models()
+    ms_fine, judge = learned.time_fine_solve(pb, 2 * coarse_steps)
+    _, vc = pb.device_models()
+    e0, e1 = _events()
+    torch.cuda.synchronize()
+    e0.record()
+    pc = learned.coarse_solve(pb, vc, coarse_steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_plain = e0.elapsed_time(e1)
+    err_plain = learned.rel_l2(pc, judge)
+    del pc
+    e0.record()
+    lc = learned.coarse_solve(pb, vc, coarse_steps, mlp)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_learned = e0.elapsed_time(e1)
+    err_learned = learned.rel_l2(lc, judge)
+    del lc
+    rep = learned.learned_solve(pb, coarse_steps, mlp, bound=1e-3, check_every=25)
+    err_judged = learned.rel_l2(rep.field, judge)
+    mlp.close()
+    pb.release()
+    torch.cuda.empty_cache()
+    return {
+        "workload": f"learned_2x_coarse_fine{learned.fine_extent(nc_eval)}^3_coarse{nc_eval}^3",
+        "coarse_steps": coarse_steps, "train_models": train_models, "train_rows": rows,
+        "train_seconds": t_train, "train_loss_first_last": [hist[0], hist[-1]],
+        "fine_ms": ms_fine, "plain_coarse_ms": ms_plain, "learned_coarse_ms": ms_learned,
+        "rel_l2_plain_coarse": err_plain, "rel_l2_learned_coarse": err_learned,
+        "time_to_solution_speedup_learned_vs_fine": ms_fine / ms_learned,
+        "judged": {"bound": 1e-3, "ms": rep.ms, "fallback_at_step": rep.fallback_at,
+                   "proxy_checks": rep.checks, "rel_l2": err_judged,
+                   "speedup_vs_fine": ms_fine / rep.ms},
+        "judge": "restricted plain FP32 fine solve",
+    }
+
+
 # ── our arm ───────────────────────────────────────────────────────────────────
 
 def run_ours(a):
@@ -363,6 +595,20 @@ def run_ours(a):
         cv, cores, sample, kind, *_ = cpu_reference_sample(n, 1, 2, a.cpu_seconds)
         cpu = {"value": cv, "unit": "Gpts/s", "cores": cores, "kind": kind, "sample": sample}
 
+    secondary = None
+    if rank == 0 and world == 1 and not a.no_secondary:
+        secondary = {}
+        for name, fn in (("heat", lambda: secondary_heat()),
+                         ("fp16_storage", lambda: secondary_fp16(n, ms_step)),
+                         ("batch", lambda: secondary_batch()),
+                         ("learned", lambda: secondary_learned())):
+            try:
+                secondary[name] = fn()
+            except Exception as exc:  # noqa: BLE001 -- report, keep the main line
+                secondary[name] = {"error": f"{type(exc).__name__}: {exc}"}
+            torch.cuda.empty_cache()
+        assert sb.device_error() == 0, "device error word set during a secondary measurement"
+
     choice = sb.pencil_choice(sb.KIND_WAVE_F32, g)
     vname = sb.variant_names()[choice[0]]
     line = {
@@ -376,6 +622,7 @@ def run_ours(a):
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
         "gpu_launches": a.steps,
         "host_issue_ms_per_step": host_issue_ms,
+        "secondary": secondary,
     }
     if pg:
         pg.barrier()
