@@ -55,6 +55,8 @@ def args_():
     ap.add_argument("--zchunks", type=int, default=1)
     ap.add_argument("--no-secondary", action="store_true",
                     help="skip the heat / FP16 / batch / learned measurements")
+    ap.add_argument("--kernel", choices=["acoustic", "heat", "fp16", "batch", "mlp"],
+                    help="run only a small case of one kernel (for profilers) and print its time")
     return ap.parse_args()
 
 
@@ -631,8 +633,77 @@ def run_ours(a):
         print(json.dumps(line), flush=True)
 
 
+def run_kernel_probe(a):
+    """A few launches of one kernel on an n^3 case (a.n), for ncu captures:
+    warm-up launches, then a.steps timed launches; prints one JSON line."""
+    import torch
+
+    import stencil_solver_b200 as sb
+
+    n = a.n
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(SEED)
+    e0, e1 = _events()
+    if a.kernel in ("acoustic", "fp16", "heat", "mlp"):
+        g, vel2, vmax, src = workload(n)
+        v = torch.from_numpy(vel2).cuda()
+        p = torch.randn(g.shape, generator=gen, device="cuda") * 0.1
+    if a.kernel == "acoustic":
+        q = p * 0.99
+        sb.set_pencil_override(sb.KIND_WAVE_F32, max(a.variant, 0), a.zchunks)
+        f = lambda: sb.wave_step(p, q, v, q, g)  # noqa: E731
+    elif a.kernel == "heat":
+        un = torch.empty_like(p)
+        sb.set_pencil_override(sb.KIND_HEAT_F32, max(a.variant, 0), a.zchunks)
+        f = lambda: sb.heat_step(p, un, g, 5.0)  # noqa: E731
+    elif a.kernel == "fp16":
+        P = torch.empty(g.shape, dtype=torch.int16, device="cuda")
+        Q = torch.empty_like(P)
+        K = torch.empty_like(P)
+        sb.f16_pack(p, P, g.size, 1024.0)
+        sb.f16_pack(p * 0.99, Q, g.size, 1024.0)
+        sb.k_field_bf16(v, K, g)
+        scale = torch.tensor([1024.0, 1.0], device="cuda")
+        sb.set_pencil_override(sb.KIND_WAVE_F16, max(a.variant, 0), a.zchunks)
+        f = lambda: sb.wave_step_f16(P, Q, K, g, scale, 0)  # noqa: E731
+    elif a.kernel == "mlp":
+        m = sb.Mlp(seed=1)
+        m.output_scale = 1e-5
+        out = torch.zeros_like(p)
+        f = lambda: m.correct(p, v, out, g)  # noqa: E731
+    else:  # batch: 12 shots with extents n/2..n in steps of 8
+        rng = np.random.default_rng(SEED)
+        shots = []
+        for _ in range(12):
+            ext = [int(rng.choice(np.arange(max(24, n // 2), n + 1, 8))) for _ in range(3)]
+            gb = sb.Grid(*ext, DX, DX, DX, 8.5e-4)
+            shots.append((gb, gb.index(ext[0] // 2, ext[1] // 2, ext[2] // 2)))
+        b = sb.Batch(shots, max_steps=a.warmup + a.steps + 2, graph_chunk=0)
+        b.set_choice(max(a.variant, 0), 64)
+        for i, (gb, _) in enumerate(shots):
+            z = np.zeros(gb.shape, np.float32)
+            b.set_fields(i, z, z, np.full(gb.shape, 9e6, np.float32))
+        st = torch.cuda.ExternalStream(b.stream)
+        f = lambda: b.steps(1)  # noqa: E731
+    for _ in range(a.warmup):
+        f()
+    torch.cuda.synchronize()
+    stream = st if a.kernel == "batch" else torch.cuda.current_stream()
+    e0.record(stream)
+    for _ in range(a.steps):
+        f()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    assert sb.device_error() == 0
+    print(json.dumps({"kernel": a.kernel, "n": n, "ms_per_launch": e0.elapsed_time(e1) / a.steps}),
+          flush=True)
+
+
 def main():
     a = args_()
+    if a.kernel:
+        run_kernel_probe(a)
+        return
     if a.impl == "reference":
         run_reference(a)
     else:
