@@ -105,7 +105,11 @@ __device__ __forceinline__ uint4 lds128h(const uint16_t* p) {
     return *reinterpret_cast<const uint4*>(p);
 }
 
-template <int TX, int TY, int RPT, int S, int AUX, int PHASE>
+// UNR = 9: the plane loop is unrolled by 9 so the z queue's slots are
+// compile-time registers that never move.  UNR = 1: one plane per iteration and
+// the queue shifts by one slot after each plane (36 register moves per row of
+// a thread) -- a ninth of the code, for kernels that stall on instruction fetch.
+template <int TX, int TY, int RPT, int S, int AUX, int PHASE, int UNR>
 __global__ void __launch_bounds__(ShapeH<TX, TY, RPT, S, AUX>::NT, ShapeH<TX, TY, RPT, S, AUX>::MINB)
     pencil_f16_kernel(const __grid_constant__ CUtensorMap pmap,
                       const __grid_constant__ CUtensorMap qmap,
@@ -213,9 +217,10 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, RPT, S, AUX>::NT, ShapeH<TX, TY
         }
     }
 
-    for (int i0 = 0; i0 < nint && !abort_run; i0 += 9) {
+    static_assert(UNR == 1 || UNR == 9, "the z queue is unrolled by 9 or rolled");
+    for (int i0 = 0; i0 < nint && !abort_run; i0 += UNR) {
 #pragma unroll
-        for (int u = 0; u < 9; ++u) {
+        for (int u = 0; u < UNR; ++u) {
             const int i = i0 + u;
             if (i < nint && !abort_run) {
                 const int cs = (u + 4) % 9;
@@ -338,6 +343,12 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, RPT, S, AUX>::NT, ShapeH<TX, TY
                     }
                     if (i + AUX < nint) issue_aux(i + AUX);
                 }
+                if (UNR == 1) {  // slot k holds plane i + 1 + k for the next plane
+#pragma unroll
+                    for (int k = 0; k < 8; ++k)
+#pragma unroll
+                        for (int j = 0; j < RPT; ++j) q[k][j] = q[k + 1][j];
+                }
             }
         }
     }
@@ -354,21 +365,21 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, RPT, S, AUX>::NT, ShapeH<TX, TY
 using LaunchFnH = cudaError_t (*)(const PencilMaps&, const F16Args&, unsigned, int, cudaStream_t);
 using ResidentFnH = int (*)();
 
-template <int TX, int TY, int RPT, int S, int AUX>
+template <int TX, int TY, int RPT, int S, int AUX, int UNR>
 int resident_f16() {
     using P = ShapeH<TX, TY, RPT, S, AUX>;
     static int cached[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (cached[dev & 63] > 0) return cached[dev & 63];
-    auto kern = pencil_f16_kernel<TX, TY, RPT, S, AUX, 0>;
+    auto kern = pencil_f16_kernel<TX, TY, RPT, S, AUX, 0, UNR>;
     const int smem = static_cast<int>(P::SMEM);
     int n = 0;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) ==
             cudaSuccess &&
-        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, RPT, S, AUX, 1>,
+        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, RPT, S, AUX, 1, UNR>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
-        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, RPT, S, AUX, 2>,
+        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, RPT, S, AUX, 2, UNR>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, P::NT, P::SMEM) == cudaSuccess &&
         n > 0) {
@@ -379,19 +390,19 @@ int resident_f16() {
     return std::max(1, std::min(int((228u * 1024u) / (P::SMEM + 1024u)), 65536 / (P::NT * 128)));
 }
 
-template <int TX, int TY, int RPT, int S, int AUX>
+template <int TX, int TY, int RPT, int S, int AUX, int UNR>
 cudaError_t launch_f16(const PencilMaps& m, const F16Args& a, unsigned ctas, int phase,
                        cudaStream_t stream) {
     using P = ShapeH<TX, TY, RPT, S, AUX>;
-    resident_f16<TX, TY, RPT, S, AUX>();  // sets the attributes once per device
+    resident_f16<TX, TY, RPT, S, AUX, UNR>();  // sets the attributes once per device
     if (phase == 1)
-        pencil_f16_kernel<TX, TY, RPT, S, AUX, 1><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
+        pencil_f16_kernel<TX, TY, RPT, S, AUX, 1, UNR><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
                                                                                    m.vel2, a);
     else if (phase == 2)
-        pencil_f16_kernel<TX, TY, RPT, S, AUX, 2><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
+        pencil_f16_kernel<TX, TY, RPT, S, AUX, 2, UNR><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
                                                                                    m.vel2, a);
     else
-        pencil_f16_kernel<TX, TY, RPT, S, AUX, 0><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
+        pencil_f16_kernel<TX, TY, RPT, S, AUX, 0, UNR><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
                                                                                    m.vel2, a);
     return cudaGetLastError();
 }
@@ -403,14 +414,22 @@ struct VariantH {
     ResidentFnH resident;
 };
 
-#define SB200_VARIANT_H(TX, TY, RPT, S, AUX, NAME) \
-    VariantH { TX, TY, RPT, S, AUX, NAME, &launch_f16<TX, TY, RPT, S, AUX>, &resident_f16<TX, TY, RPT, S, AUX> }
+#define SB200_VARIANT_H(TX, TY, RPT, S, AUX, UNR, NAME)                                   \
+    VariantH {                                                                              \
+        TX, TY, RPT, S, AUX, NAME, &launch_f16<TX, TY, RPT, S, AUX, UNR>,                   \
+            &resident_f16<TX, TY, RPT, S, AUX, UNR>                                          \
+    }
 
+// "_roll": the z queue shifts one slot per plane instead of the 9x unroll.
 const VariantH kF16[] = {
-    SB200_VARIANT_H(64, 16, 1, 8, 4, "h64x16_r1_s8_a4"),
-    SB200_VARIANT_H(64, 32, 2, 8, 3, "h64x32_r2_s8_a3"),
-    SB200_VARIANT_H(128, 16, 2, 8, 3, "h128x16_r2_s8_a3"),
-    SB200_VARIANT_H(64, 32, 1, 8, 3, "h64x32_r1_s8_a3"),
+    SB200_VARIANT_H(64, 16, 1, 8, 4, 9, "h64x16_r1_s8_a4"),
+    SB200_VARIANT_H(64, 32, 2, 8, 3, 9, "h64x32_r2_s8_a3"),
+    SB200_VARIANT_H(128, 16, 2, 8, 3, 9, "h128x16_r2_s8_a3"),
+    SB200_VARIANT_H(64, 32, 1, 8, 3, 9, "h64x32_r1_s8_a3"),
+    SB200_VARIANT_H(64, 16, 1, 8, 4, 1, "h64x16_r1_s8_a4_roll"),
+    SB200_VARIANT_H(64, 32, 2, 8, 3, 1, "h64x32_r2_s8_a3_roll"),
+    SB200_VARIANT_H(128, 16, 2, 8, 3, 1, "h128x16_r2_s8_a3_roll"),
+    SB200_VARIANT_H(64, 32, 1, 8, 3, 1, "h64x32_r1_s8_a3_roll"),
 };
 constexpr int kNumF16 = sizeof(kF16) / sizeof(kF16[0]);
 

@@ -99,7 +99,7 @@ def compare_f16(got, ref, mag):
 
 
 @pytest.mark.parametrize("phase,r", [(0, 1.0), (1, 0.5), (2, 0.5), (1, 4.0)])
-@pytest.mark.parametrize("variant", range(4))
+@pytest.mark.parametrize("variant", range(8))
 def test_f16_step_matches_oracle(torch_cuda, phase, r, variant):
     if variant >= sb.lib().sb200_pencil_variant_count(sb.KIND_WAVE_F16):
         pytest.skip("variant not compiled")
