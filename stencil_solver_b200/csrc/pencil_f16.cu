@@ -64,23 +64,6 @@ struct ShapeH {
     static constexpr int MINB = (512 / NT) > 0 ? (512 / NT) : 1;
 };
 
-__device__ __forceinline__ float h2f(uint32_t word, int hi) {
-    const unsigned short h = hi ? static_cast<unsigned short>(word >> 16)
-                                : static_cast<unsigned short>(word & 0xffffu);
-    float f;
-    asm("cvt.f32.f16 %0, %1;" : "=f"(f) : "h"(h));
-    return f;
-}
-
-// f32(a_half) + b, one instruction on sm_100.
-__device__ __forceinline__ float add_hf(uint32_t word, int hi, float b) {
-    const unsigned short h = hi ? static_cast<unsigned short>(word >> 16)
-                                : static_cast<unsigned short>(word & 0xffffu);
-    float d;
-    asm("add.rn.f32.f16 %0, %1, %2;" : "=f"(d) : "h"(h), "f"(b));
-    return d;
-}
-
 __device__ __forceinline__ float bf2f(uint32_t word, int hi) {
     return __uint_as_float(hi ? (word & 0xffff0000u) : (word << 16));
 }
@@ -89,13 +72,56 @@ __device__ __forceinline__ uint32_t get_word(const uint4& v, int k) {
     return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
 }
 
-// Element e (0..7) of a chunk of 8 halves.
-__device__ __forceinline__ float chunk_f(const uint4& v, int e) { return h2f(get_word(v, e >> 1), e & 1); }
-
 __device__ __forceinline__ uint32_t pack_h2(float lo, float hi) {
     uint32_t r;
     asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
     return r;
+}
+
+// Both halves of a word as FP32 (exact), taken apart with a register-pair move.
+__device__ __forceinline__ float2 h2f2(uint32_t w) {
+    float a, b;
+    asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\t"
+        "cvt.f32.f16 %0, lo;\n\tcvt.f32.f16 %1, hi;\n\t}"
+        : "=f"(a), "=f"(b)
+        : "r"(w));
+    return make_float2(a, b);
+}
+
+// f32(half) + b for both halves of a word (the sm_100 mixed-precision add).
+__device__ __forceinline__ float2 addhf2(uint32_t w, float2 b) {
+    float x, y;
+    asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\t"
+        "add.rn.f32.f16 %0, lo, %3;\n\tadd.rn.f32.f16 %1, hi, %4;\n\t}"
+        : "=f"(x), "=f"(y)
+        : "r"(w), "f"(b.x), "f"(b.y));
+    return make_float2(x, y);
+}
+
+// Packed FP32 pairs (sm_100 f32x2): each lane rounds as the scalar op would.
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mov.b64 rc, {%6, %7};\n\tfma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return d;
+}
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
 }
 
 __device__ __forceinline__ uint2 lds64(const uint16_t* p) {
@@ -194,6 +220,16 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, RPT, S, AUX>::NT, ShapeH<TX, TY
     float m_out = 1.f, m_q = 1.f;
     if (PHASE == 1) m_out = a.scale->r;
     if (PHASE == 2) m_q = a.scale->r;
+    float2 ax2[R], ay2[R], az2[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        ax2[r] = make_float2(ax[r], ax[r]);
+        ay2[r] = make_float2(ay[r], ay[r]);
+        az2[r] = make_float2(az[r], az[r]);
+    }
+    const float2 cx2 = make_float2(a.w.cx, a.w.cx), cy2 = make_float2(a.w.cy, a.w.cy),
+                 cz2 = make_float2(a.w.cz, a.w.cz);
+    const float2 nmq2 = make_float2(-m_q, -m_q), mout2 = make_float2(m_out, m_out);
 
     uint4 q[9][RPT];
     bool bad = false;
@@ -233,49 +269,64 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, RPT, S, AUX>::NT, ShapeH<TX, TY
                 }
                 const uint16_t* pc = sm + ((i + 4) % S) * P::PLANE + soff;
 
-                // y sums, farthest rows first, from zero.
-                float ya[RPT][8];
+                // Pairs of points (halves 2h, 2h+1 of a 16-byte chunk) as packed
+                // FP32.  y: row pairs j+d, j-d through the mixed FP16 + FP32 add;
+                // farthest pair first, from zero.
+                float2 ya[RPT][4];
 #pragma unroll
                 for (int j = 0; j < RPT; ++j)
 #pragma unroll
-                    for (int e = 0; e < 8; ++e) ya[j][e] = 0.f;
+                    for (int h = 0; h < 4; ++h) ya[j][h] = make_float2(0.f, 0.f);
 #pragma unroll
-                for (int k = -R; k < RPT + R; ++k) {
-                    const uint4 row = (k >= 0 && k < RPT) ? q[cs][k] : lds128h(pc + k * P::SX);
+                for (int d = R; d >= 1; --d) {
 #pragma unroll
-                    for (int e = 0; e < 8; ++e) {
-                        const float v = chunk_f(row, e);
+                    for (int j = 0; j < RPT; ++j) {
+                        const int ku = j + d, kd = j - d;
+                        const uint4 up = (ku < RPT) ? q[cs][ku] : lds128h(pc + ku * P::SX);
+                        const uint4 dn = (kd >= 0) ? q[cs][kd] : lds128h(pc + kd * P::SX);
 #pragma unroll
-                        for (int j = 0; j < RPT; ++j) {
-                            const int d = k > j ? k - j : j - k;
-                            if (d >= 1 && d <= R) ya[j][e] = fmaf(ay[d - 1], v, ya[j][e]);
-                        }
+                        for (int h = 0; h < 4; ++h)
+                            ya[j][h] = fma2(ay2[d - 1], addhf2(get_word(up, h), h2f2(get_word(dn, h))),
+                                            ya[j][h]);
                     }
                 }
                 // x window halves: [4 left | 8 own | 4 right] per row; z from the queue.
-                float lap[RPT][8];
+                float2 lap[RPT][4];
 #pragma unroll
                 for (int j = 0; j < RPT; ++j) {
                     const uint2 lf = lds64(pc + j * P::SX - 4);
                     const uint2 rt = lds64(pc + j * P::SX + 8);
                     const uint4 own = q[cs][j];
                     const uint32_t win[8] = {lf.x, lf.y, own.x, own.y, own.z, own.w, rt.x, rt.y};
+                    float2 xv[8];  // the window's 16 halves as 8 pairs
 #pragma unroll
-                    for (int e = 0; e < 8; ++e) {
-                        const float ce = chunk_f(own, e);
-                        float tz = a.w.cz * ce;
-                        float tx = a.w.cx * ce;
+                    for (int w = 0; w < 8; ++w) xv[w] = h2f2(win[w]);
+#pragma unroll
+                    for (int h = 0; h < 4; ++h) {
+                        const float2 c = xv[2 + h];
+                        float2 tz = mul2(cz2, c);
+                        float2 tx = mul2(cx2, c);
 #pragma unroll
                         for (int r = 1; r <= R; ++r) {
-                            const float dn = chunk_f(q[(u + 4 - r + 9) % 9][j], e);
                             const uint4& upv = q[(u + 4 + r) % 9][j];
-                            tz = fmaf(az[r - 1], add_hf(get_word(upv, e >> 1), e & 1, dn), tz);
-                            const int il = 4 + e - r, ir = 4 + e + r;  // window indices
-                            const float xl = h2f(win[il >> 1], il & 1);
-                            tx = fmaf(ax[r - 1], add_hf(win[ir >> 1], ir & 1, xl), tx);
+                            const uint4& dnv = q[(u + 4 - r + 9) % 9][j];
+                            tz = fma2(az2[r - 1], addhf2(get_word(upv, h), h2f2(get_word(dnv, h))), tz);
+                            // window halves 4 + 2h +- r and 5 + 2h +- r
+                            float2 s;
+                            if (r % 2 == 0) {
+                                s = add2(xv[2 + h + r / 2], xv[2 + h - r / 2]);
+                            } else {
+                                const int a0 = 4 + 2 * h + r, b0 = 4 + 2 * h - r;
+                                const float ra = (a0 & 1) ? xv[a0 >> 1].y : xv[a0 >> 1].x;
+                                const float rb = ((a0 + 1) & 1) ? xv[(a0 + 1) >> 1].y : xv[(a0 + 1) >> 1].x;
+                                const float la = (b0 & 1) ? xv[b0 >> 1].y : xv[b0 >> 1].x;
+                                const float lb = ((b0 + 1) & 1) ? xv[(b0 + 1) >> 1].y : xv[(b0 + 1) >> 1].x;
+                                s = make_float2(ra + la, rb + lb);
+                            }
+                            tx = fma2(ax2[r - 1], s, tx);
                         }
-                        const float ty = fmaf(a.w.cy, ce, ya[j][e]);
-                        lap[j][e] = (tx + ty) + tz;
+                        const float2 ty = fma2(cy2, c, ya[j][h]);
+                        lap[j][h] = add2(add2(tx, ty), tz);
                     }
                 }
                 if (!mbar_wait(&auxf[i % AUX], (i / AUX) & 1)) bad = true;
@@ -288,15 +339,17 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, RPT, S, AUX>::NT, ShapeH<TX, TY
                     const uint4 own = q[cs][j];
                     float o[8];
 #pragma unroll
-                    for (int e = 0; e < 8; ++e) {
-                        const float c = chunk_f(own, e);
-                        const float pq = chunk_f(qv, e);
-                        const float kk = bf2f(get_word(kv, e >> 1), e & 1);
-                        if (PHASE == 2)
-                            o[e] = fmaf(kk, lap[j][e], fmaf(-m_q, pq, 2.f * c));
-                        else
-                            o[e] = fmaf(kk, lap[j][e], fmaf(2.f, c, -pq));
-                        if (PHASE == 1) o[e] *= m_out;
+                    for (int h = 0; h < 4; ++h) {
+                        const float2 c = h2f2(get_word(own, h));
+                        const float2 pq = h2f2(get_word(qv, h));
+                        const uint32_t kw = get_word(kv, h);
+                        const float2 kk = make_float2(__uint_as_float(kw << 16),
+                                                      __uint_as_float(kw & 0xffff0000u));
+                        // 2c - m_q pq in one rounding (2c is exact), then + K lap
+                        float2 ov = fma2(kk, lap[j][h], fma2(nmq2, pq, add2(c, c)));
+                        if (PHASE == 1) ov = mul2(ov, mout2);
+                        o[2 * h] = ov.x;
+                        o[2 * h + 1] = ov.y;
                     }
                     if (src_j == j && z == a.src_z) {
                         const float wv = a.src_wavelet ? a.src_wavelet[*a.src_step + a.src_off]
