@@ -53,23 +53,6 @@ struct Shape {
     static constexpr int MINB = (512 / NT) > 0 ? (512 / NT) : 1;  // caps registers at 128
 };
 
-// ya[j][e] += weighted contributions of neighbour row k (row index relative to
-// the thread's first own row) to the y sums of the thread's own rows.
-template <int RPT>
-__device__ __forceinline__ void add_y_row(float (&ya)[RPT][4], const float4& v, int k,
-                                          const float (&ay)[R]) {
-#pragma unroll
-    for (int j = 0; j < RPT; ++j) {
-        const int d = k > j ? k - j : j - k;
-        if (d >= 1 && d <= R) {
-            ya[j][0] = fmaf(ay[d - 1], v.x, ya[j][0]);
-            ya[j][1] = fmaf(ay[d - 1], v.y, ya[j][1]);
-            ya[j][2] = fmaf(ay[d - 1], v.z, ya[j][2]);
-            ya[j][3] = fmaf(ay[d - 1], v.w, ya[j][3]);
-        }
-    }
-}
-
 // Ring position a CTA carries from one tile to the next: the sequence numbers of
 // the next p plane and the next aux iteration.  Stage = seq % ring size, phase
 // parity = (seq / ring size) & 1, so the mbarriers are initialised once per CTA
@@ -158,13 +141,14 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
         src_i = a.src_x - gx;
     }
 
-    float ax[R], ay[R], az[R];
+    float2 ax2[R], ay2[R], az2[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        ax[r] = a.w.ax[r];
-        ay[r] = a.w.ay[r];
-        az[r] = a.w.az[r];
+        ax2[r] = dup2(a.w.ax[r]);
+        ay2[r] = dup2(a.w.ay[r]);
+        az2[r] = dup2(a.w.az[r]);
     }
+    const float2 cx2 = dup2(a.w.cx), cy2 = dup2(a.w.cy), cz2 = dup2(a.w.cz), neg1 = dup2(-1.f);
 
     float4 q[9][RPT];
     bool bad = false;
@@ -214,18 +198,24 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
                 // y: neighbour rows outside the own block from shared memory, own
                 // rows from the queue centre, accumulated from zero in row order
                 // (farthest rows, smallest weights, first).
-                float ya[RPT][4];
+                // Pairs of points (lanes 0-1, 2-3 of a float4) as packed f32x2:
+                // per lane exactly the scalar operations in the same order.
+                float2 ya[RPT][2];
 #pragma unroll
-                for (int j = 0; j < RPT; ++j) ya[j][0] = ya[j][1] = ya[j][2] = ya[j][3] = 0.f;
+                for (int j = 0; j < RPT; ++j) ya[j][0] = ya[j][1] = make_float2(0.f, 0.f);
 #pragma unroll
                 for (int k = -R; k < RPT + R; ++k) {
-                    if (k >= 0 && k < RPT) {
-                        add_y_row<RPT>(ya, q[cs][k], k, ay);
-                    } else {
-                        add_y_row<RPT>(ya, lds128(pc + k * P::SX), k, ay);
+                    const float4 row = (k >= 0 && k < RPT) ? q[cs][k] : lds128(pc + k * P::SX);
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) {
+                        const int d = k > j ? k - j : j - k;
+                        if (d >= 1 && d <= R) {
+                            ya[j][0] = fma2(ay2[d - 1], pair_of(row, 0), ya[j][0]);
+                            ya[j][1] = fma2(ay2[d - 1], pair_of(row, 1), ya[j][1]);
+                        }
                     }
                 }
-                float lap[RPT][4];
+                float2 lap[RPT][2];
 #pragma unroll
                 for (int j = 0; j < RPT; ++j) {
                     const float4 c = q[cs][j];
@@ -234,19 +224,22 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
                     const float win[12] = {lf.x, lf.y, lf.z, lf.w, c.x, c.y,
                                            c.z,  c.w,  rt.x, rt.y, rt.z, rt.w};
 #pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const float ce = win[4 + e];
-                        float tz = a.w.cz * ce;
-                        float tx = a.w.cx * ce;
+                    for (int h = 0; h < 2; ++h) {
+                        const float2 ce = pair_of(c, h);
+                        float2 tz = mul2(cz2, ce);
+                        float2 tx = mul2(cx2, ce);
 #pragma unroll
                         for (int r = 1; r <= R; ++r) {
-                            const float up = f4get(q[(u + 4 + r) % 9][j], e);
-                            const float dn = f4get(q[(u + 4 - r + 9) % 9][j], e);
-                            tz = fmaf(az[r - 1], up + dn, tz);
-                            tx = fmaf(ax[r - 1], win[4 + e + r] + win[4 + e - r], tx);
+                            const float2 up = pair_of(q[(u + 4 + r) % 9][j], h);
+                            const float2 dn = pair_of(q[(u + 4 - r + 9) % 9][j], h);
+                            tz = fma2(az2[r - 1], add2(up, dn), tz);
+                            const int e = 4 + 2 * h;  // window index of the pair's first lane
+                            const float2 s = make_float2(win[e + r] + win[e - r],
+                                                         win[e + 1 + r] + win[e + 1 - r]);
+                            tx = fma2(ax2[r - 1], s, tx);
                         }
-                        const float ty = fmaf(a.w.cy, ce, ya[j][e]);
-                        lap[j][e] = (tx + ty) + tz;
+                        const float2 ty = fma2(cy2, ce, ya[j][h]);
+                        lap[j][h] = add2(add2(tx, ty), tz);
                     }
                 }
                 if (kAuxTma) {
@@ -265,15 +258,17 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
                     const float4 c = q[cs][j];
                     float4 o;
                     if (HEAT) {
-                        o.x = c.x + lap[j][0];
-                        o.y = c.y + lap[j][1];
-                        o.z = c.z + lap[j][2];
-                        o.w = c.w + lap[j][3];
+                        const float2 o0 = add2(pair_of(c, 0), lap[j][0]);
+                        const float2 o1 = add2(pair_of(c, 1), lap[j][1]);
+                        o = make_float4(o0.x, o0.y, o1.x, o1.y);
                     } else {
-                        o.x = fmaf(vv[j].x, lap[j][0], fmaf(2.f, c.x, -pv[j].x));
-                        o.y = fmaf(vv[j].y, lap[j][1], fmaf(2.f, c.y, -pv[j].y));
-                        o.z = fmaf(vv[j].z, lap[j][2], fmaf(2.f, c.z, -pv[j].z));
-                        o.w = fmaf(vv[j].w, lap[j][3], fmaf(2.f, c.w, -pv[j].w));
+                        // fmaf(vv, lap, fmaf(2, c, -pv)): 2c - pv is rounded once (2c is
+                        // exact), as fma(-1, pv, c + c)
+                        const float2 t0 = fma2(neg1, pair_of(pv[j], 0), add2(pair_of(c, 0), pair_of(c, 0)));
+                        const float2 t1 = fma2(neg1, pair_of(pv[j], 1), add2(pair_of(c, 1), pair_of(c, 1)));
+                        const float2 o0 = fma2(pair_of(vv[j], 0), lap[j][0], t0);
+                        const float2 o1 = fma2(pair_of(vv[j], 1), lap[j][1], t1);
+                        o = make_float4(o0.x, o0.y, o1.x, o1.y);
                         if (src_j == j && z == a.src_z) {
                             const float wv = a.src_wavelet
                                                  ? a.src_wavelet[*a.src_step + a.src_off]
