@@ -668,8 +668,7 @@ __global__ void __launch_bounds__(kTcThreads)
     __shared__ uint32_t s_tmem;
     __shared__ int s_flag;  // 1: the last MMA wait gave up
     __shared__ __align__(16) float sb1[H], sb2[H], sw3[H];
-    unsigned char* base = reinterpret_cast<unsigned char*>(
-        (reinterpret_cast<uintptr_t>(dyn) + 1023) & ~uintptr_t(1023));
+    unsigned char* base = smem_align<1024>(dyn);
     unsigned char* sA = base;            // 128 x 32 BF16 features
     unsigned char* sA2 = base + 8192;    // 128 x 32 BF16 h1
     unsigned char* sW1 = base + 16384;   // 32 x 32 BF16

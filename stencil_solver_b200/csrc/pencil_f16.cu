@@ -2,16 +2,30 @@
 //
 // Storage: p and p_prev in FP16, both holding a * p for one power-of-two scale
 // a (kept in a device-side F16Scale); K = vel2 * dt^2 / dx^2 in BF16.  All
-// arithmetic is FP32: every stored value is converted once at its use, the
-// z / x pair sums use the sm_100 mixed-precision add (f16 + f32 -> f32), and
-// the output is rounded to FP16 once.  DRAM traffic: 8 B per interior point
-// (read p, p_prev, K; write p_next in place over p_prev).
+// arithmetic is FP32 and the output is rounded to FP16 once.  DRAM traffic: 8 B
+// per interior point (read p, p_prev, K; write p_next in place over p_prev).
 //
 // Layout of a CTA's work is the FP32 kernel's (pencil_f32.cu) with 2-byte
-// elements: each thread owns 8 consecutive x (one 16-byte chunk) in RPT rows.
+// elements: each thread owns 8 consecutive x (one 16-byte chunk) of one row.
 // Because the interior starts at x = 4 (byte 8), tiles are aligned to x = 8k
 // and the p box starts 8 halves left of the tile (16-byte aligned TMA origin,
 // box TX + 16 wide); points of a chunk outside the interior are never stored.
+//
+// The kernel is bound by the FP32 pipe that also executes the FP16 -> FP32
+// conversions, so every choice below is about issuing fewer of them:
+//   * y neighbours come from the staged FP16 plane; each pair (up, down) costs
+//     one conversion and one mixed FP16 + FP32 add (add.f32.f16), not two
+//     conversions and an add.
+//   * the z queue is split by role.  The centre plane and the four planes above
+//     it stay FP16 in registers (the up operand of a z pair enters through the
+//     mixed add); the four planes below the centre are FP32 -- each plane is
+//     converted once, when it is the centre (the x window converts it anyway),
+//     and is then the down operand of four z pairs.  Both register rings have 4
+//     slots (plane index mod 4) and the plane loop is unrolled by 4, so every
+//     slot is a compile-time register and nothing is shifted.
+//   * arithmetic on point pairs uses the packed f32x2 instructions; the
+//     Laplacian is two FMA chains (x and y from the combined centre term, z from
+//     its first pair) added once.
 //
 // Renormalisation (driven by the FP64 statistics every few dozen steps): a
 // renorm step (PHASE 1) scales its output by r = a_new / a_old; the step after
@@ -46,16 +60,15 @@ struct F16Args {
     int* err;
 };
 
-template <int TX, int TY, int RPT, int S, int AUX>
+template <int TX, int TY, int S, int AUX>
 struct ShapeH {
     static_assert(TX % 8 == 0, "TX must be a multiple of 8 halves (16-byte chunks)");
-    static_assert(TY % RPT == 0, "TY must be a multiple of RPT");
     static_assert(S >= 8 && AUX >= 1, "rings");
     static constexpr int SX = TX + 16;  // halves per staged row: 8 left, TX, 8 right
     static constexpr int SY = TY + 2 * R;
     static_assert(SX <= 256 && SY <= 256, "TMA box extent is at most 256");
     static constexpr int TPR = TX / 8;
-    static constexpr int NT = TPR * (TY / RPT);
+    static constexpr int NT = TPR * TY;
     static constexpr uint32_t PLANE_BYTES = SX * SY * 2u;
     static constexpr int PLANE = int(((PLANE_BYTES + 127u) / 128u) * 64u);  // stride, halves
     static constexpr uint32_t TILE_BYTES = TX * TY * 2u;
@@ -98,7 +111,6 @@ __device__ __forceinline__ float2 addhf2(uint32_t w, float2 b) {
     return make_float2(x, y);
 }
 
-
 __device__ __forceinline__ uint2 lds64(const uint16_t* p) {
     return *reinterpret_cast<const uint2*>(p);
 }
@@ -106,21 +118,33 @@ __device__ __forceinline__ uint4 lds128h(const uint16_t* p) {
     return *reinterpret_cast<const uint4*>(p);
 }
 
-// UNR = 9: the plane loop is unrolled by 9 so the z queue's slots are
-// compile-time registers that never move.  UNR = 1: one plane per iteration and
-// the queue shifts by one slot after each plane (36 register moves per row of
-// a thread) -- a ninth of the code, for kernels that stall on instruction fetch.
-template <int TX, int TY, int RPT, int S, int AUX, int PHASE, int UNR>
-__global__ void __launch_bounds__(ShapeH<TX, TY, RPT, S, AUX>::NT, ShapeH<TX, TY, RPT, S, AUX>::MINB)
+__device__ __forceinline__ void stg_stream_u2(void* p, uint2 v) {
+    asm volatile("st.global.cs.v2.u32 [%0], {%1, %2};" ::"l"(p), "r"(v.x), "r"(v.y) : "memory");
+}
+
+// x pair sum (x[+r] + x[-r]) for points 2h, 2h+1 of the window xv (halves
+// [4 left | 8 own | 4 right] as 8 pairs).  Even r keeps the pair aligned (one
+// packed add); odd r straddles pairs (two scalar adds).
+__device__ __forceinline__ float2 xsum(const float2 (&xv)[8], int h, int r) {
+    if (r % 2 == 0) return add2(xv[2 + h + r / 2], xv[2 + h - r / 2]);
+    const int a0 = 4 + 2 * h + r, b0 = 4 + 2 * h - r;
+    const float ra = (a0 & 1) ? xv[a0 >> 1].y : xv[a0 >> 1].x;
+    const float rb = ((a0 + 1) & 1) ? xv[(a0 + 1) >> 1].y : xv[(a0 + 1) >> 1].x;
+    const float la = (b0 & 1) ? xv[b0 >> 1].y : xv[b0 >> 1].x;
+    const float lb = ((b0 + 1) & 1) ? xv[(b0 + 1) >> 1].y : xv[(b0 + 1) >> 1].x;
+    return make_float2(ra + la, rb + lb);
+}
+
+template <int TX, int TY, int S, int AUX, int PHASE>
+__global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, AUX>::MINB)
     pencil_f16_kernel(const __grid_constant__ CUtensorMap pmap,
                       const __grid_constant__ CUtensorMap qmap,
                       const __grid_constant__ CUtensorMap kmap, const F16Args a) {
-    using P = ShapeH<TX, TY, RPT, S, AUX>;
+    using P = ShapeH<TX, TY, S, AUX>;
     extern __shared__ unsigned char dsmem[];
     __shared__ __align__(8) uint64_t full[S];
     __shared__ __align__(8) uint64_t auxf[AUX];
-    uint16_t* sm = reinterpret_cast<uint16_t*>((reinterpret_cast<uintptr_t>(dsmem) + 127) &
-                                               ~uintptr_t(127));
+    uint16_t* sm = reinterpret_cast<uint16_t*>(smem_align<128>(dsmem));
     uint16_t* aux = sm + S * P::PLANE;  // AUX stages of [p_prev tile | K tile]
 
     const int tid = threadIdx.x;
@@ -150,7 +174,12 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, RPT, S, AUX>::NT, ShapeH<TX, TY
     }
     __syncthreads();
     int issued_hi = -1, aux_issued_hi = -1;
-    auto issue_aux = [&](int it) {
+    auto issue_plane = [&](int j) {  // thread 0 only
+        mbar_arrive_expect_tx(&full[j % S], P::PLANE_BYTES);
+        tma_load_3d(sm + (j % S) * P::PLANE, &pmap, &full[j % S], xa - 8, y0 - R, zb - R + j);
+        issued_hi = j;
+    };
+    auto issue_aux = [&](int it) {  // thread 0 only
         uint16_t* st = aux + (it % AUX) * 2 * P::TILE;
         mbar_arrive_expect_tx(&auxf[it % AUX], 2 * P::TILE_BYTES);
         tma_load_3d(st, &qmap, &auxf[it % AUX], xa, y0, zb + it);
@@ -158,175 +187,139 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, RPT, S, AUX>::NT, ShapeH<TX, TY
         aux_issued_hi = it;
     };
     if (tid == 0) {
-        for (int s = 0; s < S && s < nplanes; ++s) {
-            mbar_arrive_expect_tx(&full[s], P::PLANE_BYTES);
-            tma_load_3d(sm + s * P::PLANE, &pmap, &full[s], xa - 8, y0 - R, zb - R + s);
-            issued_hi = s;
-        }
+        for (int s = 0; s < S && s < nplanes; ++s) issue_plane(s);
         for (int it = 0; it < AUX && it < nint; ++it) issue_aux(it);
     }
 
     const int gx = xa + 8 * lx;  // first x of this thread's chunk
-    const int gy = y0 + RPT * ly;
-    // Interior x range of the chunk: [max(gx, 4), min(gx + 8, nx - 4)).
-    const int xlo = max(gx, R), xhi = min(gx + 8, a.nx - R);
-    const bool xany = xlo < xhi, xfull = gx >= R && gx + 8 <= a.nx - R;
-    bool rin[RPT];
-#pragma unroll
-    for (int j = 0; j < RPT; ++j) rin[j] = xany && (gy + j < a.ny - R);
-    const int soff = (RPT * ly + R) * P::SX + 8 + 8 * lx;
-    const int aoff = RPT * ly * TX + 8 * lx;
+    const int gy = y0 + ly;
+    // With nx % 8 == 0 a chunk is wholly interior, wholly halo, or (at the two x
+    // edges) half and half: x = 0..7 stores its upper 4 points, x = nx-8..nx-1
+    // its lower 4.
+    const bool xfull = gx >= R && gx + 8 <= a.nx - R;
+    const bool xany = gx + 8 > R && gx < a.nx - R;
+    const bool rin = xany && gy < a.ny - R;
+    const int soff = (ly + R) * P::SX + 8 + 8 * lx;
+    const int aoff = ly * TX + 8 * lx;
     int64_t goff = static_cast<int64_t>(zb) * a.sz + static_cast<int64_t>(gy) * a.sy + gx;
 
-    int src_j = -1, src_e = -1;
-    if (a.src_z >= 0 && a.src_x >= gx && a.src_x < gx + 8 && a.src_y >= gy &&
-        a.src_y < gy + RPT) {
-        src_j = a.src_y - gy;
-        src_e = a.src_x - gx;
-    }
+    // Source: a CTA-uniform test first (tile and plane), then the owning thread.
+    const bool src_tile = a.src_z >= zb && a.src_z < ze && a.src_y >= y0 && a.src_y < y0 + TY &&
+                          a.src_x >= xa && a.src_x < xa + TX;
+    const bool src_mine = src_tile && a.src_x >= gx && a.src_x < gx + 8 && a.src_y == gy;
+    const int src_e = a.src_x - gx;
+    const int src_i = a.src_z - zb;
 
-    float ax[R], ay[R], az[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        ax[r] = a.w.ax[r];
-        ay[r] = a.w.ay[r];
-        az[r] = a.w.az[r];
-    }
-    float m_out = 1.f, m_q = 1.f;
-    if (PHASE == 1) m_out = a.scale->r;
-    if (PHASE == 2) m_q = a.scale->r;
     float2 ax2[R], ay2[R], az2[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        ax2[r] = make_float2(ax[r], ax[r]);
-        ay2[r] = make_float2(ay[r], ay[r]);
-        az2[r] = make_float2(az[r], az[r]);
+        ax2[r] = dup2(a.w.ax[r]);
+        ay2[r] = dup2(a.w.ay[r]);
+        az2[r] = dup2(a.w.az[r]);
     }
-    const float2 cx2 = make_float2(a.w.cx, a.w.cx), cy2 = make_float2(a.w.cy, a.w.cy),
-                 cz2 = make_float2(a.w.cz, a.w.cz);
-    const float2 nmq2 = make_float2(-m_q, -m_q), mout2 = make_float2(m_out, m_out);
+    const float2 cxy2 = dup2(a.w.cx + a.w.cy + a.w.cz);  // combined centre weight
+    float m_out = 1.f, m_q = 1.f;
+    if (PHASE == 1) m_out = a.scale->r;
+    if (PHASE == 2) m_q = a.scale->r;
+    const float2 nmq2 = dup2(-m_q), mout2 = dup2(m_out);
 
-    uint4 q[9][RPT];
+    // Plane index p (z = zb - 4 + p) lives in slot p % 4 of both rings.
+    uint4 hq[4];      // FP16: centre and the planes above it
+    float2 dq[4][4];  // FP32: the four planes below the centre, as point pairs
     bool bad = false;
 #pragma unroll
-    for (int jj = 0; jj < 8; ++jj) {
-        if (!mbar_wait(&full[jj % S], (jj / S) & 1)) bad = true;
-        const uint16_t* pl = sm + (jj % S) * P::PLANE + soff;
+    for (int p = 0; p < 8; ++p) {
+        if (!mbar_wait(&full[p % S], (p / S) & 1)) bad = true;
+        const uint4 v = lds128h(sm + (p % S) * P::PLANE + soff);
+        if (p < R) {
 #pragma unroll
-        for (int j = 0; j < RPT; ++j) q[jj][j] = lds128h(pl + j * P::SX);
+            for (int h = 0; h < 4; ++h) dq[p][h] = h2f2(get_word(v, h));
+        } else {
+            hq[p - R] = v;
+        }
     }
     bool abort_run = __syncthreads_or(bad) != 0;
     if (!abort_run && tid == 0) {
 #pragma unroll
-        for (int jj = 0; jj < R; ++jj) {
-            const int jn = jj + S;
-            if (jn < nplanes) {
-                mbar_arrive_expect_tx(&full[jj], P::PLANE_BYTES);
-                tma_load_3d(sm + jj * P::PLANE, &pmap, &full[jj], xa - 8, y0 - R, zb - R + jn);
-                issued_hi = jn;
-            }
-        }
+        for (int p = 0; p < R; ++p)  // planes 0..3 are consumed: refill their stages
+            if (p + S < nplanes) issue_plane(p + S);
     }
 
-    static_assert(UNR == 1 || UNR == 9, "the z queue is unrolled by 9 or rolled");
-    for (int i0 = 0; i0 < nint && !abort_run; i0 += UNR) {
+    for (int i0 = 0; i0 < nint && !abort_run; i0 += 4) {
 #pragma unroll
-        for (int u = 0; u < UNR; ++u) {
+        for (int u = 0; u < 4; ++u) {
             const int i = i0 + u;
             if (i < nint && !abort_run) {
-                const int cs = (u + 4) % 9;
-                {
-                    const int jf = i + 8;
-                    if (!mbar_wait(&full[jf % S], (jf / S) & 1)) bad = true;
-                    const uint16_t* pf = sm + (jf % S) * P::PLANE + soff;
-#pragma unroll
-                    for (int j = 0; j < RPT; ++j) q[(u + 8) % 9][j] = lds128h(pf + j * P::SX);
-                }
+                // Centre plane i + 4 (slot u); it was waited for when it was fed.
                 const uint16_t* pc = sm + ((i + 4) % S) * P::PLANE + soff;
-
-                // Pairs of points (halves 2h, 2h+1 of a 16-byte chunk) as packed
-                // FP32.  y: row pairs j+d, j-d through the mixed FP16 + FP32 add;
-                // farthest pair first, from zero.
-                float2 ya[RPT][4];
-#pragma unroll
-                for (int j = 0; j < RPT; ++j)
-#pragma unroll
-                    for (int h = 0; h < 4; ++h) ya[j][h] = make_float2(0.f, 0.f);
-#pragma unroll
-                for (int d = R; d >= 1; --d) {
-#pragma unroll
-                    for (int j = 0; j < RPT; ++j) {
-                        const int ku = j + d, kd = j - d;
-                        const uint4 up = (ku < RPT) ? q[cs][ku] : lds128h(pc + ku * P::SX);
-                        const uint4 dn = (kd >= 0) ? q[cs][kd] : lds128h(pc + kd * P::SX);
-#pragma unroll
-                        for (int h = 0; h < 4; ++h)
-                            ya[j][h] = fma2(ay2[d - 1], addhf2(get_word(up, h), h2f2(get_word(dn, h))),
-                                            ya[j][h]);
-                    }
-                }
-                // x window halves: [4 left | 8 own | 4 right] per row; z from the queue.
-                float2 lap[RPT][4];
-#pragma unroll
-                for (int j = 0; j < RPT; ++j) {
-                    const uint2 lf = lds64(pc + j * P::SX - 4);
-                    const uint2 rt = lds64(pc + j * P::SX + 8);
-                    const uint4 own = q[cs][j];
+                float2 xv[8];  // x window halves [4 left | 8 own | 4 right] as 8 pairs
+                {
+                    const uint2 lf = lds64(pc - 4);
+                    const uint2 rt = lds64(pc + 8);
+                    const uint4 own = hq[u];
                     const uint32_t win[8] = {lf.x, lf.y, own.x, own.y, own.z, own.w, rt.x, rt.y};
-                    float2 xv[8];  // the window's 16 halves as 8 pairs
 #pragma unroll
                     for (int w = 0; w < 8; ++w) xv[w] = h2f2(win[w]);
-#pragma unroll
-                    for (int h = 0; h < 4; ++h) {
-                        const float2 c = xv[2 + h];
-                        float2 tz = mul2(cz2, c);
-                        float2 tx = mul2(cx2, c);
-#pragma unroll
-                        for (int r = 1; r <= R; ++r) {
-                            const uint4& upv = q[(u + 4 + r) % 9][j];
-                            const uint4& dnv = q[(u + 4 - r + 9) % 9][j];
-                            tz = fma2(az2[r - 1], addhf2(get_word(upv, h), h2f2(get_word(dnv, h))), tz);
-                            // window halves 4 + 2h +- r and 5 + 2h +- r
-                            float2 s;
-                            if (r % 2 == 0) {
-                                s = add2(xv[2 + h + r / 2], xv[2 + h - r / 2]);
-                            } else {
-                                const int a0 = 4 + 2 * h + r, b0 = 4 + 2 * h - r;
-                                const float ra = (a0 & 1) ? xv[a0 >> 1].y : xv[a0 >> 1].x;
-                                const float rb = ((a0 + 1) & 1) ? xv[(a0 + 1) >> 1].y : xv[(a0 + 1) >> 1].x;
-                                const float la = (b0 & 1) ? xv[b0 >> 1].y : xv[b0 >> 1].x;
-                                const float lb = ((b0 + 1) & 1) ? xv[(b0 + 1) >> 1].y : xv[(b0 + 1) >> 1].x;
-                                s = make_float2(ra + la, rb + lb);
-                            }
-                            tx = fma2(ax2[r - 1], s, tx);
-                        }
-                        const float2 ty = fma2(cy2, c, ya[j][h]);
-                        lap[j][h] = add2(add2(tx, ty), tz);
-                    }
                 }
+                {  // feed: plane i + 8 (z + 4) replaces the centre in slot u
+                    const int jf = i + 8;
+                    if (!mbar_wait(&full[jf % S], (jf / S) & 1)) bad = true;
+                    hq[u] = lds128h(sm + (jf % S) * P::PLANE + soff);
+                }
+                uint4 yu[R], yd[R];  // staged rows y +- d of the centre plane
+#pragma unroll
+                for (int d = 1; d <= R; ++d) {
+                    yu[d - 1] = lds128h(pc + d * P::SX);
+                    yd[d - 1] = lds128h(pc - d * P::SX);
+                }
+                // lap = [c (cx+cy+cz) + sum_r (ax_r sx_r + ay_r sy_r)] + sum_r az_r sz_r,
+                // pair sums s = p[+r] + p[-r]; up operands of y and z enter FP16.
+                float2 lap[4];
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    const float2 c = xv[2 + h];
+                    float2 txy = mul2(cxy2, c);
+                    float2 tz = mul2(az2[0], addhf2(get_word(hq[(u + 1) % 4], h),
+                                                    dq[(u + 3) % 4][h]));
+#pragma unroll
+                    for (int r = 1; r <= R; ++r) {
+                        txy = fma2(ax2[r - 1], xsum(xv, h, r), txy);
+                        txy = fma2(ay2[r - 1],
+                                   addhf2(get_word(yu[r - 1], h), h2f2(get_word(yd[r - 1], h))),
+                                   txy);
+                        // up: plane z + r (FP16, slot (u + r) % 4; r = 4 is the plane
+                        // just fed); down: plane z - r (FP32, slot (u + 4 - r) % 4)
+                        if (r > 1)
+                            tz = fma2(az2[r - 1], addhf2(get_word(hq[(u + r) % 4], h),
+                                                         dq[(u + 4 - r) % 4][h]),
+                                      tz);
+                    }
+                    lap[h] = add2(txy, tz);
+                }
+                // plane z - 4 is no longer needed: its slot takes the centre (z).
+#pragma unroll
+                for (int h = 0; h < 4; ++h) dq[u][h] = xv[2 + h];
+
                 if (!mbar_wait(&auxf[i % AUX], (i / AUX) & 1)) bad = true;
                 const uint16_t* st = aux + (i % AUX) * 2 * P::TILE + aoff;
-                const int z = zb + i;
+                const uint4 qv = lds128h(st);
+                const uint4 kv = lds128h(st + P::TILE);
+                float o[8];
 #pragma unroll
-                for (int j = 0; j < RPT; ++j) {
-                    const uint4 qv = lds128h(st + j * TX);
-                    const uint4 kv = lds128h(st + P::TILE + j * TX);
-                    const uint4 own = q[cs][j];
-                    float o[8];
-#pragma unroll
-                    for (int h = 0; h < 4; ++h) {
-                        const float2 c = h2f2(get_word(own, h));
-                        const float2 pq = h2f2(get_word(qv, h));
-                        const uint32_t kw = get_word(kv, h);
-                        const float2 kk = make_float2(__uint_as_float(kw << 16),
-                                                      __uint_as_float(kw & 0xffff0000u));
-                        // 2c - m_q pq in one rounding (2c is exact), then + K lap
-                        float2 ov = fma2(kk, lap[j][h], fma2(nmq2, pq, add2(c, c)));
-                        if (PHASE == 1) ov = mul2(ov, mout2);
-                        o[2 * h] = ov.x;
-                        o[2 * h + 1] = ov.y;
-                    }
-                    if (src_j == j && z == a.src_z) {
+                for (int h = 0; h < 4; ++h) {
+                    const float2 c = xv[2 + h];
+                    const float2 pq = h2f2(get_word(qv, h));
+                    const uint32_t kw = get_word(kv, h);
+                    const float2 kk = make_float2(__uint_as_float(kw << 16),
+                                                  __uint_as_float(kw & 0xffff0000u));
+                    // 2c - m_q pq in one rounding (2c is exact), then + K lap
+                    float2 ov = fma2(kk, lap[h], fma2(nmq2, pq, add2(c, c)));
+                    if (PHASE == 1) ov = mul2(ov, mout2);
+                    o[2 * h] = ov.x;
+                    o[2 * h + 1] = ov.y;
+                }
+                if (src_tile && i == src_i) {  // CTA-uniform
+                    if (src_mine) {
                         const float wv = a.src_wavelet ? a.src_wavelet[*a.src_step + a.src_off]
                                                        : a.src_w;
                         const float kk = bf2f(get_word(kv, src_e >> 1), src_e & 1);
@@ -341,41 +334,26 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, RPT, S, AUX>::NT, ShapeH<TX, TY
                                         __half2float(__float2half_rn(o[e])) / sa;
                             }
                     }
-                    if (rin[j]) {
-                        uint16_t* dst = a.next + goff + j * a.sy;
-                        if (xfull) {
-                            uint4 pk;
-                            pk.x = pack_h2(o[0], o[1]);
-                            pk.y = pack_h2(o[2], o[3]);
-                            pk.z = pack_h2(o[4], o[5]);
-                            pk.w = pack_h2(o[6], o[7]);
-                            stg_stream_u4(dst, pk);
-                        } else {  // chunk straddles the halo: store interior points only
-#pragma unroll
-                            for (int e = 0; e < 8; ++e)
-                                if (gx + e >= xlo && gx + e < xhi)
-                                    dst[e] = __half_as_ushort(__float2half_rn(o[e]));
-                        }
-                    }
+                }
+                if (rin) {
+                    uint16_t* dst = a.next + goff;
+                    uint4 pk;
+                    pk.x = pack_h2(o[0], o[1]);
+                    pk.y = pack_h2(o[2], o[3]);
+                    pk.z = pack_h2(o[4], o[5]);
+                    pk.w = pack_h2(o[6], o[7]);
+                    if (xfull)
+                        stg_stream_u4(dst, pk);
+                    else if (gx < R)  // x = 4..7 of the first chunk
+                        stg_stream_u2(dst + 4, make_uint2(pk.z, pk.w));
+                    else  // x = nx-8 .. nx-5 of the last chunk
+                        stg_stream_u2(dst, make_uint2(pk.x, pk.y));
                 }
                 goff += a.sz;
                 abort_run = __syncthreads_or(bad) != 0;
                 if (!abort_run && tid == 0) {
-                    const int jr = i + 4;
-                    const int jn = jr + S;
-                    if (jn < nplanes) {
-                        mbar_arrive_expect_tx(&full[jr % S], P::PLANE_BYTES);
-                        tma_load_3d(sm + (jr % S) * P::PLANE, &pmap, &full[jr % S], xa - 8,
-                                    y0 - R, zb - R + jn);
-                        issued_hi = jn;
-                    }
+                    if (i + 4 + S < nplanes) issue_plane(i + 4 + S);  // the centre's stage
                     if (i + AUX < nint) issue_aux(i + AUX);
-                }
-                if (UNR == 1) {  // slot k holds plane i + 1 + k for the next plane
-#pragma unroll
-                    for (int k = 0; k < 8; ++k)
-#pragma unroll
-                        for (int j = 0; j < RPT; ++j) q[k][j] = q[k + 1][j];
                 }
             }
         }
@@ -393,21 +371,21 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, RPT, S, AUX>::NT, ShapeH<TX, TY
 using LaunchFnH = cudaError_t (*)(const PencilMaps&, const F16Args&, unsigned, int, cudaStream_t);
 using ResidentFnH = int (*)();
 
-template <int TX, int TY, int RPT, int S, int AUX, int UNR>
+template <int TX, int TY, int S, int AUX>
 int resident_f16() {
-    using P = ShapeH<TX, TY, RPT, S, AUX>;
+    using P = ShapeH<TX, TY, S, AUX>;
     static int cached[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (cached[dev & 63] > 0) return cached[dev & 63];
-    auto kern = pencil_f16_kernel<TX, TY, RPT, S, AUX, 0, UNR>;
+    auto kern = pencil_f16_kernel<TX, TY, S, AUX, 0>;
     const int smem = static_cast<int>(P::SMEM);
     int n = 0;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) ==
             cudaSuccess &&
-        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, RPT, S, AUX, 1, UNR>,
+        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, S, AUX, 1>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
-        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, RPT, S, AUX, 2, UNR>,
+        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, S, AUX, 2>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, P::NT, P::SMEM) == cudaSuccess &&
         n > 0) {
@@ -418,46 +396,40 @@ int resident_f16() {
     return std::max(1, std::min(int((228u * 1024u) / (P::SMEM + 1024u)), 65536 / (P::NT * 128)));
 }
 
-template <int TX, int TY, int RPT, int S, int AUX, int UNR>
+template <int TX, int TY, int S, int AUX>
 cudaError_t launch_f16(const PencilMaps& m, const F16Args& a, unsigned ctas, int phase,
                        cudaStream_t stream) {
-    using P = ShapeH<TX, TY, RPT, S, AUX>;
-    resident_f16<TX, TY, RPT, S, AUX, UNR>();  // sets the attributes once per device
+    using P = ShapeH<TX, TY, S, AUX>;
+    resident_f16<TX, TY, S, AUX>();  // sets the attributes once per device
     if (phase == 1)
-        pencil_f16_kernel<TX, TY, RPT, S, AUX, 1, UNR><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
-                                                                                   m.vel2, a);
+        pencil_f16_kernel<TX, TY, S, AUX, 1><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
+                                                                                m.vel2, a);
     else if (phase == 2)
-        pencil_f16_kernel<TX, TY, RPT, S, AUX, 2, UNR><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
-                                                                                   m.vel2, a);
+        pencil_f16_kernel<TX, TY, S, AUX, 2><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
+                                                                                m.vel2, a);
     else
-        pencil_f16_kernel<TX, TY, RPT, S, AUX, 0, UNR><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
-                                                                                   m.vel2, a);
+        pencil_f16_kernel<TX, TY, S, AUX, 0><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
+                                                                                m.vel2, a);
     return cudaGetLastError();
 }
 
 struct VariantH {
-    int tx, ty, rpt, stages, aux;
+    int tx, ty, stages, aux;
     const char* name;
     LaunchFnH launch;
     ResidentFnH resident;
 };
 
-#define SB200_VARIANT_H(TX, TY, RPT, S, AUX, UNR, NAME)                                   \
-    VariantH {                                                                              \
-        TX, TY, RPT, S, AUX, NAME, &launch_f16<TX, TY, RPT, S, AUX, UNR>,                   \
-            &resident_f16<TX, TY, RPT, S, AUX, UNR>                                          \
-    }
+#define SB200_VARIANT_H(TX, TY, S, AUX, NAME) \
+    VariantH { TX, TY, S, AUX, NAME, &launch_f16<TX, TY, S, AUX>, &resident_f16<TX, TY, S, AUX> }
 
-// "_roll": the z queue shifts one slot per plane instead of the 9x unroll.
 const VariantH kF16[] = {
-    SB200_VARIANT_H(64, 16, 1, 8, 4, 9, "h64x16_r1_s8_a4"),
-    SB200_VARIANT_H(64, 32, 2, 8, 3, 9, "h64x32_r2_s8_a3"),
-    SB200_VARIANT_H(128, 16, 2, 8, 3, 9, "h128x16_r2_s8_a3"),
-    SB200_VARIANT_H(64, 32, 1, 8, 3, 9, "h64x32_r1_s8_a3"),
-    SB200_VARIANT_H(64, 16, 1, 8, 4, 1, "h64x16_r1_s8_a4_roll"),
-    SB200_VARIANT_H(64, 32, 2, 8, 3, 1, "h64x32_r2_s8_a3_roll"),
-    SB200_VARIANT_H(128, 16, 2, 8, 3, 1, "h128x16_r2_s8_a3_roll"),
-    SB200_VARIANT_H(64, 32, 1, 8, 3, 1, "h64x32_r1_s8_a3_roll"),
+    SB200_VARIANT_H(64, 16, 8, 4, "h64x16_s8_a4"),
+    SB200_VARIANT_H(64, 32, 8, 4, "h64x32_s8_a4"),
+    SB200_VARIANT_H(128, 16, 8, 4, "h128x16_s8_a4"),
+    SB200_VARIANT_H(64, 8, 8, 4, "h64x8_s8_a4"),
+    SB200_VARIANT_H(32, 16, 8, 4, "h32x16_s8_a4"),
+    SB200_VARIANT_H(64, 16, 12, 4, "h64x16_s12_a4"),
 };
 constexpr int kNumF16 = sizeof(kF16) / sizeof(kF16[0]);
 

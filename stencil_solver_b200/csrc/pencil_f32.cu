@@ -329,7 +329,7 @@ __device__ __forceinline__ float* setup_rings(unsigned char* dsmem, uint64_t* fu
         fence_barrier_init();
     }
     __syncthreads();
-    return reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(dsmem) + 127) & ~uintptr_t(127));
+    return reinterpret_cast<float*>(smem_align<128>(dsmem));
 }
 
 // One grid: CTA b owns tile (b % tiles_x, (b / tiles_x) % tiles_y) and z chunk

@@ -45,6 +45,15 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
+// Rounds a pointer into dynamic shared memory up to A bytes (A a power of two) by
+// pointer arithmetic on the pointer itself: a round trip through an integer
+// would hide the shared address space from the compiler and turn every access
+// through the result into a generic load or store.
+template <unsigned A>
+__device__ __forceinline__ unsigned char* smem_align(unsigned char* p) {
+    return p + ((A - (smem_u32(p) & (A - 1u))) & (A - 1u));
+}
+
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
                  : "memory");

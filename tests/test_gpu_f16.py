@@ -161,14 +161,22 @@ def test_f16_tuner_picks_a_variant(torch_cuda):
     assert zc.value >= 1 and ms.value > 0
 
 
-def test_f16_source_injection(torch_cuda):
+@pytest.mark.parametrize("variant", [0, 3, 4])
+def test_f16_source_injection(torch_cuda, variant):
+    """Source injection under three tile shapes (64x16, 64x8, 32x16)."""
+    if variant >= sb.lib().sb200_pencil_variant_count(sb.KIND_WAVE_F16):
+        pytest.skip("variant not compiled")
     shape = (24, 24, 32)
     P, Q, K = f16_case(shape, 9, scale=64.0)
     g = sb.Grid(32, 24, 24, 10.0, 10.0, 10.0, 1e-3)
     src = g.index(13, 11, 12)
     out = dev(torch_cuda, Q.view(np.int16))
-    sb.wave_step_f16(dev(torch_cuda, P.view(np.int16)), out, dev(torch_cuda, K.view(np.int16)), g,
-                     scale_state(torch_cuda, 64.0), 0, src, 0.75)
+    sb.set_pencil_override(sb.KIND_WAVE_F16, variant, 1)
+    try:
+        sb.wave_step_f16(dev(torch_cuda, P.view(np.int16)), out, dev(torch_cuda, K.view(np.int16)),
+                         g, scale_state(torch_cuda, 64.0), 0, src, 0.75)
+    finally:
+        sb.set_pencil_override(sb.KIND_WAVE_F16, -1, 1)
     ref = oracle.wave_step_f16(P, Q, K, 10.0, 10.0, 10.0, src=src, w=0.75, a=64.0)
     mag = step_magnitude(P, Q, K)
     kk = float((K.astype(np.uint32) << 16).view(np.float32).ravel()[src])
