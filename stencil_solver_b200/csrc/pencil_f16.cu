@@ -63,7 +63,7 @@ struct F16Args {
 template <int TX, int TY, int S, int AUX>
 struct ShapeH {
     static_assert(TX % 8 == 0, "TX must be a multiple of 8 halves (16-byte chunks)");
-    static_assert(S >= 8 && AUX >= 1, "rings");
+    static_assert(S >= 8 && S % 4 == 0 && 4 % AUX == 0, "rings (the plane loop is unrolled by 4)");
     static constexpr int SX = TX + 16;  // halves per staged row: 8 left, TX, 8 right
     static constexpr int SY = TY + 2 * R;
     static_assert(SX <= 256 && SY <= 256, "TMA box extent is at most 256");
@@ -122,20 +122,39 @@ __device__ __forceinline__ void stg_stream_u2(void* p, uint2 v) {
     asm volatile("st.global.cs.v2.u32 [%0], {%1, %2};" ::"l"(p), "r"(v.x), "r"(v.y) : "memory");
 }
 
-// x pair sum (x[+r] + x[-r]) for points 2h, 2h+1 of the window xv (halves
-// [4 left | 8 own | 4 right] as 8 pairs).  Even r keeps the pair aligned (one
-// packed add); odd r straddles pairs (two scalar adds).
-__device__ __forceinline__ float2 xsum(const float2 (&xv)[8], int h, int r) {
-    if (r % 2 == 0) return add2(xv[2 + h + r / 2], xv[2 + h - r / 2]);
-    const int a0 = 4 + 2 * h + r, b0 = 4 + 2 * h - r;
-    const float ra = (a0 & 1) ? xv[a0 >> 1].y : xv[a0 >> 1].x;
-    const float rb = ((a0 + 1) & 1) ? xv[(a0 + 1) >> 1].y : xv[(a0 + 1) >> 1].x;
-    const float la = (b0 & 1) ? xv[b0 >> 1].y : xv[b0 >> 1].x;
-    const float lb = ((b0 + 1) & 1) ? xv[(b0 + 1) >> 1].y : xv[(b0 + 1) >> 1].x;
-    return make_float2(ra + la, rb + lb);
+// f32(half `hi` of word w) + c (the mixed add on one point).
+__device__ __forceinline__ float addhf(uint32_t w, int hi, float c) {
+    float d;
+    if (hi)
+        asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %1;\n\tadd.rn.f32.f16 %0, hi, %2;\n\t}"
+            : "=f"(d)
+            : "r"(w), "f"(c));
+    else
+        asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %1;\n\tadd.rn.f32.f16 %0, lo, %2;\n\t}"
+            : "=f"(d)
+            : "r"(w), "f"(c));
+    return d;
 }
 
-template <int TX, int TY, int S, int AUX, int PHASE>
+// x pair sum x[e+r] + x[e-r] for point e of a chunk: own points as FP32 (c,
+// 8 values), the 4 halves left (lf) and right (rt) of the chunk as FP16.  No pair
+// reaches both sides (r <= 4), so a pair with a side value takes it through the
+// mixed add and the side halves are never converted; the sum is the same FP32
+// add either way.
+__device__ __forceinline__ float xsum1(const float (&c)[8], uint2 lf, uint2 rt, int e, int r) {
+    const int up = e + r, dn = e - r;
+    if (up >= 8) {
+        const int k = up - 8;  // right half k: word k / 2, half k % 2
+        return addhf(k < 2 ? rt.x : rt.y, k & 1, c[dn]);
+    }
+    if (dn < 0) {
+        const int k = dn + 4;  // left half k
+        return addhf(k < 2 ? lf.x : lf.y, k & 1, c[up]);
+    }
+    return c[up] + c[dn];
+}
+
+template <int TX, int TY, int S, int AUX, int PHASE, int UNR>
 __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, AUX>::MINB)
     pencil_f16_kernel(const __grid_constant__ CUtensorMap pmap,
                       const __grid_constant__ CUtensorMap qmap,
@@ -245,27 +264,35 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
             if (p + S < nplanes) issue_plane(p + S);
     }
 
-    for (int i0 = 0; i0 < nint && !abort_run; i0 += 4) {
+    // The plane loop is unrolled by UNR (4 or 8).  i0 is a multiple of 4 and so
+    // is S: the fed plane's stage is a block base + u, wrapping at most once
+    // (UNR = 8), and its phase is a block constant or flips with the wrap; the aux
+    // ring (AUX | 4) has compile-time stages and a block-constant phase.
+    static_assert(UNR == 4 || UNR == 8, "unroll");
+    static_assert(UNR == 4 || S == 8, "an unroll of 8 needs an 8-stage ring");
+    for (int i0 = 0; i0 < nint && !abort_run; i0 += UNR) {
+        const int cbase = (i0 + 4) % S, fbase = (i0 + 8) % S;
+        const uint32_t fpar = ((i0 + 8) / S) & 1u, apar = (i0 / AUX) & 1u;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < UNR; ++u) {
             const int i = i0 + u;
             if (i < nint && !abort_run) {
                 // Centre plane i + 4 (slot u); it was waited for when it was fed.
-                const uint16_t* pc = sm + ((i + 4) % S) * P::PLANE + soff;
-                float2 xv[8];  // x window halves [4 left | 8 own | 4 right] as 8 pairs
-                {
-                    const uint2 lf = lds64(pc - 4);
-                    const uint2 rt = lds64(pc + 8);
-                    const uint4 own = hq[u];
-                    const uint32_t win[8] = {lf.x, lf.y, own.x, own.y, own.z, own.w, rt.x, rt.y};
+                const int cst = (cbase + u) % S, fst = (fbase + u) % S;
+                const uint32_t fph = fpar ^ (fbase + u >= S ? 1u : 0u);
+                const uint16_t* pc = sm + cst * P::PLANE + soff;
+                // x window: 4 halves left and right of the chunk stay FP16; the
+                // own 8 points (the centre) are converted once.
+                const uint2 lf = lds64(pc - 4);
+                const uint2 rt = lds64(pc + 8);
+                float2 cv[4];
 #pragma unroll
-                    for (int w = 0; w < 8; ++w) xv[w] = h2f2(win[w]);
-                }
-                {  // feed: plane i + 8 (z + 4) replaces the centre in slot u
-                    const int jf = i + 8;
-                    if (!mbar_wait(&full[jf % S], (jf / S) & 1)) bad = true;
-                    hq[u] = lds128h(sm + (jf % S) * P::PLANE + soff);
-                }
+                for (int h = 0; h < 4; ++h) cv[h] = h2f2(get_word(hq[u % 4], h));
+                const float cf[8] = {cv[0].x, cv[0].y, cv[1].x, cv[1].y,
+                                     cv[2].x, cv[2].y, cv[3].x, cv[3].y};
+                // feed: plane i + 8 (z + 4) replaces the centre in slot u
+                if (!mbar_wait(&full[fst], fph)) bad = true;
+                hq[u % 4] = lds128h(sm + fst * P::PLANE + soff);
                 uint4 yu[R], yd[R];  // staged rows y +- d of the centre plane
 #pragma unroll
                 for (int d = 1; d <= R; ++d) {
@@ -277,13 +304,18 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
                 float2 lap[4];
 #pragma unroll
                 for (int h = 0; h < 4; ++h) {
-                    const float2 c = xv[2 + h];
+                    const float2 c = cv[h];
                     float2 txy = mul2(cxy2, c);
                     float2 tz = mul2(az2[0], addhf2(get_word(hq[(u + 1) % 4], h),
                                                     dq[(u + 3) % 4][h]));
 #pragma unroll
                     for (int r = 1; r <= R; ++r) {
-                        txy = fma2(ax2[r - 1], xsum(xv, h, r), txy);
+                        // an aligned pair of own points (even r) adds as one pair
+                        const bool own2 = r % 2 == 0 && 2 * h - r >= 0 && 2 * h + 1 + r <= 7;
+                        const float2 sx = own2 ? add2(cv[h + r / 2], cv[h - r / 2])
+                                               : make_float2(xsum1(cf, lf, rt, 2 * h, r),
+                                                             xsum1(cf, lf, rt, 2 * h + 1, r));
+                        txy = fma2(ax2[r - 1], sx, txy);
                         txy = fma2(ay2[r - 1],
                                    addhf2(get_word(yu[r - 1], h), h2f2(get_word(yd[r - 1], h))),
                                    txy);
@@ -298,16 +330,16 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
                 }
                 // plane z - 4 is no longer needed: its slot takes the centre (z).
 #pragma unroll
-                for (int h = 0; h < 4; ++h) dq[u][h] = xv[2 + h];
+                for (int h = 0; h < 4; ++h) dq[u % 4][h] = cv[h];
 
-                if (!mbar_wait(&auxf[i % AUX], (i / AUX) & 1)) bad = true;
-                const uint16_t* st = aux + (i % AUX) * 2 * P::TILE + aoff;
+                if (!mbar_wait(&auxf[u % AUX], apar ^ ((u / AUX) & 1u))) bad = true;
+                const uint16_t* st = aux + (u % AUX) * 2 * P::TILE + aoff;
                 const uint4 qv = lds128h(st);
                 const uint4 kv = lds128h(st + P::TILE);
                 float o[8];
 #pragma unroll
                 for (int h = 0; h < 4; ++h) {
-                    const float2 c = xv[2 + h];
+                    const float2 c = cv[h];
                     const float2 pq = h2f2(get_word(qv, h));
                     const uint32_t kw = get_word(kv, h);
                     const float2 kk = make_float2(__uint_as_float(kw << 16),
@@ -371,21 +403,21 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
 using LaunchFnH = cudaError_t (*)(const PencilMaps&, const F16Args&, unsigned, int, cudaStream_t);
 using ResidentFnH = int (*)();
 
-template <int TX, int TY, int S, int AUX>
+template <int TX, int TY, int S, int AUX, int UNR>
 int resident_f16() {
     using P = ShapeH<TX, TY, S, AUX>;
     static int cached[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (cached[dev & 63] > 0) return cached[dev & 63];
-    auto kern = pencil_f16_kernel<TX, TY, S, AUX, 0>;
+    auto kern = pencil_f16_kernel<TX, TY, S, AUX, 0, UNR>;
     const int smem = static_cast<int>(P::SMEM);
     int n = 0;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) ==
             cudaSuccess &&
-        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, S, AUX, 1>,
+        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, S, AUX, 1, UNR>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
-        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, S, AUX, 2>,
+        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, S, AUX, 2, UNR>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, P::NT, P::SMEM) == cudaSuccess &&
         n > 0) {
@@ -396,20 +428,20 @@ int resident_f16() {
     return std::max(1, std::min(int((228u * 1024u) / (P::SMEM + 1024u)), 65536 / (P::NT * 128)));
 }
 
-template <int TX, int TY, int S, int AUX>
+template <int TX, int TY, int S, int AUX, int UNR>
 cudaError_t launch_f16(const PencilMaps& m, const F16Args& a, unsigned ctas, int phase,
                        cudaStream_t stream) {
     using P = ShapeH<TX, TY, S, AUX>;
-    resident_f16<TX, TY, S, AUX>();  // sets the attributes once per device
+    resident_f16<TX, TY, S, AUX, UNR>();  // sets the attributes once per device
     if (phase == 1)
-        pencil_f16_kernel<TX, TY, S, AUX, 1><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
-                                                                                m.vel2, a);
+        pencil_f16_kernel<TX, TY, S, AUX, 1, UNR><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
+                                                                                     m.vel2, a);
     else if (phase == 2)
-        pencil_f16_kernel<TX, TY, S, AUX, 2><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
-                                                                                m.vel2, a);
+        pencil_f16_kernel<TX, TY, S, AUX, 2, UNR><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
+                                                                                     m.vel2, a);
     else
-        pencil_f16_kernel<TX, TY, S, AUX, 0><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
-                                                                                m.vel2, a);
+        pencil_f16_kernel<TX, TY, S, AUX, 0, UNR><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
+                                                                                     m.vel2, a);
     return cudaGetLastError();
 }
 
@@ -420,16 +452,22 @@ struct VariantH {
     ResidentFnH resident;
 };
 
-#define SB200_VARIANT_H(TX, TY, S, AUX, NAME) \
-    VariantH { TX, TY, S, AUX, NAME, &launch_f16<TX, TY, S, AUX>, &resident_f16<TX, TY, S, AUX> }
+#define SB200_VARIANT_H(TX, TY, S, AUX, UNR, NAME)                                         \
+    VariantH {                                                                               \
+        TX, TY, S, AUX, NAME, &launch_f16<TX, TY, S, AUX, UNR>,                             \
+            &resident_f16<TX, TY, S, AUX, UNR>                                               \
+    }
 
+// "_u8": the plane loop unrolled by 8 instead of 4.
 const VariantH kF16[] = {
-    SB200_VARIANT_H(64, 16, 8, 4, "h64x16_s8_a4"),
-    SB200_VARIANT_H(64, 32, 8, 4, "h64x32_s8_a4"),
-    SB200_VARIANT_H(128, 16, 8, 4, "h128x16_s8_a4"),
-    SB200_VARIANT_H(64, 8, 8, 4, "h64x8_s8_a4"),
-    SB200_VARIANT_H(32, 16, 8, 4, "h32x16_s8_a4"),
-    SB200_VARIANT_H(64, 16, 12, 4, "h64x16_s12_a4"),
+    SB200_VARIANT_H(64, 16, 8, 4, 4, "h64x16_s8_a4"),
+    SB200_VARIANT_H(64, 32, 8, 4, 4, "h64x32_s8_a4"),
+    SB200_VARIANT_H(128, 16, 8, 4, 4, "h128x16_s8_a4"),
+    SB200_VARIANT_H(64, 8, 8, 4, 4, "h64x8_s8_a4"),
+    SB200_VARIANT_H(32, 16, 8, 4, 4, "h32x16_s8_a4"),
+    SB200_VARIANT_H(64, 16, 8, 4, 8, "h64x16_s8_a4_u8"),
+    SB200_VARIANT_H(64, 32, 8, 4, 8, "h64x32_s8_a4_u8"),
+    SB200_VARIANT_H(128, 16, 8, 4, 8, "h128x16_s8_a4_u8"),
 };
 constexpr int kNumF16 = sizeof(kF16) / sizeof(kF16[0]);
 
