@@ -55,7 +55,7 @@ def args_():
     ap.add_argument("--zchunks", type=int, default=1)
     ap.add_argument("--no-secondary", action="store_true",
                     help="skip the heat / FP16 / batch / learned measurements")
-    ap.add_argument("--kernel", choices=["acoustic", "heat", "fp16", "batch", "mlp"],
+    ap.add_argument("--kernel", choices=["acoustic", "heat", "fp16", "batch", "mlp", "learned"],
                     help="run only a small case of one kernel (for profilers) and print its time")
     return ap.parse_args()
 
@@ -644,7 +644,7 @@ def run_kernel_probe(a):
     gen = torch.Generator(device="cuda")
     gen.manual_seed(SEED)
     e0, e1 = _events()
-    if a.kernel in ("acoustic", "fp16", "heat", "mlp"):
+    if a.kernel in ("acoustic", "fp16", "heat", "mlp", "learned"):
         g, vel2, vmax, src = workload(n)
         v = torch.from_numpy(vel2).cuda()
         p = torch.randn(g.shape, generator=gen, device="cuda") * 0.1
@@ -671,6 +671,11 @@ def run_kernel_probe(a):
         m.output_scale = 1e-5
         out = torch.zeros_like(p)
         f = lambda: m.correct(p, v, out, g)  # noqa: E731
+    elif a.kernel == "learned":
+        m = sb.Mlp(seed=1)
+        m.output_scale = 1e-5
+        q = p * 0.99
+        f = lambda: m.learned_step(p, q, v, g)  # noqa: E731
     else:  # batch: 12 shots with extents n/2..n in steps of 8
         rng = np.random.default_rng(SEED)
         shots = []

@@ -355,6 +355,15 @@ int sb200_mlp_train_step(void* handle, const uint16_t* X, const float* t, int64_
  * sb200_mlp_set_kernel selected the mma.sync kernel. */
 int sb200_mlp_correct(void* handle, const float* p, const float* vel2, float* p_next,
                       const sb200_grid* grid, void* stream);
+/* One learned coarse step in one fused launch: p_prev_next <- acoustic step of
+ * (p, p_prev_next, vel2) + s * c * MLP(features of p), in place over p_prev (no
+ * source term: inject it afterwards).  Bit for bit sb200_wave_step_f32 followed
+ * by sb200_mlp_correct (tcgen05).  Needs nx % 4 == 0 and 16-byte aligned fields
+ * (SB200_ERR_UNSUPPORTED otherwise); p_prev_next must not alias p.  After a
+ * train_step the first call copies the parameters to the host (synchronising
+ * the stream). */
+int sb200_mlp_learned_step(void* handle, const float* p, float* p_prev_next, const float* vel2,
+                           const sb200_grid* grid, void* stream);
 /* Correction kernel of the handle: 0 = tcgen05 (default), 1 = mma.sync. */
 int sb200_mlp_set_kernel(void* handle, int kernel);
 /* Training rows at n cells (device int64 flat indices, interior only):

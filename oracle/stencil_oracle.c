@@ -311,19 +311,29 @@ float oracle_mlp_features(const float* p, const float* vel2, int64_t nx, int64_t
         if (r) v[k++] = p[c + r * sy];
     for (int r = -4; r <= 4; ++r)
         if (r) v[k++] = p[c + r * sz];
+    float m = 0.f;
+    for (int j = 0; j < 25; ++j) m = fabsf(v[j]) > m ? fabsf(v[j]) : m;
+    /* s: the smallest power of two above m (0 for m = 0), from m's exponent
+     * field (subnormal m counts as 2^-126; clamped below 2^126) */
     float s = 0.f;
-    for (int j = 0; j < 25; ++j) s = fabsf(v[j]) > s ? fabsf(v[j]) : s;
+    if (m > 0.f) {
+        uint32_t e = f32_bits(m) & 0x7f800000u;
+        if (e < 0x00800000u) e = 0x00800000u;
+        if (e > 0x7e000000u) e = 0x7e000000u;
+        s = bits_f32(e + 0x00800000u);
+    }
     const float inv = s > 0.f ? 1.f / s : 0.f;
-    /* difference basis: p_c, then (p_+r - p_-r) and (p_+r + p_-r - 2 p_c) per axis
-     * and radius, all / s; v[1 + 8a + k] holds axis a's offset k - 4 (k < 4) or
-     * k - 3 (k >= 4) */
-    row[0] = oracle_f32_to_bf16(v[0] * inv);
+    /* difference basis: per axis a and radius r the pair (p_+r - p_-r,
+     * p_+r + p_-r - 2 p_c) at features 2k, 2k + 1 (k = 4a + r - 1), then p_c, all
+     * / s; v[1 + 8a + k] holds axis a's offset k - 4 (k < 4) or k - 3 (k >= 4) */
     for (int a = 0; a < 3; ++a)
         for (int r = 1; r <= 4; ++r) {
             const float up = v[1 + 8 * a + 3 + r], dn = v[1 + 8 * a + 4 - r];
-            row[1 + 4 * a + r - 1] = oracle_f32_to_bf16((up - dn) * inv);
-            row[13 + 4 * a + r - 1] = oracle_f32_to_bf16(((up + dn) - 2.f * v[0]) * inv);
+            const int k = 4 * a + r - 1;
+            row[2 * k] = oracle_f32_to_bf16((up - dn) * inv);
+            row[2 * k + 1] = oracle_f32_to_bf16(((up + dn) - 2.f * v[0]) * inv);
         }
+    row[24] = oracle_f32_to_bf16(v[0] * inv);
     row[25] = oracle_f32_to_bf16(sqrtf(vel2[c]) * dt_over_dx);
     for (int j = 26; j < 32; ++j) row[j] = 0;
     return s;

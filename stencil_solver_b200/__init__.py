@@ -185,6 +185,7 @@ _SIGNATURES = {
     "sb200_mlp_train_step": ([C.c_void_p] * 3 + [C.c_int64, C.c_float, C.c_void_p, C.c_void_p],
                              C.c_int),
     "sb200_mlp_correct": ([C.c_void_p] * 4 + [C.POINTER(sb200_grid), C.c_void_p], C.c_int),
+    "sb200_mlp_learned_step": ([C.c_void_p] * 4 + [C.POINTER(sb200_grid), C.c_void_p], C.c_int),
     "sb200_mlp_samples": ([C.c_void_p] * 4 + [C.POINTER(sb200_grid), C.c_void_p, C.c_int64,
                                                C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "sb200_add_box": ([C.c_void_p, C.POINTER(sb200_grid)] + [C.c_int] * 6 +
@@ -679,6 +680,12 @@ class Mlp:
     def correct(self, p, vel2, p_next, grid: Grid, stream=None) -> None:
         _check(lib().sb200_mlp_correct(self._h, _ptr(p), _ptr(vel2), _ptr(p_next), _g(grid),
                                         _stream(stream)))
+
+    def learned_step(self, p, p_prev_next, vel2, grid: Grid, stream=None) -> None:
+        """p_prev_next <- acoustic step of p + the learned correction, in one fused
+        launch (no source term); the same bits as wave_step then correct."""
+        _check(lib().sb200_mlp_learned_step(self._h, _ptr(p), _ptr(p_prev_next), _ptr(vel2),
+                                             _g(grid), _stream(stream)))
 
 
 def mlp_samples(p, vel2, p_true, p_plain, grid: Grid, cells, X, t, stream=None) -> None:

@@ -68,6 +68,28 @@ struct PencilBoxes {
 int pencil_f32_variant_count(bool heat);
 const char* pencil_f32_variant_name(bool heat, int v);
 PencilBoxes pencil_f32_boxes(bool heat, int v);
+struct Weights;  // sb200_common.cuh
+
+// Network of the fused learned coarse step (learned_step.cu): BF16 W1, W2 on the
+// device, biases and w3 by value, the output scale c.
+struct LearnedNet {
+    const uint16_t* w1b = nullptr;
+    const uint16_t* w2b = nullptr;
+    float b1[32] = {}, b2[32] = {}, w3[32] = {};
+    float b3 = 0.f;
+    float out_scale = 1.f;
+};
+// Boxes of its tensor maps, resident CTAs per SM, and the launch: p_next =
+// acoustic step of p + learned correction, in place over p_prev.
+PencilBoxes learned_step_boxes();
+int learned_step_resident();
+cudaError_t launch_learned_step(const PencilMaps& maps, float* next, const GridDesc& g,
+                                const LearnedNet& net, int sms, int* err, cudaStream_t stream);
+
+// Laplacian weights of the pencil kernels (C_r / dx_a^2, times `scale`: dt^2 for
+// the acoustic step, alpha dt for heat), rounded once from double.
+Weights fold_weights(const GridDesc& g, float scale);
+
 cudaError_t launch_wave_pencil_f32(const PencilMaps& maps, const float* prev, const float* vel2,
                                    float* next, const GridDesc& g, const SourceDesc& src,
                                    const PencilConfig& cfg, int* err, cudaStream_t stream);

@@ -1,0 +1,482 @@
+// Fused learned coarse step for sm_100a: the FP32 acoustic leapfrog and the
+// learned correction of the same plane in one z-marching pass,
+//   p_next = [2 p - p_prev + vel2 dt^2 lap(p)] + s c MLP(features of p),
+// bit for bit the composition of the FP32 pencil step and the tcgen05
+// correction kernel (sb200_wave_step_f32, then sb200_mlp_correct).  No
+// reference counterpart: the correction is this project's learned layer.
+//
+// Work unit: a CTA owns a 32 x 16 tile of interior columns and marches z, as the
+// FP32 pencil kernel does: planes of p (with the 4-cell halo) arrive by TMA in
+// a 6-stage ring, the p_prev / vel2 tiles in a 3-stage ring, z neighbours come
+// from a 9-deep register queue (shifted one slot per plane).  Each thread owns 4
+// consecutive x of one row.  Per plane:
+//   1. the stencil (the pencil kernel's arithmetic and order) and the 26
+//      features of each of the thread's 4 points: the differences are rounded to
+//      BF16 unscaled and 1/s is applied to the first layer's accumulator (s is a
+//      power of two, so this is exact);
+//   2. the feature row of the thread's point e goes to row `tid` of A tile e
+//      (4 tiles x 128 rows, K-major BF16), so TMEM lane `tid` of tile e's
+//      accumulator is this thread's own point: the correction lands in the
+//      thread that holds the stencil value and one store writes p_next;
+//   3. one thread issues tcgen05.mma (M = 128, N = 32, K = 16: 2 per tile and
+//      layer) into TMEM columns 32 e, commits to an mbarrier that every thread
+//      waits on (two CTA barriers per plane in all); the epilogue of
+//      layer 1 (1/s, bias, ReLU, BF16) writes layer 2's A tiles over the
+//      features, layer 2 overwrites the accumulators, its epilogue (bias, ReLU,
+//      w3 dot product) finishes the correction.
+// A plane whose points are all exactly zero skips the network (its correction
+// is exactly zero).  Every wait is bounded; on timeout the CTA records the
+// error, lets its copies and MMAs land, releases TMEM and exits.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "kernels.h"
+#include "mlp_device.cuh"
+#include "sb200_common.cuh"
+
+namespace sb200 {
+
+namespace {
+
+using namespace mlp;
+
+constexpr int LTX = 32, LTY = 16;  // tile of columns
+constexpr int LTPR = LTX / 4;      // threads per row (4 x each)
+constexpr int LNT = LTPR * LTY;    // 128 threads: one per A-tile row
+constexpr int LS = 6, LAUX = 3;    // staged planes of p; p_prev / vel2 stages
+static_assert(LS >= 6 && LS <= 8, "planes z..z+4 staged, plus one in flight");
+constexpr int LSX = LTX + 2 * R, LSY = LTY + 2 * R;
+constexpr uint32_t LPLANE_BYTES = LSX * LSY * 4u;
+constexpr int LPLANE = int(((LPLANE_BYTES + 127u) / 128u) * 32u);  // stride, floats
+constexpr uint32_t LTILE_BYTES = LTX * LTY * 4u;
+constexpr int LTILE = int(LTILE_BYTES / 4u);
+constexpr uint32_t kLCols = 128;  // TMEM: tile e's 32 accumulator columns at 32 e
+constexpr int kTileA = 128 * 64;  // one A tile: 128 rows x 32 BF16
+// Shared memory from a 1024-byte aligned base: A tiles, W1, W2, staged planes, aux.
+constexpr int kOffW1 = 4 * kTileA, kOffW2 = kOffW1 + H * F * 2, kOffP = kOffW2 + H * H * 2;
+constexpr int kOffAux = kOffP + LS * LPLANE * 4;
+constexpr int kLSmem = kOffAux + LAUX * 2 * LTILE * 4 + 1024;
+static_assert(LNT == 128, "one thread per TMEM lane of an M = 128 tile");
+
+struct LearnedArgs {
+    float* next;  // p_next, in place over p_prev (read through qmap)
+    int nx, ny, nz;
+    int64_t sy, sz;
+    int tiles_x, tiles_y, zlen;
+    Weights w;         // Laplacian weights x dt^2 (the FP32 pencil kernel's)
+    float dt_over_dx;  // Courant feature: sqrt(vel2) dt / min(dx, dy, dz)
+    float out_scale;   // c
+    const uint16_t* w1b;  // BF16 W1, W2 (out x in)
+    const uint16_t* w2b;
+    float b1[H], b2[H], w3[H];
+    float b3;
+    int* err;
+};
+
+__device__ __forceinline__ float lane_of(const float4& v, int e) {
+    return e == 0 ? v.x : (e == 1 ? v.y : (e == 2 ? v.z : v.w));
+}
+
+__global__ void __launch_bounds__(LNT, 3)
+    learned_step_kernel(const __grid_constant__ CUtensorMap pmap,
+                        const __grid_constant__ CUtensorMap qmap,
+                        const __grid_constant__ CUtensorMap vmap, const LearnedArgs a) {
+    extern __shared__ unsigned char dyn[];
+    __shared__ __align__(8) uint64_t full[LS];
+    __shared__ __align__(8) uint64_t auxf[LAUX];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_flag;  // a bounded wait gave up
+    unsigned char* base = smem_align<1024>(dyn);
+    unsigned char* sA = base;
+    unsigned char* sW1 = base + kOffW1;
+    unsigned char* sW2 = base + kOffW2;
+    float* sm = reinterpret_cast<float*>(base + kOffP);
+    float* aux = reinterpret_cast<float*>(base + kOffAux);
+
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int lx = tid % LTPR, ly = tid / LTPR;
+    int b = blockIdx.x;
+    const int tx = b % a.tiles_x;
+    b /= a.tiles_x;
+    const int ty = b % a.tiles_y;
+    b /= a.tiles_y;
+    const int x0 = R + tx * LTX, y0 = R + ty * LTY;
+    const int zb = R + b * a.zlen;
+    const int ze = min(zb + a.zlen, a.nz - R);
+    const int nint = ze - zb, nplanes = nint + 2 * R;
+
+    for (int i = tid; i < H * F; i += LNT) {
+        *reinterpret_cast<uint16_t*>(sW1 + core_off(i / F, i % F)) = a.w1b[i];
+        *reinterpret_cast<uint16_t*>(sW2 + core_off(i / H, i % H)) = a.w2b[i];
+    }
+    if (tid == 0) {
+        prefetch_tmap(&pmap);
+        prefetch_tmap(&qmap);
+        prefetch_tmap(&vmap);
+#pragma unroll
+        for (int s = 0; s < LS; ++s) mbar_init(&full[s], 1);
+#pragma unroll
+        for (int s = 0; s < LAUX; ++s) mbar_init(&auxf[s], 1);
+        mbar_init(&mbar, 1);
+        fence_barrier_init();
+        s_flag = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&s_tmem)),
+                     "r"(kLCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const uint32_t lane_base = tmem + (uint32_t(32 * warp) << 16);
+    const uint32_t aA = smem_u32(sA), aW1 = smem_u32(sW1), aW2 = smem_u32(sW2);
+
+    int issued_hi = -1, aux_issued_hi = -1;
+    auto plane = [&](int j) -> const float* { return sm + (j % LS) * LPLANE; };
+    auto issue_plane = [&](int j) {  // thread 0 only
+        mbar_arrive_expect_tx(&full[j % LS], LPLANE_BYTES);
+        tma_load_3d(sm + (j % LS) * LPLANE, &pmap, &full[j % LS], x0 - R, y0 - R, zb - R + j);
+        issued_hi = j;
+    };
+    auto issue_aux = [&](int it) {  // thread 0 only
+        float* st = aux + (it % LAUX) * 2 * LTILE;
+        mbar_arrive_expect_tx(&auxf[it % LAUX], 2 * LTILE_BYTES);
+        tma_load_3d(st, &qmap, &auxf[it % LAUX], x0, y0, zb + it);
+        tma_load_3d(st + LTILE, &vmap, &auxf[it % LAUX], x0, y0, zb + it);
+        aux_issued_hi = it;
+    };
+    if (tid == 0) {
+        for (int s = 0; s < LS && s < nplanes; ++s) issue_plane(s);
+        for (int it = 0; it < LAUX && it < nint; ++it) issue_aux(it);
+    }
+
+    const int gx = x0 + 4 * lx, gy = y0 + ly;
+    const bool rin = gx < a.nx - R && gy < a.ny - R;
+    const int soff = (ly + R) * LSX + 4 * lx + R;
+    const int aoff = ly * LTX + 4 * lx;
+    int64_t goff = static_cast<int64_t>(zb) * a.sz + static_cast<int64_t>(gy) * a.sy + gx;
+
+
+    float4 q[9];  // planes z-4 .. z+4: slot k holds plane z - 4 + k
+    bool bad = false;
+    // Start-up: planes 0..5 are staged; 0..3 only feed the queue, so their stages
+    // take planes 6..9 at once; 4..7 stay staged as the first centre planes.
+#pragma unroll
+    for (int jj = 0; jj < LS; ++jj) {
+        if (!mbar_wait(&full[jj], 0)) bad = true;
+        q[jj] = lds128(plane(jj) + soff);
+    }
+    bool abort_run = __syncthreads_or(bad) != 0;
+    if (!abort_run && tid == 0) {
+#pragma unroll
+        for (int jj = 0; jj < R; ++jj)
+            if (jj + LS < nplanes) issue_plane(jj + LS);
+    }
+#pragma unroll
+    for (int jj = LS; jj < 8; ++jj) {
+        if (!mbar_wait(&full[jj % LS], (jj / LS) & 1)) bad = true;
+        q[jj] = lds128(plane(jj) + soff);
+    }
+    uint32_t ncommit = 0;    // MMA commits issued (uniform): the mbarrier's phases
+    uint32_t completed = 0;  // thread 0: commits seen complete
+    auto wait_mma = [&]() {
+        const bool ok = mbar_wait(&mbar, (ncommit - 1u) & 1u);
+        tc_fence_after();
+        if (!ok) bad = true;
+        if (ok && tid == 0) completed = ncommit;
+    };
+
+    // One plane per iteration; the queue shifts by one slot at the end (the body
+    // is too large to unroll 9 times and still fit the instruction cache).
+    for (int i = 0; i < nint && !abort_run; ++i) {
+        {
+            const int jf = i + 8;  // queue feed: plane z + 4
+            if (!mbar_wait(&full[jf % LS], (jf / LS) & 1)) bad = true;
+            q[8] = lds128(plane(jf) + soff);
+        }
+        const float* pc = plane(i + 4) + soff;
+        const float4 c = q[4];
+        // Weights from the kernel parameters (constant bank) each plane, so they
+        // hold no registers through the network epilogues.
+        float2 ax2[R], ay2[R], az2[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            ax2[r] = dup2(a.w.ax[r]);
+            ay2[r] = dup2(a.w.ay[r]);
+            az2[r] = dup2(a.w.az[r]);
+        }
+        const float2 cx2 = dup2(a.w.cx), cy2 = dup2(a.w.cy), cz2 = dup2(a.w.cz),
+                     neg1 = dup2(-1.f), neg2 = dup2(-2.f);
+
+        // Stencil: the FP32 pencil kernel's arithmetic in its order (y per row
+        // from zero, farthest rows first; x and z pair sums; (x + y) + z).
+        float2 ya[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+#pragma unroll
+        for (int k = -R; k <= R; ++k) {
+            if (k == 0) continue;
+            const float4 row = lds128(pc + k * LSX);
+            const int d = k > 0 ? k : -k;
+            ya[0] = fma2(ay2[d - 1], pair_of(row, 0), ya[0]);
+            ya[1] = fma2(ay2[d - 1], pair_of(row, 1), ya[1]);
+        }
+        const float4 lf = lds128(pc - 4);
+        const float4 rt = lds128(pc + 4);
+        const float win[12] = {lf.x, lf.y, lf.z, lf.w, c.x, c.y, c.z, c.w, rt.x, rt.y, rt.z, rt.w};
+        float2 lap[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const float2 ce = pair_of(c, h);
+            float2 tz = mul2(cz2, ce);
+            float2 tx = mul2(cx2, ce);
+#pragma unroll
+            for (int r = 1; r <= R; ++r) {
+                tz = fma2(az2[r - 1], add2(pair_of(q[4 + r], h), pair_of(q[4 - r], h)), tz);
+                const int e = 4 + 2 * h;
+                const float2 s = make_float2(win[e + r] + win[e - r], win[e + 1 + r] + win[e + 1 - r]);
+                tx = fma2(ax2[r - 1], s, tx);
+            }
+            const float2 tyv = fma2(cy2, ce, ya[h]);
+            lap[h] = add2(add2(tx, tyv), tz);
+        }
+        if (!mbar_wait(&auxf[i % LAUX], (i / LAUX) & 1)) bad = true;
+        const float* st = aux + (i % LAUX) * 2 * LTILE + aoff;
+        const float4 pv = lds128(st);
+        const float4 vv = lds128(st + LTILE);
+        float4 o;
+        {
+            const float2 t0 = fma2(neg1, pair_of(pv, 0), add2(pair_of(c, 0), pair_of(c, 0)));
+            const float2 t1 = fma2(neg1, pair_of(pv, 1), add2(pair_of(c, 1), pair_of(c, 1)));
+            const float2 o0 = fma2(pair_of(vv, 0), lap[0], t0);
+            const float2 o1 = fma2(pair_of(vv, 1), lap[1], t1);
+            o = make_float4(o0.x, o0.y, o1.x, o1.y);
+        }
+
+        // Features, one pair of points at a time: per axis and radius the word
+        // (up - dn, (up + dn) - 2c), unscaled, packed as soon as it is computed;
+        // the star's largest magnitude gives s, and the last word is (c, Courant
+        // number x s).  Point e's row is row tid of A tile e.
+        float inv[4], sc[4];
+        bool act = false;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const float2 ce = pair_of(c, h);
+            float2 mx = make_float2(fabsf(ce.x), fabsf(ce.y));
+            uint32_t row0[16], row1[16];  // points 2h, 2h + 1
+#pragma unroll
+            for (int a3 = 0; a3 < 3; ++a3)
+#pragma unroll
+                for (int r = 1; r <= R; ++r) {
+                    float2 up, dn;
+                    if (a3 == 0) {
+                        const int e = 4 + 2 * h;
+                        up = make_float2(win[e + r], win[e + 1 + r]);
+                        dn = make_float2(win[e - r], win[e + 1 - r]);
+                    } else if (a3 == 1) {
+                        up = *reinterpret_cast<const float2*>(pc + r * LSX + 2 * h);
+                        dn = *reinterpret_cast<const float2*>(pc - r * LSX + 2 * h);
+                    } else {
+                        up = pair_of(q[4 + r], h);
+                        dn = pair_of(q[4 - r], h);
+                    }
+                    const float2 dif = fma2(neg1, dn, up);
+                    const float2 sec = fma2(neg2, ce, add2(up, dn));
+                    const int k = 4 * a3 + r - 1;
+                    row0[k] = pack_bf2(dif.x, sec.x);
+                    row1[k] = pack_bf2(dif.y, sec.y);
+                    mx.x = fmaxf(mx.x, fmaxf(fabsf(up.x), fabsf(dn.x)));
+                    mx.y = fmaxf(mx.y, fmaxf(fabsf(up.y), fabsf(dn.y)));
+                }
+#pragma unroll
+            for (int l = 0; l < 2; ++l) {
+                const int e = 2 * h + l;
+                float s;
+                pow2_scale(rin ? (l ? mx.y : mx.x) : 0.f, s, inv[e]);
+                sc[e] = s * a.out_scale;
+                act = act || s > 0.f;
+                uint32_t(&row)[16] = l ? row1 : row0;
+                row[12] = pack_bf2(l ? ce.y : ce.x, (sqrtf(lane_of(vv, e)) * a.dt_over_dx) * s);
+                row[13] = row[14] = row[15] = 0u;
+                store_row(sA + e * kTileA, tid, row);
+            }
+        }
+        fence_async_smem();  // feature rows visible to the tensor cores
+        if (bad) s_flag = 1;
+        tc_fence_before();
+        const bool any = __syncthreads_or(act) != 0;
+        tc_fence_after();
+        abort_run = s_flag != 0;
+        if (!abort_run && tid == 0) {
+            // The staged plane z and the aux stage of this plane are free now.
+            if (i + 4 + LS < nplanes) issue_plane(i + 4 + LS);
+            if (i + LAUX < nint) issue_aux(i + LAUX);
+            if (any) {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    tc_mma(tmem + 32 * e, umma_desc(aA + e * kTileA), umma_desc(aW1), 0u);
+                    tc_mma(tmem + 32 * e, umma_desc(aA + e * kTileA + 256), umma_desc(aW1 + 256), 1u);
+                }
+                tc_commit(&mbar);
+            }
+        }
+        if (!abort_run && any) {
+            ++ncommit;
+            wait_mma();  // every thread waits for the layer-1 accumulators
+            // Layer 1 epilogue: h1 = relu(acc / s + b1) as BF16, over the features.
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                float d[32];
+                tc_ld32(lane_base + 32 * e, d);
+                const float2 iv = dup2(inv[e]);
+                uint32_t hw[16];
+#pragma unroll
+                for (int k = 0; k < 16; ++k) {
+                    const float2 t = fma2(make_float2(d[2 * k], d[2 * k + 1]), iv,
+                                          make_float2(a.b1[2 * k], a.b1[2 * k + 1]));
+                    hw[k] = relu_bf2(t.x, t.y);
+                }
+                store_row(sA + e * kTileA, tid, hw);
+            }
+            fence_async_smem();
+            tc_fence_before();
+            __syncthreads();
+            tc_fence_after();
+            if (tid == 0) {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    tc_mma(tmem + 32 * e, umma_desc(aA + e * kTileA), umma_desc(aW2), 0u);
+                    tc_mma(tmem + 32 * e, umma_desc(aA + e * kTileA + 256), umma_desc(aW2 + 256), 1u);
+                }
+                tc_commit(&mbar);
+            }
+            ++ncommit;
+            wait_mma();
+            // Layer 2 epilogue and the output layer, in the correction kernel's
+            // order; then p_next = stencil + s c y.
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                float d[32];
+                tc_ld32(lane_base + 32 * e, d);
+                float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int q4 = 0; q4 < 8; ++q4) {
+                    const float2 uu = add2(make_float2(d[4 * q4], d[4 * q4 + 1]),
+                                           make_float2(a.b2[4 * q4], a.b2[4 * q4 + 1]));
+                    const float2 vw = add2(make_float2(d[4 * q4 + 2], d[4 * q4 + 3]),
+                                           make_float2(a.b2[4 * q4 + 2], a.b2[4 * q4 + 3]));
+                    acc = fma2(make_float2(a.w3[4 * q4], a.w3[4 * q4 + 1]),
+                               make_float2(fmaxf(uu.x, 0.f), fmaxf(uu.y, 0.f)), acc);
+                    acc = fma2(make_float2(a.w3[4 * q4 + 2], a.w3[4 * q4 + 3]),
+                               make_float2(fmaxf(vw.x, 0.f), fmaxf(vw.y, 0.f)), acc);
+                }
+                const float yv = (acc.x + acc.y) + a.b3;
+                if (sc[e] > 0.f) {
+                    if (e == 0) o.x = fmaf(sc[e], yv, o.x);
+                    if (e == 1) o.y = fmaf(sc[e], yv, o.y);
+                    if (e == 2) o.z = fmaf(sc[e], yv, o.z);
+                    if (e == 3) o.w = fmaf(sc[e], yv, o.w);
+                }
+            }
+            tc_fence_before();
+        }
+        if (!bad && rin) stg_stream(a.next + goff, o);
+        goff += a.sz;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) q[k] = q[k + 1];
+    }
+
+    if (abort_run && tid == 0) {
+        record_error(a.err, kDevWaitTimeout);
+        // Let every copy and MMA still in flight land before shared memory and
+        // TMEM are released.
+        for (int jj = max(0, issued_hi - LS + 1); jj <= issued_hi; ++jj)
+            (void)mbar_wait(&full[jj % LS], (jj / LS) & 1);
+        for (int it = max(0, aux_issued_hi - LAUX + 1); it <= aux_issued_hi; ++it)
+            (void)mbar_wait(&auxf[it % LAUX], (it / LAUX) & 1);
+        for (uint32_t k = completed; k < ncommit; ++k) (void)mbar_wait(&mbar, k & 1u);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(kLCols)
+                     : "memory");
+}
+
+}  // namespace
+
+int learned_step_resident() {
+    static int cached[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cached[dev & 63] > 0) return cached[dev & 63];
+    int n = 0;
+    if (cudaFuncSetAttribute(learned_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kLSmem) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, learned_step_kernel, LNT, kLSmem) ==
+            cudaSuccess &&
+        n > 0) {
+        cached[dev & 63] = n;
+        return n;
+    }
+    cudaGetLastError();
+    return 1;
+}
+
+PencilBoxes learned_step_boxes() {
+    PencilBoxes b;
+    b.halo_x = LSX;
+    b.halo_y = LSY;
+    b.tile_x = LTX;
+    b.tile_y = LTY;
+    b.aux_tma = true;
+    return b;
+}
+
+cudaError_t launch_learned_step(const PencilMaps& maps, float* next, const GridDesc& g,
+                                const LearnedNet& net, int sms, int* err, cudaStream_t stream) {
+    if (!g.has_interior()) return cudaSuccess;
+    const int resident = learned_step_resident();
+    LearnedArgs a{};
+    a.next = next;
+    a.nx = static_cast<int>(g.nx);
+    a.ny = static_cast<int>(g.ny);
+    a.nz = static_cast<int>(g.nz);
+    a.sy = g.nx;
+    a.sz = g.nx * g.ny;
+    a.tiles_x = static_cast<int>((g.nx - 2 * R + LTX - 1) / LTX);
+    a.tiles_y = static_cast<int>((g.ny - 2 * R + LTY - 1) / LTY);
+    // z split: the smallest one that gives every resident CTA slot about four
+    // tiles' worth of work (each split re-reads 8 halo planes of p).
+    const int inz = static_cast<int>(g.nz - 2 * R);
+    const int64_t tiles = int64_t(a.tiles_x) * a.tiles_y;
+    const int64_t slots = int64_t(std::max(1, sms)) * std::max(1, resident);
+    int zc = static_cast<int>(std::min<int64_t>(16, std::max<int64_t>(1, (4 * slots + tiles - 1) / tiles)));
+    zc = std::min(zc, inz);
+    a.zlen = (inz + zc - 1) / zc;
+    const unsigned ctas =
+        static_cast<unsigned>(tiles * ((inz + a.zlen - 1) / a.zlen));
+    a.w = fold_weights(g, g.dt * g.dt);
+    a.dt_over_dx = g.dt / std::min(g.dx, std::min(g.dy, g.dz));
+    a.out_scale = net.out_scale;
+    a.w1b = net.w1b;
+    a.w2b = net.w2b;
+    for (int k = 0; k < H; ++k) {
+        a.b1[k] = net.b1[k];
+        a.b2[k] = net.b2[k];
+        a.w3[k] = net.w3[k];
+    }
+    a.b3 = net.b3;
+    a.err = err;
+    learned_step_kernel<<<ctas, LNT, kLSmem, stream>>>(maps.p, maps.prev, maps.vel2, a);
+    return cudaGetLastError();
+}
+
+}  // namespace sb200

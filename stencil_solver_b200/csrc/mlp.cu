@@ -6,9 +6,10 @@
 //   p_next[i] += s_i * c * MLP(f_i),   c a fixed output scale (the training
 // targets' RMS, so the network itself works on O(1) values),
 // where f_i is the 25-point star of p around i (in a difference basis, see
-// feature_row) divided by its largest magnitude s_i, plus the local Courant
-// number sqrt(vel2) dt / dx, padded to 32 features.  The correction is
-// positively homogeneous in p (scaling the field scales the correction).
+// feature_row in mlp_device.cuh) divided by s_i, the smallest power of two
+// above its largest magnitude, plus the local Courant number sqrt(vel2) dt / dx,
+// padded to 32 features.  The correction is positively homogeneous in p under
+// power-of-two scalings of the field.
 //
 // Parameters: FP32 masters [W1 (32x32, out x in; input columns 26..31 stay 0),
 // b1, W2 (32x32), b2, w3 (32), b3] and BF16 copies of W1, W2 and W2^T that the
@@ -34,33 +35,16 @@
 
 #include "dispatch.h"
 #include "kernels.h"
+#include "mlp_device.cuh"
 #include "sb200_common.cuh"
 #include "stencil_b200.h"
 
 namespace sb200 {
 namespace {
 
-constexpr int H = 32;    // hidden width
-constexpr int F = 32;    // padded input width
-constexpr int NIN = 26;  // real inputs
-constexpr int OFF_W1 = 0;
-constexpr int OFF_B1 = OFF_W1 + H * F;
-constexpr int OFF_W2 = OFF_B1 + H;
-constexpr int OFF_B2 = OFF_W2 + H * H;
-constexpr int OFF_W3 = OFF_B2 + H;
-constexpr int OFF_B3 = OFF_W3 + H;
-constexpr int NPARAM = OFF_B3 + 1;  // 2145
-constexpr int NSLOT = NPARAM + 1;   // + loss
-static_assert(NPARAM == SB200_MLP_NPARAM, "parameter count");
+using namespace mlp;
 
-__device__ __forceinline__ uint32_t pack_bf2(float lo, float hi) {
-    uint32_t r;
-    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
-    return r;
-}
-__device__ __forceinline__ uint16_t bf16_bits(float x) {
-    return static_cast<uint16_t>(pack_bf2(x, 0.f) & 0xffffu);
-}
+static_assert(NPARAM == SB200_MLP_NPARAM, "parameter count");
 
 __device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4],
                                          const uint32_t (&b)[2]) {
@@ -403,58 +387,6 @@ __global__ void mlp_bf16_kernel(const float* __restrict__ prm, uint16_t* __restr
 
 // ── features ──────────────────────────────────────────────────────────────────
 
-// The 25-point star of p around c (centre, then x-4..x-1, x+1..x+4, then y and
-// z likewise) and its largest magnitude.
-struct Star {
-    float v[25];
-    float s;
-};
-
-__device__ __forceinline__ void gather_star(Star& st, const float* __restrict__ p, int64_t c,
-                                            int64_t sy, int64_t sz) {
-    st.v[0] = p[c];
-    int k = 1;
-#pragma unroll
-    for (int r = -4; r <= 4; ++r)
-        if (r) st.v[k++] = p[c + r];
-#pragma unroll
-    for (int r = -4; r <= 4; ++r)
-        if (r) st.v[k++] = p[c + r * sy];
-#pragma unroll
-    for (int r = -4; r <= 4; ++r)
-        if (r) st.v[k++] = p[c + r * sz];
-    float m = 0.f;
-#pragma unroll
-    for (int j = 0; j < 25; ++j) m = fmaxf(m, fabsf(st.v[j]));
-    st.s = m;
-}
-
-// Feature row (32 BF16) of a star, in a difference basis computed in FP32
-// before the rounding: [p_c, (p_+r - p_-r) for axis x, y, z and r = 1..4,
-// (p_+r + p_-r - 2 p_c) likewise] / s, then the Courant number, then zeros.
-// The same information as the 25 values, but the small differences that the
-// scheme's error is made of survive the BF16 rounding.
-__device__ __forceinline__ void feature_row(uint32_t* row, const Star& st, float courant) {
-    const float inv = st.s > 0.f ? 1.f / st.s : 0.f;
-    const float c = st.v[0];
-    float f[26];
-    f[0] = c * inv;
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int r = 1; r <= 4; ++r) {
-            const float up = st.v[1 + 8 * a + 3 + r];  // +r: slot 4 + r - 1 of the axis' 8
-            const float dn = st.v[1 + 8 * a + 4 - r];  // -r: slot 4 - r
-            f[1 + 4 * a + (r - 1)] = (up - dn) * inv;
-            f[13 + 4 * a + (r - 1)] = ((up + dn) - 2.f * c) * inv;
-        }
-    f[25] = courant;
-#pragma unroll
-    for (int j = 0; j < 13; ++j) row[j] = pack_bf2(f[2 * j], f[2 * j + 1]);
-#pragma unroll
-    for (int j = 13; j < 16; ++j) row[j] = 0u;
-}
-
 __global__ void mlp_samples_kernel(const float* __restrict__ p, const float* __restrict__ vel2,
                                    const float* __restrict__ p_true,
                                    const float* __restrict__ p_plain, int64_t nx, int64_t ny,
@@ -576,88 +508,6 @@ constexpr uint32_t kTcCols = 64;  // TMEM columns: layer 1 in 0..31, layer 2 in 
 // most 8 CTAs then fit on one SM, 8 x 64 = 512 TMEM columns, so tcgen05.alloc
 // never waits for another CTA.
 constexpr int kTcSmem = 26 * 1024;
-constexpr uint32_t kTcIdesc = (1u << 4)                   // D: FP32
-                              | (1u << 7) | (1u << 10)   // A, B: BF16 (both K-major)
-                              | (uint32_t(32 >> 3) << 17)  // N = 32
-                              | (uint32_t(128 >> 4) << 24);  // M = 128
-
-// Byte offset of element (row, k) of a K-major BF16 operand in the no-swizzle
-// canonical layout: 8-row x 16-byte core matrices, the 4 K-chunks of a row
-// group 128 B apart (leading byte offset), row groups 512 B apart (stride byte
-// offset).  A K = 16 step starts 256 B further.
-__device__ __forceinline__ uint32_t core_off(int row, int k) {
-    return uint32_t((row >> 3) * 512 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
-}
-
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
-    return uint64_t((saddr >> 4) & 0x3FFFu)  // start address
-           | (uint64_t(128 >> 4) << 16)      // leading byte offset
-           | (uint64_t(512 >> 4) << 32)      // stride byte offset
-           | (uint64_t(1) << 46);            // descriptor version; no swizzle
-}
-
-__device__ __forceinline__ void tc_fence_before() {
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void fence_async_smem() {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
-                                       uint32_t accumulate) {
-    const uint32_t mask = 0;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
-        :
-        : "r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate), "r"(mask)
-        : "memory");
-}
-
-__device__ __forceinline__ void tc_commit(uint64_t* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                     smem_u32(bar))
-                 : "memory");
-}
-
-// 32 consecutive FP32 columns of this thread's TMEM lane.
-__device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
-    uint32_t r[32];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-        "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
-        "%28, %29, %30, %31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
-          "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
-          "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr)
-        : "memory");
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-__device__ __forceinline__ uint32_t relu_bf2(float lo, float hi) {
-    uint32_t r;
-    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
-    return r;
-}
-
-// One feature / activation row (16 words = 32 BF16) into a K-major operand tile.
-__device__ __forceinline__ void store_row(unsigned char* tile, int row, const uint32_t (&w)[16]) {
-#pragma unroll
-    for (int kc = 0; kc < 4; ++kc)
-        *reinterpret_cast<uint4*>(tile + core_off(row, 8 * kc)) =
-            make_uint4(w[4 * kc], w[4 * kc + 1], w[4 * kc + 2], w[4 * kc + 3]);
-}
-
-
 __global__ void __launch_bounds__(kTcThreads)
     mlp_correct_tc_kernel(const float* __restrict__ prm, const uint16_t* __restrict__ w1b,
                           const uint16_t* __restrict__ w2b, const float* __restrict__ p,
@@ -853,6 +703,10 @@ struct Mlp {
     int sms = 148;
     float out_scale = 1.f;  // the correction is s * out_scale * y
     int kernel = 0;         // correction kernel: 0 = tcgen05, 1 = mma.sync
+    // Host copy of the FP32 parameters for the fused step, which takes biases
+    // and w3 by value; stale after a device-side update (train_step).
+    std::vector<float> host;
+    bool host_valid = false;
 };
 
 int cuda_err(cudaError_t e, const char* where) {
@@ -930,6 +784,8 @@ int sb200_mlp_set_params(void* h, const float* params) {
         for (int i = NIN; i < F; ++i) w[OFF_W1 + o * F + i] = 0.f;  // padding inputs
     int rc = cuda_err(cudaMemcpy(m->prm, w.data(), NPARAM * 4, cudaMemcpyHostToDevice),
                       "sb200_mlp_set_params");
+    m->host = w;
+    m->host_valid = !rc;
     if (!rc) rc = cuda_err(cudaMemset(m->m1, 0, NPARAM * 4), "sb200_mlp_set_params");
     if (!rc) rc = cuda_err(cudaMemset(m->m2, 0, NPARAM * 4), "sb200_mlp_set_params");
     if (rc) return rc;
@@ -994,6 +850,7 @@ int sb200_mlp_train_step(void* h, const uint16_t* X, const float* t, int64_t n, 
     if (!(lr > 0.f)) return set_error(SB200_ERR_INVALID, "sb200_mlp_train_step: lr must be positive");
     if (int rc = sb200_mlp_gradients(h, X, t, n, m->grad, stream)) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    m->host_valid = false;
     m->adam_t += 1;
     const float b1 = 0.9f, b2 = 0.999f;
     const float c1 = 1.f - std::pow(b1, float(m->adam_t)), c2 = 1.f - std::pow(b2, float(m->adam_t));
@@ -1048,6 +905,64 @@ int sb200_mlp_correct(void* h, const float* p, const float* vel2, float* p_next,
         m->prm, m->w1b, m->w2b, p, vel2, p_next, static_cast<int>(grid->nx),
         static_cast<int>(grid->ny), static_cast<int>(grid->nz), grid->dt / dx, m->out_scale, err);
     return cuda_err(cudaGetLastError(), "sb200_mlp_correct");
+}
+
+int sb200_mlp_learned_step(void* h, const float* p, float* p_prev_next, const float* vel2,
+                           const sb200_grid* grid, void* stream) {
+    const char* where = "sb200_mlp_learned_step";
+    Mlp* m = static_cast<Mlp*>(h);
+    if (!m || !p || !p_prev_next || !vel2 || !grid)
+        return set_error(SB200_ERR_INVALID, std::string(where) + ": NULL argument");
+    if (p == p_prev_next)
+        return set_error(SB200_ERR_INVALID, std::string(where) + ": p_next must not alias p");
+    if (!(grid->dx > 0.f && grid->dy > 0.f && grid->dz > 0.f && grid->dt > 0.f) ||
+        grid->nx < 0 || grid->ny < 0 || grid->nz < 0)
+        return set_error(SB200_ERR_INVALID, std::string(where) + ": bad grid");
+    GridDesc g;
+    g.nx = grid->nx;
+    g.ny = grid->ny;
+    g.nz = grid->nz;
+    g.dx = grid->dx;
+    g.dy = grid->dy;
+    g.dz = grid->dz;
+    g.dt = grid->dt;
+    if (!g.has_interior()) return SB200_OK;
+    auto a16 = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
+    if (g.nx % 4 != 0 || !a16(p) || !a16(p_prev_next) || !a16(vel2) || g.nx > (1 << 20) ||
+        g.ny > (1 << 20) || g.nz > (1 << 20))
+        return set_error(SB200_ERR_UNSUPPORTED,
+                         std::string(where) + ": needs nx % 4 == 0 and 16-byte aligned fields");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (!m->host_valid) {  // parameters changed on the device since the last copy
+        m->host.resize(NPARAM);
+        int rc = cuda_err(cudaMemcpyAsync(m->host.data(), m->prm, NPARAM * 4,
+                                          cudaMemcpyDeviceToHost, st),
+                          where);
+        if (!rc) rc = cuda_err(cudaStreamSynchronize(st), where);
+        if (rc) return rc;
+        m->host_valid = true;
+    }
+    int* err = device_error_word();
+    if (!err) return set_error(SB200_ERR_CUDA, std::string(where) + ": device error word unavailable");
+    const PencilBoxes b = learned_step_boxes();
+    PencilMaps maps;
+    int rc = tensor_map_3d(&maps.p, p, g.nx, g.ny, g.nz, 4, b.halo_x, b.halo_y);
+    if (!rc) rc = tensor_map_3d(&maps.prev, p_prev_next, g.nx, g.ny, g.nz, 4, b.tile_x, b.tile_y);
+    if (!rc) rc = tensor_map_3d(&maps.vel2, vel2, g.nx, g.ny, g.nz, 4, b.tile_x, b.tile_y);
+    if (rc)
+        return set_error(SB200_ERR_CUDA, std::string(where) + ": tensor map encode failed (" +
+                                             std::to_string(rc) + ")");
+    LearnedNet net;
+    net.w1b = m->w1b;
+    net.w2b = m->w2b;
+    for (int k = 0; k < H; ++k) {
+        net.b1[k] = m->host[OFF_B1 + k];
+        net.b2[k] = m->host[OFF_B2 + k];
+        net.w3[k] = m->host[OFF_W3 + k];
+    }
+    net.b3 = m->host[OFF_B3];
+    net.out_scale = m->out_scale;
+    return cuda_err(launch_learned_step(maps, p_prev_next, g, net, m->sms, err, st), where);
 }
 
 int sb200_mlp_set_kernel(void* h, int kernel) {

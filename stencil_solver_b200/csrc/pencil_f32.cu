@@ -492,6 +492,8 @@ unsigned ctas_of(const PencilArgs& a, const GridDesc& g) {
     return static_cast<unsigned>(int64_t(a.tiles_x) * a.tiles_y * zc);
 }
 
+}  // namespace
+
 Weights fold_weights(const GridDesc& g, float scale) {
     const float c[R] = {C1, C2, C3, C4};
     const float ix2 = 1.0f / (g.dx * g.dx);
@@ -509,7 +511,6 @@ Weights fold_weights(const GridDesc& g, float scale) {
     return w;
 }
 
-}  // namespace
 
 int pencil_f32_variant_count(bool heat) { return heat ? kNumHeat : kNumWave; }
 

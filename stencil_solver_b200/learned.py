@@ -196,13 +196,20 @@ def fine_solve(pb: Problem, vf, steps: int, on_even=None):
     return p
 
 
-def coarse_step(pb: Problem, vc, p, q, src, w, m, mlp: Mlp | None = None) -> None:
-    """One coarse step from level m (p) over level m-1 (q, overwritten with m+1)."""
+def coarse_step(pb: Problem, vc, p, q, src, w, m, mlp: Mlp | None = None,
+                fused: bool = True) -> None:
+    """One coarse step from level m (p) over level m-1 (q, overwritten with m+1):
+    the acoustic step, the learned correction (mlp given; one fused launch unless
+    fused is False), then the source."""
     g = pb.coarse
-    wave_step(p, q, vc, q, g)
-    _inject(pb, False, q, src, w, m)
-    if mlp is not None:
+    if mlp is None:
+        wave_step(p, q, vc, q, g)
+    elif fused:
+        mlp.learned_step(p, q, vc, g)
+    else:
+        wave_step(p, q, vc, q, g)
         mlp.correct(p, vc, q, g)
+    _inject(pb, False, q, src, w, m)
 
 
 def coarse_solve(pb: Problem, vc, steps: int, mlp: Mlp | None = None):

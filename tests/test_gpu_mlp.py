@@ -215,3 +215,47 @@ def test_tcgen05_and_mma_correction_agree(torch_cuda):
     assert np.max(np.abs(a - b)) <= 2e-2 * scale
     assert np.median(np.abs(a - b)) <= 1e-5 * scale
     assert np.array_equal(outs["tcgen05"][0], outs["tcgen05"][1])  # deterministic
+
+
+@pytest.mark.parametrize("shape", [(40, 36, 72), (29, 45, 40)])
+def test_learned_step_is_step_plus_correction(torch_cuda, shape):
+    """The fused learned step gives the same bits as the FP32 acoustic step
+    followed by the tcgen05 correction: ragged tiles in x and y, unequal
+    spacings, and an all-zero slab whose planes skip the network."""
+    torch = torch_cuda
+    rng = np.random.default_rng(13)
+    nz, ny, nx = shape
+    p = rng.standard_normal(shape).astype(np.float32)
+    p[: nz // 3] = 0.0
+    q = rng.standard_normal(shape).astype(np.float32)
+    v2 = rng.uniform(1500, 4500, shape).astype(np.float32) ** 2
+    g = sb.Grid(nx, ny, nz, 10.0, 12.0, 9.0, 8e-4)
+    w, X, t = net_and_rows(14, 4096)
+    with sb.Mlp() as m:
+        m.set_params(w)
+        m.output_scale = 0.3
+        m.set_kernel("tcgen05")
+        P, V = dev(torch, p), dev(torch, v2)
+        for trained in (False, True):
+            if trained:  # parameters changed on the device: the fused step re-reads them
+                loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+                m.train_step(dev(torch, X.view(np.int16)), dev(torch, t), 1e-2, loss)
+            ref = dev(torch, q)
+            sb.wave_step(P, ref, V, ref, g)
+            m.correct(P, V, ref, g)
+            got = dev(torch, q)
+            m.learned_step(P, got, V, g)
+            plain = dev(torch, q)
+            sb.wave_step(P, plain, V, plain, g)
+            assert not torch.equal(ref, plain)  # the correction is not zero
+            assert torch.equal(got, ref), float((got - ref).abs().max())
+
+
+def test_learned_step_needs_aligned_rows(torch_cuda):
+    torch = torch_cuda
+    g = sb.Grid(38, 20, 20)  # nx % 4 != 0
+    z = torch.zeros(g.shape, device="cuda")
+    with sb.Mlp() as m:
+        with pytest.raises(sb.StencilError) as e:
+            m.learned_step(z, z.clone(), z.clone(), g)
+    assert e.value.status == sb.SB200_ERR_UNSUPPORTED

@@ -51,17 +51,18 @@ def test_mlp_features_match_numpy():
     star = [p[z, y, x]] + [p[z, y, x + r] for r in range(-4, 5) if r] + \
            [p[z, y + r, x] for r in range(-4, 5) if r] + [p[z + r, y, x] for r in range(-4, 5) if r]
     star = np.array(star, np.float32)
-    assert s == np.abs(star).max()
+    m = np.abs(star).max()
+    # s: the smallest power of two above max |star|
+    assert s == 2.0 ** (np.floor(np.log2(m)) + 1) and s > m >= s / 2
     inv = np.float32(1.0) / np.float32(s)
     c0 = star[0]
-    f = [c0 * inv]
+    f = []
     axes = [star[1:9], star[9:17], star[17:25]]  # offsets -4..-1, 1..4
-    for ax in axes:
+    for ax in axes:  # per axis and radius: difference, second difference
         for r in range(1, 5):
             f.append((ax[3 + r] - ax[4 - r]) * inv)
-    for ax in axes:
-        for r in range(1, 5):
             f.append(((ax[3 + r] + ax[4 - r]) - np.float32(2) * c0) * inv)
+    f.append(c0 * inv)
     assert np.array_equal(row[:25], oracle.to_bf16(np.array(f, np.float32)))
     assert row[25] == oracle.to_bf16(np.sqrt(v2[z, y, x]) * np.float32(1e-3 / 10.0))
     assert not row[26:].any()
