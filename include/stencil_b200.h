@@ -364,6 +364,13 @@ int sb200_mlp_correct(void* handle, const float* p, const float* vel2, float* p_
  * the stream). */
 int sb200_mlp_learned_step(void* handle, const float* p, float* p_prev_next, const float* vel2,
                            const sb200_grid* grid, void* stream);
+/* Correction floor: a point whose 25-point star has largest magnitude below
+ * `floor` gets no correction (default 0: every point with a nonzero star).  Ahead
+ * of a wavefront the stencil leaves values that decay and underflow; a correction
+ * proportional to them keeps them alive, so a floor far below the field's scale
+ * keeps those regions exactly zero (and lets the fused step skip them). */
+int sb200_mlp_set_min_scale(void* handle, float floor);
+float sb200_mlp_min_scale(void* handle);
 /* Correction kernel of the handle: 0 = tcgen05 (default), 1 = mma.sync. */
 int sb200_mlp_set_kernel(void* handle, int kernel);
 /* Training rows at n cells (device int64 flat indices, interior only):

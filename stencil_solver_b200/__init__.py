@@ -186,6 +186,8 @@ _SIGNATURES = {
                              C.c_int),
     "sb200_mlp_correct": ([C.c_void_p] * 4 + [C.POINTER(sb200_grid), C.c_void_p], C.c_int),
     "sb200_mlp_learned_step": ([C.c_void_p] * 4 + [C.POINTER(sb200_grid), C.c_void_p], C.c_int),
+    "sb200_mlp_set_min_scale": ([C.c_void_p, C.c_float], C.c_int),
+    "sb200_mlp_min_scale": ([C.c_void_p], C.c_float),
     "sb200_mlp_samples": ([C.c_void_p] * 4 + [C.POINTER(sb200_grid), C.c_void_p, C.c_int64,
                                                C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "sb200_add_box": ([C.c_void_p, C.POINTER(sb200_grid)] + [C.c_int] * 6 +
@@ -658,6 +660,16 @@ class Mlp:
     @output_scale.setter
     def output_scale(self, c: float) -> None:
         _check(lib().sb200_mlp_set_output_scale(self._h, c))
+
+    @property
+    def min_scale(self) -> float:
+        """Correction floor: points whose star's largest magnitude is below it get
+        no correction (0, the default: every point with a nonzero star)."""
+        return float(lib().sb200_mlp_min_scale(self._h))
+
+    @min_scale.setter
+    def min_scale(self, floor: float) -> None:
+        _check(lib().sb200_mlp_set_min_scale(self._h, floor))
 
     def set_kernel(self, kernel: str) -> None:
         """Correction kernel: "tcgen05" (default) or "mma"."""

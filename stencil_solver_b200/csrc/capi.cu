@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <cmath>
 #include <cstdio>
 #include <map>
@@ -95,6 +96,23 @@ int sm_count() {
     return n;
 }
 
+// Untuned default tile of a kind: the tuner's usual pick on large grids
+// (1024^3 acoustic: t64x32_r2_s8_a3; 512^3 heat: t64x16_r2_s8), found by name so
+// the tables can be reordered.
+int default_variant(int kind) {
+    const char* want = kind == SB200_KIND_WAVE_F32 ? "t64x32_r2_s8_a3"
+                       : kind == SB200_KIND_HEAT_F32 ? "t64x16_r2_s8"
+                                                     : "h64x16_s8_a4";
+    const int n = variant_count(kind);
+    for (int v = 0; v < n; ++v) {
+        const char* name = kind == SB200_KIND_WAVE_F16
+                               ? pencil_f16_variant_name(v)
+                               : pencil_f32_variant_name(kind == SB200_KIND_HEAT_F32, v);
+        if (name && std::strcmp(name, want) == 0) return v;
+    }
+    return 0;
+}
+
 PencilConfig choose(int kind, const GridDesc& g) {
     {
         std::lock_guard<std::mutex> lock(g_cfg_mu);
@@ -118,8 +136,8 @@ PencilConfig choose(int kind, const GridDesc& g) {
     std::lock_guard<std::mutex> lock(memo_mu);
     auto it = memo.find(key);
     if (it != memo.end()) return it->second;
-    c.variant = 0;
-    c.zchunks = zchunk_ranking(kind, 0, g, 1).front();
+    c.variant = default_variant(kind);
+    c.zchunks = zchunk_ranking(kind, c.variant, g, 1).front();
     memo[key] = c;
     return c;
 }

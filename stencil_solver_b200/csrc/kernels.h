@@ -78,6 +78,7 @@ struct LearnedNet {
     float b1[32] = {}, b2[32] = {}, w3[32] = {};
     float b3 = 0.f;
     float out_scale = 1.f;
+    float min_scale = 0.f;  // correction floor (stars below it: no correction)
 };
 // Boxes of its tensor maps, resident CTAs per SM, and the launch: p_next =
 // acoustic step of p + learned correction, in place over p_prev.

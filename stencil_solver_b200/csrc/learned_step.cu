@@ -24,8 +24,9 @@
 //      layer 1 (1/s, bias, ReLU, BF16) writes layer 2's A tiles over the
 //      features, layer 2 overwrites the accumulators, its epilogue (bias, ReLU,
 //      w3 dot product) finishes the correction.
-// A plane whose points are all exactly zero skips the network (its correction
-// is exactly zero).  Every wait is bounded; on timeout the CTA records the
+// Points whose star stays below the network's correction floor (by default: is
+// exactly zero) get no correction; threads with no such point skip the features,
+// warps the epilogues, and a plane-tile with none skips the network.  Every wait is bounded; on timeout the CTA records the
 // error, lets its copies and MMAs land, releases TMEM and exits.
 #include <cuda_runtime.h>
 
@@ -67,6 +68,8 @@ struct LearnedArgs {
     Weights w;         // Laplacian weights x dt^2 (the FP32 pencil kernel's)
     float dt_over_dx;  // Courant feature: sqrt(vel2) dt / min(dx, dy, dz)
     float out_scale;   // c
+    float min_scale;   // correction floor: stars whose largest magnitude is below it
+                       // get no correction (0: every nonzero star)
     const uint16_t* w1b;  // BF16 W1, W2 (out x in)
     const uint16_t* w2b;
     float b1[H], b2[H], w3[H];
@@ -184,13 +187,18 @@ __global__ void __launch_bounds__(LNT, 3)
         if (!mbar_wait(&full[jj % LS], (jj / LS) & 1)) bad = true;
         q[jj] = lds128(plane(jj) + soff);
     }
-    uint32_t ncommit = 0;    // MMA commits issued (uniform): the mbarrier's phases
-    uint32_t completed = 0;  // thread 0: commits seen complete
-    auto wait_mma = [&]() {
+    // A tiles start zeroed: rows of points that never become active are read by
+    // the MMAs (their results are discarded) and must hold finite values.
+    for (int i = tid; i < 4 * kTileA / 16; i += LNT)
+        reinterpret_cast<uint4*>(sA)[i] = make_uint4(0u, 0u, 0u, 0u);
+    fence_async_smem();
+    uint32_t ncommit = 0;  // MMA commits issued (uniform): the mbarrier's phases
+    uint32_t waited = 0;   // commits this thread has seen complete (phases complete in order)
+    auto wait_mma = [&]() {  // the latest commit
         const bool ok = mbar_wait(&mbar, (ncommit - 1u) & 1u);
         tc_fence_after();
         if (!ok) bad = true;
-        if (ok && tid == 0) completed = ncommit;
+        if (ok) waited = ncommit;
     };
 
     // One plane per iteration; the queue shifts by one slot at the end (the body
@@ -217,17 +225,31 @@ __global__ void __launch_bounds__(LNT, 3)
 
         // Stencil: the FP32 pencil kernel's arithmetic in its order (y per row
         // from zero, farthest rows first; x and z pair sums; (x + y) + z).
+        // mag: the largest magnitude in the thread's 4 stars, as float bits with
+        // the sign cleared (an unsigned compare of such bits orders magnitudes).
+        auto bits4 = [](const float4& v) {
+            return max(max(__float_as_uint(v.x) & 0x7fffffffu, __float_as_uint(v.y) & 0x7fffffffu),
+                       max(__float_as_uint(v.z) & 0x7fffffffu, __float_as_uint(v.w) & 0x7fffffffu));
+        };
+        uint32_t mag = 0u;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) mag = max(mag, bits4(q[k]));
         float2 ya[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
 #pragma unroll
         for (int k = -R; k <= R; ++k) {
             if (k == 0) continue;
             const float4 row = lds128(pc + k * LSX);
+            mag = max(mag, bits4(row));
             const int d = k > 0 ? k : -k;
             ya[0] = fma2(ay2[d - 1], pair_of(row, 0), ya[0]);
             ya[1] = fma2(ay2[d - 1], pair_of(row, 1), ya[1]);
         }
         const float4 lf = lds128(pc - 4);
         const float4 rt = lds128(pc + 4);
+        mag = max(mag, max(bits4(lf), bits4(rt)));
+        // Some star of the thread reaches the floor (a zero floor admits any
+        // nonzero star).
+        const bool tact = rin && mag >= max(1u, __float_as_uint(a.min_scale));
         const float win[12] = {lf.x, lf.y, lf.z, lf.w, c.x, c.y, c.z, c.w, rt.x, rt.y, rt.z, rt.w};
         float2 lap[2];
 #pragma unroll
@@ -262,10 +284,14 @@ __global__ void __launch_bounds__(LNT, 3)
         // (up - dn, (up + dn) - 2c), unscaled, packed as soon as it is computed;
         // the star's largest magnitude gives s, and the last word is (c, Courant
         // number x s).  Point e's row is row tid of A tile e.
-        float inv[4], sc[4];
+        // A thread whose stars are all zero writes no rows (its points' corrections
+        // are exactly zero); one that writes first makes sure no MMA of the
+        // previous plane still reads the tiles (it may have skipped that wait).
+        float inv[4] = {0.f, 0.f, 0.f, 0.f}, sc[4] = {0.f, 0.f, 0.f, 0.f};
         bool act = false;
+        if (tact && waited < ncommit) wait_mma();
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < 2 && tact; ++h) {
             const float2 ce = pair_of(c, h);
             float2 mx = make_float2(fabsf(ce.x), fabsf(ce.y));
             uint32_t row0[16], row1[16];  // points 2h, 2h + 1
@@ -297,7 +323,8 @@ __global__ void __launch_bounds__(LNT, 3)
             for (int l = 0; l < 2; ++l) {
                 const int e = 2 * h + l;
                 float s;
-                pow2_scale(rin ? (l ? mx.y : mx.x) : 0.f, s, inv[e]);
+                const float mm = l ? mx.y : mx.x;
+                pow2_scale(rin && mm >= a.min_scale ? mm : 0.f, s, inv[e]);
                 sc[e] = s * a.out_scale;
                 act = act || s > 0.f;
                 uint32_t(&row)[16] = l ? row1 : row0;
@@ -325,9 +352,12 @@ __global__ void __launch_bounds__(LNT, 3)
                 tc_commit(&mbar);
             }
         }
-        if (!abort_run && any) {
-            ++ncommit;
-            wait_mma();  // every thread waits for the layer-1 accumulators
+        // Warps without an active point skip the epilogues (TMEM loads are
+        // warp-wide): their rows' results are discarded.
+        const bool wact = __any_sync(0xffffffffu, act);
+        if (!abort_run && any) ++ncommit;
+        if (!abort_run && any && wact) {
+            wait_mma();  // the layer-1 accumulators
             // Layer 1 epilogue: h1 = relu(acc / s + b1) as BF16, over the features.
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
@@ -344,6 +374,8 @@ __global__ void __launch_bounds__(LNT, 3)
                 store_row(sA + e * kTileA, tid, hw);
             }
             fence_async_smem();
+        }
+        if (!abort_run && any) {
             tc_fence_before();
             __syncthreads();
             tc_fence_after();
@@ -356,6 +388,8 @@ __global__ void __launch_bounds__(LNT, 3)
                 tc_commit(&mbar);
             }
             ++ncommit;
+        }
+        if (!abort_run && any && wact) {
             wait_mma();
             // Layer 2 epilogue and the output layer, in the correction kernel's
             // order; then p_next = stencil + s c y.
@@ -399,7 +433,7 @@ __global__ void __launch_bounds__(LNT, 3)
             (void)mbar_wait(&full[jj % LS], (jj / LS) & 1);
         for (int it = max(0, aux_issued_hi - LAUX + 1); it <= aux_issued_hi; ++it)
             (void)mbar_wait(&auxf[it % LAUX], (it / LAUX) & 1);
-        for (uint32_t k = completed; k < ncommit; ++k) (void)mbar_wait(&mbar, k & 1u);
+        if (waited < ncommit) (void)mbar_wait(&mbar, (ncommit - 1u) & 1u);
     }
     tc_fence_before();
     __syncthreads();
@@ -466,6 +500,7 @@ cudaError_t launch_learned_step(const PencilMaps& maps, float* next, const GridD
     a.w = fold_weights(g, g.dt * g.dt);
     a.dt_over_dx = g.dt / std::min(g.dx, std::min(g.dy, g.dz));
     a.out_scale = net.out_scale;
+    a.min_scale = net.min_scale;
     a.w1b = net.w1b;
     a.w2b = net.w2b;
     for (int k = 0; k < H; ++k) {

@@ -438,7 +438,7 @@ __global__ void __launch_bounds__(32 * kCorrWarps)
     mlp_correct_kernel(const float* __restrict__ prm, const uint32_t* __restrict__ w1b,
                        const uint32_t* __restrict__ w2b, const float* __restrict__ p,
                        const float* __restrict__ vel2, float* __restrict__ p_next, int64_t nx,
-                       int64_t ny, int64_t nz, float dt_over_dx, float out_scale) {
+                       int64_t ny, int64_t nz, float dt_over_dx, float out_scale, float floor) {
     __shared__ __align__(16) uint16_t feat[kCorrWarps][32][CP];
     __shared__ float scale[kCorrWarps][32];
     NetFrag net;
@@ -459,7 +459,7 @@ __global__ void __launch_bounds__(32 * kCorrWarps)
         float s = 0.f;
         if (live) {
             Star st;
-            gather_star(st, p, c, sy, sz);
+            gather_star(st, p, c, sy, sz, floor);
             feature_row(fr, st, sqrtf(vel2[c]) * dt_over_dx);
             s = st.s;
         } else {
@@ -512,7 +512,8 @@ __global__ void __launch_bounds__(kTcThreads)
     mlp_correct_tc_kernel(const float* __restrict__ prm, const uint16_t* __restrict__ w1b,
                           const uint16_t* __restrict__ w2b, const float* __restrict__ p,
                           const float* __restrict__ vel2, float* __restrict__ p_next, int nx,
-                          int ny, int nz, float dt_over_dx, float out_scale, int* err) {
+                          int ny, int nz, float dt_over_dx, float out_scale, float floor,
+                          int* err) {
     extern __shared__ unsigned char dyn[];
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t s_tmem;
@@ -591,7 +592,7 @@ __global__ void __launch_bounds__(kTcThreads)
             if (x < nx - 4) {
                 c = (int64_t(z) * ny + y) * nx + x;
                 Star st;
-                gather_star(st, p, c, sy, sz);
+                gather_star(st, p, c, sy, sz, floor);
                 feature_row(fr, st, sqrtf(vel2[c]) * dt_over_dx);
                 sc = st.s * out_scale;
             }
@@ -702,6 +703,7 @@ struct Mlp {
     int64_t adam_t = 0;
     int sms = 148;
     float out_scale = 1.f;  // the correction is s * out_scale * y
+    float min_scale = 0.f;  // correction floor: stars below it get no correction
     int kernel = 0;         // correction kernel: 0 = tcgen05, 1 = mma.sync
     // Host copy of the FP32 parameters for the fused step, which takes biases
     // and w3 by value; stale after a device-side update (train_step).
@@ -811,6 +813,19 @@ int sb200_mlp_set_output_scale(void* h, float scale) {
     return SB200_OK;
 }
 
+int sb200_mlp_set_min_scale(void* h, float floor) {
+    Mlp* m = static_cast<Mlp*>(h);
+    if (!m || !(floor >= 0.f) || !std::isfinite(floor))
+        return set_error(SB200_ERR_INVALID, "sb200_mlp_set_min_scale: bad arguments");
+    m->min_scale = floor;
+    return SB200_OK;
+}
+
+float sb200_mlp_min_scale(void* h) {
+    Mlp* m = static_cast<Mlp*>(h);
+    return m ? m->min_scale : 0.f;
+}
+
 float sb200_mlp_output_scale(void* h) {
     Mlp* m = static_cast<Mlp*>(h);
     return m ? m->out_scale : 0.f;
@@ -881,7 +896,7 @@ int sb200_mlp_correct(void* h, const float* p, const float* vel2, float* p_next,
         mlp_correct_kernel<<<blocks, 32 * kCorrWarps, 0, st>>>(
             m->prm, reinterpret_cast<const uint32_t*>(m->w1b),
             reinterpret_cast<const uint32_t*>(m->w2b), p, vel2, p_next, grid->nx, grid->ny,
-            grid->nz, grid->dt / dx, m->out_scale);
+            grid->nz, grid->dt / dx, m->out_scale, m->min_scale);
         return cuda_err(cudaGetLastError(), "sb200_mlp_correct");
     }
     int* err = device_error_word();
@@ -903,7 +918,8 @@ int sb200_mlp_correct(void* h, const float* p, const float* vel2, float* p_next,
     const int blocks = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(tiles, int64_t(m->sms) * 8)));
     mlp_correct_tc_kernel<<<blocks, kTcThreads, kTcSmem, st>>>(
         m->prm, m->w1b, m->w2b, p, vel2, p_next, static_cast<int>(grid->nx),
-        static_cast<int>(grid->ny), static_cast<int>(grid->nz), grid->dt / dx, m->out_scale, err);
+        static_cast<int>(grid->ny), static_cast<int>(grid->nz), grid->dt / dx, m->out_scale,
+        m->min_scale, err);
     return cuda_err(cudaGetLastError(), "sb200_mlp_correct");
 }
 
@@ -962,6 +978,7 @@ int sb200_mlp_learned_step(void* h, const float* p, float* p_prev_next, const fl
     }
     net.b3 = m->host[OFF_B3];
     net.out_scale = m->out_scale;
+    net.min_scale = m->min_scale;
     return cuda_err(launch_learned_step(maps, p_prev_next, g, net, m->sms, err, st), where);
 }
 

@@ -59,14 +59,17 @@ __device__ __forceinline__ void pow2_scale(float m, float& s, float& inv) {
 }
 
 // The 25-point star of p around c (centre, then x-4..x-1, x+1..x+4, then y and
-// z likewise) and its scale s.
+// z likewise) and its scale s.  A star whose largest magnitude is below `floor`
+// (the network's correction floor; 0 admits every nonzero star) gets s = 0, so
+// its correction is exactly zero: ahead of a wavefront the field holds values
+// that only underflow if nothing keeps feeding them.
 struct Star {
     float v[25];
     float s;
 };
 
 __device__ __forceinline__ void gather_star(Star& st, const float* __restrict__ p, int64_t c,
-                                            int64_t sy, int64_t sz) {
+                                            int64_t sy, int64_t sz, float floor = 0.f) {
     st.v[0] = p[c];
     int k = 1;
 #pragma unroll
@@ -82,7 +85,7 @@ __device__ __forceinline__ void gather_star(Star& st, const float* __restrict__ 
 #pragma unroll
     for (int j = 0; j < 25; ++j) m = fmaxf(m, fabsf(st.v[j]));
     float inv;
-    pow2_scale(m, st.s, inv);
+    pow2_scale(m >= floor ? m : 0.f, st.s, inv);
 }
 
 // Feature row (32 BF16) of a star (see the file comment): word 4a + r - 1 holds

@@ -43,6 +43,12 @@ import numpy as np
 from . import Grid, Mlp, _check, add_box, lib, mlp_samples, restrict2, smooth3, wave_step
 
 OFFSET = -4  # coarse cell i <-> fine cell 2 i + OFFSET
+# Correction floor of a trained network (Mlp.min_scale).  A Problem's source is
+# normalised so that its fields are O(1); points whose star stays below 2^-64 of
+# that get no correction, so the values the stencil leaves ahead of the wavefront
+# decay and underflow as in the plain solve (a correction proportional to them
+# would keep the whole numerical light cone, 4 cells per step, nonzero).
+CORRECTION_FLOOR = 2.0 ** -64
 
 
 def _torch():
@@ -301,14 +307,16 @@ def make_pairs(problems, fine_steps: int, samples_per_pair: int = 4096, every: i
 def train(ds: Dataset, mlp: Mlp, epochs: int = 4, batch: int = 8192, lr: float = 2e-3,
           lr_final: float = 1e-4, seed: int = 0, log=None) -> list:
     """Adam over shuffled mini-batches with a cosine learning-rate decay.  The
-    targets are divided by their RMS, which becomes the network's output scale.
-    Returns the mean batch loss (in units of that RMS squared) of every epoch."""
+    targets are divided by their RMS, which becomes the network's output scale;
+    the network's correction floor becomes CORRECTION_FLOOR.  Returns the mean
+    batch loss (in units of that RMS squared) of every epoch."""
     torch = _torch()
     gen = torch.Generator(device="cuda")
     gen.manual_seed(seed)
     n = ds.n
     rms = float(ds.t.double().pow(2).mean().sqrt())
     mlp.output_scale = rms if rms > 0 else 1.0
+    mlp.min_scale = CORRECTION_FLOOR
     tn = ds.t / mlp.output_scale
     steps_per_epoch = max(1, n // batch)
     total = epochs * steps_per_epoch
@@ -443,9 +451,11 @@ def learned_solve(pb: Problem, coarse_steps: int, mlp: Mlp, bound: float = 1e-3,
 
 
 def time_fine_solve(pb: Problem, fine_steps: int):
-    """(device ms, restricted result) of the plain fine solve."""
+    """(device ms, restricted result) of the plain fine solve.  Two untimed steps
+    first, so the pencil tuner's first-use work stays outside."""
     torch = _torch()
     vf, _ = pb.device_models()
+    fine_solve(pb, vf, 2)
     e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
     torch.cuda.synchronize()
     e0.record()

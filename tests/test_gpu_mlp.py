@@ -217,16 +217,23 @@ def test_tcgen05_and_mma_correction_agree(torch_cuda):
     assert np.array_equal(outs["tcgen05"][0], outs["tcgen05"][1])  # deterministic
 
 
-@pytest.mark.parametrize("shape", [(40, 36, 72), (29, 45, 40)])
-def test_learned_step_is_step_plus_correction(torch_cuda, shape):
+@pytest.mark.parametrize("shape,sparse", [((40, 36, 72), False), ((29, 45, 40), False),
+                                          ((36, 52, 80), True)])
+def test_learned_step_is_step_plus_correction(torch_cuda, shape, sparse):
     """The fused learned step gives the same bits as the FP32 acoustic step
     followed by the tcgen05 correction: ragged tiles in x and y, unequal
-    spacings, and an all-zero slab whose planes skip the network."""
+    spacings, an all-zero slab whose planes skip the network, and (sparse) a
+    field that is zero but for a small blob, so most threads and warps of the
+    active planes skip the features and epilogues."""
     torch = torch_cuda
     rng = np.random.default_rng(13)
     nz, ny, nx = shape
     p = rng.standard_normal(shape).astype(np.float32)
     p[: nz // 3] = 0.0
+    if sparse:
+        blob = p[14:21, 20:27, 33:41].copy()
+        p[:] = 0.0
+        p[14:21, 20:27, 33:41] = blob
     q = rng.standard_normal(shape).astype(np.float32)
     v2 = rng.uniform(1500, 4500, shape).astype(np.float32) ** 2
     g = sb.Grid(nx, ny, nz, 10.0, 12.0, 9.0, 8e-4)
@@ -259,3 +266,59 @@ def test_learned_step_needs_aligned_rows(torch_cuda):
         with pytest.raises(sb.StencilError) as e:
             m.learned_step(z, z.clone(), z.clone(), g)
     assert e.value.status == sb.SB200_ERR_UNSUPPORTED
+
+
+def test_correction_floor(torch_cuda):
+    """Points whose star stays below the floor get no correction, in the
+    standalone kernels and the fused step alike (bitwise), and the others are
+    corrected as without a floor: a field ramped over five decades along x."""
+    torch = torch_cuda
+    rng = np.random.default_rng(17)
+    shape = (28, 24, 96)
+    nz, ny, nx = shape
+    ramp = (10.0 ** np.linspace(-5, 0, nx)).astype(np.float32)
+    p = rng.standard_normal(shape).astype(np.float32) * ramp
+    q = rng.standard_normal(shape).astype(np.float32) * ramp
+    v2 = rng.uniform(1500, 4500, shape).astype(np.float32) ** 2
+    g = sb.Grid(nx, ny, nz, 10.0, 10.0, 10.0, 8e-4)
+    w, _, _ = net_and_rows(18, 1)
+    P, V = dev(torch, p), dev(torch, v2)
+    outs = {}
+    with sb.Mlp() as m:
+        m.set_params(w)
+        m.output_scale = 0.3
+        for floor in (0.0, 1e-2):
+            m.min_scale = floor
+            assert m.min_scale == np.float32(floor)
+            for kern in ("tcgen05", "mma"):
+                m.set_kernel(kern)
+                ref = dev(torch, q)
+                sb.wave_step(P, ref, V, ref, g)
+                m.correct(P, V, ref, g)
+                outs[(floor, kern)] = ref.cpu().numpy()
+            got = dev(torch, q)
+            m.learned_step(P, got, V, g)
+            outs[(floor, "fused")] = got.cpu().numpy()
+        with pytest.raises(sb.StencilError):
+            m.min_scale = -1.0
+    plain = dev(torch, q)
+    sb.wave_step(P, plain, V, plain, g)
+    plain = plain.cpu().numpy()
+    for floor in (0.0, 1e-2):
+        assert np.array_equal(outs[(floor, "fused")], outs[(floor, "tcgen05")])
+    # star maxima: points below the floor are plain steps; the rest match no floor
+    pad = np.pad(np.abs(p), 4)
+    m_star = np.zeros(shape, np.float32)
+    for axis in range(3):
+        for r in range(-4, 5):
+            m_star = np.maximum(m_star, np.roll(pad, r, axis)[4:-4, 4:-4, 4:-4])
+    inner = np.zeros(shape, bool)
+    inner[4:-4, 4:-4, 4:-4] = True
+    fl = np.float32(1e-2)
+    low, high = inner & (m_star < fl), inner & (m_star >= fl)
+    assert low.sum() > 1000 and high.sum() > 1000
+    for kern in ("tcgen05", "mma"):
+        f, nf = outs[(1e-2, kern)], outs[(0.0, kern)]
+        assert np.array_equal(f[low], plain[low])
+        assert np.array_equal(f[high], nf[high])
+        assert not np.array_equal(nf[low], plain[low])
