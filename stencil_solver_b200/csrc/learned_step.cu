@@ -225,31 +225,28 @@ __global__ void __launch_bounds__(LNT, 3)
 
         // Stencil: the FP32 pencil kernel's arithmetic in its order (y per row
         // from zero, farthest rows first; x and z pair sums; (x + y) + z).
-        // mag: the largest magnitude in the thread's 4 stars, as float bits with
-        // the sign cleared (an unsigned compare of such bits orders magnitudes).
-        auto bits4 = [](const float4& v) {
-            return max(max(__float_as_uint(v.x) & 0x7fffffffu, __float_as_uint(v.y) & 0x7fffffffu),
-                       max(__float_as_uint(v.z) & 0x7fffffffu, __float_as_uint(v.w) & 0x7fffffffu));
+        // mag: the largest magnitude in the thread's 4 stars.
+        auto absmax4 = [](const float4& v) {
+            return fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w)));
         };
-        uint32_t mag = 0u;
+        float mag = absmax4(q[0]);
 #pragma unroll
-        for (int k = 0; k < 9; ++k) mag = max(mag, bits4(q[k]));
+        for (int k = 1; k < 9; ++k) mag = fmaxf(mag, absmax4(q[k]));
         float2 ya[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
 #pragma unroll
         for (int k = -R; k <= R; ++k) {
             if (k == 0) continue;
             const float4 row = lds128(pc + k * LSX);
-            mag = max(mag, bits4(row));
+            mag = fmaxf(mag, absmax4(row));
             const int d = k > 0 ? k : -k;
             ya[0] = fma2(ay2[d - 1], pair_of(row, 0), ya[0]);
             ya[1] = fma2(ay2[d - 1], pair_of(row, 1), ya[1]);
         }
         const float4 lf = lds128(pc - 4);
         const float4 rt = lds128(pc + 4);
-        mag = max(mag, max(bits4(lf), bits4(rt)));
-        // Some star of the thread reaches the floor (a zero floor admits any
-        // nonzero star).
-        const bool tact = rin && mag >= max(1u, __float_as_uint(a.min_scale));
+        mag = fmaxf(mag, fmaxf(absmax4(lf), absmax4(rt)));
+        // Some star of the thread is nonzero and reaches the floor.
+        const bool tact = rin && mag > 0.f && mag >= a.min_scale;
         const float win[12] = {lf.x, lf.y, lf.z, lf.w, c.x, c.y, c.z, c.w, rt.x, rt.y, rt.z, rt.w};
         float2 lap[2];
 #pragma unroll
