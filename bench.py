@@ -55,6 +55,8 @@ def args_():
     ap.add_argument("--zchunks", type=int, default=1)
     ap.add_argument("--no-secondary", action="store_true",
                     help="skip the heat / FP16 / batch / learned measurements")
+    ap.add_argument("--sparse", action="store_true",
+                    help="--kernel learned: a small random cube in a zero field (floor 2^-64)")
     ap.add_argument("--kernel", choices=["acoustic", "heat", "fp16", "batch", "mlp", "learned"],
                     help="run only a small case of one kernel (for profilers) and print its time")
     return ap.parse_args()
@@ -682,6 +684,12 @@ def run_kernel_probe(a):
     elif a.kernel == "learned":
         m = sb.Mlp(seed=1)
         m.output_scale = 1e-5
+        if a.sparse:  # a random cube of side 40 n / 256 in a zero field, floor 2^-64
+            lo, hi = n * 100 // 256, n * 140 // 256
+            blob = p[lo:hi, lo:hi, lo:hi].clone()
+            p.zero_()
+            p[lo:hi, lo:hi, lo:hi] = blob
+            m.min_scale = 2.0 ** -64
         q = p * 0.99
         f = lambda: m.learned_step(p, q, v, g)  # noqa: E731
     else:  # batch: 12 shots with extents n/2..n in steps of 8
