@@ -320,6 +320,40 @@ def secondary_fp16(n: int, fp32_ms: float, steps: int = 30):
            "gpts_per_s": g.interior / (ms * 1e-3) / 1e9, "speedup_vs_fp32": fp32_ms / ms,
            "achieved_gbs": gbs, "frac_of_measured_hbm": gbs / peak, "bytes_per_point": 8,
            "tile": sb.variant_names(sb.KIND_WAVE_F16)[ch[0]], "zchunks": ch[1]}
+    # 2048^3: the same kernel over 8x the points (51.5 GB of FP16 / BF16 fields).
+    # Its work does not depend on the velocity values, so K is uniform here
+    # (v = 3000 m/s) instead of a 34 GB host-built layered model.
+    try:
+        n2 = 2048
+        g2 = sb.Grid(n2, n2, n2, DX, DX, DX, g.dt)
+        K2 = torch.empty(g2.shape, dtype=torch.int16, device="cuda")
+        kval = np.float32(3000.0 ** 2 * g.dt * g.dt / (DX * DX))
+        K2.fill_(int(np.array([kval], np.float32).view(np.uint32)[0] >> 16))
+        P2 = torch.zeros(g2.shape, dtype=torch.int16, device="cuda")
+        Q2 = torch.zeros_like(P2)
+        S2 = torch.empty_like(P2)  # the tuner's output buffer (68.7 GB in all)
+        sb.tune(sb.KIND_WAVE_F16, g2, P2, Q2, K2, S2, reps=2)
+        del S2
+        for _ in range(3):
+            sb.wave_step_f16(P2, Q2, K2, g2, scale, 0)
+            P2, Q2 = Q2, P2
+        e0.record()
+        for _ in range(10):
+            sb.wave_step_f16(P2, Q2, K2, g2, scale, 0)
+            P2, Q2 = Q2, P2
+        e1.record()
+        torch.cuda.synchronize()
+        ms2 = e0.elapsed_time(e1) / 10
+        gbs2 = 8 * g2.interior / (ms2 * 1e-3) / 1e9
+        ch2 = sb.pencil_choice(sb.KIND_WAVE_F16, g2)
+        out["at_2048^3"] = {"ms_per_step": ms2, "gpts_per_s": g2.interior / (ms2 * 1e-3) / 1e9,
+                            "achieved_gbs": gbs2, "frac_of_measured_hbm": gbs2 / peak,
+                            "tile": sb.variant_names(sb.KIND_WAVE_F16)[ch2[0]], "zchunks": ch2[1],
+                            "k_field": "uniform (v = 3000 m/s): timing only"}
+        del P2, Q2, K2
+    except Exception as exc:  # noqa: BLE001 -- e.g. a GPU with less memory
+        out["at_2048^3"] = {"error": f"{type(exc).__name__}: {exc}"}
+    torch.cuda.empty_cache()
     # accuracy: 256^3 instance, 500 steps, source at the centre
     m = 256
     vel2s, vmaxs = sb.model_layered(m, m, m, SEED)

@@ -287,8 +287,11 @@ typedef struct {
 } sb200_shot;
 
 typedef struct {
-    int precision;     /* SB200_PRECISION_F32 */
-    int graph_chunk;   /* steps per captured graph; 0 = one launch per step */
+    int precision;     /* SB200_PRECISION_F32, or SB200_PRECISION_F16: p / p_prev in
+                          FP16 at per-shot power-of-two scales renormalised every 50
+                          steps (FP64 statistics), K in BF16; every nx % 8 == 0 */
+    int graph_chunk;   /* steps per captured graph; 0 = one launch per step (FP16:
+                          a multiple of 50 so that each chunk starts on a renorm) */
     int64_t max_steps; /* capacity of the per-shot wavelet and trace tables */
 } sb200_batch_config;
 
@@ -314,8 +317,12 @@ int sb200_batch_set_choice(void* handle, int variant, int zlen);
 int sb200_batch_choice(void* handle, int* variant, int* zlen, int* n_items, int* ctas);
 int64_t sb200_batch_steps_done(void* handle);
 void* sb200_batch_stream(void* handle);
+/* Tile variants of FP32 batches (set_choice / choice index these; an FP16
+ * batch indexes its own table, named by sb200_batch_variant_name_f16). */
 int sb200_batch_variant_count(void);
 const char* sb200_batch_variant_name(int variant);
+int sb200_batch_variant_count_f16(void);
+const char* sb200_batch_variant_name_f16(int variant);
 
 /* ── learned coarse correction ─────────────────────────────────────────────
  * No reference counterpart.  A per-point MLP 26 -> 32 -> 32 -> 1 (ReLU), BF16

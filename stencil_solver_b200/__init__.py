@@ -172,6 +172,8 @@ _SIGNATURES = {
     "sb200_batch_steps_done": ([C.c_void_p], C.c_int64),
     "sb200_batch_stream": ([C.c_void_p], C.c_void_p),
     "sb200_batch_variant_count": ([], C.c_int),
+    "sb200_batch_variant_count_f16": ([], C.c_int),
+    "sb200_batch_variant_name_f16": ([C.c_int], C.c_char_p),
     "sb200_batch_variant_name": ([C.c_int], C.c_char_p),
     "sb200_mlp_create": ([C.c_uint64, C.POINTER(C.c_void_p)], C.c_int),
     "sb200_mlp_destroy": ([C.c_void_p], C.c_int),
@@ -521,9 +523,13 @@ def pencil_choice(kind: int, grid: Grid):
 class Batch:
     """Independent acoustic shots of uneven sizes advanced together by one
     persistent launch per step (C-ABI handle sb200_batch_*).  shots is a list of
-    (Grid, src_index) pairs; max_steps bounds the run (source and trace tables)."""
+    (Grid, src_index) pairs; max_steps bounds the run (source and trace tables).
+    precision PRECISION_F16 stores p / p_prev in FP16 at per-shot power-of-two
+    scales (renormalised every 50 steps from FP64 statistics) and K in BF16
+    (every nx a multiple of 8); fields and traces cross the boundary in FP32."""
 
-    def __init__(self, shots, max_steps: int, graph_chunk: int = 100):
+    def __init__(self, shots, max_steps: int, graph_chunk: int = 100,
+                 precision: int = PRECISION_F32):
         arr = (sb200_shot * len(shots))()
         for i, (g, src) in enumerate(shots):
             arr[i].grid = g.c()
@@ -532,11 +538,13 @@ class Batch:
         lib().sb200_batch_config_init(C.byref(cfg))
         cfg.graph_chunk = graph_chunk
         cfg.max_steps = max_steps
+        cfg.precision = precision
         h = C.c_void_p()
         _check(lib().sb200_batch_create(arr, len(shots), C.byref(cfg), C.byref(h)))
         self._h = h
         self._destroy = lib().sb200_batch_destroy  # still callable at interpreter exit
         self.grids = [g for g, _ in shots]
+        self.precision = precision
 
     def close(self):
         if getattr(self, "_h", None):
@@ -594,8 +602,10 @@ class Batch:
     def choice(self) -> dict:
         v, z, n, c = C.c_int(), C.c_int(), C.c_int(), C.c_int()
         _check(lib().sb200_batch_choice(self._h, C.byref(v), C.byref(z), C.byref(n), C.byref(c)))
+        name = (lib().sb200_batch_variant_name_f16 if self.precision == PRECISION_F16
+                else lib().sb200_batch_variant_name)(v.value)
         return {"variant": v.value, "zlen": z.value, "items": n.value, "ctas": c.value,
-                "name": lib().sb200_batch_variant_name(v.value).decode()}
+                "name": name.decode()}
 
     @property
     def steps_done(self) -> int:

@@ -14,10 +14,19 @@
 //
 // The tile shape and z-chunk length come from a small autotuner (sb200_batch_tune)
 // that times each candidate on the batch itself; choices are cached per process
-// by the set of shot extents.
+// by the precision and the set of shot extents.
+//
+// FP16 storage (batch_f16_kernel): the levels hold p / p_prev in FP16 at a
+// per-shot power-of-two scale and the third array K = vel2 dt^2 / dx^2 in BF16.
+// Every 50 steps each shot's FP64 statistics and source bound set its new scale
+// (sb200_f16_renorm, reading the device step counter), the launch after that
+// rescales the output (phase 1) and the next one p_prev (phase 2); a captured
+// 100-step chunk holds two such windows.  Fields cross the boundary in FP32
+// through a one-shot staging buffer (pack on set_fields, unpack on get_field).
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -51,11 +60,16 @@ class Batch {
 public:
     int init(const sb200_shot* shots, int n, const sb200_batch_config& cfg) {
         if (!shots || n <= 0) return set_error(SB200_ERR_INVALID, "sb200_batch_create: no shots");
-        if (cfg.precision != SB200_PRECISION_F32)
-            return set_error(SB200_ERR_UNSUPPORTED, "sb200_batch_create: FP32 batches only");
+        if (cfg.precision != SB200_PRECISION_F32 && cfg.precision != SB200_PRECISION_F16)
+            return set_error(SB200_ERR_UNSUPPORTED, "sb200_batch_create: unknown precision");
+        f16_ = cfg.precision == SB200_PRECISION_F16;
+        esz_ = f16_ ? 2 : 4;
         if (cfg.max_steps <= 0)
             return set_error(SB200_ERR_INVALID, "sb200_batch_create: max_steps must be positive");
         chunk_ = cfg.graph_chunk > 0 ? cfg.graph_chunk : 0;
+        if (f16_ && chunk_ % kRenorm != 0)
+            return set_error(SB200_ERR_INVALID,
+                             "sb200_batch_create: FP16 graph_chunk must be a multiple of 50");
         cap_ = cfg.max_steps;
         size_t off = 0;
         for (int s = 0; s < n; ++s) {
@@ -63,9 +77,10 @@ public:
             if (g.nx <= 8 || g.ny <= 8 || g.nz <= 8)
                 return set_error(SB200_ERR_INVALID, "sb200_batch_create: shot " + std::to_string(s) +
                                                         ": every extent must exceed 8");
-            if (g.nx % 4 != 0)
-                return set_error(SB200_ERR_UNSUPPORTED, "sb200_batch_create: shot " + std::to_string(s) +
-                                                            ": nx must be a multiple of 4");
+            if (g.nx % (f16_ ? 8 : 4) != 0)
+                return set_error(SB200_ERR_UNSUPPORTED,
+                                 "sb200_batch_create: shot " + std::to_string(s) + ": nx must be a multiple of " +
+                                     std::to_string(f16_ ? 8 : 4));
             if (g.nx > 4096 || g.ny > 4096 || g.nz > 4096)
                 return set_error(SB200_ERR_INVALID, "sb200_batch_create: shot " + std::to_string(s) +
                                                         ": extent above 4096");
@@ -89,7 +104,8 @@ public:
                                                             std::to_string(s) +
                                                             ": the source must be an interior cell");
             }
-            const size_t bytes = round_up(static_cast<size_t>(h.g.size()) * 4);
+            const size_t bytes = round_up(static_cast<size_t>(h.g.size()) * esz_);
+            max_points_ = std::max<int64_t>(max_points_, h.g.size());
             h.off[0] = off;
             h.off[1] = off + bytes;
             h.off[2] = off + 2 * bytes;
@@ -102,14 +118,37 @@ public:
         if (int rc = cuda(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking))) return rc;
         if (int rc = alloc(reinterpret_cast<void**>(&arena_), arena_bytes_)) return rc;
         for (int p = 0; p < 2; ++p)
-            if (int rc = alloc(reinterpret_cast<void**>(&table_[p]), sizeof(ShotF32) * n)) return rc;
+            if (int rc = alloc(&table_[p], shot_bytes() * n)) return rc;
         if (int rc = alloc(reinterpret_cast<void**>(&queue_), sizeof(BatchQueue))) return rc;
         if (int rc = alloc(reinterpret_cast<void**>(&wave_), sizeof(float) * cap_ * n)) return rc;
         if (int rc = alloc(reinterpret_cast<void**>(&trace_), sizeof(float) * cap_ * n)) return rc;
+        if (f16_) {
+            // scales, FP64 statistics and their scratch, source bounds, FP32 staging
+            if (int rc = alloc(reinterpret_cast<void**>(&scale_), sizeof(F16Scale) * n)) return rc;
+            if (int rc = alloc(reinterpret_cast<void**>(&stats_), sizeof(double) * 3 * n)) return rc;
+            for (const Shot& h : shots_) {
+                sb200_grid gg = to_grid(h.g);
+                scratch_len_ = std::max(scratch_len_, sb200_field_stats_scratch_len(&gg));
+            }
+            if (int rc = alloc(reinterpret_cast<void**>(&scratch_), sizeof(double) * scratch_len_)) return rc;
+            if (int rc = alloc(reinterpret_cast<void**>(&bound_), sizeof(float) * cap_ * n)) return rc;
+            if (int rc = alloc(reinterpret_cast<void**>(&staging_), sizeof(float) * max_points_)) return rc;
+            if (int rc = cuda(cudaMemsetAsync(bound_, 0, sizeof(float) * cap_ * n, st_))) return rc;
+            std::vector<F16Scale> ones(n, F16Scale{1.f, 1.f});
+            if (int rc = cuda(cudaMemcpyAsync(scale_, ones.data(), sizeof(F16Scale) * n,
+                                              cudaMemcpyHostToDevice, st_)))
+                return rc;
+            if (int rc = cuda(cudaStreamSynchronize(st_))) return rc;
+            wave_host_.assign(n, {});
+            vel2_src_.assign(n, 0.f);
+        }
         if (int rc = cuda(cudaMemsetAsync(arena_, 0, arena_bytes_, st_))) return rc;
         if (int rc = cuda(cudaMemsetAsync(wave_, 0, sizeof(float) * cap_ * n, st_))) return rc;
         if (int rc = reset_clock()) return rc;
-        batch_f32_prepare();
+        if (f16_)
+            batch_f16_prepare();
+        else
+            batch_f32_prepare();
         BatchChoice c;
         if (cached_choice(&c)) {
             variant_ = c.variant;
@@ -125,7 +164,9 @@ public:
         for (void* p : {static_cast<void*>(arena_), static_cast<void*>(table_[0]),
                         static_cast<void*>(table_[1]), static_cast<void*>(queue_),
                         static_cast<void*>(wave_), static_cast<void*>(trace_),
-                        static_cast<void*>(items_)})
+                        static_cast<void*>(items_), static_cast<void*>(scale_),
+                        static_cast<void*>(stats_), static_cast<void*>(scratch_),
+                        static_cast<void*>(bound_), static_cast<void*>(staging_)})
             if (p) cudaFree(p);
         if (st_) cudaStreamDestroy(st_);
     }
@@ -137,6 +178,7 @@ public:
         const Shot& h = shots_[s];
         const size_t bytes = static_cast<size_t>(h.g.size()) * 4;
         const int cur = static_cast<int>(step_ & 1);  // level that is current now
+        if (f16_) return set_fields_f16(s, p, p_prev, vel2, cur);
         if (int rc = cuda(cudaMemcpyAsync(arena_ + h.off[cur], p, bytes, cudaMemcpyHostToDevice, st_)))
             return rc;
         if (int rc = cuda(cudaMemcpyAsync(arena_ + h.off[cur ^ 1], p_prev, bytes,
@@ -154,6 +196,10 @@ public:
         if (int rc = cuda(cudaMemcpyAsync(wave_ + s * cap_, w, sizeof(float) * n,
                                           cudaMemcpyHostToDevice, st_)))
             return rc;
+        if (f16_) {
+            wave_host_[s].assign(w, w + n);
+            if (int rc = upload_bound(s)) return rc;
+        }
         return cuda(cudaStreamSynchronize(st_));
     }
 
@@ -164,7 +210,9 @@ public:
                                                     std::to_string(cap_) + ")");
         int64_t done = 0;
         while (done < n) {
-            if (chunk_ > 0 && n - done >= chunk_) {
+            // FP16: a graph chunk starts on a renormalisation step (its phase
+            // pattern is then the same every time).
+            if (chunk_ > 0 && n - done >= chunk_ && (!f16_ || step_ % kRenorm == 0)) {
                 const int par = static_cast<int>(step_ & 1);
                 if (!graph_[par])
                     if (int rc = capture(par, &graph_[par])) return rc;
@@ -173,7 +221,7 @@ public:
                 done += chunk_;
                 continue;
             }
-            if (int rc = launch(static_cast<int>(step_ & 1))) return rc;
+            if (int rc = step_once(step_, static_cast<int>(step_ & 1))) return rc;
             ++step_;
             ++done;
         }
@@ -193,6 +241,16 @@ public:
             return set_error(SB200_ERR_INVALID, "sb200_batch_get_field: bad shot or NULL output");
         if (int rc = synchronize()) return rc;
         const Shot& h = shots_[s];
+        if (f16_) {  // FP16 level -> FP32 in p's units (divided by the shot's scale)
+            F16Scale sc;
+            if (int rc = cuda(cudaMemcpy(&sc, scale_ + s, sizeof(sc), cudaMemcpyDeviceToHost)))
+                return rc;
+            if (int rc = sb200_f16_unpack(reinterpret_cast<const uint16_t*>(arena_ + h.off[step_ & 1]),
+                                          staging_, h.g.size(), sc.a, st_))
+                return rc;
+            return cuda(cudaMemcpy(out, staging_, static_cast<size_t>(h.g.size()) * 4,
+                                   cudaMemcpyDeviceToHost));
+        }
         return cuda(cudaMemcpy(out, arena_ + h.off[step_ & 1], static_cast<size_t>(h.g.size()) * 4,
                                cudaMemcpyDeviceToHost));
     }
@@ -221,16 +279,16 @@ public:
         BatchChoice best;
         best.ms = 1e30f;
         int rc = SB200_OK;
-        for (int v = 0; v < batch_f32_variant_count() && !rc; ++v) {
+        for (int v = 0; v < variant_count() && !rc; ++v) {
             for (int zl : kZlens) {
                 variant_ = v;
                 zlen_ = zl;
                 if ((rc = build())) break;
                 if ((rc = reset_clock())) break;
-                if ((rc = launch(0))) break;  // warm-up
-                if ((rc = launch(1))) break;
+                if ((rc = launch(0, 0))) break;  // warm-up
+                if ((rc = launch(1, 0))) break;
                 if ((rc = cuda(cudaEventRecord(e0, st_)))) break;
-                for (int k = 0; k < 2 * reps && !rc; ++k) rc = launch(k & 1);
+                for (int k = 0; k < 2 * reps && !rc; ++k) rc = launch(k & 1, 0);
                 if (rc || (rc = cuda(cudaEventRecord(e1, st_)))) break;
                 if ((rc = cuda(cudaEventSynchronize(e1)))) break;
                 float ms = 0.f;
@@ -262,7 +320,7 @@ public:
     }
 
     int set_choice(int v, int zlen) {
-        if (v < 0 || v >= batch_f32_variant_count() || zlen < 0)
+        if (v < 0 || v >= variant_count() || zlen < 0)
             return set_error(SB200_ERR_INVALID, "sb200_batch_set_choice: bad variant or z length");
         if (int rc = synchronize()) return rc;
         variant_ = v;
@@ -301,7 +359,7 @@ private:
     }
 
     std::string key() const {
-        std::string k = "f32";
+        std::string k = f16_ ? "f16" : "f32";
         for (const Shot& h : shots_)
             k += ":" + std::to_string(h.g.nx) + "x" + std::to_string(h.g.ny) + "x" +
                  std::to_string(h.g.nz);
@@ -323,16 +381,22 @@ private:
     int build() {
         drop_graphs();
         const int n = n_shots();
-        const PencilBoxes bx = batch_f32_boxes(variant_);
+        const PencilBoxes bx = f16_ ? batch_f16_boxes(variant_) : batch_f32_boxes(variant_);
         std::vector<ShotF32> tab[2];
-        tab[0].resize(n);
-        tab[1].resize(n);
+        std::vector<ShotF16> tab16[2];
+        for (int par = 0; par < 2; ++par) {
+            if (f16_)
+                tab16[par].resize(n);
+            else
+                tab[par].resize(n);
+        }
         std::vector<int> order(n);
         std::iota(order.begin(), order.end(), 0);
         std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
             return shots_[a].g.interior() > shots_[b].g.interior();
         });
         std::vector<int4> items;
+        std::vector<int> tiles_x(n), tiles_y(n), zlen(n);
         for (int s = 0; s < n; ++s) {
             const Shot& h = shots_[s];
             const int inz = static_cast<int>(h.g.nz - 8);
@@ -341,14 +405,6 @@ private:
                 char* cur = arena_ + h.off[par];
                 char* prev = arena_ + h.off[par ^ 1];
                 char* vel = arena_ + h.off[2];
-                ShotF32& d = tab[par][s];
-                std::memset(&d, 0, sizeof(d));
-                int rc = tensor_map_3d(&d.p, cur, h.g.nx, h.g.ny, h.g.nz, 4, bx.halo_x, bx.halo_y);
-                if (!rc) rc = tensor_map_3d(&d.prev, prev, h.g.nx, h.g.ny, h.g.nz, 4, bx.tile_x, bx.tile_y);
-                if (!rc) rc = tensor_map_3d(&d.vel2, vel, h.g.nx, h.g.ny, h.g.nz, 4, bx.tile_x, bx.tile_y);
-                if (rc)
-                    return set_error(SB200_ERR_CUDA, "sb200_batch: tensor map encoding failed (" +
-                                                         std::to_string(rc) + ")");
                 SourceDesc src;
                 if (h.src >= 0) {
                     src.idx = h.src;
@@ -357,23 +413,53 @@ private:
                     src.step_offset = 0;
                     src.trace = trace_ + s * cap_;
                 }
-                d.args = batch_f32_shot_args(variant_, h.g, zc, reinterpret_cast<float*>(prev), src,
-                                             err_);
-                d.args.vel2 = reinterpret_cast<const float*>(vel);
+                CUtensorMap *mp, *mq, *mv;
+                if (f16_) {
+                    ShotF16& d = tab16[par][s];
+                    std::memset(&d, 0, sizeof(d));
+                    mp = &d.p;
+                    mq = &d.prev;
+                    mv = &d.k;
+                    d.args = batch_f16_shot_args(variant_, h.g, zc, reinterpret_cast<uint16_t*>(prev),
+                                                 src, scale_ + s, err_);
+                    tiles_x[s] = d.args.tiles_x;
+                    tiles_y[s] = d.args.tiles_y;
+                    zlen[s] = d.args.zlen;
+                } else {
+                    ShotF32& d = tab[par][s];
+                    std::memset(&d, 0, sizeof(d));
+                    mp = &d.p;
+                    mq = &d.prev;
+                    mv = &d.vel2;
+                    d.args = batch_f32_shot_args(variant_, h.g, zc, reinterpret_cast<float*>(prev), src,
+                                                 err_);
+                    d.args.vel2 = reinterpret_cast<const float*>(vel);
+                    tiles_x[s] = d.args.tiles_x;
+                    tiles_y[s] = d.args.tiles_y;
+                    zlen[s] = d.args.zlen;
+                }
+                int rc = tensor_map_3d(mp, cur, h.g.nx, h.g.ny, h.g.nz, esz_, bx.halo_x, bx.halo_y);
+                if (!rc) rc = tensor_map_3d(mq, prev, h.g.nx, h.g.ny, h.g.nz, esz_, bx.tile_x, bx.tile_y);
+                if (!rc) rc = tensor_map_3d(mv, vel, h.g.nx, h.g.ny, h.g.nz, esz_, bx.tile_x, bx.tile_y);
+                if (rc)
+                    return set_error(SB200_ERR_CUDA, "sb200_batch: tensor map encoding failed (" +
+                                                         std::to_string(rc) + ")");
             }
         }
         for (int s : order) {
-            const PencilArgs& a = tab[0][s].args;
             const int inz = static_cast<int>(shots_[s].g.nz - 8);
-            const int zc = (inz + a.zlen - 1) / a.zlen;
+            const int zc = (inz + zlen[s] - 1) / zlen[s];
             for (int z = 0; z < zc; ++z)
-                for (int y = 0; y < a.tiles_y; ++y)
-                    for (int x = 0; x < a.tiles_x; ++x) items.push_back(make_int4(s, x, y, z));
+                for (int y = 0; y < tiles_y[s]; ++y)
+                    for (int x = 0; x < tiles_x[s]; ++x) items.push_back(make_int4(s, x, y, z));
         }
-        for (int par = 0; par < 2; ++par)
-            if (int rc = cuda(cudaMemcpyAsync(table_[par], tab[par].data(), sizeof(ShotF32) * n,
+        for (int par = 0; par < 2; ++par) {
+            const void* src = f16_ ? static_cast<const void*>(tab16[par].data())
+                                   : static_cast<const void*>(tab[par].data());
+            if (int rc = cuda(cudaMemcpyAsync(table_[par], src, shot_bytes() * n,
                                               cudaMemcpyHostToDevice, st_)))
                 return rc;
+        }
         if (static_cast<int>(items.size()) > items_cap_) {
             if (items_) cudaFree(items_);
             items_ = nullptr;
@@ -389,23 +475,57 @@ private:
         if (cudaGetDevice(&dev) == cudaSuccess)
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaGetLastError();
-        ctas_ = static_cast<unsigned>(std::min<int64_t>(
-            int64_t(sms) * batch_f32_resident(variant_), std::max(1, n_items_)));
+        const int resident = f16_ ? batch_f16_resident(variant_) : batch_f32_resident(variant_);
+        ctas_ = static_cast<unsigned>(std::min<int64_t>(int64_t(sms) * resident, std::max(1, n_items_)));
         // the host copies above read std::vectors that go out of scope here
         return cuda(cudaStreamSynchronize(st_));
     }
 
-    int launch(int par) {
+    int launch(int par, int phase) {
         const cudaError_t e =
-            launch_batch_f32(variant_, table_[par], items_, n_items_, queue_, ctas_, st_);
+            f16_ ? launch_batch_f16(variant_, static_cast<const ShotF16*>(table_[par]), items_,
+                                    n_items_, queue_, ctas_, phase, st_)
+                 : launch_batch_f32(variant_, static_cast<const ShotF32*>(table_[par]), items_,
+                                    n_items_, queue_, ctas_, st_);
         return cuda(e);
+    }
+
+    // Step number k of the run (level parity par).  FP16: step k % kRenorm == 0
+    // renormalises every shot's scale from its FP64 statistics first and runs
+    // as phase 1, the next step as phase 2.
+    int step_once(int64_t k, int par) {
+        int phase = 0;
+        if (f16_) {
+            const int64_t r = k % kRenorm;
+            if (r == 0) {
+                if (int rc = renorm_all(par)) return rc;
+                phase = 1;
+            } else if (r == 1) {
+                phase = 2;
+            }
+        }
+        return launch(par, phase);
+    }
+
+    int renorm_all(int par) {
+        for (int s = 0; s < n_shots(); ++s) {
+            const Shot& h = shots_[s];
+            const sb200_grid gg = to_grid(h.g);
+            if (int rc = sb200_field_stats_f16(reinterpret_cast<const uint16_t*>(arena_ + h.off[par]),
+                                               &gg, 1.f, stats_ + 3 * s, scratch_, scratch_len_, st_))
+                return rc;
+            if (int rc = sb200_f16_renorm(stats_ + 3 * s, reinterpret_cast<sb200_f16_scale*>(scale_ + s),
+                                          bound_ + s * cap_, &queue_->step, 0.f, kTarget, st_))
+                return rc;
+        }
+        return SB200_OK;
     }
 
     int capture(int par, cudaGraphExec_t* out) {
         cudaGraph_t g = nullptr;
         if (int rc = cuda(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal))) return rc;
         int rc = SB200_OK;
-        for (int k = 0; k < chunk_ && !rc; ++k) rc = launch((par + k) & 1);
+        for (int k = 0; k < chunk_ && !rc; ++k) rc = step_once(k, (par + k) & 1);
         const cudaError_t e = cudaStreamEndCapture(st_, &g);
         if (rc) {
             if (g) cudaGraphDestroy(g);
@@ -417,6 +537,87 @@ private:
         return rc;
     }
 
+    int variant_count() const { return f16_ ? batch_f16_variant_count() : batch_f32_variant_count(); }
+    size_t shot_bytes() const { return f16_ ? sizeof(ShotF16) : sizeof(ShotF32); }
+
+    static sb200_grid to_grid(const GridDesc& g) {
+        sb200_grid gg{};
+        gg.nx = g.nx;
+        gg.ny = g.ny;
+        gg.nz = g.nz;
+        gg.dx = g.dx;
+        gg.dy = g.dy;
+        gg.dz = g.dz;
+        gg.dt = g.dt;
+        return gg;
+    }
+
+    // FP16: the shot's fields go through the FP32 staging buffer: p and p_prev
+    // packed at the initial power-of-two scale (target / (max |p| + the source
+    // bound of the first window)), vel2 to K in BF16.
+    int set_fields_f16(int s, const float* p, const float* p_prev, const float* vel2, int cur) {
+        const Shot& h = shots_[s];
+        const int64_t n = h.g.size();
+        double m = 0.0;
+        for (int64_t i = 0; i < n; ++i)
+            m = std::max(m, std::max(std::fabs(double(p[i])), std::fabs(double(p_prev[i]))));
+        vel2_src_[s] = h.src >= 0 ? vel2[h.src] : 0.f;
+        const std::vector<float> b = host_bound(s);
+        const double bnd = b.empty() ? 0.0 : b[0];
+        double a0 = 1.0;
+        if (m + bnd > 0.0)
+            a0 = std::ldexp(1.0, std::max(-120, std::min(120, int(std::floor(std::log2(
+                                                                  double(kTarget) / (m + bnd)))))));
+        const F16Scale s0{static_cast<float>(a0), 1.f};
+        if (int rc = cuda(cudaMemcpyAsync(scale_ + s, &s0, sizeof(s0), cudaMemcpyHostToDevice, st_)))
+            return rc;
+        const size_t bytes = static_cast<size_t>(n) * 4;
+        const sb200_grid gg = to_grid(h.g);
+        struct Part {
+            const float* host;
+            int level;  // index into the shot's offsets: current, previous, K (2)
+        };
+        const Part parts[3] = {{p, cur}, {p_prev, cur ^ 1}, {vel2, 2}};
+        for (const Part& part : parts) {
+            if (int rc = cuda(cudaMemcpyAsync(staging_, part.host, bytes, cudaMemcpyHostToDevice, st_)))
+                return rc;
+            uint16_t* dst = reinterpret_cast<uint16_t*>(arena_ + h.off[part.level]);
+            const int rc = part.level == 2 ? sb200_k_field_bf16(staging_, dst, &gg, st_)
+                                           : sb200_f16_pack(staging_, dst, n, float(a0), st_);
+            if (rc) return rc;
+            // the staging buffer is reused by the next part
+            if (int r2 = cuda(cudaStreamSynchronize(st_))) return r2;
+        }
+        return upload_bound(s);
+    }
+
+    // bound[k] = 2 x sum over the renormalisation window from step k of
+    // |dt^2 vel2[src] w|: the most the source can add to |p| before the next
+    // renormalisation (2x: the wave can focus).
+    std::vector<float> host_bound(int s) const {
+        const std::vector<float>& w = wave_host_[s];
+        const int64_t n = static_cast<int64_t>(w.size());
+        std::vector<float> b(std::max<int64_t>(n, 1), 0.f);
+        if (shots_[s].src < 0 || n == 0) return b;
+        const double k = double(shots_[s].g.dt) * shots_[s].g.dt * vel2_src_[s];
+        double acc = 0.0;
+        for (int64_t j = n - 1; j >= 0; --j) {
+            acc += std::fabs(k * w[j]);
+            if (j + kRenorm < n) acc -= std::fabs(k * w[j + kRenorm]);
+            b[j] = static_cast<float>(2.0 * acc);
+        }
+        return b;
+    }
+
+    int upload_bound(int s) {
+        std::vector<float> b = host_bound(s);
+        b.resize(static_cast<size_t>(cap_), 0.f);
+        if (int rc = cuda(cudaMemcpyAsync(bound_ + s * cap_, b.data(), sizeof(float) * cap_,
+                                          cudaMemcpyHostToDevice, st_)))
+            return rc;
+        return cuda(cudaStreamSynchronize(st_));
+    }
+
     void drop_graphs() {
         for (auto& g : graph_)
             if (g) {
@@ -425,10 +626,25 @@ private:
             }
     }
 
+    static constexpr int kRenorm = 50;        // FP16: steps between renormalisations
+    static constexpr float kTarget = 4096.f;  // FP16: scaled max |p| aimed for
+
     std::vector<Shot> shots_;
     char* arena_ = nullptr;
     size_t arena_bytes_ = 0;
-    ShotF32* table_[2] = {nullptr, nullptr};
+    void* table_[2] = {nullptr, nullptr};  // ShotF32 or ShotF16 tables
+    bool f16_ = false;
+    int esz_ = 4;
+    int64_t max_points_ = 0;
+    F16Scale* scale_ = nullptr;  // FP16: per-shot scale
+    double* stats_ = nullptr;    // FP16: per-shot FP64 statistics (3 each)
+    double* scratch_ = nullptr;
+    int64_t scratch_len_ = 0;
+    float* bound_ = nullptr;    // FP16: per-shot source bound per step (max_steps each)
+    float* staging_ = nullptr;  // FP16: one shot's FP32 field
+    std::vector<std::vector<float>> wave_host_;
+    std::vector<float> vel2_src_;
+
     BatchQueue* queue_ = nullptr;
     int4* items_ = nullptr;
     int items_cap_ = 0;
@@ -542,5 +758,9 @@ void* sb200_batch_stream(void* h) { return h ? static_cast<void*>(as_batch(h)->s
 int sb200_batch_variant_count(void) { return batch_f32_variant_count(); }
 
 const char* sb200_batch_variant_name(int v) { return batch_f32_variant_name(v); }
+
+int sb200_batch_variant_count_f16(void) { return batch_f16_variant_count(); }
+
+const char* sb200_batch_variant_name_f16(int v) { return batch_f16_variant_name(v); }
 
 }  // extern "C"

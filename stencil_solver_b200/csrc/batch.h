@@ -47,6 +47,32 @@ struct alignas(64) ShotF32 {
     PencilArgs args;
 };
 
+// Arguments of one FP16-storage sweep over one grid (pencil_f16.cu): p and
+// p_prev FP16 at the power-of-two scale scale->a, K = vel2 dt^2 / dx^2 in BF16.
+struct F16Args {
+    uint16_t* next;  // p_next (aliases the p_prev buffer read through qmap)
+    int nx, ny, nz;
+    int64_t sy, sz;
+    int tiles_x, tiles_y, zlen;
+    Weights w;   // Laplacian weights relative to K: ax = c_r, ay = c_r (dx/dy)^2, ...
+    float dx2;   // dx^2: the source term dt^2 vel2 w = K dx^2 w
+    int src_x, src_y, src_z;
+    float src_w;
+    const float* src_wavelet;
+    const int* src_step;
+    int src_off;
+    float* trace;
+    const F16Scale* scale;
+    int* err;
+};
+
+// One shot of the FP16 batch, in device memory: p with the halo box, p_prev and
+// K with the tile box, and the sweep's arguments (next = prev: in place).
+struct alignas(64) ShotF16 {
+    CUtensorMap p, prev, k;
+    F16Args args;
+};
+
 // Work item: x = shot, y = tile x, z = tile y, w = z chunk.
 int batch_f32_variant_count();
 const char* batch_f32_variant_name(int v);
@@ -59,5 +85,18 @@ PencilArgs batch_f32_shot_args(int v, const GridDesc& g, int zchunks, float* nex
                                const SourceDesc& src, int* err);
 cudaError_t launch_batch_f32(int v, const ShotF32* shots, const int4* items, int n_items,
                              BatchQueue* queue, unsigned ctas, cudaStream_t stream);
+
+int batch_f16_variant_count();
+const char* batch_f16_variant_name(int v);
+PencilBoxes batch_f16_boxes(int v);
+int batch_f16_resident(int v);
+void batch_f16_prepare();
+// Sweep arguments of one FP16 shot for variant v split into zchunks z chunks;
+// scale: the shot's device scale, next: its p_prev / p_next level.
+F16Args batch_f16_shot_args(int v, const GridDesc& g, int zchunks, uint16_t* next,
+                            const SourceDesc& src, const F16Scale* scale, int* err);
+// phase: 0 plain, 1 renormalisation step, 2 the step after it (every shot).
+cudaError_t launch_batch_f16(int v, const ShotF16* shots, const int4* items, int n_items,
+                             BatchQueue* queue, unsigned ctas, int phase, cudaStream_t stream);
 
 }  // namespace sb200

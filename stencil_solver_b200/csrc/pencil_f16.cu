@@ -36,6 +36,7 @@
 #include <algorithm>
 #include <mutex>
 
+#include "batch.h"
 #include "kernels.h"
 #include "sb200_common.cuh"
 
@@ -43,22 +44,6 @@ namespace sb200 {
 
 namespace {
 
-struct F16Args {
-    uint16_t* next;  // p_next (aliases the p_prev buffer read through qmap)
-    int nx, ny, nz;
-    int64_t sy, sz;
-    int tiles_x, tiles_y, zlen;
-    Weights w;   // Laplacian weights relative to K: ax = c_r, ay = c_r (dx/dy)^2, ...
-    float dx2;   // dx^2: the source term dt^2 vel2 w = K dx^2 w
-    int src_x, src_y, src_z;
-    float src_w;
-    const float* src_wavelet;
-    const int* src_step;
-    int src_off;
-    float* trace;
-    const F16Scale* scale;
-    int* err;
-};
 
 template <int TX, int TY, int S, int AUX>
 struct ShapeH {
@@ -154,55 +139,45 @@ __device__ __forceinline__ float xsum1(const float (&c)[8], uint2 lf, uint2 rt, 
     return c[up] + c[dn];
 }
 
+// One tile: columns [tx TX, tx TX + TX) x rows [4 + ty TY, ...) of the interior,
+// marched over z chunk zc.  All threads of the CTA call it; `sm`, `full` and
+// `auxf` are the CTA's rings, their mbarriers freshly initialised by the caller
+// (phase 0 on every stage).  Every copy it issues has landed when it returns;
+// false means a bounded wait gave up (the error is recorded).
 template <int TX, int TY, int S, int AUX, int PHASE, int UNR>
-__global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, AUX>::MINB)
-    pencil_f16_kernel(const __grid_constant__ CUtensorMap pmap,
-                      const __grid_constant__ CUtensorMap qmap,
-                      const __grid_constant__ CUtensorMap kmap, const F16Args a) {
+__device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const CUtensorMap* qmap,
+                                                const CUtensorMap* kmap, const F16Args& a,
+                                                int tx, int ty, int zc, uint16_t* sm,
+                                                uint64_t* full, uint64_t* auxf) {
     using P = ShapeH<TX, TY, S, AUX>;
-    extern __shared__ unsigned char dsmem[];
-    __shared__ __align__(8) uint64_t full[S];
-    __shared__ __align__(8) uint64_t auxf[AUX];
-    uint16_t* sm = reinterpret_cast<uint16_t*>(smem_align<128>(dsmem));
     uint16_t* aux = sm + S * P::PLANE;  // AUX stages of [p_prev tile | K tile]
 
     const int tid = threadIdx.x;
     const int lx = tid % P::TPR;
     const int ly = tid / P::TPR;
-    int b = blockIdx.x;
-    const int tx = b % a.tiles_x;
-    b /= a.tiles_x;
-    const int ty = b % a.tiles_y;
-    b /= a.tiles_y;
     const int xa = tx * TX;      // first x of the tile (multiple of 8)
     const int y0 = R + ty * TY;  // first interior row of the tile
-    const int zb = R + b * a.zlen;
+    const int zb = R + zc * a.zlen;
     const int ze = min(zb + a.zlen, a.nz - R);
     const int nint = ze - zb;
     const int nplanes = nint + 2 * R;
 
     if (tid == 0) {
-        prefetch_tmap(&pmap);
-        prefetch_tmap(&qmap);
-        prefetch_tmap(&kmap);
-#pragma unroll
-        for (int s = 0; s < S; ++s) mbar_init(&full[s], 1);
-#pragma unroll
-        for (int s = 0; s < AUX; ++s) mbar_init(&auxf[s], 1);
-        fence_barrier_init();
+        prefetch_tmap(pmap);
+        prefetch_tmap(qmap);
+        prefetch_tmap(kmap);
     }
-    __syncthreads();
     int issued_hi = -1, aux_issued_hi = -1;
     auto issue_plane = [&](int j) {  // thread 0 only
         mbar_arrive_expect_tx(&full[j % S], P::PLANE_BYTES);
-        tma_load_3d(sm + (j % S) * P::PLANE, &pmap, &full[j % S], xa - 8, y0 - R, zb - R + j);
+        tma_load_3d(sm + (j % S) * P::PLANE, pmap, &full[j % S], xa - 8, y0 - R, zb - R + j);
         issued_hi = j;
     };
     auto issue_aux = [&](int it) {  // thread 0 only
         uint16_t* st = aux + (it % AUX) * 2 * P::TILE;
         mbar_arrive_expect_tx(&auxf[it % AUX], 2 * P::TILE_BYTES);
-        tma_load_3d(st, &qmap, &auxf[it % AUX], xa, y0, zb + it);
-        tma_load_3d(st + P::TILE, &kmap, &auxf[it % AUX], xa, y0, zb + it);
+        tma_load_3d(st, qmap, &auxf[it % AUX], xa, y0, zb + it);
+        tma_load_3d(st + P::TILE, kmap, &auxf[it % AUX], xa, y0, zb + it);
         aux_issued_hi = it;
     };
     if (tid == 0) {
@@ -398,7 +373,91 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
         for (int it = max(0, aux_issued_hi - AUX + 1); it <= aux_issued_hi; ++it)
             (void)mbar_wait(&auxf[it % AUX], (it / AUX) & 1);
     }
+    return !abort_run;
 }
+
+// (Re)initialises the CTA's ring barriers (thread 0); the caller synchronises.
+// A barrier is invalidated before it is initialised again: by then every copy
+// that completed on it has been waited for.
+template <int S, int AUX>
+__device__ __forceinline__ void init_rings_f16(uint64_t* full, uint64_t* auxf, bool again) {
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        if (again) mbar_inval(&full[s]);
+        mbar_init(&full[s], 1);
+    }
+#pragma unroll
+    for (int s = 0; s < AUX; ++s) {
+        if (again) mbar_inval(&auxf[s]);
+        mbar_init(&auxf[s], 1);
+    }
+    fence_barrier_init();
+}
+
+// One grid: CTA b owns tile (b % tiles_x, (b / tiles_x) % tiles_y) and z chunk
+// b / (tiles_x * tiles_y).
+template <int TX, int TY, int S, int AUX, int PHASE, int UNR>
+__global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, AUX>::MINB)
+    pencil_f16_kernel(const __grid_constant__ CUtensorMap pmap,
+                      const __grid_constant__ CUtensorMap qmap,
+                      const __grid_constant__ CUtensorMap kmap, const F16Args a) {
+    extern __shared__ unsigned char dsmem[];
+    __shared__ __align__(8) uint64_t full[S];
+    __shared__ __align__(8) uint64_t auxf[AUX];
+    uint16_t* sm = reinterpret_cast<uint16_t*>(smem_align<128>(dsmem));
+    if (threadIdx.x == 0) init_rings_f16<S, AUX>(full, auxf, false);
+    __syncthreads();
+    int b = blockIdx.x;
+    const int tx = b % a.tiles_x;
+    b /= a.tiles_x;
+    const int ty = b % a.tiles_y;
+    b /= a.tiles_y;
+    (void)pencil_f16_tile<TX, TY, S, AUX, PHASE, UNR>(&pmap, &qmap, &kmap, a, tx, ty, b, sm, full,
+                                                      auxf);
+}
+
+// Many grids (shots) in one persistent launch, as batch_f32_kernel: CTAs take
+// (shot, tile x, tile y, z chunk) items from the queue; the rings' barriers are
+// re-initialised for every item; the last CTA to finish resets the queue and
+// advances the step counter the sources read.
+template <int TX, int TY, int S, int AUX, int PHASE, int UNR>
+__global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, AUX>::MINB)
+    batch_f16_kernel(const ShotF16* __restrict__ shots, const int4* __restrict__ items,
+                     int n_items, BatchQueue* queue) {
+    extern __shared__ unsigned char dsmem[];
+    __shared__ __align__(8) uint64_t full[S];
+    __shared__ __align__(8) uint64_t auxf[AUX];
+    __shared__ int s_item;
+    uint16_t* sm = reinterpret_cast<uint16_t*>(smem_align<128>(dsmem));
+    bool first = true;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            s_item = atomicAdd(&queue->next, 1);
+            init_rings_f16<S, AUX>(full, auxf, !first);
+        }
+        first = false;
+        __syncthreads();
+        const int it = s_item;
+        __syncthreads();  // every thread has read s_item before it is replaced
+        if (it >= n_items) break;
+        const int4 w = items[it];
+        const ShotF16* sh = shots + w.x;
+        const F16Args a = sh->args;
+        if (!pencil_f16_tile<TX, TY, S, AUX, PHASE, UNR>(&sh->p, &sh->prev, &sh->k, a, w.y, w.z,
+                                                         w.w, sm, full, auxf))
+            break;
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&queue->done, 1) == static_cast<int>(gridDim.x) - 1) {
+            queue->next = 0;
+            queue->done = 0;
+            queue->step += 1;
+            __threadfence();
+        }
+    }
+}
+
 
 using LaunchFnH = cudaError_t (*)(const PencilMaps&, const F16Args&, unsigned, int, cudaStream_t);
 using ResidentFnH = int (*)();
@@ -499,11 +558,12 @@ int64_t pencil_f16_ctas(int v, const GridDesc& g, int zchunks) {
     return int64_t(tiles_x) * tiles_y * ((inz + zlen - 1) / zlen);
 }
 
-cudaError_t launch_wave_pencil_f16(const PencilMaps& maps, uint16_t* next, const GridDesc& g,
-                                   const SourceDesc& src, const F16Scale* scale, int phase,
-                                   const PencilConfig& cfg, int* err, cudaStream_t stream) {
-    if (!g.has_interior()) return cudaSuccess;
-    const VariantH& v = kF16[cfg.variant];
+namespace {
+
+// Sweep arguments of a TX x TY tile shape over grid g split into zchunks z
+// chunks: tile counts, weights relative to K, source, scale.
+F16Args make_f16_args(int TX, int TY, const GridDesc& g, int zchunks, uint16_t* next,
+                      const SourceDesc& src, const F16Scale* scale, int* err) {
     F16Args a{};
     a.next = next;
     a.nx = static_cast<int>(g.nx);
@@ -512,13 +572,11 @@ cudaError_t launch_wave_pencil_f16(const PencilMaps& maps, uint16_t* next, const
     a.sy = g.nx;
     a.sz = g.nx * g.ny;
     // x tiles start at 0 and cover every x below nx - 4.
-    a.tiles_x = static_cast<int>((g.nx - R + v.tx - 1) / v.tx);
-    a.tiles_y = static_cast<int>((g.ny - 2 * R + v.ty - 1) / v.ty);
+    a.tiles_x = static_cast<int>((g.nx - R + TX - 1) / TX);
+    a.tiles_y = static_cast<int>((g.ny - 2 * R + TY - 1) / TY);
     const int inz = static_cast<int>(g.nz - 2 * R);
-    const int zc = std::max(1, std::min(cfg.zchunks, inz));
+    const int zc = std::max(1, std::min(zchunks, inz));
     a.zlen = (inz + zc - 1) / zc;
-    const unsigned ctas = static_cast<unsigned>(int64_t(a.tiles_x) * a.tiles_y *
-                                                ((inz + a.zlen - 1) / a.zlen));
     const double ry = double(g.dx) * g.dx / (double(g.dy) * g.dy);
     const double rz = double(g.dx) * g.dx / (double(g.dz) * g.dz);
     const double c[R + 1] = {C0, C1, C2, C3, C4};
@@ -544,7 +602,111 @@ cudaError_t launch_wave_pencil_f16(const PencilMaps& maps, uint16_t* next, const
     }
     a.scale = scale;
     a.err = err;
+    return a;
+}
+
+// ── batched FP16 shots ────────────────────────────────────────────────────────
+
+using LaunchFnB16 = cudaError_t (*)(const ShotF16*, const int4*, int, BatchQueue*, unsigned, int,
+                                    cudaStream_t);
+
+template <int TX, int TY, int S, int AUX, int UNR>
+int resident_batch_f16() {
+    using P = ShapeH<TX, TY, S, AUX>;
+    static int cached[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cached[dev & 63] > 0) return cached[dev & 63];
+    const int smem = static_cast<int>(P::SMEM);
+    int n = 0;
+    if (cudaFuncSetAttribute(batch_f16_kernel<TX, TY, S, AUX, 0, UNR>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
+        cudaFuncSetAttribute(batch_f16_kernel<TX, TY, S, AUX, 1, UNR>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
+        cudaFuncSetAttribute(batch_f16_kernel<TX, TY, S, AUX, 2, UNR>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_f16_kernel<TX, TY, S, AUX, 0, UNR>,
+                                                      P::NT, P::SMEM) == cudaSuccess &&
+        n > 0) {
+        cached[dev & 63] = n;
+        return n;
+    }
+    cudaGetLastError();
+    return std::max(1, std::min(int((228u * 1024u) / (P::SMEM + 1024u)), 65536 / (P::NT * 128)));
+}
+
+template <int TX, int TY, int S, int AUX, int UNR>
+cudaError_t launch_batch_f16_t(const ShotF16* shots, const int4* items, int n_items,
+                               BatchQueue* queue, unsigned ctas, int phase, cudaStream_t stream) {
+    using P = ShapeH<TX, TY, S, AUX>;
+    resident_batch_f16<TX, TY, S, AUX, UNR>();  // sets the attributes once per device
+    if (phase == 1)
+        batch_f16_kernel<TX, TY, S, AUX, 1, UNR><<<ctas, P::NT, P::SMEM, stream>>>(shots, items,
+                                                                                    n_items, queue);
+    else if (phase == 2)
+        batch_f16_kernel<TX, TY, S, AUX, 2, UNR><<<ctas, P::NT, P::SMEM, stream>>>(shots, items,
+                                                                                    n_items, queue);
+    else
+        batch_f16_kernel<TX, TY, S, AUX, 0, UNR><<<ctas, P::NT, P::SMEM, stream>>>(shots, items,
+                                                                                    n_items, queue);
+    return cudaGetLastError();
+}
+
+struct VariantB16 {
+    int tx, ty;
+    const char* name;
+    LaunchFnB16 launch;
+    ResidentFnH resident;
+};
+
+const VariantB16 kBatchF16[] = {
+    {64, 16, "bh64x16_s8_a4", &launch_batch_f16_t<64, 16, 8, 4, 4>,
+     &resident_batch_f16<64, 16, 8, 4, 4>},
+    {32, 16, "bh32x16_s8_a4", &launch_batch_f16_t<32, 16, 8, 4, 4>,
+     &resident_batch_f16<32, 16, 8, 4, 4>},
+    {64, 8, "bh64x8_s8_a4", &launch_batch_f16_t<64, 8, 8, 4, 4>,
+     &resident_batch_f16<64, 8, 8, 4, 4>},
+};
+constexpr int kNumBatchF16 = sizeof(kBatchF16) / sizeof(kBatchF16[0]);
+
+}  // namespace
+
+cudaError_t launch_wave_pencil_f16(const PencilMaps& maps, uint16_t* next, const GridDesc& g,
+                                   const SourceDesc& src, const F16Scale* scale, int phase,
+                                   const PencilConfig& cfg, int* err, cudaStream_t stream) {
+    if (!g.has_interior()) return cudaSuccess;
+    const VariantH& v = kF16[cfg.variant];
+    const F16Args a = make_f16_args(v.tx, v.ty, g, cfg.zchunks, next, src, scale, err);
+    const int inz = static_cast<int>(g.nz - 2 * R);
+    const unsigned ctas = static_cast<unsigned>(int64_t(a.tiles_x) * a.tiles_y *
+                                                ((inz + a.zlen - 1) / a.zlen));
     return v.launch(maps, a, ctas, phase, stream);
+}
+
+int batch_f16_variant_count() { return kNumBatchF16; }
+const char* batch_f16_variant_name(int v) {
+    return (v >= 0 && v < kNumBatchF16) ? kBatchF16[v].name : nullptr;
+}
+PencilBoxes batch_f16_boxes(int v) {
+    PencilBoxes b;
+    b.halo_x = kBatchF16[v].tx + 16;
+    b.halo_y = kBatchF16[v].ty + 2 * R;
+    b.tile_x = kBatchF16[v].tx;
+    b.tile_y = kBatchF16[v].ty;
+    b.aux_tma = true;
+    return b;
+}
+int batch_f16_resident(int v) { return kBatchF16[v].resident(); }
+void batch_f16_prepare() {
+    for (int v = 0; v < kNumBatchF16; ++v) kBatchF16[v].resident();
+}
+F16Args batch_f16_shot_args(int v, const GridDesc& g, int zchunks, uint16_t* next,
+                            const SourceDesc& src, const F16Scale* scale, int* err) {
+    return make_f16_args(kBatchF16[v].tx, kBatchF16[v].ty, g, zchunks, next, src, scale, err);
+}
+cudaError_t launch_batch_f16(int v, const ShotF16* shots, const int4* items, int n_items,
+                             BatchQueue* queue, unsigned ctas, int phase, cudaStream_t stream) {
+    return kBatchF16[v].launch(shots, items, n_items, queue, ctas, phase, stream);
 }
 
 }  // namespace sb200

@@ -59,6 +59,12 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
                  : "memory");
 }
 
+// Invalidates a barrier whose phases have all completed, before it is
+// initialised again.
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // Make barrier initialisation visible to the async (TMA) proxy.
 __device__ __forceinline__ void fence_barrier_init() {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");

@@ -116,3 +116,65 @@ def test_batch_rejects_bad_shots():
         with pytest.raises(sb.StencilError) as e:
             b.steps(1)
         assert e.value.status == sb.SB200_ERR_INVALID
+
+
+def run_batch_f16(shots, steps=120, chunk=50, choice=None, split=(7, 113)):
+    with sb.Batch([(g, s) for g, s, _, _ in shots], max_steps=steps, graph_chunk=chunk,
+                  precision=sb.PRECISION_F16) as b:
+        if choice is not None:
+            b.set_choice(*choice)
+        for i, (g, _, v, w) in enumerate(shots):
+            z = np.zeros(g.shape, np.float32)
+            b.set_fields(i, z, z, v)
+            b.set_wavelet(i, w)
+        for k in split:
+            b.steps(k)
+        b.synchronize()
+        return [(b.field(i), b.trace(i, steps)) for i in range(len(shots))]
+
+
+def test_f16_batch_matches_single_grid_f16_runs_bitwise():
+    """FP16-storage batch: per-shot power-of-two scales renormalised every 50
+    steps (eager steps and a captured 50-step chunk), bit for bit the FP16 run
+    engine on each shot alone."""
+    steps = 120
+    shots = make_shots(seed=21)
+    shots = [(g, s, v, np.pad(w, (0, steps - len(w)))) for g, s, v, w in shots]
+    got = run_batch_f16(shots, steps=steps)
+    for (g, src, v, w), (p, tr) in zip(shots, got):
+        z = np.zeros(g.shape, np.float32)
+        with sb.Run(g, src_index=src, graph_chunk=0, precision=sb.PRECISION_F16) as r:
+            r.set_fields(z, z, v)
+            r.set_wavelet(w)
+            r.steps(steps)
+            ref_p, ref_tr = r.field(), r.trace(steps)
+        assert np.abs(p).max() > 0
+        assert np.array_equal(p, ref_p)
+        assert np.array_equal(tr, ref_tr)
+
+
+@pytest.mark.parametrize("zlen", [0, 16])
+def test_f16_batch_every_variant_agrees(zlen):
+    steps = 60
+    shots = make_shots(seed=23)
+    base = run_batch_f16(shots, steps=steps, choice=(0, 64), split=(60,))
+    for v in range(sb.lib().sb200_batch_variant_count_f16()):
+        got = run_batch_f16(shots, steps=steps, choice=(v, zlen), split=(60,))
+        for (p0, t0), (p1, t1) in zip(base, got):
+            assert np.array_equal(p0, p1), v
+            assert np.array_equal(t0, t1), v
+
+
+def test_f16_batch_tune_and_validation():
+    shots = make_shots(seed=25)
+    with sb.Batch([(g, s) for g, s, _, _ in shots], max_steps=20, graph_chunk=0,
+                  precision=sb.PRECISION_F16) as b:
+        b.tune(reps=1)
+        c = b.choice()
+        assert 0 <= c["variant"] < sb.lib().sb200_batch_variant_count_f16() and c["items"] > 0
+    g = sb.Grid(36, 32, 32)  # nx % 8 != 0
+    with pytest.raises(sb.StencilError):
+        sb.Batch([(g, None)], max_steps=10, graph_chunk=0, precision=sb.PRECISION_F16)
+    g = sb.Grid(40, 32, 32)
+    with pytest.raises(sb.StencilError):  # a chunk that does not start on a renorm
+        sb.Batch([(g, None)], max_steps=100, graph_chunk=30, precision=sb.PRECISION_F16)
