@@ -379,7 +379,8 @@ def secondary_batch(n_shots: int = 48, steps: int = 400):
     """48 independent acoustic shots, extents U{96..320 step 8} per axis, each its
     own seeded layered model, a Ricker (U[10, 25] Hz) at a random interior cell,
     400 steps in 100-step CUDA-graph chunks, tuned: one persistent launch per
-    step, against the same shots as separate runs (one graph chain each)."""
+    step, against the same shots as separate runs (one graph chain each); then
+    the same shots with FP16 storage."""
     import torch
 
     import stencil_solver_b200 as sb
@@ -397,7 +398,7 @@ def secondary_batch(n_shots: int = 48, steps: int = 400):
         shots.append((g, src))
         fields.append((vel2, sb.ricker(f, 1.0 / f, dt, steps)))
     pts = sum(g.interior for g, _ in shots)
-    out = {"workload": f"batch_{n_shots}_shots_fp32", "shots": n_shots, "steps": steps,
+    out = {"workload": f"batch_{n_shots}_shots_fp32_and_fp16", "shots": n_shots, "steps": steps,
            "interior_points": pts}
     with sb.Batch(shots, max_steps=steps, graph_chunk=100) as b:
         b.tune(reps=3)
@@ -433,6 +434,25 @@ def secondary_batch(n_shots: int = 48, steps: int = 400):
         r.close()
     out["separate_runs"] = {"ms_per_step_wall": wall, "gpts_per_s": pts / (wall * 1e-3) / 1e9}
     out["speedup_batched_vs_separate"] = wall / ms
+    # FP16-storage variant of the same shots: per-shot power-of-two scales
+    # renormalised every 50 steps inside the 100-step graphs (8 B per point).
+    with sb.Batch(shots, max_steps=steps, graph_chunk=100, precision=sb.PRECISION_F16) as b:
+        b.tune(reps=3)
+        for i, ((g, _), (vel2, w)) in enumerate(zip(shots, fields)):
+            z = np.zeros(g.shape, np.float32)
+            b.set_fields(i, z, z, vel2)
+            b.set_wavelet(i, w)
+        st = torch.cuda.ExternalStream(b.stream)
+        e0, e1 = _events()
+        torch.cuda.synchronize()
+        e0.record(st)
+        b.steps(steps)
+        e1.record(st)
+        b.synchronize()
+        ms16 = e0.elapsed_time(e1) / steps
+        out["batched_fp16"] = {"ms_per_step": ms16, "gpts_per_s": pts / (ms16 * 1e-3) / 1e9,
+                               "achieved_gbs": 8 * pts / (ms16 * 1e-3) / 1e9,
+                               "speedup_vs_fp32_batch": ms / ms16, **b.choice()}
     return out
 
 
