@@ -55,6 +55,8 @@ def args_():
     ap.add_argument("--zchunks", type=int, default=1)
     ap.add_argument("--no-secondary", action="store_true",
                     help="skip the heat / FP16 / batch / learned measurements")
+    ap.add_argument("--f16", action="store_true",
+                    help="--kernel batch: the FP16-storage batch")
     ap.add_argument("--sparse", action="store_true",
                     help="--kernel learned: a small random cube in a zero field (floor 2^-64)")
     ap.add_argument("--kernel", choices=["acoustic", "heat", "fp16", "batch", "mlp", "learned"],
@@ -753,7 +755,8 @@ def run_kernel_probe(a):
             ext = [int(rng.choice(np.arange(max(24, n // 2), n + 1, 8))) for _ in range(3)]
             gb = sb.Grid(*ext, DX, DX, DX, 8.5e-4)
             shots.append((gb, gb.index(ext[0] // 2, ext[1] // 2, ext[2] // 2)))
-        b = sb.Batch(shots, max_steps=a.warmup + a.steps + 2, graph_chunk=0)
+        b = sb.Batch(shots, max_steps=a.warmup + a.steps + 2, graph_chunk=0,
+                     precision=sb.PRECISION_F16 if a.f16 else sb.PRECISION_F32)
         b.set_choice(max(a.variant, 0), 64)
         for i, (gb, _) in enumerate(shots):
             z = np.zeros(gb.shape, np.float32)

@@ -11,9 +11,10 @@
 // from a 9-deep register queue (shifted one slot per plane).  Each thread owns 4
 // consecutive x of one row.  Per plane:
 //   1. the stencil (the pencil kernel's arithmetic and order) and the 26
-//      features of each of the thread's 4 points: the differences are rounded to
-//      BF16 unscaled and 1/s is applied to the first layer's accumulator (s is a
-//      power of two, so this is exact);
+//      features of each of the thread's 4 points, in the correction kernel's
+//      arithmetic: the star's largest magnitude first, then the differences
+//      times 1/s, rounded to BF16 (rounding the unscaled differences and
+//      applying 1/s to the accumulator would differ where they are subnormal);
 //   2. the feature row of the thread's point e goes to row `tid` of A tile e
 //      (4 tiles x 128 rows, K-major BF16), so TMEM lane `tid` of tile e's
 //      accumulator is this thread's own point: the correction lands in the
@@ -21,7 +22,7 @@
 //   3. one thread issues tcgen05.mma (M = 128, N = 32, K = 16: 2 per tile and
 //      layer) into TMEM columns 32 e, commits to an mbarrier that every thread
 //      waits on (two CTA barriers per plane in all); the epilogue of
-//      layer 1 (1/s, bias, ReLU, BF16) writes layer 2's A tiles over the
+//      layer 1 (bias, ReLU, BF16) writes layer 2's A tiles over the
 //      features, layer 2 overwrites the accumulators, its epilogue (bias, ReLU,
 //      w3 dot product) finishes the correction.
 // Points whose star stays below the network's correction floor (by default: is
@@ -277,55 +278,63 @@ __global__ void __launch_bounds__(LNT, 3)
             o = make_float4(o0.x, o0.y, o1.x, o1.y);
         }
 
-        // Features, one pair of points at a time: per axis and radius the word
-        // (up - dn, (up + dn) - 2c), unscaled, packed as soon as it is computed;
-        // the star's largest magnitude gives s, and the last word is (c, Courant
-        // number x s).  Point e's row is row tid of A tile e.
+        // Features, one pair of points at a time, in the correction kernel's
+        // arithmetic: the star's largest magnitude gives s first, then per axis
+        // and radius the word ((up - dn) / s, ((up + dn) - 2c) / s), rounded to
+        // BF16 after the (exact, power-of-two) scaling so that tiny and
+        // subnormal stars round as they do there; the last word is (c / s,
+        // Courant number).  Point e's row is row tid of A tile e.
         // A thread whose stars are all zero writes no rows (its points' corrections
         // are exactly zero); one that writes first makes sure no MMA of the
         // previous plane still reads the tiles (it may have skipped that wait).
-        float inv[4] = {0.f, 0.f, 0.f, 0.f}, sc[4] = {0.f, 0.f, 0.f, 0.f};
+        float sc[4] = {0.f, 0.f, 0.f, 0.f};
         bool act = false;
+        // Star arm of axis a3 at offset r (+-1..4) for points 2h, 2h + 1.
+        auto arm = [&](int a3, int r, int h) -> float2 {
+            if (a3 == 0) return make_float2(win[4 + 2 * h + r], win[5 + 2 * h + r]);
+            if (a3 == 1) return *reinterpret_cast<const float2*>(pc + r * LSX + 2 * h);
+            return pair_of(q[4 + r], h);
+        };
         if (tact && waited < ncommit) wait_mma();
 #pragma unroll
         for (int h = 0; h < 2 && tact; ++h) {
             const float2 ce = pair_of(c, h);
             float2 mx = make_float2(fabsf(ce.x), fabsf(ce.y));
+#pragma unroll
+            for (int a3 = 0; a3 < 3; ++a3)
+#pragma unroll
+                for (int r = 1; r <= R; ++r) {
+                    const float2 up = arm(a3, r, h);
+                    const float2 dn = arm(a3, -r, h);
+                    mx.x = fmaxf(mx.x, fmaxf(fabsf(up.x), fabsf(dn.x)));
+                    mx.y = fmaxf(mx.y, fmaxf(fabsf(up.y), fabsf(dn.y)));
+                }
+            float2 iv;
+            float s0, s1;
+            pow2_scale(rin && mx.x >= a.min_scale ? mx.x : 0.f, s0, iv.x);
+            pow2_scale(rin && mx.y >= a.min_scale ? mx.y : 0.f, s1, iv.y);
+            sc[2 * h] = s0 * a.out_scale;
+            sc[2 * h + 1] = s1 * a.out_scale;
+            act = act || s0 > 0.f || s1 > 0.f;
             uint32_t row0[16], row1[16];  // points 2h, 2h + 1
 #pragma unroll
             for (int a3 = 0; a3 < 3; ++a3)
 #pragma unroll
                 for (int r = 1; r <= R; ++r) {
-                    float2 up, dn;
-                    if (a3 == 0) {
-                        const int e = 4 + 2 * h;
-                        up = make_float2(win[e + r], win[e + 1 + r]);
-                        dn = make_float2(win[e - r], win[e + 1 - r]);
-                    } else if (a3 == 1) {
-                        up = *reinterpret_cast<const float2*>(pc + r * LSX + 2 * h);
-                        dn = *reinterpret_cast<const float2*>(pc - r * LSX + 2 * h);
-                    } else {
-                        up = pair_of(q[4 + r], h);
-                        dn = pair_of(q[4 - r], h);
-                    }
-                    const float2 dif = fma2(neg1, dn, up);
-                    const float2 sec = fma2(neg2, ce, add2(up, dn));
+                    const float2 up = arm(a3, r, h);
+                    const float2 dn = arm(a3, -r, h);
+                    const float2 dif = mul2(fma2(neg1, dn, up), iv);
+                    const float2 sec = mul2(fma2(neg2, ce, add2(up, dn)), iv);
                     const int k = 4 * a3 + r - 1;
                     row0[k] = pack_bf2(dif.x, sec.x);
                     row1[k] = pack_bf2(dif.y, sec.y);
-                    mx.x = fmaxf(mx.x, fmaxf(fabsf(up.x), fabsf(dn.x)));
-                    mx.y = fmaxf(mx.y, fmaxf(fabsf(up.y), fabsf(dn.y)));
                 }
+            const float2 cs = mul2(ce, iv);
 #pragma unroll
             for (int l = 0; l < 2; ++l) {
                 const int e = 2 * h + l;
-                float s;
-                const float mm = l ? mx.y : mx.x;
-                pow2_scale(rin && mm >= a.min_scale ? mm : 0.f, s, inv[e]);
-                sc[e] = s * a.out_scale;
-                act = act || s > 0.f;
                 uint32_t(&row)[16] = l ? row1 : row0;
-                row[12] = pack_bf2(l ? ce.y : ce.x, (sqrtf(lane_of(vv, e)) * a.dt_over_dx) * s);
+                row[12] = pack_bf2(l ? cs.y : cs.x, sqrtf(lane_of(vv, e)) * a.dt_over_dx);
                 row[13] = row[14] = row[15] = 0u;
                 store_row(sA + e * kTileA, tid, row);
             }
@@ -355,16 +364,15 @@ __global__ void __launch_bounds__(LNT, 3)
         if (!abort_run && any) ++ncommit;
         if (!abort_run && any && wact) {
             wait_mma();  // the layer-1 accumulators
-            // Layer 1 epilogue: h1 = relu(acc / s + b1) as BF16, over the features.
+            // Layer 1 epilogue: h1 = relu(acc + b1) as BF16.
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
                 float d[32];
                 tc_ld32(lane_base + 32 * e, d);
-                const float2 iv = dup2(inv[e]);
                 uint32_t hw[16];
 #pragma unroll
                 for (int k = 0; k < 16; ++k) {
-                    const float2 t = fma2(make_float2(d[2 * k], d[2 * k + 1]), iv,
+                    const float2 t = add2(make_float2(d[2 * k], d[2 * k + 1]),
                                           make_float2(a.b1[2 * k], a.b1[2 * k + 1]));
                     hw[k] = relu_bf2(t.x, t.y);
                 }

@@ -8,9 +8,9 @@
 // and r = 1..4 the pair (p_+r - p_-r, p_+r + p_-r - 2 p_c), then p_c, all / s,
 // then the local Courant number sqrt(vel2) dt / dx, padded to 32 -- where s is
 // the smallest power of two above the star's largest magnitude (0 for an all-zero
-// star).  With s a power of two, dividing by s commutes exactly with every FP32
-// and BF16 rounding, so a kernel may round the unscaled differences and apply
-// 1/s to the first layer's accumulator instead: the result is the same bits.
+// star).  Every kernel scales by 1/s (exact: a power of two) before the BF16
+// rounding; rounding the unscaled differences instead gives other bits where
+// they are FP32 or BF16 subnormals (the decaying tail ahead of a wave front).
 #pragma once
 
 #include <cuda_runtime.h>

@@ -217,23 +217,29 @@ def test_tcgen05_and_mma_correction_agree(torch_cuda):
     assert np.array_equal(outs["tcgen05"][0], outs["tcgen05"][1])  # deterministic
 
 
-@pytest.mark.parametrize("shape,sparse", [((40, 36, 72), False), ((29, 45, 40), False),
-                                          ((36, 52, 80), True)])
-def test_learned_step_is_step_plus_correction(torch_cuda, shape, sparse):
+@pytest.mark.parametrize("shape,mode", [((40, 36, 72), "dense"), ((29, 45, 40), "dense"),
+                                        ((36, 52, 80), "sparse"), ((32, 40, 64), "wide")])
+def test_learned_step_is_step_plus_correction(torch_cuda, shape, mode):
     """The fused learned step gives the same bits as the FP32 acoustic step
     followed by the tcgen05 correction: ragged tiles in x and y, unequal
-    spacings, an all-zero slab whose planes skip the network, and (sparse) a
+    spacings, an all-zero slab whose planes skip the network, (sparse) a
     field that is zero but for a small blob, so most threads and warps of the
-    active planes skip the features and epilogues."""
+    active planes skip the features and epilogues, and (wide) magnitudes
+    spread from 2^10 down into the FP32 subnormals, as in the tail of a wave
+    front, where the features must be scaled before their BF16 rounding."""
     torch = torch_cuda
     rng = np.random.default_rng(13)
     nz, ny, nx = shape
     p = rng.standard_normal(shape).astype(np.float32)
     p[: nz // 3] = 0.0
-    if sparse:
+    if mode == "sparse":
         blob = p[14:21, 20:27, 33:41].copy()
         p[:] = 0.0
         p[14:21, 20:27, 33:41] = blob
+    elif mode == "wide":
+        e2 = rng.uniform(-149.0, 10.0, shape)
+        p = np.where(p != 0.0, np.sign(p) * np.exp2(e2), 0.0).astype(np.float32)
+        assert (np.abs(p[p != 0]) < np.finfo(np.float32).tiny).any()
     q = rng.standard_normal(shape).astype(np.float32)
     v2 = rng.uniform(1500, 4500, shape).astype(np.float32) ** 2
     g = sb.Grid(nx, ny, nz, 10.0, 12.0, 9.0, 8e-4)
