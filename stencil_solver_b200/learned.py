@@ -12,7 +12,14 @@ Source: both grids discretise the same continuum term S(x, t) = A v^2 w(t) g(x),
 w a Ricker wavelet and g a Gaussian of width sigma (2 coarse cells by default)
 around the source point: each step adds dt^2 S(x_j, t_n) on a box of cells
 (the coarse grid's w samples are the [1, 2, 1] / 4 average of the fine ones,
-see Problem.wavelet).  A
+see Problem.wavelet).  Two fine leapfrog steps of h = dt / 2 compose to
+
+    p(t + 2h) - 2 p(t) + p(t - 2h) = (2h)^2 [L p + S-bar] + h^4 L^2 p + h^4 L S(t),
+
+L = v^2 lap and S-bar the [1, 2, 1] / 4 average: the coarse step has the first
+term; the network learns the h^4 L^2 p part of the rest (a function of the
+state); the coarse source adds the state-independent h^4 L S(t) term, computed
+once as the pattern v^2 lap(v^2 g) on the coarse grid (Problem.source).  A
 point source (the reference's rule, one cell) puts energy above the coarse
 grid's Nyquist wavenumber, which no coarse state can represent; the Gaussian
 keeps the field band-limited, so the coarse-grid error is the scheme's
@@ -37,6 +44,7 @@ from __future__ import annotations
 import ctypes as C
 import math
 from dataclasses import dataclass, field
+from typing import NamedTuple
 
 import numpy as np
 
@@ -61,6 +69,23 @@ def fine_extent(nc: int) -> int:
     return 2 * nc - 8
 
 
+# 8th-order central second-derivative weights (the library's FD coefficients)
+_FD8 = (-205.0 / 72, 8.0 / 5, -1.0 / 5, 8.0 / 315, -1.0 / 560)
+
+
+class Source(NamedTuple):
+    """A grid's source term: each step adds dt^2 amp w pattern on the box
+    (origin (x, y, z), dims); on the coarse grid also h^4 amp w(t) comp_pattern
+    on the box (comp_origin, comp_dims), h the fine step (the composition term)."""
+    origin: tuple
+    dims: tuple
+    pattern: object
+    amp: float
+    comp_origin: tuple = None
+    comp_dims: tuple = None
+    comp_pattern: object = None
+
+
 @dataclass
 class Problem:
     """One velocity model on the coarse / fine pair of grids."""
@@ -79,12 +104,14 @@ class Problem:
     perturbation: float = 0.05
     corr_cells: float = 20.0
     vel2_window: object = None  # device fine model to use instead of generating one
+    compose_source: bool = True  # the coarse source's h^4 L S term (see the module doc)
 
     def __post_init__(self):
         if self.src_c is None:
             c = self.nc // 2
             self.src_c = (c, c, c)
         self._vf = self._vc = None
+        self._wc = None  # cached wavelet_centre samples
 
     @property
     def coarse(self) -> Grid:
@@ -148,10 +175,18 @@ class Problem:
     def release(self) -> None:
         """Drops the cached device models."""
         self._vf = self._vc = None
+        self._wc = None  # cached wavelet_centre samples
 
-    def source(self, fine: bool):
-        """(origin, dims, pattern on the device, amplitude A): pattern_j = vel2_j g(x_j)
-        on the box of cells within 3.5 sigma of the source point."""
+    def wavelet_centre(self, n: int) -> np.ndarray:
+        """w(t_m) at the first n coarse times t_m = m dt (the centre sample of the
+        coarse [1, 2, 1] / 4 average): the fine samples of even index."""
+        return self.wavelet(True, 2 * n)[0::2]
+
+    def source(self, fine: bool) -> Source:
+        """The grid's Source: pattern_j = vel2_j g(x_j) on the box of cells within
+        3.5 sigma of the source point, amplitude A; on the coarse grid also the
+        composition pattern vel2 lap(vel2 g) (8th-order Laplacian of the coarse
+        grid) on that box widened by the stencil radius."""
         torch = _torch()
         vf, vc = self.device_models()
         sig = self.sigma_cells  # in coarse cells
@@ -173,13 +208,42 @@ class Problem:
         box = v[zs, ys, xs].cpu().numpy().astype(np.float64)
         pat = (box * gx).astype(np.float32)
         amp = 1.0 / (self.dt * self.dt * 3000.0 * 3000.0)  # O(1) fields
-        return tuple(origin), (n, n, n), torch.from_numpy(np.ascontiguousarray(pat)).cuda(), amp
+        pat_d = torch.from_numpy(np.ascontiguousarray(pat)).cuda()
+        if fine or not self.compose_source:
+            return Source(tuple(origin), (n, n, n), pat_d, amp)
+        # v^2 lap(v^2 g) on the box widened by 4; v^2 g on a box widened by 8
+        # (cells outside the grid take the nearest edge value of v^2)
+        R = 4
+        ext = rad + 2 * R
+        idx = [np.clip(np.arange(c - ext, c + ext + 1), 0, d - 1)
+               for c, d in zip(centre[::-1], v.shape)]
+        iz, iy, ix = (torch.as_tensor(i, device=v.device) for i in idx)
+        vbox = v.index_select(0, iz).index_select(1, iy).index_select(2, ix)
+        vbox = vbox.cpu().numpy().astype(np.float64)
+        offe = np.arange(2 * ext + 1) - ext
+        r2e = offe[None, None, :] ** 2 + offe[None, :, None] ** 2 + offe[:, None, None] ** 2
+        u = vbox * np.exp(-r2e / (2 * sig * sig))
+        lap = 3 * _FD8[0] * u
+        for r in range(1, R + 1):
+            for ax in range(3):
+                lap = lap + _FD8[r] * (np.roll(u, r, ax) + np.roll(u, -r, ax))
+        inner = slice(R, 2 * ext + 1 - R)
+        comp = (vbox * lap / (self.h * self.h))[inner, inner, inner].astype(np.float32)
+        nw = comp.shape[0]
+        return Source(tuple(origin), (n, n, n), pat_d, amp,
+                      tuple(c - rad - R for c in centre), (nw, nw, nw),
+                      torch.from_numpy(np.ascontiguousarray(comp)).cuda())
 
 
-def _inject(pb: Problem, fine: bool, fld, src, w, k) -> None:
-    origin, dims, pat, amp = src
+def _inject(pb: Problem, fine: bool, fld, src: Source, w, k) -> None:
     g = pb.fine if fine else pb.coarse
-    add_box(fld, g, origin, dims, pat, float(g.dt * g.dt * amp * w[k]))
+    add_box(fld, g, src.origin, src.dims, src.pattern, float(g.dt * g.dt * src.amp * w[k]))
+    if src.comp_pattern is not None:
+        h = pb.fine.dt
+        wc = pb._wc if pb._wc is not None and pb._wc.size > k else pb.wavelet_centre(2 * k + 64)
+        pb._wc = wc
+        add_box(fld, g, src.comp_origin, src.comp_dims, src.comp_pattern,
+                float(h ** 4 * src.amp * wc[k]))
 
 
 def fine_solve(pb: Problem, vf, steps: int, on_even=None):
@@ -244,15 +308,26 @@ class Dataset:
 
 
 def make_pairs(problems, fine_steps: int, samples_per_pair: int = 4096, every: int = 4,
-               first: int = 8, wall: int = 12, amp_floor: float = 0.05, src_clear: float = 3.5,
-               seed: int = 0) -> Dataset:
+               first: int = 8, wall: int = 12, amp_floor: float = 0.05, src_clear: float = 0.0,
+               seed: int = 0, policy: Mlp | None = None, weighting: str = "uniform") -> Dataset:
     """Training rows from the plain fine solver on each problem: every `every`
     coarse steps from `first` on, samples_per_pair random coarse cells at least
     `wall` cells from the walls and src_clear source widths from the source point,
-    whose local field exceeds amp_floor x the field's largest magnitude.  (Inside
-    the source the two grids' time sampling of the wavelet differs, and where the
-    field is small its round-off dominates the normalised residual: neither is a
-    function of the local state.)"""
+    whose local field exceeds amp_floor x the field's largest magnitude (where
+    the field is small its round-off dominates the normalised residual, which is
+    then not a function of the local state).  With the coarse source's
+    composition term (Problem.compose_source) the residual inside the source is
+    a function of the state too, and rows there (src_clear 0) halve the
+    corrected solve's early error.  weighting "energy" draws the cells with
+    probability proportional to the squared field value instead of uniformly,
+    so the rows weigh as the cells weigh in the field's L2 error (the
+    correction is s c y, s the star's scale).
+
+    With a policy network, the coarse states are the corrected coarse solve's own
+    (run in step with the fine solve) instead of the restricted fine states, and
+    the target is the restricted fine state minus the plain step of that state:
+    rows from the states the corrected solver actually visits, whose targets also
+    pull its accumulated drift back toward the fine solution."""
     torch = _torch()
     gen = torch.Generator(device="cuda")
     gen.manual_seed(seed)
@@ -275,27 +350,47 @@ def make_pairs(problems, fine_steps: int, samples_per_pair: int = 4096, every: i
         del zz, yy, xx, d2
         before = sum(x.shape[0] for x in Xs)
 
+        roll = [torch.zeros(gc.shape, device="cuda"), torch.zeros(gc.shape, device="cuda")]
+
         def on_even(m, f):
             c = torch.empty(gc.shape, device="cuda")
             restrict2(f, pb.fine, c, gc, OFFSET)
             ring[m] = c
             ring.pop(m - 3, None)
-            if m >= max(first, 2) and (m - first) % every == 0:
+            sample = m >= max(first, 2) and (m - first) % every == 0
+            if policy is not None and m >= 1:
+                # roll = [level m - 1, level m - 2] of the corrected coarse solve
+                if sample:
+                    plain.copy_(roll[1])
+                    coarse_step(pb, vc, roll[0], plain, src_c, w_c, m - 1)
+                    sample_rows(roll[0], c, m)
+                coarse_step(pb, vc, roll[0], roll[1], src_c, w_c, m - 1, policy)
+                roll.reverse()
+                return
+            if sample:
                 cm2, cm1, cm = ring[m - 2], ring[m - 1], ring[m]
                 plain.copy_(cm2)  # in-place leapfrog writes over the older level
                 coarse_step(pb, vc, cm1, plain, src_c, w_c, m - 1)
-                mag = cm1.abs()
-                ok = box & (mag > amp_floor * float(mag.max()))
-                cand = torch.nonzero(ok.view(-1)).view(-1)
-                if cand.numel() == 0:
-                    return
-                pick = cand[torch.randint(0, cand.numel(), (min(samples_per_pair, cand.numel()),),
-                                          generator=gen, device="cuda")]
-                X = torch.empty((pick.numel(), 32), dtype=torch.int16, device="cuda")
-                t = torch.empty(pick.numel(), dtype=torch.float32, device="cuda")
-                mlp_samples(cm1, vc, cm, plain, gc, pick.to(torch.int64), X, t)
-                Xs.append(X)
-                ts.append(t)
+                sample_rows(cm1, cm, m)
+
+        def sample_rows(state, target, m):
+            """Rows at random cells of `state` (level m - 1); `plain` holds its plain step."""
+            mag = state.abs()
+            ok = box & (mag > amp_floor * float(mag.max()))
+            cand = torch.nonzero(ok.view(-1)).view(-1)
+            if cand.numel() == 0:
+                return
+            k = min(samples_per_pair, cand.numel())
+            if weighting == "energy":
+                wgt = mag.view(-1)[cand].double().pow(2)
+                pick = cand[torch.multinomial(wgt, k, replacement=True, generator=gen)]
+            else:
+                pick = cand[torch.randint(0, cand.numel(), (k,), generator=gen, device="cuda")]
+            X = torch.empty((pick.numel(), 32), dtype=torch.int16, device="cuda")
+            t = torch.empty(pick.numel(), dtype=torch.float32, device="cuda")
+            mlp_samples(state, vc, target, plain, gc, pick.to(torch.int64), X, t)
+            Xs.append(X)
+            ts.append(t)
 
         fine_solve(pb, vf, fine_steps, on_even)
         counts.append(sum(x.shape[0] for x in Xs) - before)
@@ -381,7 +476,7 @@ def proxy_of(pb: Problem, nc_proxy: int = 64) -> Problem:
     win = vf[z0:z0 + nfp, y0:y0 + nfp, x0:x0 + nfp].contiguous()
     src = (pb.src_c[0] - x0 // 2, pb.src_c[1] - y0 // 2, pb.src_c[2] - z0 // 2)
     return Problem(nc_proxy, pb.h, pb.dt, pb.seed, freq=pb.freq, src_c=src,
-                   sigma_cells=pb.sigma_cells, vel2_window=win)
+                   sigma_cells=pb.sigma_cells, vel2_window=win, compose_source=pb.compose_source)
 
 
 @dataclass

@@ -34,7 +34,7 @@ def test_geometry_and_source_agree_between_grids(torch_cuda):
     avg = (wf[1:18:2].astype(np.float64) + 2 * wf[2:19:2] + wf[3:20:2]) / 4  # m = 1..9
     assert np.allclose(wc[1:10], avg, rtol=1e-5, atol=1e-7)
     # the two source patterns sample the same function: equal on shared cells
-    (of, df, pf, af), (oc, dc, pc, ac) = pb.source(True), pb.source(False)
+    (of, df, pf, af), (oc, dc, pc, ac) = pb.source(True)[:4], pb.source(False)[:4]
     assert af == ac
     pf, pc = pf.cpu().numpy(), pc.cpu().numpy()
     rc, rf = (dc[0] - 1) // 2, (df[0] - 1) // 2
@@ -45,6 +45,27 @@ def test_geometry_and_source_agree_between_grids(torch_cuda):
             assert np.isclose(pc[rc, rc, k], pf[rf, rf, j], rtol=1e-6)
             hits += 1
     assert hits >= dc[0] - 1
+
+
+def test_source_composition_pattern(torch_cuda):
+    """The coarse source's composition pattern is v^2 lap(v^2 g): on a constant
+    model, v^4 g (r^2 / sigma^4 - 3 / sigma^2) / h^2 to the 8th-order stencil's
+    accuracy; the fine grid has none."""
+    pb = learned.Problem(NC, H, DT, seed=3, model="constant")
+    assert pb.source(True).comp_pattern is None
+    s = pb.source(False)
+    v2 = float(pb.device_models()[1][NC // 2, NC // 2, NC // 2])
+    comp = s.comp_pattern.cpu().numpy().astype(np.float64)
+    n = s.comp_dims[0]
+    assert s.comp_dims == (n, n, n) and n == s.dims[0] + 8
+    assert tuple(o + n // 2 for o in s.comp_origin) == tuple(pb.src_c)
+    off = np.arange(n) - n // 2
+    r2 = off[None, None, :] ** 2 + off[None, :, None] ** 2 + off[:, None, None] ** 2
+    sig = pb.sigma_cells
+    ref = v2 * v2 * np.exp(-r2 / (2 * sig * sig)) * (r2 / sig ** 4 - 3 / sig ** 2) / (H * H)
+    assert np.max(np.abs(comp - ref)) <= 2e-3 * np.max(np.abs(ref))
+    off_pb = learned.Problem(NC, H, DT, seed=3, model="constant", compose_source=False)
+    assert off_pb.source(False).comp_pattern is None
 
 
 NC80, C80 = 80, 40
@@ -69,11 +90,25 @@ def trained(torch_cuda):
 
 def test_learned_correction_beats_plain_coarse(trained):
     mlp, hist = trained
-    assert hist[-1] < 0.2 * hist[0]
+    # rows inside the source region (the default) are the hardest: the last
+    # epoch's loss ends near 0.22 of the first one's (0.15 without them)
+    assert hist[-1] < 0.3 * hist[0]
     errs = {k: learned.evaluate(mk80(99), k, mlp) for k in (40, 120)}
     print("ablation", errs, "loss", hist[0], hist[-1])
     for k, e in errs.items():
         assert e["learned"] < 0.8 * e["plain"], (k, e)
+
+
+def test_source_composition_lowers_the_early_corrected_error(trained):
+    """Two fine steps compose to a coarse step plus h^4 L^2 p + h^4 L S: the
+    network (trained with the composition term in the coarse source) supplies
+    the state's part, the source term the rest.  While the source is on, the
+    corrected solve is closer to the fine one with the term than without."""
+    mlp, _ = trained
+    errs = {comp: learned.evaluate(mk80(98, compose_source=comp), 30, mlp)["learned"]
+            for comp in (False, True)}
+    print("composition", errs)
+    assert errs[True] < 0.8 * errs[False], errs
 
 
 def test_judged_solve_without_fallback_is_the_corrected_solve(trained):
