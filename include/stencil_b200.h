@@ -246,6 +246,11 @@ int sb200_run_steps(void* handle, int64_t n);
 int sb200_run_synchronize(void* handle);
 /* Current field in physical units into host memory (synchronous). */
 int sb200_run_get_field(void* handle, float* p);
+/* XY plane z of the current field (nx*ny floats, x fastest) in physical units
+ * into host memory (synchronous).  Only that plane crosses to the host: the
+ * per-frame read of the reference's slice writer (src/main_slice.cpp:112-121,
+ * which downloads the whole grid and keeps plane nz/2). */
+int sb200_run_get_plane(void* handle, int64_t z, float* plane);
 /* First n source-trace samples (p at the source after each step) to host memory. */
 int sb200_run_get_trace(void* handle, float* trace, int64_t n);
 /* FP64 statistics {sum p^2, max |p|, non-finite count} of the current field. */

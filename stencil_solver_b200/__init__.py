@@ -152,6 +152,7 @@ _SIGNATURES = {
     "sb200_run_steps": ([C.c_void_p, C.c_int64], C.c_int),
     "sb200_run_synchronize": ([C.c_void_p], C.c_int),
     "sb200_run_get_field": ([C.c_void_p, C.c_void_p], C.c_int),
+    "sb200_run_get_plane": ([C.c_void_p, C.c_int64, C.c_void_p], C.c_int),
     "sb200_run_get_trace": ([C.c_void_p, C.c_void_p, C.c_int64], C.c_int),
     "sb200_run_stats": ([C.c_void_p, C.c_void_p], C.c_int),
     "sb200_run_steps_done": ([C.c_void_p], C.c_int64),
@@ -460,6 +461,16 @@ class Run:
             out = np.empty(self.grid.shape, np.float32)
         ptr = out.data_ptr() if hasattr(out, "data_ptr") else out.ctypes.data
         _check(lib().sb200_run_get_field(self._h, ptr))
+        return out
+
+    def plane(self, z: int, out=None):
+        """XY plane z of the current field, (ny, nx) float32, physical units."""
+        import numpy as np
+
+        g = self.grid
+        if out is None:
+            out = np.empty((g.ny, g.nx), np.float32)
+        _check(lib().sb200_run_get_plane(self._h, int(z), out.ctypes.data))
         return out
 
     def trace(self, n: int):

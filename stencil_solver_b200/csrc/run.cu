@@ -233,6 +233,32 @@ public:
         return cuda(cudaStreamSynchronize(st_));
     }
 
+    // XY plane z (nx * ny floats, x fastest) of the current field in physical
+    // units: one contiguous range of the z-major field, so only that range
+    // crosses to the host (FP16: unpacked on the device first).
+    int get_plane(int64_t z, float* host) {
+        if (!host) return set_error(SB200_ERR_INVALID, "sb200_run_get_plane: NULL destination");
+        const int64_t plane = c_.grid.nx * c_.grid.ny;
+        if (z < 0 || z >= c_.grid.nz)
+            return set_error(SB200_ERR_INVALID, "sb200_run_get_plane: z outside [0, nz)");
+        if (int rc = synchronize()) return rc;
+        if (!fp16_)
+            return cuda(cudaMemcpy(host, static_cast<const float*>(a_) + z * plane, plane * 4,
+                                   cudaMemcpyDeviceToHost));
+        F16Scale s;
+        if (int rc = cuda(cudaMemcpy(&s, scale_dev_, sizeof(s), cudaMemcpyDeviceToHost))) return rc;
+        if (int rc = ensure_stage()) return rc;
+        for (int64_t off = 0; off < plane; off += kStageFloats) {
+            const int64_t m = std::min(kStageFloats, plane - off);
+            if (int rc = sb200_f16_unpack(static_cast<const uint16_t*>(a_) + z * plane + off, stage_,
+                                          m, s.a, st_))
+                return rc;
+            if (int rc = cuda(cudaMemcpyAsync(host + off, stage_, m * 4, cudaMemcpyDeviceToHost, st_)))
+                return rc;
+        }
+        return cuda(cudaStreamSynchronize(st_));
+    }
+
     int get_trace(float* host, int64_t n) {
         if (!host || n < 0) return set_error(SB200_ERR_INVALID, "sb200_run_get_trace: bad arguments");
         if (!trace_dev_ || n > cap_ || n > step_)
@@ -572,6 +598,11 @@ int sb200_run_synchronize(void* h) {
 int sb200_run_get_field(void* h, float* p) {
     if (!h) return set_error(SB200_ERR_INVALID, "NULL run handle");
     return as_run(h)->get_field(p);
+}
+
+int sb200_run_get_plane(void* h, int64_t z, float* p) {
+    if (!h) return set_error(SB200_ERR_INVALID, "NULL run handle");
+    return as_run(h)->get_plane(z, p);
 }
 
 int sb200_run_get_trace(void* h, float* trace, int64_t n) {

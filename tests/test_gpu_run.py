@@ -56,6 +56,38 @@ def test_run_exact_mode_is_bit_identical_to_reference():
     assert np.array_equal(p[64], f["mid32"])
 
 
+def test_slices_hold_the_reference_mid_plane(tmp_path):
+    """Frames written through the plane read-back (exact mode): the frame after
+    300 steps is the reference's mid plane bit for bit, frame 0 the initial state."""
+    from stencil_solver_b200.slices import read_slices, write_slices
+
+    f, run = acoustic128(graph_chunk=100, exact=1)
+    with run:
+        run.set_wavelet(f["wavelet"])
+        n = write_slices(run, tmp_path / "wave", 300, 100, velocity=2000.0)
+        full = run.field()
+    meta, frames = read_slices(tmp_path / "wave")
+    assert n == 4 and meta["plane_index"] == 64
+    assert not frames[0].any()
+    assert np.array_equal(frames[3], f["mid32"])
+    assert np.array_equal(frames[3], full[64])
+
+
+def test_plane_readback_fp16_is_the_field_plane():
+    n = 40
+    g = sb.Grid(n, n, n, 10.0, 10.0, 10.0, 1e-3)
+    p0 = gaussian_field(g.shape, sigma=4.0)
+    v = np.full(g.shape, 1800.0 ** 2, np.float32)
+    with sb.Run(g, precision=sb.PRECISION_F16, graph_chunk=0) as r:
+        r.set_fields(p0, p0, v)
+        r.steps(7)
+        full = r.field()
+        for z in (0, 17, n - 1):
+            assert np.array_equal(r.plane(z), full[z])
+        with pytest.raises(sb.StencilError):
+            r.plane(n)
+
+
 def test_run_graph_and_eager_agree_across_parity():
     n = 48
     g = sb.Grid(n, n, n, 10.0, 10.0, 10.0, 1e-3)
