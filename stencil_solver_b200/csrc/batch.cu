@@ -248,8 +248,12 @@ public:
             if (int rc = sb200_f16_unpack(reinterpret_cast<const uint16_t*>(arena_ + h.off[step_ & 1]),
                                           staging_, h.g.size(), sc.a, st_))
                 return rc;
-            return cuda(cudaMemcpy(out, staging_, static_cast<size_t>(h.g.size()) * 4,
-                                   cudaMemcpyDeviceToHost));
+            // on the batch's (non-blocking) stream, behind the unpack: a plain
+            // cudaMemcpy would not wait for it
+            if (int rc = cuda(cudaMemcpyAsync(out, staging_, static_cast<size_t>(h.g.size()) * 4,
+                                              cudaMemcpyDeviceToHost, st_)))
+                return rc;
+            return cuda(cudaStreamSynchronize(st_));
         }
         return cuda(cudaMemcpy(out, arena_ + h.off[step_ & 1], static_cast<size_t>(h.g.size()) * 4,
                                cudaMemcpyDeviceToHost));

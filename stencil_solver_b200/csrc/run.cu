@@ -150,7 +150,9 @@ public:
             a0 = std::ldexp(1.0, std::max(-120, std::min(120, int(std::floor(std::log2(
                                                                   double(c_.f16_target) / (m + bnd)))))));
         const F16Scale s0{static_cast<float>(a0), 1.f};
-        if (int rc = cuda(cudaMemcpy(scale_dev_, &s0, sizeof(s0), cudaMemcpyHostToDevice))) return rc;
+        // on the run's stream: steps still queued there read the scale
+        if (int rc = cuda(cudaMemcpyAsync(scale_dev_, &s0, sizeof(s0), cudaMemcpyHostToDevice, st_)))
+            return rc;
         if (int rc = stage_in(p, a_, float(a0), false)) return rc;
         if (int rc = stage_in(p_prev, b_, float(a0), false)) return rc;
         if (int rc = stage_in(vel2, k_, 1.f, true)) return rc;
