@@ -58,7 +58,7 @@ def args_():
     ap.add_argument("--f16", action="store_true",
                     help="--kernel batch: the FP16-storage batch")
     ap.add_argument("--sparse", action="store_true",
-                    help="--kernel learned: a small random cube in a zero field (floor 2^-64)")
+                    help="--kernel learned / mlp: a small random cube in a zero field (floor 2^-64)")
     ap.add_argument("--kernel", choices=["acoustic", "heat", "fp16", "batch", "mlp", "learned"],
                     help="run only a small case of one kernel (for profilers) and print its time")
     return ap.parse_args()
@@ -753,12 +753,7 @@ def run_kernel_probe(a):
         scale = torch.tensor([1024.0, 1.0], device="cuda")
         sb.set_pencil_override(sb.KIND_WAVE_F16, max(a.variant, 0), a.zchunks)
         f = lambda: sb.wave_step_f16(P, Q, K, g, scale, 0)  # noqa: E731
-    elif a.kernel == "mlp":
-        m = sb.Mlp(seed=1)
-        m.output_scale = 1e-5
-        out = torch.zeros_like(p)
-        f = lambda: m.correct(p, v, out, g)  # noqa: E731
-    elif a.kernel == "learned":
+    elif a.kernel in ("mlp", "learned"):
         m = sb.Mlp(seed=1)
         m.output_scale = 1e-5
         if a.sparse:  # a random cube of side 40 n / 256 in a zero field, floor 2^-64
@@ -767,9 +762,13 @@ def run_kernel_probe(a):
             p.zero_()
             p[lo:hi, lo:hi, lo:hi] = blob
             m.min_scale = 2.0 ** -64
+    if a.kernel == "mlp":
+        out = torch.zeros_like(p)
+        f = lambda: m.correct(p, v, out, g)  # noqa: E731
+    elif a.kernel == "learned":
         q = p * 0.99
         f = lambda: m.learned_step(p, q, v, g)  # noqa: E731
-    else:  # batch: 12 shots with extents n/2..n in steps of 8
+    elif a.kernel == "batch":  # 12 shots with extents n/2..n in steps of 8
         rng = np.random.default_rng(SEED)
         shots = []
         for _ in range(12):
