@@ -456,17 +456,28 @@ int learned_step_resident() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (cached[dev & 63] > 0) return cached[dev & 63];
-    int n = 0;
+    // From the kernel's registers and shared memory and the SM's budgets (the
+    // occupancy query answers 1 for this kernel, while 3 CTAs run per SM).
+    cudaFuncAttributes fa{};
+    int regs_sm = 0, smem_sm = 0, reserved = 0;
     if (cudaFuncSetAttribute(learned_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             kLSmem) == cudaSuccess &&
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, learned_step_kernel, LNT, kLSmem) ==
-            cudaSuccess &&
-        n > 0) {
-        cached[dev & 63] = n;
-        return n;
+                             kLSmem) != cudaSuccess ||
+        cudaFuncGetAttributes(&fa, learned_step_kernel) != cudaSuccess ||
+        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        return 1;
     }
-    cudaGetLastError();
-    return 1;
+    const int warp_regs = ((fa.numRegs * 32 + 255) / 256) * 256;  // allocated per warp
+    const int by_regs = regs_sm / (warp_regs * (LNT / 32));
+    const int by_smem = smem_sm / (kLSmem + int(fa.sharedSizeBytes) + reserved);
+    const int n = std::max(1, std::min(by_regs, by_smem));
+    cached[dev & 63] = n;
+    return n;
 }
 
 PencilBoxes learned_step_boxes() {
