@@ -189,6 +189,9 @@ _SIGNATURES = {
                              C.c_int),
     "sb200_mlp_correct": ([C.c_void_p] * 4 + [C.POINTER(sb200_grid), C.c_void_p], C.c_int),
     "sb200_mlp_learned_step": ([C.c_void_p] * 4 + [C.POINTER(sb200_grid), C.c_void_p], C.c_int),
+    "sb200_mlp_flags_bytes": ([C.c_void_p, C.POINTER(sb200_grid)], C.c_int64),
+    "sb200_mlp_learned_step_flags": ([C.c_void_p] * 4 + [C.POINTER(sb200_grid)] + [C.c_void_p] * 4,
+                                     C.c_int),
     "sb200_mlp_set_min_scale": ([C.c_void_p, C.c_float], C.c_int),
     "sb200_mlp_min_scale": ([C.c_void_p], C.c_float),
     "sb200_mlp_samples": ([C.c_void_p] * 4 + [C.POINTER(sb200_grid), C.c_void_p, C.c_int64,
@@ -714,11 +717,32 @@ class Mlp:
         _check(lib().sb200_mlp_correct(self._h, _ptr(p), _ptr(vel2), _ptr(p_next), _g(grid),
                                         _stream(stream)))
 
-    def learned_step(self, p, p_prev_next, vel2, grid: Grid, stream=None) -> None:
+    def learned_step(self, p, p_prev_next, vel2, grid: Grid, stream=None, flags=None,
+                     box=None) -> None:
         """p_prev_next <- acoustic step of p + the learned correction, in one fused
-        launch (no source term); the same bits as wave_step then correct."""
-        _check(lib().sb200_mlp_learned_step(self._h, _ptr(p), _ptr(p_prev_next), _ptr(vel2),
-                                             _g(grid), _stream(stream)))
+        launch (no source term); the same bits as wave_step then correct.
+
+        flags = (flags_in, flags_out): uint8 device tensors of flags_bytes(grid)
+        bytes (flags_in None: every chunk active); chunks whose neighbourhood holds
+        no flagged chunk skip the network.  box = (x0, x1, y0, y1, z0, z1) cells
+        that count as flagged (a source added to p after its flags were written)."""
+        if flags is None:
+            _check(lib().sb200_mlp_learned_step(self._h, _ptr(p), _ptr(p_prev_next), _ptr(vel2),
+                                                 _g(grid), _stream(stream)))
+            return
+        fin, fout = flags
+        bx = None if box is None else (C.c_int64 * 6)(*[int(v) for v in box])
+        _check(lib().sb200_mlp_learned_step_flags(
+            self._h, _ptr(p), _ptr(p_prev_next), _ptr(vel2), _g(grid),
+            None if fin is None else _ptr(fin), None if fout is None else _ptr(fout),
+            None if bx is None else C.cast(bx, C.c_void_p), _stream(stream)))
+
+    def flags_bytes(self, grid: Grid) -> int:
+        """Bytes of the activity flags of learned_step on `grid`."""
+        n = lib().sb200_mlp_flags_bytes(self._h, _g(grid))
+        if n < 0:
+            _check(int(n))
+        return int(n)
 
 
 def mlp_samples(p, vel2, p_true, p_plain, grid: Grid, cells, X, t, stream=None) -> None:

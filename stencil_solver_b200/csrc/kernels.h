@@ -84,8 +84,19 @@ struct LearnedNet {
 // acoustic step of p + learned correction, in place over p_prev.
 PencilBoxes learned_step_boxes();
 int learned_step_resident();
+// Its work split: 32 x 16 column tiles x zchunks z chunks of zlen planes (one
+// activity flag byte per tile and chunk).
+struct LearnedChunks {
+    int tiles_x = 0, tiles_y = 0, zchunks = 0, zlen = 0;
+};
+LearnedChunks learned_step_chunks(const GridDesc& g, int sms);
+// flags_in: per chunk, whether p may hold a value at or above the floor (NULL:
+// all may); box (x0, x1, y0, y1, z0, z1 cells, or NULL) counts as flagged;
+// flags_out receives the flags of p_next (NULL: none).
 cudaError_t launch_learned_step(const PencilMaps& maps, float* next, const GridDesc& g,
-                                const LearnedNet& net, int sms, int* err, cudaStream_t stream);
+                                const LearnedNet& net, int sms, int* err, cudaStream_t stream,
+                                const uint8_t* flags_in = nullptr, uint8_t* flags_out = nullptr,
+                                const int64_t* box = nullptr);
 
 // Laplacian weights of the pencil kernels (C_r / dx_a^2, times `scale`: dt^2 for
 // the acoustic step, alpha dt for heat), rounded once from double.

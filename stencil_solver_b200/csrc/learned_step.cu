@@ -59,6 +59,12 @@ constexpr int kTileA = 128 * 64;  // one A tile: 128 rows x 32 BF16
 constexpr int kOffW1 = 4 * kTileA, kOffW2 = kOffW1 + H * F * 2, kOffP = kOffW2 + H * H * 2;
 constexpr int kOffAux = kOffP + LS * LPLANE * 4;
 constexpr int kLSmem = kOffAux + LAUX * 2 * LTILE * 4 + 1024;
+// The plain path of an idle chunk has no network: its rings take the whole
+// dynamic shared memory (PS staged planes, PAUX p_prev / vel2 stages), so the
+// short plain iterations still have PS - 4 planes of copy lead.
+constexpr int PS = 12, PAUX = 4;
+constexpr int kOffPAux = PS * LPLANE * 4;
+static_assert(kOffPAux + PAUX * 2 * LTILE * 4 + 1024 <= kLSmem, "plain rings fit");
 static_assert(LNT == 128, "one thread per TMEM lane of an M = 128 tile");
 
 struct LearnedArgs {
@@ -76,10 +82,186 @@ struct LearnedArgs {
     float b1[H], b2[H], w3[H];
     float b3;
     int* err;
+    // Activity flags (one byte per tile and z chunk; zchunks chunks of zlen):
+    // flags_in[c] != 0 when chunk c of p may hold a value at or above the floor
+    // (NULL: every chunk may), box [x0, x1) x [y0, y1) x [z0, z1) cells counts as
+    // flagged too (a source added after the previous step); flags_out[c] receives
+    // the same for p_next (NULL: not written).
+    const uint8_t* flags_in;
+    uint8_t* flags_out;
+    int zchunks;
+    int box[6];
 };
+
+// Whether chunk (tx, ty, zc) of the launch may hold an active value: its flag,
+// or it meets the forced box.
+__device__ __forceinline__ bool chunk_flagged(const LearnedArgs& a, int tx, int ty, int zc) {
+    if (a.flags_in[(int64_t(zc) * a.tiles_y + ty) * a.tiles_x + tx]) return true;
+    const int x0 = R + tx * LTX, y0 = R + ty * LTY, z0 = R + zc * a.zlen;
+    return a.box[0] < x0 + LTX && x0 < a.box[1] && a.box[2] < y0 + LTY && y0 < a.box[3] &&
+           a.box[4] < z0 + a.zlen && z0 < a.box[5];
+}
 
 __device__ __forceinline__ float lane_of(const float4& v, int e) {
     return e == 0 ? v.x : (e == 1 ? v.y : (e == 2 ? v.z : v.w));
+}
+
+// A chunk with no active star: the plain FP32 acoustic step (the pencil kernel's
+// arithmetic in its order, as in the fused path), with the z queue in
+// compile-time slots (plane loop unrolled by 9), the same rings, and the
+// chunk's activity flag of p_next.  All threads of the CTA call it.
+__device__ __forceinline__ void plain_chunk(const CUtensorMap& pmap, const CUtensorMap& qmap,
+                                            const CUtensorMap& vmap, const LearnedArgs& a,
+                                            int x0, int y0, int zb, int nint, unsigned char* base,
+                                            uint64_t* full, uint64_t* auxf, int zc, int tx,
+                                            int ty) {
+    constexpr int LS = PS, LAUX = PAUX;  // this path's rings (shadow the fused path's)
+    float* sm = reinterpret_cast<float*>(base);
+    float* aux = reinterpret_cast<float*>(base + kOffPAux);
+    const int tid = threadIdx.x;
+    const int lx = tid % LTPR, ly = tid / LTPR;
+    const int nplanes = nint + 2 * R;
+    if (tid == 0) {
+        prefetch_tmap(&pmap);
+        prefetch_tmap(&qmap);
+        prefetch_tmap(&vmap);
+#pragma unroll
+        for (int s = 0; s < LS; ++s) mbar_init(&full[s], 1);
+#pragma unroll
+        for (int s = 0; s < LAUX; ++s) mbar_init(&auxf[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    int issued_hi = -1, aux_issued_hi = -1;
+    auto plane = [&](int j) -> const float* { return sm + (j % LS) * LPLANE; };
+    auto issue_plane = [&](int j) {  // thread 0 only
+        mbar_arrive_expect_tx(&full[j % LS], LPLANE_BYTES);
+        tma_load_3d(sm + (j % LS) * LPLANE, &pmap, &full[j % LS], x0 - R, y0 - R, zb - R + j);
+        issued_hi = j;
+    };
+    auto issue_aux = [&](int it) {  // thread 0 only
+        float* st = aux + (it % LAUX) * 2 * LTILE;
+        mbar_arrive_expect_tx(&auxf[it % LAUX], 2 * LTILE_BYTES);
+        tma_load_3d(st, &qmap, &auxf[it % LAUX], x0, y0, zb + it);
+        tma_load_3d(st + LTILE, &vmap, &auxf[it % LAUX], x0, y0, zb + it);
+        aux_issued_hi = it;
+    };
+    if (tid == 0) {
+        for (int s = 0; s < LS && s < nplanes; ++s) issue_plane(s);
+        for (int it = 0; it < LAUX && it < nint; ++it) issue_aux(it);
+    }
+    const int gx = x0 + 4 * lx, gy = y0 + ly;
+    const bool rin = gx < a.nx - R && gy < a.ny - R;
+    const int soff = (ly + R) * LSX + 4 * lx + R;
+    const int aoff = ly * LTX + 4 * lx;
+    int64_t goff = static_cast<int64_t>(zb) * a.sz + static_cast<int64_t>(gy) * a.sy + gx;
+
+    float2 ax2[R], ay2[R], az2[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        ax2[r] = dup2(a.w.ax[r]);
+        ay2[r] = dup2(a.w.ay[r]);
+        az2[r] = dup2(a.w.az[r]);
+    }
+    const float2 cx2 = dup2(a.w.cx), cy2 = dup2(a.w.cy), cz2 = dup2(a.w.cz), neg1 = dup2(-1.f);
+
+    float4 q[9];  // slot (i + k) % 9 holds plane z - 4 + k at plane i
+    bool bad = false;
+    // Start-up: planes 0..7 fill slots 0..7 (all staged: PS >= 8); 0..3 only feed
+    // the queue, so their stages take planes PS .. PS + 3 at once.
+    static_assert(PS >= 8, "the start-up reads planes 0..7 from the first fill");
+#pragma unroll
+    for (int jj = 0; jj < 8; ++jj) {
+        if (!mbar_wait(&full[jj], 0)) bad = true;
+        q[jj] = lds128(plane(jj) + soff);
+    }
+    bool abort_run = __syncthreads_or(bad) != 0;
+    if (!abort_run && tid == 0) {
+#pragma unroll
+        for (int jj = 0; jj < R; ++jj)
+            if (jj + LS < nplanes) issue_plane(jj + LS);
+    }
+    float omax = 0.f;
+    for (int i0 = 0; i0 < nint && !abort_run; i0 += 9) {
+#pragma unroll
+        for (int u = 0; u < 9; ++u) {
+            const int i = i0 + u;
+            if (i < nint && !abort_run) {
+                {
+                    const int jf = i + 8;  // queue feed: plane z + 4
+                    if (!mbar_wait(&full[jf % LS], (jf / LS) & 1)) bad = true;
+                    q[(u + 8) % 9] = lds128(plane(jf) + soff);
+                }
+                const float* pc = plane(i + 4) + soff;
+                const float4 c = q[(u + 4) % 9];
+                float2 ya[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+#pragma unroll
+                for (int k = -R; k <= R; ++k) {
+                    if (k == 0) continue;
+                    const float4 row = lds128(pc + k * LSX);
+                    const int d = k > 0 ? k : -k;
+                    ya[0] = fma2(ay2[d - 1], pair_of(row, 0), ya[0]);
+                    ya[1] = fma2(ay2[d - 1], pair_of(row, 1), ya[1]);
+                }
+                const float4 lf = lds128(pc - 4);
+                const float4 rt = lds128(pc + 4);
+                const float win[12] = {lf.x, lf.y, lf.z, lf.w, c.x, c.y,
+                                       c.z,  c.w,  rt.x, rt.y, rt.z, rt.w};
+                float2 lap[2];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const float2 ce = pair_of(c, h);
+                    float2 tz = mul2(cz2, ce);
+                    float2 txv = mul2(cx2, ce);
+#pragma unroll
+                    for (int r = 1; r <= R; ++r) {
+                        tz = fma2(az2[r - 1],
+                                  add2(pair_of(q[(u + 4 + r) % 9], h), pair_of(q[(u + 4 - r + 9) % 9], h)),
+                                  tz);
+                        const int e = 4 + 2 * h;
+                        const float2 sx = make_float2(win[e + r] + win[e - r], win[e + 1 + r] + win[e + 1 - r]);
+                        txv = fma2(ax2[r - 1], sx, txv);
+                    }
+                    const float2 tyv = fma2(cy2, ce, ya[h]);
+                    lap[h] = add2(add2(txv, tyv), tz);
+                }
+                if (!mbar_wait(&auxf[i % LAUX], (i / LAUX) & 1)) bad = true;
+                const float* st = aux + (i % LAUX) * 2 * LTILE + aoff;
+                const float4 pv = lds128(st);
+                const float4 vv = lds128(st + LTILE);
+                const float2 t0 = fma2(neg1, pair_of(pv, 0), add2(pair_of(c, 0), pair_of(c, 0)));
+                const float2 t1 = fma2(neg1, pair_of(pv, 1), add2(pair_of(c, 1), pair_of(c, 1)));
+                const float2 o0 = fma2(pair_of(vv, 0), lap[0], t0);
+                const float2 o1 = fma2(pair_of(vv, 1), lap[1], t1);
+                const float4 o = make_float4(o0.x, o0.y, o1.x, o1.y);
+                if (!bad && rin) {
+                    stg_stream(a.next + goff, o);
+                    omax = fmaxf(omax, fmaxf(fmaxf(fabsf(o.x), fabsf(o.y)),
+                                             fmaxf(fabsf(o.z), fabsf(o.w))));
+                }
+                goff += a.sz;
+                abort_run = __syncthreads_or(bad) != 0;
+                if (!abort_run && tid == 0) {
+                    // the staged plane z and the aux stage of this plane are free now
+                    if (i + 4 + LS < nplanes) issue_plane(i + 4 + LS);
+                    if (i + LAUX < nint) issue_aux(i + LAUX);
+                }
+            }
+        }
+    }
+    const bool act_out = __syncthreads_or(omax > 0.f && omax >= a.min_scale) != 0;
+    if (abort_run) {
+        if (tid == 0) {
+            record_error(a.err, kDevWaitTimeout);
+            for (int jj = max(0, issued_hi - LS + 1); jj <= issued_hi; ++jj)
+                (void)mbar_wait(&full[jj % LS], (jj / LS) & 1);
+            for (int it = max(0, aux_issued_hi - LAUX + 1); it <= aux_issued_hi; ++it)
+                (void)mbar_wait(&auxf[it % LAUX], (it / LAUX) & 1);
+        }
+        return;
+    }
+    if (a.flags_out && tid == 0)
+        a.flags_out[(int64_t(zc) * a.tiles_y + ty) * a.tiles_x + tx] = act_out ? 1 : 0;
 }
 
 __global__ void __launch_bounds__(LNT, 3)
@@ -87,8 +269,8 @@ __global__ void __launch_bounds__(LNT, 3)
                         const __grid_constant__ CUtensorMap qmap,
                         const __grid_constant__ CUtensorMap vmap, const LearnedArgs a) {
     extern __shared__ unsigned char dyn[];
-    __shared__ __align__(8) uint64_t full[LS];
-    __shared__ __align__(8) uint64_t auxf[LAUX];
+    __shared__ __align__(8) uint64_t full[PS];  // the fused path uses the first LS
+    __shared__ __align__(8) uint64_t auxf[PAUX];
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t s_tmem;
     __shared__ int s_flag;  // a bounded wait gave up
@@ -111,6 +293,30 @@ __global__ void __launch_bounds__(LNT, 3)
     const int ze = min(zb + a.zlen, a.nz - R);
     const int nint = ze - zb, nplanes = nint + 2 * R;
 
+    // No star of this chunk can reach the floor when no chunk within one tile /
+    // one z chunk of it is flagged (a star reaches 4 cells; tiles and full
+    // chunks are at least that long): then the plain step is the whole answer.
+    bool skip = false;
+    if (a.flags_in) {
+        skip = true;
+        for (int dz = -1; dz <= 1 && skip; ++dz)
+            for (int dy = -1; dy <= 1 && skip; ++dy)
+                for (int dx = -1; dx <= 1 && skip; ++dx) {
+                    const int nx_ = tx + dx, ny_ = ty + dy, nz_ = b + dz;
+                    if (nx_ >= 0 && nx_ < a.tiles_x && ny_ >= 0 && ny_ < a.tiles_y && nz_ >= 0 &&
+                        nz_ < a.zchunks && chunk_flagged(a, nx_, ny_, nz_))
+                        skip = false;
+                }
+    }
+    if (skip) {
+        // No TMEM here: give up the allocation permit at once, as the network
+        // path does after its allocation (the SM starts no further CTA of this
+        // kernel while a resident one still holds it).
+        if (warp == 0)
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        plain_chunk(pmap, qmap, vmap, a, x0, y0, zb, nint, base, full, auxf, b, tx, ty);
+        return;
+    }
     for (int i = tid; i < H * F; i += LNT) {
         *reinterpret_cast<uint16_t*>(sW1 + core_off(i / F, i % F)) = a.w1b[i];
         *reinterpret_cast<uint16_t*>(sW2 + core_off(i / H, i % H)) = a.w2b[i];
@@ -202,6 +408,7 @@ __global__ void __launch_bounds__(LNT, 3)
         if (ok) waited = ncommit;
     };
 
+    float omax = 0.f;  // largest |p_next| this thread stores (activity flag of the chunk)
     // One plane per iteration; the queue shifts by one slot at the end (the body
     // is too large to unroll 9 times and still fit the instruction cache).
     for (int i = 0; i < nint && !abort_run; ++i) {
@@ -424,10 +631,18 @@ __global__ void __launch_bounds__(LNT, 3)
             }
             tc_fence_before();
         }
-        if (!bad && rin) stg_stream(a.next + goff, o);
+        if (!bad && rin) {
+            stg_stream(a.next + goff, o);
+            omax = fmaxf(omax, fmaxf(fmaxf(fabsf(o.x), fabsf(o.y)), fmaxf(fabsf(o.z), fabsf(o.w))));
+        }
         goff += a.sz;
 #pragma unroll
         for (int k = 0; k < 8; ++k) q[k] = q[k + 1];
+    }
+    {
+        const bool act_out = __syncthreads_or(omax > 0.f && omax >= a.min_scale) != 0;
+        if (a.flags_out && tid == 0 && !abort_run)
+            a.flags_out[(int64_t(b) * a.tiles_y + ty) * a.tiles_x + tx] = act_out ? 1 : 0;
     }
 
     if (abort_run && tid == 0) {
@@ -490,10 +705,29 @@ PencilBoxes learned_step_boxes() {
     return b;
 }
 
-cudaError_t launch_learned_step(const PencilMaps& maps, float* next, const GridDesc& g,
-                                const LearnedNet& net, int sms, int* err, cudaStream_t stream) {
-    if (!g.has_interior()) return cudaSuccess;
+LearnedChunks learned_step_chunks(const GridDesc& g, int sms) {
+    LearnedChunks c;
+    if (!g.has_interior()) return c;
     const int resident = learned_step_resident();
+    c.tiles_x = static_cast<int>((g.nx - 2 * R + LTX - 1) / LTX);
+    c.tiles_y = static_cast<int>((g.ny - 2 * R + LTY - 1) / LTY);
+    // z split: the smallest one that gives every resident CTA slot about four
+    // tiles' worth of work (each split re-reads 8 halo planes of p).
+    const int inz = static_cast<int>(g.nz - 2 * R);
+    const int64_t tiles = int64_t(c.tiles_x) * c.tiles_y;
+    const int64_t slots = int64_t(std::max(1, sms)) * std::max(1, resident);
+    int zc = static_cast<int>(std::min<int64_t>(16, std::max<int64_t>(1, (4 * slots + tiles - 1) / tiles)));
+    zc = std::min(zc, inz);
+    c.zlen = (inz + zc - 1) / zc;
+    c.zchunks = (inz + c.zlen - 1) / c.zlen;
+    return c;
+}
+
+cudaError_t launch_learned_step(const PencilMaps& maps, float* next, const GridDesc& g,
+                                const LearnedNet& net, int sms, int* err, cudaStream_t stream,
+                                const uint8_t* flags_in, uint8_t* flags_out, const int64_t* box) {
+    if (!g.has_interior()) return cudaSuccess;
+    const LearnedChunks ch = learned_step_chunks(g, sms);
     LearnedArgs a{};
     a.next = next;
     a.nx = static_cast<int>(g.nx);
@@ -501,18 +735,20 @@ cudaError_t launch_learned_step(const PencilMaps& maps, float* next, const GridD
     a.nz = static_cast<int>(g.nz);
     a.sy = g.nx;
     a.sz = g.nx * g.ny;
-    a.tiles_x = static_cast<int>((g.nx - 2 * R + LTX - 1) / LTX);
-    a.tiles_y = static_cast<int>((g.ny - 2 * R + LTY - 1) / LTY);
-    // z split: the smallest one that gives every resident CTA slot about four
-    // tiles' worth of work (each split re-reads 8 halo planes of p).
-    const int inz = static_cast<int>(g.nz - 2 * R);
-    const int64_t tiles = int64_t(a.tiles_x) * a.tiles_y;
-    const int64_t slots = int64_t(std::max(1, sms)) * std::max(1, resident);
-    int zc = static_cast<int>(std::min<int64_t>(16, std::max<int64_t>(1, (4 * slots + tiles - 1) / tiles)));
-    zc = std::min(zc, inz);
-    a.zlen = (inz + zc - 1) / zc;
-    const unsigned ctas =
-        static_cast<unsigned>(tiles * ((inz + a.zlen - 1) / a.zlen));
+    a.tiles_x = ch.tiles_x;
+    a.tiles_y = ch.tiles_y;
+    a.zlen = ch.zlen;
+    a.zchunks = ch.zchunks;
+    // Flags need chunks at least as long as a star's reach; shorter ones (tiny
+    // grids) run every chunk through the network.
+    a.flags_in = ch.zlen >= R ? flags_in : nullptr;
+    a.flags_out = flags_out;
+    a.box[0] = a.box[2] = a.box[4] = 0;
+    a.box[1] = a.box[3] = a.box[5] = 0;  // empty
+    if (box && box[1] > box[0] && box[3] > box[2] && box[5] > box[4])
+        for (int k = 0; k < 6; ++k)
+            a.box[k] = static_cast<int>(std::max<int64_t>(-(1 << 30), std::min<int64_t>(1 << 30, box[k])));
+    const unsigned ctas = static_cast<unsigned>(int64_t(ch.tiles_x) * ch.tiles_y * ch.zchunks);
     a.w = fold_weights(g, g.dt * g.dt);
     a.dt_over_dx = g.dt / std::min(g.dx, std::min(g.dy, g.dz));
     a.out_scale = net.out_scale;

@@ -923,9 +923,22 @@ int sb200_mlp_correct(void* h, const float* p, const float* vel2, float* p_next,
     return cuda_err(cudaGetLastError(), "sb200_mlp_correct");
 }
 
-int sb200_mlp_learned_step(void* h, const float* p, float* p_prev_next, const float* vel2,
-                           const sb200_grid* grid, void* stream) {
-    const char* where = "sb200_mlp_learned_step";
+namespace {
+GridDesc grid_desc(const sb200_grid& grid) {
+    GridDesc g;
+    g.nx = grid.nx;
+    g.ny = grid.ny;
+    g.nz = grid.nz;
+    g.dx = grid.dx;
+    g.dy = grid.dy;
+    g.dz = grid.dz;
+    g.dt = grid.dt;
+    return g;
+}
+
+int learned_step_impl(void* h, const float* p, float* p_prev_next, const float* vel2,
+                      const sb200_grid* grid, const uint8_t* flags_in, uint8_t* flags_out,
+                      const int64_t* box, void* stream, const char* where) {
     Mlp* m = static_cast<Mlp*>(h);
     if (!m || !p || !p_prev_next || !vel2 || !grid)
         return set_error(SB200_ERR_INVALID, std::string(where) + ": NULL argument");
@@ -934,14 +947,7 @@ int sb200_mlp_learned_step(void* h, const float* p, float* p_prev_next, const fl
     if (!(grid->dx > 0.f && grid->dy > 0.f && grid->dz > 0.f && grid->dt > 0.f) ||
         grid->nx < 0 || grid->ny < 0 || grid->nz < 0)
         return set_error(SB200_ERR_INVALID, std::string(where) + ": bad grid");
-    GridDesc g;
-    g.nx = grid->nx;
-    g.ny = grid->ny;
-    g.nz = grid->nz;
-    g.dx = grid->dx;
-    g.dy = grid->dy;
-    g.dz = grid->dz;
-    g.dt = grid->dt;
+    const GridDesc g = grid_desc(*grid);
     if (!g.has_interior()) return SB200_OK;
     auto a16 = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
     if (g.nx % 4 != 0 || !a16(p) || !a16(p_prev_next) || !a16(vel2) || g.nx > (1 << 20) ||
@@ -979,7 +985,33 @@ int sb200_mlp_learned_step(void* h, const float* p, float* p_prev_next, const fl
     net.b3 = m->host[OFF_B3];
     net.out_scale = m->out_scale;
     net.min_scale = m->min_scale;
-    return cuda_err(launch_learned_step(maps, p_prev_next, g, net, m->sms, err, st), where);
+    return cuda_err(launch_learned_step(maps, p_prev_next, g, net, m->sms, err, st, flags_in,
+                                        flags_out, box),
+                    where);
+}
+}  // namespace
+
+int sb200_mlp_learned_step(void* h, const float* p, float* p_prev_next, const float* vel2,
+                           const sb200_grid* grid, void* stream) {
+    return learned_step_impl(h, p, p_prev_next, vel2, grid, nullptr, nullptr, nullptr, stream,
+                             "sb200_mlp_learned_step");
+}
+
+int64_t sb200_mlp_flags_bytes(void* h, const sb200_grid* grid) {
+    Mlp* m = static_cast<Mlp*>(h);
+    if (!m || !grid) return set_error(SB200_ERR_INVALID, "sb200_mlp_flags_bytes: NULL argument");
+    const LearnedChunks c = learned_step_chunks(grid_desc(*grid), m->sms);
+    return int64_t(c.tiles_x) * c.tiles_y * c.zchunks;
+}
+
+int sb200_mlp_learned_step_flags(void* h, const float* p, float* p_prev_next, const float* vel2,
+                                 const sb200_grid* grid, const uint8_t* flags_in,
+                                 uint8_t* flags_out, const int64_t* box, void* stream) {
+    if (flags_in && flags_in == flags_out)
+        return set_error(SB200_ERR_INVALID,
+                         "sb200_mlp_learned_step_flags: flags_in and flags_out must differ");
+    return learned_step_impl(h, p, p_prev_next, vel2, grid, flags_in, flags_out, box, stream,
+                             "sb200_mlp_learned_step_flags");
 }
 
 int sb200_mlp_set_kernel(void* h, int kernel) {

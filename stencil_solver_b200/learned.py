@@ -85,6 +85,15 @@ class Source(NamedTuple):
     comp_dims: tuple = None
     comp_pattern: object = None
 
+    def box(self) -> tuple:
+        """(x0, x1, y0, y1, z0, z1): the cells the source writes (both boxes)."""
+        lo = list(self.origin)
+        hi = [o + d for o, d in zip(self.origin, self.dims)]
+        if self.comp_pattern is not None:
+            lo = [min(a, b) for a, b in zip(lo, self.comp_origin)]
+            hi = [max(a, o + d) for a, o, d in zip(hi, self.comp_origin, self.comp_dims)]
+        return (lo[0], hi[0], lo[1], hi[1], lo[2], hi[2])
+
 
 @dataclass
 class Problem:
@@ -267,32 +276,46 @@ def fine_solve(pb: Problem, vf, steps: int, on_even=None):
 
 
 def coarse_step(pb: Problem, vc, p, q, src, w, m, mlp: Mlp | None = None,
-                fused: bool = True) -> None:
+                fused: bool = True, flags=None) -> None:
     """One coarse step from level m (p) over level m-1 (q, overwritten with m+1):
     the acoustic step, the learned correction (mlp given; one fused launch unless
-    fused is False), then the source."""
+    fused is False), then the source.  flags = (flags of p, flags for q): the
+    fused step's activity flags (chunks far from any value at the correction
+    floor skip the network; the source box counts as active)."""
     g = pb.coarse
     if mlp is None:
         wave_step(p, q, vc, q, g)
     elif fused:
-        mlp.learned_step(p, q, vc, g)
+        mlp.learned_step(p, q, vc, g, flags=flags, box=None if flags is None else src.box())
     else:
         wave_step(p, q, vc, q, g)
         mlp.correct(p, vc, q, g)
     _inject(pb, False, q, src, w, m)
 
 
-def coarse_solve(pb: Problem, vc, steps: int, mlp: Mlp | None = None):
-    """Plain (mlp None) or corrected coarse solve from rest for `steps` coarse steps."""
+def new_flags(mlp: Mlp, g: Grid):
+    """A pair of activity-flag buffers for the fused step on g, all active."""
+    torch = _torch()
+    n = mlp.flags_bytes(g)
+    return [torch.ones(n, dtype=torch.uint8, device="cuda"),
+            torch.ones(n, dtype=torch.uint8, device="cuda")]
+
+
+def coarse_solve(pb: Problem, vc, steps: int, mlp: Mlp | None = None, use_flags: bool = True):
+    """Plain (mlp None) or corrected coarse solve from rest for `steps` coarse steps
+    (corrected: with activity flags unless use_flags is False; the same bits)."""
     torch = _torch()
     g = pb.coarse
     p = torch.zeros(g.shape, device="cuda")
     q = torch.zeros(g.shape, device="cuda")
     w = pb.wavelet(False, steps)
     src = pb.source(False)
+    fl = new_flags(mlp, g) if mlp is not None and use_flags else None
     for m in range(steps):
-        coarse_step(pb, vc, p, q, src, w, m, mlp)
+        coarse_step(pb, vc, p, q, src, w, m, mlp, flags=None if fl is None else (fl[0], fl[1]))
         p, q = q, p
+        if fl is not None:
+            fl.reverse()
     return p
 
 
@@ -517,12 +540,15 @@ def learned_solve(pb: Problem, coarse_steps: int, mlp: Mlp, bound: float = 1e-3,
     wp = px.wavelet(False, coarse_steps)
     wf = px.wavelet(True, 2 * coarse_steps)
     src, psrc, pfsrc = pb.source(False), px.source(False), px.source(True)
+    fl, pfl = new_flags(mlp, g), new_flags(mlp, gp)
     checks, fallback = [], None
     for m in range(coarse_steps):
-        coarse_step(pb, vc, p, q, src, w, m, mlp)
+        coarse_step(pb, vc, p, q, src, w, m, mlp, flags=(fl[0], fl[1]))
         p, q = q, p
-        coarse_step(px, pvc, pp, pq, psrc, wp, m, mlp)
+        fl.reverse()
+        coarse_step(px, pvc, pp, pq, psrc, wp, m, mlp, flags=(pfl[0], pfl[1]))
         pp, pq = pq, pp
+        pfl.reverse()
         for k in (2 * m, 2 * m + 1):
             wave_step(fp, fq, pvf, fq, gpf)
             _inject(px, True, fq, pfsrc, wf, k)

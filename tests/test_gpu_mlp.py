@@ -328,3 +328,57 @@ def test_correction_floor(torch_cuda):
         assert np.array_equal(f[low], plain[low])
         assert np.array_equal(f[high], nf[high])
         assert not np.array_equal(nf[low], plain[low])
+
+
+@pytest.mark.parametrize("floor", [0.0, 2.0 ** -20])
+def test_learned_step_flags_keep_the_bits(torch_cuda, floor):
+    """Activity flags: over 14 steps of a sparse field with a source box added
+    after every step, the flagged fused step (chunks far from any value at the
+    floor take the plain path) gives the same bits as the unflagged one and as
+    the acoustic step followed by the correction; the flags mark some chunks
+    idle and some active."""
+    torch = torch_cuda
+    nz, ny, nx = 100, 64, 96
+    rng = np.random.default_rng(31)
+    p0 = np.zeros((nz, ny, nx), np.float32)
+    p0[10:18, 8:14, 10:20] = rng.standard_normal((8, 6, 10))
+    v2 = rng.uniform(1500, 4500, (nz, ny, nx)).astype(np.float32) ** 2
+    g = sb.Grid(nx, ny, nz, 10.0, 10.0, 10.0, 8e-4)
+    w, _, _ = net_and_rows(15, 1)
+    origin, dims = (60, 40, 70), (5, 4, 3)  # a source box far from the blob
+    pat = torch.from_numpy(rng.uniform(0.5, 1.0, dims[::-1]).astype(np.float32)).cuda()
+    box = (origin[0], origin[0] + dims[0], origin[1], origin[1] + dims[1], origin[2],
+           origin[2] + dims[2])
+    V = dev(torch, v2)
+    with sb.Mlp() as m:
+        m.set_params(w)
+        m.output_scale = 0.3
+        m.min_scale = floor
+        m.set_kernel("tcgen05")
+        n = m.flags_bytes(g)
+        assert n > 0
+        states = {k: [dev(torch, p0), dev(torch, p0)] for k in ("ref", "fused", "flags")}
+        fl = [torch.ones(n, dtype=torch.uint8, device="cuda"),
+              torch.zeros(n, dtype=torch.uint8, device="cuda")]
+        idle = active = 0
+        for step in range(14):
+            for k, (p, q) in states.items():
+                if k == "ref":
+                    sb.wave_step(p, q, V, q, g)
+                    m.correct(p, V, q, g)
+                elif k == "fused":
+                    m.learned_step(p, q, V, g)
+                else:
+                    m.learned_step(p, q, V, g, flags=(fl[0], fl[1]), box=box)
+                sb.add_box(q, g, origin, dims, pat, 0.25 * (step % 3 + 1))
+                states[k] = [q, p]
+            f = fl[1].cpu().numpy()
+            idle += int((f == 0).sum())
+            active += int((f != 0).sum())
+            fl.reverse()
+        torch.cuda.synchronize()
+        for k in ("fused", "flags"):
+            for a, b in zip(states[k], states["ref"]):
+                assert torch.equal(a, b), (k, float((a - b).abs().max()))
+        assert idle > 0 and active > 0, (idle, active)
+        assert not torch.equal(states["ref"][0], dev(torch, p0))
