@@ -59,6 +59,10 @@ def args_():
                     help="--kernel batch: the FP16-storage batch")
     ap.add_argument("--sparse", action="store_true",
                     help="--kernel learned / mlp: a small random cube in a zero field (floor 2^-64)")
+    ap.add_argument("--zero", action="store_true",
+                    help="--kernel learned: an all-zero field (floor 2^-64)")
+    ap.add_argument("--flags", action="store_true",
+                    help="--kernel learned --zero: with activity flags (all clear: the plain path)")
     ap.add_argument("--kernel", choices=["acoustic", "heat", "fp16", "batch", "mlp", "learned"],
                     help="run only a small case of one kernel (for profilers) and print its time")
     return ap.parse_args()
@@ -762,12 +766,20 @@ def run_kernel_probe(a):
             p.zero_()
             p[lo:hi, lo:hi, lo:hi] = blob
             m.min_scale = 2.0 ** -64
+        elif a.zero:
+            p.zero_()
+            m.min_scale = 2.0 ** -64
     if a.kernel == "mlp":
         out = torch.zeros_like(p)
         f = lambda: m.correct(p, v, out, g)  # noqa: E731
     elif a.kernel == "learned":
         q = p * 0.99
-        f = lambda: m.learned_step(p, q, v, g)  # noqa: E731
+        fl = None
+        if a.flags and a.zero:  # the true flags of a zero field: all clear
+            nb = m.flags_bytes(g)
+            fl = (torch.zeros(nb, dtype=torch.uint8, device="cuda"),
+                  torch.zeros(nb, dtype=torch.uint8, device="cuda"))
+        f = lambda: m.learned_step(p, q, v, g, flags=fl)  # noqa: E731
     elif a.kernel == "batch":  # 12 shots with extents n/2..n in steps of 8
         rng = np.random.default_rng(SEED)
         shots = []
