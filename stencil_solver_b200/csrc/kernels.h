@@ -89,7 +89,7 @@ int learned_step_resident();
 struct LearnedChunks {
     int tiles_x = 0, tiles_y = 0, zchunks = 0, zlen = 0;
 };
-LearnedChunks learned_step_chunks(const GridDesc& g, int sms);
+LearnedChunks learned_step_chunks(const GridDesc& g, int sms, bool flagged);
 // flags_in: per chunk, whether p may hold a value at or above the floor (NULL:
 // all may); box (x0, x1, y0, y1, z0, z1 cells, or NULL) counts as flagged;
 // flags_out receives the flags of p_next (NULL: none).

@@ -1000,7 +1000,7 @@ int sb200_mlp_learned_step(void* h, const float* p, float* p_prev_next, const fl
 int64_t sb200_mlp_flags_bytes(void* h, const sb200_grid* grid) {
     Mlp* m = static_cast<Mlp*>(h);
     if (!m || !grid) return set_error(SB200_ERR_INVALID, "sb200_mlp_flags_bytes: NULL argument");
-    const LearnedChunks c = learned_step_chunks(grid_desc(*grid), m->sms);
+    const LearnedChunks c = learned_step_chunks(grid_desc(*grid), m->sms, true);
     return int64_t(c.tiles_x) * c.tiles_y * c.zchunks;
 }
 
