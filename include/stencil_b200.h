@@ -311,7 +311,17 @@ int sb200_batch_set_fields(void* handle, int shot, const float* p, const float* 
 int sb200_batch_set_wavelet(void* handle, int shot, const float* w, int64_t n);
 /* Enqueues n steps of every shot; the run may not pass max_steps in total. */
 int sb200_batch_steps(void* handle, int64_t n);
+/* Waits for the enqueued steps.  Returns SB200_ERR_MONITOR when a shot's
+ * stability monitor tripped: a non-finite value, or (FP32) max |p| above the
+ * limit, in the FP64 statistics taken at every graph-chunk end (FP32), at every
+ * renormalisation (FP16) and at synchronisation; SB200_ERR_DEVICE on a device
+ * error.  The run handle's monitor per shot (sb200_run_synchronize). */
 int sb200_batch_synchronize(void* handle);
+/* Largest |p| the FP32 monitor accepts (default 1e30). */
+int sb200_batch_set_monitor_limit(void* handle, float limit);
+/* Per-shot monitor flags (n_shots ints, 1 = tripped) to host memory after the
+ * check of the current level (synchronous; set_fields clears a shot's flag). */
+int sb200_batch_monitor_flags(void* handle, int* flags);
 int sb200_batch_get_field(void* handle, int shot, float* p);
 int sb200_batch_get_trace(void* handle, int shot, float* trace, int64_t n);
 /* Times every (tile variant, z-chunk length) on the batch's own buffers and

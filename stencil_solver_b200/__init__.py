@@ -168,6 +168,8 @@ _SIGNATURES = {
     "sb200_batch_get_field": ([C.c_void_p, C.c_int, C.c_void_p], C.c_int),
     "sb200_batch_get_trace": ([C.c_void_p, C.c_int, C.c_void_p, C.c_int64], C.c_int),
     "sb200_batch_tune": ([C.c_void_p, C.c_int], C.c_int),
+    "sb200_batch_set_monitor_limit": ([C.c_void_p, C.c_float], C.c_int),
+    "sb200_batch_monitor_flags": ([C.c_void_p, C.c_void_p], C.c_int),
     "sb200_batch_set_choice": ([C.c_void_p, C.c_int, C.c_int], C.c_int),
     "sb200_batch_choice": ([C.c_void_p] + [C.POINTER(C.c_int)] * 4, C.c_int),
     "sb200_batch_steps_done": ([C.c_void_p], C.c_int64),
@@ -592,6 +594,18 @@ class Batch:
 
     def synchronize(self) -> None:
         _check(lib().sb200_batch_synchronize(self._h))
+
+    def set_monitor_limit(self, limit: float) -> None:
+        """Largest |p| the FP32 stability monitor accepts (default 1e30)."""
+        _check(lib().sb200_batch_set_monitor_limit(self._h, float(limit)))
+
+    def monitor_flags(self):
+        """Per-shot monitor flags (1: non-finite value or |p| above the limit)."""
+        import numpy as np
+
+        out = np.zeros(len(self.grids), np.int32)
+        _check(lib().sb200_batch_monitor_flags(self._h, out.ctypes.data))
+        return out
 
     def field(self, shot: int):
         import numpy as np

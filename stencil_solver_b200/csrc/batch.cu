@@ -48,6 +48,12 @@ size_t round_up(size_t b) { return (b + kAlign - 1) / kAlign * kAlign; }
 // z-chunk lengths the tuner tries (0: one chunk per column).
 constexpr int kZlens[] = {0, 128, 64, 32};
 
+// Stability monitor of one shot: a non-finite value or max |p| above the limit
+// (FP64 statistics {sum p^2, max |p|, non-finite count}) sets its flag.
+__global__ void batch_monitor_kernel(const double* stats3, int* flag, double limit) {
+    if (!(stats3[2] == 0.0) || !(stats3[1] <= limit)) *flag = 1;
+}
+
 struct BatchChoice {
     int variant = 0;
     int zlen = 64;
@@ -122,15 +128,19 @@ public:
         if (int rc = alloc(reinterpret_cast<void**>(&queue_), sizeof(BatchQueue))) return rc;
         if (int rc = alloc(reinterpret_cast<void**>(&wave_), sizeof(float) * cap_ * n)) return rc;
         if (int rc = alloc(reinterpret_cast<void**>(&trace_), sizeof(float) * cap_ * n)) return rc;
+        // FP64 statistics (monitor; FP16: renormalisation too), their scratch,
+        // and one monitor flag per shot
+        if (int rc = alloc(reinterpret_cast<void**>(&stats_), sizeof(double) * 3 * n)) return rc;
+        for (const Shot& h : shots_) {
+            sb200_grid gg = to_grid(h.g);
+            scratch_len_ = std::max(scratch_len_, sb200_field_stats_scratch_len(&gg));
+        }
+        if (int rc = alloc(reinterpret_cast<void**>(&scratch_), sizeof(double) * scratch_len_)) return rc;
+        if (int rc = alloc(reinterpret_cast<void**>(&mon_), sizeof(int) * n)) return rc;
+        if (int rc = cuda(cudaMemsetAsync(mon_, 0, sizeof(int) * n, st_))) return rc;
         if (f16_) {
-            // scales, FP64 statistics and their scratch, source bounds, FP32 staging
+            // scales, source bounds, FP32 staging
             if (int rc = alloc(reinterpret_cast<void**>(&scale_), sizeof(F16Scale) * n)) return rc;
-            if (int rc = alloc(reinterpret_cast<void**>(&stats_), sizeof(double) * 3 * n)) return rc;
-            for (const Shot& h : shots_) {
-                sb200_grid gg = to_grid(h.g);
-                scratch_len_ = std::max(scratch_len_, sb200_field_stats_scratch_len(&gg));
-            }
-            if (int rc = alloc(reinterpret_cast<void**>(&scratch_), sizeof(double) * scratch_len_)) return rc;
             if (int rc = alloc(reinterpret_cast<void**>(&bound_), sizeof(float) * cap_ * n)) return rc;
             if (int rc = alloc(reinterpret_cast<void**>(&staging_), sizeof(float) * max_points_)) return rc;
             if (int rc = cuda(cudaMemsetAsync(bound_, 0, sizeof(float) * cap_ * n, st_))) return rc;
@@ -166,7 +176,8 @@ public:
                         static_cast<void*>(wave_), static_cast<void*>(trace_),
                         static_cast<void*>(items_), static_cast<void*>(scale_),
                         static_cast<void*>(stats_), static_cast<void*>(scratch_),
-                        static_cast<void*>(bound_), static_cast<void*>(staging_)})
+                        static_cast<void*>(bound_), static_cast<void*>(staging_),
+                        static_cast<void*>(mon_)})
             if (p) cudaFree(p);
         if (st_) cudaStreamDestroy(st_);
     }
@@ -178,6 +189,9 @@ public:
         const Shot& h = shots_[s];
         const size_t bytes = static_cast<size_t>(h.g.size()) * 4;
         const int cur = static_cast<int>(step_ & 1);  // level that is current now
+        // new fields: the shot's monitor starts clear (and is checked again)
+        if (int rc = cuda(cudaMemsetAsync(mon_ + s, 0, sizeof(int), st_))) return rc;
+        checked_step_ = -1;
         if (f16_) return set_fields_f16(s, p, p_prev, vel2, cur);
         if (int rc = cuda(cudaMemcpyAsync(arena_ + h.off[cur], p, bytes, cudaMemcpyHostToDevice, st_)))
             return rc;
@@ -229,11 +243,59 @@ public:
     }
 
     int synchronize() {
+        if (checked_step_ != step_) {  // the monitor over the current level of every shot
+            if (int rc = enqueue_monitor(static_cast<int>(step_ & 1))) return rc;
+            checked_step_ = step_;
+        }
         if (int rc = cuda(cudaStreamSynchronize(st_))) return rc;
         int e = 0;
         if (int rc = cuda(cudaMemcpy(&e, err_, sizeof(int), cudaMemcpyDeviceToHost))) return rc;
         if (e) return set_error(SB200_ERR_DEVICE, "sb200_batch: a kernel's bounded wait gave up");
+        std::vector<int> f(static_cast<size_t>(n_shots()));
+        if (int rc = cuda(cudaMemcpy(f.data(), mon_, sizeof(int) * f.size(), cudaMemcpyDeviceToHost)))
+            return rc;
+        for (int k = 0; k < n_shots(); ++k)
+            if (f[k])
+                return set_error(SB200_ERR_MONITOR,
+                                 "sb200_batch: stability monitor tripped on shot " + std::to_string(k) +
+                                     " (non-finite value or |p| above the limit)");
         return SB200_OK;
+    }
+
+    // Per-shot FP64 statistics of level `par` and the monitor check: a
+    // non-finite value, or (FP32) |p| above the limit, sets the shot's flag.
+    // FP16 checks for non-finite values (the stored field is scaled).
+    int enqueue_monitor(int par) {
+        for (int s = 0; s < n_shots(); ++s) {
+            const Shot& h = shots_[s];
+            const sb200_grid gg = to_grid(h.g);
+            const int rc =
+                f16_ ? sb200_field_stats_f16(reinterpret_cast<const uint16_t*>(arena_ + h.off[par]),
+                                             &gg, 1.f, stats_ + 3 * s, scratch_, scratch_len_, st_)
+                     : sb200_field_stats_f32(reinterpret_cast<const float*>(arena_ + h.off[par]),
+                                             &gg, stats_ + 3 * s, scratch_, scratch_len_, st_);
+            if (rc) return rc;
+            batch_monitor_kernel<<<1, 1, 0, st_>>>(stats_ + 3 * s, mon_ + s,
+                                                   f16_ ? 1e300 : monitor_limit_);
+        }
+        return cuda(cudaGetLastError());
+    }
+
+    int set_monitor_limit(float limit) {
+        if (!(limit > 0.f)) return set_error(SB200_ERR_INVALID, "sb200_batch_set_monitor_limit: limit <= 0");
+        monitor_limit_ = limit;
+        return SB200_OK;
+    }
+
+    int monitor_flags(int* out) {
+        if (!out) return set_error(SB200_ERR_INVALID, "sb200_batch_monitor_flags: NULL output");
+        if (checked_step_ != step_) {
+            if (int rc = enqueue_monitor(static_cast<int>(step_ & 1))) return rc;
+            checked_step_ = step_;
+        }
+        if (int rc = cuda(cudaMemcpyAsync(out, mon_, sizeof(int) * n_shots(), cudaMemcpyDeviceToHost, st_)))
+            return rc;
+        return cuda(cudaStreamSynchronize(st_));
     }
 
     int get_field(int s, float* out) {
@@ -518,6 +580,7 @@ private:
             if (int rc = sb200_field_stats_f16(reinterpret_cast<const uint16_t*>(arena_ + h.off[par]),
                                                &gg, 1.f, stats_ + 3 * s, scratch_, scratch_len_, st_))
                 return rc;
+            batch_monitor_kernel<<<1, 1, 0, st_>>>(stats_ + 3 * s, mon_ + s, 1e300);
             if (int rc = sb200_f16_renorm(stats_ + 3 * s, reinterpret_cast<sb200_f16_scale*>(scale_ + s),
                                           bound_ + s * cap_, &queue_->step, 0.f, kTarget, st_))
                 return rc;
@@ -530,6 +593,7 @@ private:
         if (int rc = cuda(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal))) return rc;
         int rc = SB200_OK;
         for (int k = 0; k < chunk_ && !rc; ++k) rc = step_once(k, (par + k) & 1);
+        if (!rc && !f16_) rc = enqueue_monitor((par + chunk_) & 1);  // FP32: at every chunk end
         const cudaError_t e = cudaStreamEndCapture(st_, &g);
         if (rc) {
             if (g) cudaGraphDestroy(g);
@@ -641,7 +705,10 @@ private:
     int esz_ = 4;
     int64_t max_points_ = 0;
     F16Scale* scale_ = nullptr;  // FP16: per-shot scale
-    double* stats_ = nullptr;    // FP16: per-shot FP64 statistics (3 each)
+    double* stats_ = nullptr;    // per-shot FP64 statistics (3 each)
+    int* mon_ = nullptr;         // per-shot monitor flags (1: tripped)
+    double monitor_limit_ = 1e30;
+    int64_t checked_step_ = -1;  // step count at the last monitor check
     double* scratch_ = nullptr;
     int64_t scratch_len_ = 0;
     float* bound_ = nullptr;    // FP16: per-shot source bound per step (max_steps each)
@@ -739,6 +806,16 @@ int sb200_batch_get_trace(void* h, int shot, float* out, int64_t n) {
 int sb200_batch_tune(void* h, int reps) {
     SB200_BATCH_OR_FAIL(h);
     return as_batch(h)->tune(reps);
+}
+
+int sb200_batch_set_monitor_limit(void* h, float limit) {
+    if (!h) return set_error(SB200_ERR_INVALID, "NULL batch handle");
+    return as_batch(h)->set_monitor_limit(limit);
+}
+
+int sb200_batch_monitor_flags(void* h, int* flags) {
+    if (!h) return set_error(SB200_ERR_INVALID, "NULL batch handle");
+    return as_batch(h)->monitor_flags(flags);
 }
 
 int sb200_batch_set_choice(void* h, int variant, int zlen) {

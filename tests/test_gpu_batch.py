@@ -178,3 +178,48 @@ def test_f16_batch_tune_and_validation():
     g = sb.Grid(40, 32, 32)
     with pytest.raises(sb.StencilError):  # a chunk that does not start on a renorm
         sb.Batch([(g, None)], max_steps=100, graph_chunk=30, precision=sb.PRECISION_F16)
+
+
+@pytest.mark.parametrize("precision,chunk", [(sb.PRECISION_F32, 0), (sb.PRECISION_F32, 10),
+                                             (sb.PRECISION_F16, 50)])
+def test_batch_monitor_flags_the_shot_that_blows_up(precision, chunk):
+    """A non-finite value in one shot trips that shot's monitor (eager steps,
+    graph chunks, FP16 renormalisation statistics) and synchronize fails; the
+    other shots stay clear, and new fields clear the flag."""
+    shots = make_shots(seed=27)[:3]
+    with sb.Batch([(g, s) for g, s, _, _ in shots], max_steps=120, graph_chunk=chunk,
+                  precision=precision) as b:
+        for i, (g, _, v, w) in enumerate(shots):
+            p = np.zeros(g.shape, np.float32)
+            if i == 1:
+                p[g.nz // 2, g.ny // 2, g.nx // 2] = np.nan
+            b.set_fields(i, p, p, v)
+            b.set_wavelet(i, w)
+        b.steps(60 if precision == sb.PRECISION_F16 else 20)
+        with pytest.raises(sb.StencilError) as e:
+            b.synchronize()
+        assert e.value.status == sb.SB200_ERR_MONITOR and "shot 1" in str(e.value)
+        assert list(b.monitor_flags()) == [0, 1, 0]
+        g, _, v, _ = shots[1]
+        z = np.zeros(g.shape, np.float32)
+        b.set_fields(1, z, z, v)
+        assert list(b.monitor_flags()) == [0, 0, 0]
+
+
+def test_batch_monitor_limit():
+    shots = make_shots(seed=29)[:2]
+    with sb.Batch([(g, s) for g, s, _, _ in shots], max_steps=STEPS, graph_chunk=0) as b:
+        for i, (g, _, v, w) in enumerate(shots):
+            z = np.zeros(g.shape, np.float32)
+            b.set_fields(i, z, z, v)
+            b.set_wavelet(i, w)
+        b.steps(20)
+        b.synchronize()
+        peak = max(float(np.abs(b.field(i)).max()) for i in range(2))
+        assert peak > 0
+        b.set_monitor_limit(peak / 2)
+        b.steps(1)
+        with pytest.raises(sb.StencilError) as e:
+            b.synchronize()
+        assert e.value.status == sb.SB200_ERR_MONITOR
+        assert b.monitor_flags().sum() >= 1
