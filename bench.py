@@ -558,6 +558,24 @@ def secondary_learned(train_models: int = 16, nc_eval: int = 516, coarse_steps: 
 
 # ── our arm ───────────────────────────────────────────────────────────────────
 
+def max_over_ranks(pg, ms: float, device: str = "cuda") -> float:
+    """The largest of every rank's `ms` (a device time): the job is as slow as
+    its slowest replica.  Without a process group, `ms` itself."""
+    if pg is None:
+        return ms
+    import torch
+
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_gpts(world: int, interior: int, steps: int, ms_max: float) -> float:
+    """Whole-job throughput of `world` replicas that each update `interior`
+    points `steps` times, over the slowest replica's time."""
+    return world * interior * steps / (ms_max * 1e-3) / 1e9
+
+
 def run_ours(a):
     import torch
 
@@ -621,15 +639,11 @@ def run_ours(a):
         pg.barrier()
     clk = clocks.stop()
     ms = e0.elapsed_time(e1)
-    ms_max = ms
-    if pg:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms_max = float(t.item())
+    ms_max = max_over_ranks(pg, ms)
     assert sb.device_error() == 0, "device error word set during the timed run"
 
     ms_step = ms_max / a.steps
-    value = world * g.interior * a.steps / (ms_max * 1e-3) / 1e9
+    value = job_gpts(world, g.interior, a.steps, ms_max)
     peak, peak_src = measured_peak()
     achieved = BYTES_PER_POINT * g.interior / (ms / a.steps * 1e-3) / 1e9
     tpp = profiled_traffic_per_point()
@@ -667,15 +681,11 @@ def run_ours(a):
     hout.copy_(dp, non_blocking=True)
     f1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = f0.elapsed_time(f1)
-    if pg:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(pg, f0.elapsed_time(f1))
     assert np.isfinite(htrace.numpy()).all()
     h2d = 3 * g.size * 4 + 0  # vel2, p, p_prev (the per-step source sample is a kernel argument)
     d2h = g.size * 4 + E * 4  # final field + one trace sample per step
-    e2e = {"value": world * g.interior * E / (e2e_ms * 1e-3) / 1e9, "unit": "Gpts/s",
+    e2e = {"value": job_gpts(world, g.interior, E, e2e_ms), "unit": "Gpts/s",
            "h2d_bytes_per_step": h2d / E, "d2h_bytes_per_step": d2h / E,
            "steps": E, "ms_total": e2e_ms,
            "api": "sb200_wave_step_f32 per step; fields uploaded from / downloaded to pinned "
