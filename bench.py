@@ -463,7 +463,7 @@ def secondary_batch(n_shots: int = 48, steps: int = 400):
 
 
 def secondary_learned(train_models: int = 16, nc_eval: int = 516, coarse_steps: int = 200,
-                      horizon: int = 80, src_clear: float = 0.0):
+                      horizon: int = 80, src_clear: float = 0.0, samples_per_pair: int = 4096):
     """Learned 2x-coarse stepping: the network is trained (hand-written forward /
     backward / Adam kernels) on pairs from the plain fine solver over
     train_models seeded 256^3 fine / 132^3 coarse models (600 fine steps each),
@@ -486,7 +486,7 @@ def secondary_learned(train_models: int = 16, nc_eval: int = 516, coarse_steps: 
                            src_c=tuple(int(v) for v in rng.integers(c - 20, c + 20, 3)))
            for k in range(train_models)]
     t0 = time.perf_counter()
-    ds = learned.make_pairs(pbs, fine_steps=600, samples_per_pair=4096, every=6,
+    ds = learned.make_pairs(pbs, fine_steps=600, samples_per_pair=samples_per_pair, every=6,
                             src_clear=src_clear)
     mlp = sb.Mlp(seed=3)
     hist = learned.train(ds, mlp, epochs=8, batch=16384, lr=2e-3)
