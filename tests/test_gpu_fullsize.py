@@ -3,8 +3,8 @@ that do not need a full-size oracle run: one step of the 1024^3 FP32 acoustic
 grid (2^30 cells, byte offsets past 2^32) and of the 2048^3 FP16 grid (2^33
 cells) at 4096 sampled interior points against a float64 restatement of the
 stencil from the gathered stars (tolerance: FP32 rounding of the terms, plus
-one FP16 ulp for the stored halves), and linearity of the FP32 step under a
-power-of-two scaling (bit for bit)."""
+one FP16 ulp for the stored halves), linearity of the FP32 step under a
+power-of-two scaling (bit for bit), and one heat step of the 512^3 grid."""
 from __future__ import annotations
 
 import numpy as np
@@ -124,4 +124,31 @@ def test_fp16_2048_sampled(torch_cuda):
     ref = 2 * st[:, 0] - qs + ks * lap
     ulp = np.spacing(np.abs(ref).astype(np.float16)).astype(np.float64)
     tol = ulp + 64 * 2.0 ** -24 * (2 * np.abs(st[:, 0]) + np.abs(qs) + ks * mag)
+    assert np.all(np.abs(got - ref) <= tol), float(np.max(np.abs(got - ref) / tol))
+
+
+def test_heat_512_sampled(torch_cuda):
+    """The heat configuration's grid (512^3, alpha dt / dx^2 = 0.05, U[0, 1)
+    interior, zero walls): one step at sampled points against float64."""
+    torch = torch_cuda
+    n = 512
+    g = sb.Grid(n, n, n, 1.0, 1.0, 1.0, 0.05)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(31)
+    u = torch.rand(g.shape, generator=gen, device="cuda")
+    u[:R] = 0
+    u[-R:] = 0
+    u[:, :R] = 0
+    u[:, -R:] = 0
+    u[:, :, :R] = 0
+    u[:, :, -R:] = 0
+    out = torch.zeros_like(u)
+    sb.heat_step(u, out, g, 1.0)
+    idx = sample_points(torch, g.shape, 4096, 32)
+    st = stars(torch, u, idx, g.shape)
+    got = out.reshape(-1)[idx].double().cpu().numpy()
+    lap, mag = lap_terms(st, 1.0, 1.0, 1.0, oracle.fd_coefficients()[0])
+    k = float(np.float32(0.05))
+    ref = st[:, 0] + k * lap
+    tol = 4e-6 * (np.abs(st[:, 0]) + k * mag) + 1e-30
     assert np.all(np.abs(got - ref) <= tol), float(np.max(np.abs(got - ref) / tol))
