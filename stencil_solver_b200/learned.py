@@ -332,7 +332,7 @@ class Dataset:
 
 def make_pairs(problems, fine_steps: int, samples_per_pair: int = 4096, every: int = 4,
                first: int = 8, wall: int = 12, amp_floor: float = 0.05, src_clear: float = 0.0,
-               seed: int = 0, policy: Mlp | None = None, weighting: str = "uniform") -> Dataset:
+               seed: int = 0) -> Dataset:
     """Training rows from the plain fine solver on each problem: every `every`
     coarse steps from `first` on, samples_per_pair random coarse cells at least
     `wall` cells from the walls and src_clear source widths from the source point,
@@ -341,16 +341,7 @@ def make_pairs(problems, fine_steps: int, samples_per_pair: int = 4096, every: i
     then not a function of the local state).  With the coarse source's
     composition term (Problem.compose_source) the residual inside the source is
     a function of the state too, and rows there (src_clear 0) halve the
-    corrected solve's early error.  weighting "energy" draws the cells with
-    probability proportional to the squared field value instead of uniformly,
-    so the rows weigh as the cells weigh in the field's L2 error (the
-    correction is s c y, s the star's scale).
-
-    With a policy network, the coarse states are the corrected coarse solve's own
-    (run in step with the fine solve) instead of the restricted fine states, and
-    the target is the restricted fine state minus the plain step of that state:
-    rows from the states the corrected solver actually visits, whose targets also
-    pull its accumulated drift back toward the fine solution."""
+    corrected solve's early error."""
     torch = _torch()
     gen = torch.Generator(device="cuda")
     gen.manual_seed(seed)
@@ -373,24 +364,12 @@ def make_pairs(problems, fine_steps: int, samples_per_pair: int = 4096, every: i
         del zz, yy, xx, d2
         before = sum(x.shape[0] for x in Xs)
 
-        roll = [torch.zeros(gc.shape, device="cuda"), torch.zeros(gc.shape, device="cuda")]
-
         def on_even(m, f):
             c = torch.empty(gc.shape, device="cuda")
             restrict2(f, pb.fine, c, gc, OFFSET)
             ring[m] = c
             ring.pop(m - 3, None)
-            sample = m >= max(first, 2) and (m - first) % every == 0
-            if policy is not None and m >= 1:
-                # roll = [level m - 1, level m - 2] of the corrected coarse solve
-                if sample:
-                    plain.copy_(roll[1])
-                    coarse_step(pb, vc, roll[0], plain, src_c, w_c, m - 1)
-                    sample_rows(roll[0], c, m)
-                coarse_step(pb, vc, roll[0], roll[1], src_c, w_c, m - 1, policy)
-                roll.reverse()
-                return
-            if sample:
+            if m >= max(first, 2) and (m - first) % every == 0:
                 cm2, cm1, cm = ring[m - 2], ring[m - 1], ring[m]
                 plain.copy_(cm2)  # in-place leapfrog writes over the older level
                 coarse_step(pb, vc, cm1, plain, src_c, w_c, m - 1)
@@ -404,11 +383,7 @@ def make_pairs(problems, fine_steps: int, samples_per_pair: int = 4096, every: i
             if cand.numel() == 0:
                 return
             k = min(samples_per_pair, cand.numel())
-            if weighting == "energy":
-                wgt = mag.view(-1)[cand].double().pow(2)
-                pick = cand[torch.multinomial(wgt, k, replacement=True, generator=gen)]
-            else:
-                pick = cand[torch.randint(0, cand.numel(), (k,), generator=gen, device="cuda")]
+            pick = cand[torch.randint(0, cand.numel(), (k,), generator=gen, device="cuda")]
             X = torch.empty((pick.numel(), 32), dtype=torch.int16, device="cuda")
             t = torch.empty(pick.numel(), dtype=torch.float32, device="cuda")
             mlp_samples(state, vc, target, plain, gc, pick.to(torch.int64), X, t)
