@@ -27,8 +27,18 @@
 //      w3 dot product) finishes the correction.
 // Points whose star stays below the network's correction floor (by default: is
 // exactly zero) get no correction; threads with no such point skip the features,
-// warps the epilogues, and a plane-tile with none skips the network.  Every wait is bounded; on timeout the CTA records the
-// error, lets its copies and MMAs land, releases TMEM and exits.
+// warps the epilogues, and a plane-tile with none skips the network.
+//
+// Activity flags (optional): one byte per tile and z chunk says whether the
+// chunk of p may hold a value at or above the floor; the kernel writes the same
+// for p_next.  A CTA with no flagged chunk among its 26 neighbours can have no
+// active star and takes a plain path: the same stencil with the queue in
+// compile-time slots (unrolled by 9), 12-stage rings in the shared memory the
+// network would use, no TMEM -- after giving up the TMEM allocation permit, which
+// the SM otherwise waits on before it starts another CTA of this kernel.
+//
+// Every wait is bounded; on timeout the CTA records the error, lets its copies
+// and MMAs land, releases TMEM and exits.
 #include <cuda_runtime.h>
 
 #include <algorithm>
