@@ -391,14 +391,15 @@ int sb200_mlp_learned_step(void* handle, const float* p, float* p_prev_next, con
  * and the device). */
 int64_t sb200_mlp_flags_bytes(void* handle, const sb200_grid* grid);
 /* sb200_mlp_learned_step with activity flags (the same bits).  flags_in (device,
- * sb200_mlp_flags_bytes bytes, or NULL: every chunk active) says which chunks
- * of p may hold a value at or above the correction floor; cells of `box` (x0,
- * x1, y0, y1, z0, z1, half-open; NULL: none) count as flagged too -- pass the
- * box of whatever was added to p after the step that wrote its flags (a
- * source).  Chunks with no flagged chunk within one tile / z chunk of them take
- * the plain step with no network work.  flags_out (or NULL) receives the flags
- * of p_next; it must not be flags_in.  Start a run with flags_in all ones (or
- * NULL). */
+ * sb200_mlp_flags_bytes bytes, or NULL: every chunk active) describes p, one
+ * byte per chunk: bit 0 = some value at or above the correction floor, bits 1-6
+ * = such a value within 4 cells of the chunk's -x, +x, -y, +y, -z, +z face;
+ * 0xFF when unknown.  Cells of `box` (x0, x1, y0, y1, z0, z1, half-open; NULL:
+ * none) count as active too -- pass the box of whatever was added to p after
+ * the step that wrote its flags (a source).  A chunk whose own bit 0 and whose
+ * face neighbours' facing bits are clear takes the plain step with no network
+ * work.  flags_out (or NULL) receives the flags of p_next; it must not be
+ * flags_in.  Start a run with flags_in all 0xFF (or NULL). */
 int sb200_mlp_learned_step_flags(void* handle, const float* p, float* p_prev_next,
                                  const float* vel2, const sb200_grid* grid, const uint8_t* flags_in,
                                  uint8_t* flags_out, const int64_t* box, void* stream);

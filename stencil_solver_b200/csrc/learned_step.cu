@@ -103,17 +103,54 @@ struct LearnedArgs {
     int box[6];
 };
 
-// Whether chunk (tx, ty, zc) of the launch may hold an active value: its flag,
-// or it meets the forced box.
-__device__ __forceinline__ bool chunk_flagged(const LearnedArgs& a, int tx, int ty, int zc) {
-    if (a.flags_in[(int64_t(zc) * a.tiles_y + ty) * a.tiles_x + tx]) return true;
+// Activity flag bits of a chunk: any value at or above the floor (kAny), and
+// such a value within R cells of its -x, +x, -y, +y, -z, +z face.
+constexpr uint32_t kAny = 1u, kXlo = 2u, kXhi = 4u, kYlo = 8u, kYhi = 16u, kZlo = 32u, kZhi = 64u;
+
+// Whether some star of chunk (tx, ty, zc) may be active.  A 25-point star reaches
+// R cells along one axis, so only the chunk itself and the facing R-cell slabs
+// of its six face neighbours matter (tiles and full chunks are longer than R);
+// the forced box counts as active where it meets the chunk grown by R.
+__device__ __forceinline__ bool chunk_active(const LearnedArgs& a, int tx, int ty, int zc) {
+    auto flag = [&](int x, int y, int z) -> uint32_t {
+        if (x < 0 || x >= a.tiles_x || y < 0 || y >= a.tiles_y || z < 0 || z >= a.zchunks)
+            return 0u;
+        return a.flags_in[(int64_t(z) * a.tiles_y + y) * a.tiles_x + x];
+    };
+    if ((flag(tx, ty, zc) & kAny) || (flag(tx - 1, ty, zc) & kXhi) ||
+        (flag(tx + 1, ty, zc) & kXlo) || (flag(tx, ty - 1, zc) & kYhi) ||
+        (flag(tx, ty + 1, zc) & kYlo) || (flag(tx, ty, zc - 1) & kZhi) ||
+        (flag(tx, ty, zc + 1) & kZlo))
+        return true;
     const int x0 = R + tx * LTX, y0 = R + ty * LTY, z0 = R + zc * a.zlen;
-    return a.box[0] < x0 + LTX && x0 < a.box[1] && a.box[2] < y0 + LTY && y0 < a.box[3] &&
-           a.box[4] < z0 + a.zlen && z0 < a.box[5];
+    return a.box[0] < x0 + LTX + R && x0 - R < a.box[1] && a.box[2] < y0 + LTY + R &&
+           y0 - R < a.box[3] && a.box[4] < z0 + a.zlen + R && z0 - R < a.box[5];
+}
+
+// Flag bits of a thread's stored plane i of nint (its 4 points at column lx,
+// row ly of the tile) when one of them is active.
+__device__ __forceinline__ uint32_t face_bits(int lx, int ly, int i, int nint) {
+    return kAny | (lx == 0 ? kXlo : 0u) | (lx == LTPR - 1 ? kXhi : 0u) | (ly < R ? kYlo : 0u) |
+           (ly >= LTY - R ? kYhi : 0u) | (i < R ? kZlo : 0u) | (i >= nint - R ? kZhi : 0u);
 }
 
 __device__ __forceinline__ float lane_of(const float4& v, int e) {
     return e == 0 ? v.x : (e == 1 ? v.y : (e == 2 ? v.z : v.w));
+}
+
+// OR of every thread's bits (all threads of the CTA call it).
+__device__ __forceinline__ uint32_t block_or(uint32_t bits) {
+    __shared__ uint32_t s_or;
+    if (threadIdx.x == 0) s_or = 0u;
+    __syncthreads();
+    bits |= __shfl_xor_sync(0xffffffffu, bits, 16);
+    bits |= __shfl_xor_sync(0xffffffffu, bits, 8);
+    bits |= __shfl_xor_sync(0xffffffffu, bits, 4);
+    bits |= __shfl_xor_sync(0xffffffffu, bits, 2);
+    bits |= __shfl_xor_sync(0xffffffffu, bits, 1);
+    if ((threadIdx.x & 31) == 0 && bits) atomicOr(&s_or, bits);
+    __syncthreads();
+    return s_or;
 }
 
 // A chunk with no active star: the plain FP32 acoustic step (the pencil kernel's
@@ -191,7 +228,7 @@ __device__ __forceinline__ void plain_chunk(const CUtensorMap& pmap, const CUten
         for (int jj = 0; jj < R; ++jj)
             if (jj + LS < nplanes) issue_plane(jj + LS);
     }
-    float omax = 0.f;
+    uint32_t bits = 0u;  // activity flag bits of the stored points
     for (int i0 = 0; i0 < nint && !abort_run; i0 += 9) {
 #pragma unroll
         for (int u = 0; u < 9; ++u) {
@@ -246,8 +283,8 @@ __device__ __forceinline__ void plain_chunk(const CUtensorMap& pmap, const CUten
                 const float4 o = make_float4(o0.x, o0.y, o1.x, o1.y);
                 if (!bad && rin) {
                     stg_stream(a.next + goff, o);
-                    omax = fmaxf(omax, fmaxf(fmaxf(fabsf(o.x), fabsf(o.y)),
-                                             fmaxf(fabsf(o.z), fabsf(o.w))));
+                    const float m = fmaxf(fmaxf(fabsf(o.x), fabsf(o.y)), fmaxf(fabsf(o.z), fabsf(o.w)));
+                    if (m > 0.f && m >= a.min_scale) bits |= face_bits(lx, ly, i, nint);
                 }
                 goff += a.sz;
                 abort_run = __syncthreads_or(bad) != 0;
@@ -259,7 +296,7 @@ __device__ __forceinline__ void plain_chunk(const CUtensorMap& pmap, const CUten
             }
         }
     }
-    const bool act_out = __syncthreads_or(omax > 0.f && omax >= a.min_scale) != 0;
+    const uint32_t out_bits = block_or(bits);
     if (abort_run) {
         if (tid == 0) {
             record_error(a.err, kDevWaitTimeout);
@@ -271,7 +308,7 @@ __device__ __forceinline__ void plain_chunk(const CUtensorMap& pmap, const CUten
         return;
     }
     if (a.flags_out && tid == 0)
-        a.flags_out[(int64_t(zc) * a.tiles_y + ty) * a.tiles_x + tx] = act_out ? 1 : 0;
+        a.flags_out[(int64_t(zc) * a.tiles_y + ty) * a.tiles_x + tx] = uint8_t(out_bits);
 }
 
 __global__ void __launch_bounds__(LNT, 3)
@@ -303,21 +340,10 @@ __global__ void __launch_bounds__(LNT, 3)
     const int ze = min(zb + a.zlen, a.nz - R);
     const int nint = ze - zb, nplanes = nint + 2 * R;
 
-    // No star of this chunk can reach the floor when no chunk within one tile /
-    // one z chunk of it is flagged (a star reaches 4 cells; tiles and full
-    // chunks are at least that long): then the plain step is the whole answer.
-    bool skip = false;
-    if (a.flags_in) {
-        skip = true;
-        for (int dz = -1; dz <= 1 && skip; ++dz)
-            for (int dy = -1; dy <= 1 && skip; ++dy)
-                for (int dx = -1; dx <= 1 && skip; ++dx) {
-                    const int nx_ = tx + dx, ny_ = ty + dy, nz_ = b + dz;
-                    if (nx_ >= 0 && nx_ < a.tiles_x && ny_ >= 0 && ny_ < a.tiles_y && nz_ >= 0 &&
-                        nz_ < a.zchunks && chunk_flagged(a, nx_, ny_, nz_))
-                        skip = false;
-                }
-    }
+    // No star of this chunk can reach the floor when neither the chunk nor the
+    // facing slab of a face neighbour is flagged: then the plain step is the
+    // whole answer.
+    const bool skip = a.flags_in && !chunk_active(a, tx, ty, b);
     if (skip) {
         // No TMEM here: give up the allocation permit at once, as the network
         // path does after its allocation (the SM starts no further CTA of this
@@ -418,7 +444,7 @@ __global__ void __launch_bounds__(LNT, 3)
         if (ok) waited = ncommit;
     };
 
-    float omax = 0.f;  // largest |p_next| this thread stores (activity flag of the chunk)
+    uint32_t bits = 0u;  // activity flag bits of the points this thread stores
     // One plane per iteration; the queue shifts by one slot at the end (the body
     // is too large to unroll 9 times and still fit the instruction cache).
     for (int i = 0; i < nint && !abort_run; ++i) {
@@ -643,16 +669,17 @@ __global__ void __launch_bounds__(LNT, 3)
         }
         if (!bad && rin) {
             stg_stream(a.next + goff, o);
-            omax = fmaxf(omax, fmaxf(fmaxf(fabsf(o.x), fabsf(o.y)), fmaxf(fabsf(o.z), fabsf(o.w))));
+            const float m = fmaxf(fmaxf(fabsf(o.x), fabsf(o.y)), fmaxf(fabsf(o.z), fabsf(o.w)));
+            if (m > 0.f && m >= a.min_scale) bits |= face_bits(lx, ly, i, nint);
         }
         goff += a.sz;
 #pragma unroll
         for (int k = 0; k < 8; ++k) q[k] = q[k + 1];
     }
     {
-        const bool act_out = __syncthreads_or(omax > 0.f && omax >= a.min_scale) != 0;
+        const uint32_t out_bits = block_or(bits);
         if (a.flags_out && tid == 0 && !abort_run)
-            a.flags_out[(int64_t(b) * a.tiles_y + ty) * a.tiles_x + tx] = act_out ? 1 : 0;
+            a.flags_out[(int64_t(b) * a.tiles_y + ty) * a.tiles_x + tx] = uint8_t(out_bits);
     }
 
     if (abort_run && tid == 0) {

@@ -294,11 +294,12 @@ def coarse_step(pb: Problem, vc, p, q, src, w, m, mlp: Mlp | None = None,
 
 
 def new_flags(mlp: Mlp, g: Grid):
-    """A pair of activity-flag buffers for the fused step on g, all active."""
+    """A pair of activity-flag buffers for the fused step on g, every bit set
+    (every chunk and face active)."""
     torch = _torch()
     n = mlp.flags_bytes(g)
-    return [torch.ones(n, dtype=torch.uint8, device="cuda"),
-            torch.ones(n, dtype=torch.uint8, device="cuda")]
+    return [torch.full((n,), 255, dtype=torch.uint8, device="cuda"),
+            torch.full((n,), 255, dtype=torch.uint8, device="cuda")]
 
 
 def coarse_solve(pb: Problem, vc, steps: int, mlp: Mlp | None = None, use_flags: bool = True):

@@ -358,7 +358,7 @@ def test_learned_step_flags_keep_the_bits(torch_cuda, floor):
         n = m.flags_bytes(g)
         assert n > 0
         states = {k: [dev(torch, p0), dev(torch, p0)] for k in ("ref", "fused", "flags")}
-        fl = [torch.ones(n, dtype=torch.uint8, device="cuda"),
+        fl = [torch.full((n,), 255, dtype=torch.uint8, device="cuda"),
               torch.zeros(n, dtype=torch.uint8, device="cuda")]
         idle = active = 0
         for step in range(14):
