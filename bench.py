@@ -552,6 +552,8 @@ def secondary_learned(train_models: int = 16, nc_eval: int = 516, coarse_steps: 
                          "rel_l2_judged": err_h, "rel_l2_plain_coarse": err_plain_h,
                          "time_to_solution_speedup_vs_fine": ms_fine_h / rep_h.ms},
         "train_src_clear_sigmas": src_clear,
+        "correction_floor": learned.CORRECTION_FLOOR,
+        "fused_step": "learned_step_kernel with activity flags (idle chunks take the plain path)",
         "judge": "restricted plain FP32 fine solve",
     }
 
