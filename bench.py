@@ -37,7 +37,6 @@ FREQ = 15.0
 SEED = 1234
 CONFIG_STEPS = 1000
 BYTES_PER_POINT = 16  # read p, p_prev, vel2; write p_next (FP32)
-CPU_SAMPLE_NZ = 72    # z-slab of the same grid for the CPU reference timing
 
 
 def args_():
@@ -84,47 +83,70 @@ def workload(n: int, rank: int = 0):
 
 
 def workload_desc(n, dt, vmax):
+    """The workload both arms report as `config` (identical keys and values)."""
     return {
         "workload": f"acoustic_fp32_{n}^3_layered",
         "grid": [n, n, n],
         "interior_points": (n - 8) ** 3,
         "dx_m": DX, "dt_s": dt, "v_max_mps": round(vmax, 2),
         "source": {"type": "ricker", "freq_hz": FREQ, "cell": [n // 2, n // 2, 16]},
-        "model": f"8 layers 1500-4500 m/s x (1+0.05 g), corr 20 cells, seed {SEED}+rank",
+        "velocity": (f"8 layers 1500-4500 m/s x (1+0.05 g), corr 20 cells, seed {SEED} "
+                     "(replica r of a multi-GPU run: seed + r)"),
+        "initial_state": "p = p_prev = 0",
         "l2_policy": "inputs larger than L2 (three 4 GiB fields), no flush",
     }
 
 
-# ── reference CPU path (oracle/_ref) on a bounded sample ───────────────────────
+def host_cores():
+    """(logical CPUs this process may run on, physical cores behind them)."""
+    try:
+        cpus = sorted(os.sched_getaffinity(0))
+    except AttributeError:
+        cpus = list(range(os.cpu_count() or 1))
+    phys = set()
+    try:
+        for c in cpus:
+            topo = pathlib.Path(f"/sys/devices/system/cpu/cpu{c}/topology")
+            phys.add(((topo / "physical_package_id").read_text().strip(),
+                      (topo / "core_id").read_text().strip()))
+    except OSError:
+        return len(cpus), None
+    return len(cpus), len(phys)
 
-def cpu_reference_sample(n: int, steps: int, warmup: int, seconds: float | None):
-    """Times the reference's CPU launch_naive (OpenMP, the reference's Release flags)
-    on a z-slab [0, CPU_SAMPLE_NZ) of the same model with the same source, started
-    from rest.  Returns (gpts_per_s, cores, sample_text, kind, steps_done)."""
+
+# ── reference CPU path (oracle/_ref): the reference's launch_naive ─────────────
+
+def cpu_reference_sample(n: int, steps: int, warmup: int, seconds: float | None,
+                         vel2=None, vmax=None):
+    """Times the reference's CPU launch_naive (src/kernels/stencil_naive.cu:136-170,
+    OpenMP, compiled from the reference's sources with its Release flags) on the
+    whole n^3 workload: the reference solver's three-buffer ring
+    (src/solver/wave_prop.cpp:67-75), the source added after each step, from rest.
+    The velocity model and the wavelet come from the oracle's restatement
+    (bit-equal to the product's), unless the caller passes the model.  `warmup`
+    untimed steps, then `steps` timed steps, or as many as fit in `seconds`.
+    Returns a dict."""
     import oracle
-    import stencil_solver_b200 as sb
 
     variant = "f32" if oracle.ref_available("f32") else None
-    nz = CPU_SAMPLE_NZ
-    vel2_full, vmax = sb.model_layered(n, n, n, SEED)
-    vel2 = np.ascontiguousarray(vel2_full[:nz])
-    del vel2_full
+    if vel2 is None:
+        vel2, vmax = oracle.model_layered(n, n, n, SEED)
     dt = float(np.float32(0.4 * DX / vmax))
     src = (16 * n + n // 2) * n + n // 2
-    w = sb.ricker(FREQ, 1.0 / FREQ, dt, 100000)
-    p = np.zeros((nz, n, n), np.float32)
-    q = np.zeros_like(p)
-    interior = (n - 8) * (n - 8) * (nz - 8)
+    w = oracle.ricker(FREQ, 1.0 / FREQ, dt, warmup + max(steps, 1) * 64 + 64).astype(np.float32)
+    ring = [np.zeros((n, n, n), np.float32) for _ in range(3)]  # prev, cur, next
+    ip, ic, inx = 0, 1, 2
+    k_src = np.float32(np.float32(np.float32(dt) * np.float32(dt)) * vel2.flat[src])
 
     def one(step_i):
-        nonlocal p, q
+        nonlocal ip, ic, inx
         if variant:
-            oracle.ref_wave_step(p, q, vel2, DX, DX, DX, dt, variant=variant, out=q)
+            oracle.ref_wave_step(ring[ic], ring[ip], vel2, DX, DX, DX, dt, variant=variant,
+                                 out=ring[inx])
         else:
-            oracle.wave_step(p, q, vel2, DX, DX, DX, dt, out=q)
-        k = np.float32(np.float32(dt) * np.float32(dt)) * vel2.flat[src]
-        q.flat[src] = np.float32(q.flat[src] + np.float32(k * w[step_i]))
-        p, q = q, p
+            oracle.wave_step(ring[ic], ring[ip], vel2, DX, DX, DX, dt, out=ring[inx])
+        ring[inx].flat[src] = np.float32(ring[inx].flat[src] + np.float32(k_src * w[step_i]))
+        ip, ic, inx = ic, inx, ip
 
     for s in range(warmup):
         one(s)
@@ -136,33 +158,44 @@ def cpu_reference_sample(n: int, steps: int, warmup: int, seconds: float | None)
         el = time.perf_counter() - t0
         if seconds is None and done >= steps:
             break
-        if seconds is not None and (el >= seconds or done >= max(steps, 1) * 50):
-            if done >= 1:
-                break
+        if seconds is not None and (el >= seconds or done >= len(w) - warmup - 1):
+            break
     el = time.perf_counter() - t0
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    kind = "reference" if variant else "port"
-    sample = (f"{done} steps of a {n}x{n}x{nz} z-slab (interior {n-8}x{n-8}x{nz-8}) of the "
-              f"same layered model and source, from rest; "
-              f"{'reference launch_naive CPU path (-O3 -march=x86-64-v4 -fopenmp)' if variant else 'oracle port'}")
-    return interior * done / el / 1e9, cores, sample, kind, done, el, dt, vmax
+    logical, physical = host_cores()
+    threads = oracle.ref_omp_threads(variant) if variant else logical
+    interior = (n - 8) ** 3
+    what = ("reference launch_naive CPU path (-O3 -march=x86-64-v4 -fopenmp)" if variant
+            else "oracle port of launch_naive")
+    sample = (f"{done} timed steps (after {warmup} untimed) of the whole {n}^3 grid, "
+              f"three-buffer ring, from rest; {what}; {threads} OpenMP threads on "
+              f"{physical} physical cores")
+    del ring
+    return {"gpts": interior * done / el / 1e9, "threads": threads, "physical_cores": physical,
+            "logical_cpus": logical, "sample": sample,
+            "kind": "reference" if variant else "port", "steps": done, "seconds": el,
+            "dt": dt, "vmax": vmax}
 
 
 def run_reference(a):
+    """The reference arm: rank 0 alone times the reference's CPU path on the whole
+    workload; it loads only numpy and oracle/ (never the product library)."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    v, cores, sample, kind, done, el, dt, vmax = cpu_reference_sample(a.n, a.steps, a.warmup,
-                                                                       None)
+    r = cpu_reference_sample(a.n, a.steps, a.warmup, None)
+    v = r["gpts"]
     line = {
         "metric": "acoustic interior grid-point updates per second",
         "value": v, "unit": "Gpts/s", "impl": "reference", "n_gpus": world,
-        "steps": a.steps, "warmup": a.warmup, "ms_per_step": el / max(done, 1) * 1e3,
+        "steps": r["steps"], "warmup": a.warmup, "ms_per_step": r["seconds"] / r["steps"] * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": workload_desc(a.n, dt, vmax) | {"sample": sample},
-        "cpu_baseline": {"value": v, "unit": "Gpts/s", "cores": cores, "kind": kind,
-                         "sample": sample},
+        "config": workload_desc(a.n, r["dt"], r["vmax"]),
+        "parallelism": f"cpu_openmp{r['threads']}",
+        "cpu_baseline": {"value": v, "unit": "Gpts/s", "cores": r["threads"],
+                         "physical_cores": r["physical_cores"],
+                         "logical_cpus": r["logical_cpus"], "kind": r["kind"],
+                         "sample": r["sample"]},
         "e2e": {"value": v, "unit": "Gpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -719,8 +752,10 @@ def run_ours(a):
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        cv, cores, sample, kind, *_ = cpu_reference_sample(n, 1, 2, a.cpu_seconds)
-        cpu = {"value": cv, "unit": "Gpts/s", "cores": cores, "kind": kind, "sample": sample}
+        r = cpu_reference_sample(n, 1, 2, a.cpu_seconds, vel2, vmax)
+        cpu = {"value": r["gpts"], "unit": "Gpts/s", "cores": r["threads"],
+               "physical_cores": r["physical_cores"], "logical_cpus": r["logical_cpus"],
+               "kind": r["kind"], "sample": r["sample"]}
 
     secondary = None
     if rank == 0 and world == 1 and not a.no_secondary:
@@ -744,9 +779,9 @@ def run_ours(a):
         "value": value, "unit": "Gpts/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": workload_desc(n, g.dt, vmax) | {"parallelism": f"replicas{world}",
-                                               "tile": vname, "zchunks": choice[1],
-                                               "tuned": tuned is not None},
+        "config": workload_desc(n, g.dt, vmax),
+        "parallelism": f"replicas{world}",
+        "kernel_choice": {"tile": vname, "zchunks": choice[1], "tuned": tuned is not None},
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
         "gpu_launches": a.steps,
         "host_issue_ms_per_step": host_issue_ms,

@@ -186,7 +186,12 @@ int sb200_field_stats_f16(const uint16_t* field, const sb200_grid* grid, float s
  * so the same bits.  Nothing in the array must start at zero.  The array is
  * shared per device: calls that overlap on the device (unordered streams) race.
  * The first call per device looks up the array's address
- * (cudaGetSymbolAddress); make it before any stream capture starts. */
+ * (cudaGetSymbolAddress); make it before any stream capture starts.  The
+ * looked-up address is kept for the life of the process and does not survive
+ * cudaDeviceReset.  While another stream of the process is being captured, pass
+ * an explicit stream created with cudaStreamNonBlocking: stream NULL is the
+ * legacy default stream, whose implicit synchronisation with blocking streams
+ * would invalidate that capture. */
 int sb200_field_stats_f32_noalloc(const float* field, const sb200_grid* grid, double* out3,
                                   void* stream);
 

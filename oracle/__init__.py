@@ -68,6 +68,12 @@ def lib() -> C.CDLL:
         L.oracle_mlp_forward.restype = None
         L.oracle_mlp_grad.argtypes = [_f32p, _u16p, _f32p, _i64, C.c_int, _f64p]
         L.oracle_mlp_grad.restype = C.c_double
+        L.oracle_model_layered.argtypes = [_f32p, _i64, _i64, _i64, C.c_uint64, C.c_int,
+                                           C.c_float, C.c_float, C.c_float, C.c_float,
+                                           C.POINTER(C.c_float)]
+        L.oracle_model_layered.restype = C.c_int
+        L.oracle_mt64_nth.argtypes = [C.c_uint64, _i64]
+        L.oracle_mt64_nth.restype = C.c_uint64
         L.oracle_rms_diff_f32.argtypes = [_f32p, _f32p, _i64]
         L.oracle_rms_diff_f32.restype = C.c_double
         L.oracle_max_abs_diff_f32.argtypes = [_f32p, _f32p, _i64]
@@ -181,6 +187,24 @@ def ricker(f, t0, dt, n_steps) -> np.ndarray:
     return out
 
 
+def model_layered(nx, ny, nz, seed, n_layers=8, v_top=1500.0, v_bottom=4500.0,
+                  perturbation=0.05, corr_cells=20.0):
+    """Seeded layered v^2 model, (nz, ny, nx) float32, and v_max: the oracle's
+    restatement of the benchmark's velocity model (model_oracle.c)."""
+    out = np.empty((nz, ny, nx), np.float32)
+    vmax = C.c_float()
+    rc = lib().oracle_model_layered(out, nx, ny, nz, seed, n_layers, v_top, v_bottom,
+                                    perturbation, corr_cells, C.byref(vmax))
+    if rc != 0:
+        raise ValueError("oracle_model_layered: invalid arguments")
+    return out, float(vmax.value)
+
+
+def mt64_nth(seed: int, n: int) -> int:
+    """The n-th output (1-based) of the MT19937-64 engine seeded with `seed`."""
+    return int(lib().oracle_mt64_nth(seed, n))
+
+
 def rms_diff(a, b) -> float:
     return lib().oracle_rms_diff_f32(np.ascontiguousarray(a, np.float32),
                                      np.ascontiguousarray(b, np.float32), a.size)
@@ -249,6 +273,13 @@ def ref_wave_run(cur, prev, vel2, dx, dy, dz, dt, n_steps, src=-1, wavelet=None,
     ref(variant).ref_wave_run(cur, prev, scratch, vel2, nx, ny, nz, dx, dy, dz, dt, n_steps,
                               src, wl.ctypes.data if wl is not None else None)
     return cur, prev
+
+
+def ref_omp_threads(variant: str = "f32") -> int:
+    """OpenMP threads the reference CPU launcher uses in this process."""
+    L = ref(variant)
+    L.ref_omp_threads.restype = C.c_int
+    return int(L.ref_omp_threads())
 
 
 def ref_init_gaussian(shape, cx, cy, cz, sigma, variant="f32_strict"):

@@ -1,8 +1,8 @@
 """Build recipe for the oracle (test infrastructure only).
 
 Produces
-  oracle/liboracle.so                 -- the C restatement (stencil_oracle.c),
-                                         -ffp-contract=off, OpenMP.
+  oracle/liboracle.so                 -- the C restatements (stencil_oracle.c,
+                                         model_oracle.c), -ffp-contract=off, OpenMP.
   oracle/_ref/libstencil_ref_*.so     -- the reference's own CPU path, compiled
                                          from its sources where they lie (only
                                          when the reference checkout exists):
@@ -23,7 +23,11 @@ import subprocess
 import sys
 
 HERE = pathlib.Path(__file__).resolve().parent
-REF_ROOT = pathlib.Path(os.environ.get("STENCIL_REF_ROOT", "/root/reference"))
+
+# The reference checkout this recipe compiles from: $STENCIL_REF_ROOT, else the
+# path where this build environment mounts it.  Hosts without the checkout use
+# prebuilt oracle/_ref/ files if they have them, and otherwise build the oracle only.
+REF_ROOT = pathlib.Path(os.environ.get("STENCIL_REF_ROOT") or "/root/reference")
 
 # Reference translation units that make up its CPU path (kernels + solver + utils).
 REF_SOURCES = [
@@ -60,10 +64,10 @@ def _run(cmd):
 
 def build_oracle(force: bool = False) -> pathlib.Path:
     out = HERE / "liboracle.so"
-    src = HERE / "stencil_oracle.c"
-    if force or _newer(out, [src]):
+    srcs = [HERE / "stencil_oracle.c", HERE / "model_oracle.c"]
+    if force or _newer(out, srcs):
         _run(["gcc", "-O2", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared", "-std=c11",
-              "-Wall", "-Wextra", str(src), "-o", str(out), "-lm"])
+              "-Wall", "-Wextra", *map(str, srcs), "-o", str(out), "-lm"])
     return out
 
 

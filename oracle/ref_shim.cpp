@@ -9,6 +9,8 @@
 //   stencil::upload_fd_coefficients   src/kernels/stencil_naive.cu:129-134 (CPU branch)
 //   stencil::launch_naive             src/kernels/stencil_naive.cu:136-170 (CPU branch)
 //   stencil::make_solver / ISolver    src/solver/solver_base.cpp:119-133
+#include <omp.h>
+
 #include <cstdint>
 #include <cstring>
 #include <memory>
@@ -118,5 +120,8 @@ void ref_init_gaussian(real_t* out, int64_t nx, int64_t ny, int64_t nz, double c
                            static_cast<real_t>(cz), static_cast<real_t>(sigma));
     std::memcpy(out, h.ptr(), h.bytes());
 }
+
+// Threads an OpenMP region of the reference's CPU launcher uses in this process.
+int ref_omp_threads() { return omp_get_max_threads(); }
 
 }  // extern "C"

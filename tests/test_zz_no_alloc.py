@@ -64,11 +64,33 @@ def test_noalloc_on_a_stream_matches(torch_cuda):
     ref = _with_scratch(torch, f, g)
     s = torch.cuda.Stream()
     out = torch.zeros(3, dtype=torch.float64, device="cuda")
+    s.wait_stream(torch.cuda.current_stream())  # f and out were written on the default stream
     with torch.cuda.stream(s):
         sb.field_stats_noalloc(f, g, out, stream=s)
         sb.field_stats_noalloc(f, g, out, stream=s)
     s.synchronize()
     assert np.array_equal(out.cpu().numpy(), ref)
+
+
+def test_noalloc_allocates_nothing(torch_cuda):
+    """After the first call on the device (which may load the library's module),
+    further calls leave the device's free memory and torch's allocator as they
+    were: the partials live in the static array."""
+    torch = torch_cuda
+    g = sb.Grid(200, 136, 96)
+    f = _field(torch, g, 4)
+    out = torch.zeros(3, dtype=torch.float64, device="cuda")
+    sb.field_stats_noalloc(f, g, out)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    alloc0, reserved0 = torch.cuda.memory_allocated(), torch.cuda.memory_reserved()
+    for _ in range(20):
+        sb.field_stats_noalloc(f, g, out)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert (torch.cuda.memory_allocated(), torch.cuda.memory_reserved()) == (alloc0, reserved0)
+    assert np.array_equal(out.cpu().numpy(), _with_scratch(torch, f, g))
 
 
 def test_noalloc_rejects_bad_arguments(torch_cuda):
