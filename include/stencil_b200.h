@@ -109,6 +109,19 @@ int sb200_set_device_int(int* dst, int value, void* stream);
 int sb200_heat_step_f32(const float* u, float* u_next, const sb200_grid* grid, float alpha,
                         void* stream);
 
+/* No reference counterpart.  First half of a coarse acoustic step that carries
+ * the composition term of two leapfrog steps of dt/2 (the learned 2x-coarse
+ * path).  With L = vel2 * lap (the 8th-order Laplacian of the grid), writes
+ *   r      = p + beta dt^2 L p                  (interior; halo untouched)
+ *   p_prev = p_prev + 2 beta dt^2 L p           (in place, interior)
+ * so that a plain step of (r, p_prev) -- sb200_wave_step_f32 or
+ * sb200_mlp_learned_step -- gives 2 p - p_prev + dt^2 L p + beta dt^4 L^2 p.
+ * beta = 1/16 is the dt^4 term of two steps of dt/2.  r, p and p_prev must be
+ * distinct; r's halo cells must hold zeros (they are never written); nx % 4 == 0
+ * and 16-byte aligned fields (the pencil kernel).  20 B per interior point. */
+int sb200_wave_prepass_f32(const float* p, float* p_prev, const float* vel2, float* r,
+                           const sb200_grid* grid, float beta, void* stream);
+
 /* ── inputs of the benchmark configurations (host memory; no reference counterpart:
  *    the reference has only a constant / two-layer velocity and a Gaussian pulse,
  *    include/stencil/grid.hpp:57-99) ─────────────────────────────────────────── */
@@ -397,7 +410,7 @@ int sb200_mlp_learned_step(void* handle, const float* p, float* p_prev_next, con
 int64_t sb200_mlp_flags_bytes(void* handle, const sb200_grid* grid);
 /* sb200_mlp_learned_step with activity flags (the same bits).  flags_in (device,
  * sb200_mlp_flags_bytes bytes, or NULL: every chunk active) describes p, one
- * byte per chunk: bit 0 = some value at or above the correction floor, bits 1-6
+ * byte per chunk: bit 0 = some value at or above half the correction floor, bits 1-6
  * = such a value within 4 cells of the chunk's -x, +x, -y, +y, -z, +z face;
  * 0xFF when unknown.  Cells of `box` (x0, x1, y0, y1, z0, z1, half-open; NULL:
  * none) count as active too -- pass the box of whatever was added to p after
@@ -408,6 +421,14 @@ int64_t sb200_mlp_flags_bytes(void* handle, const sb200_grid* grid);
 int sb200_mlp_learned_step_flags(void* handle, const float* p, float* p_prev_next,
                                  const float* vel2, const sb200_grid* grid, const uint8_t* flags_in,
                                  uint8_t* flags_out, const int64_t* box, void* stream);
+/* Activity flags for the field r = p + c L p of sb200_wave_prepass_f32, from the
+ * flags of p (both in the layout of sb200_mlp_flags_bytes): a chunk gets every
+ * bit when a 25-point star of p reaches it (p's chunk or a face neighbour's
+ * facing slab is flagged), else none.  The learned step of r then takes these as
+ * flags_in; its box argument must be grown by the stencil radius (4 cells),
+ * since the pre-pass spreads a box's values that far.  flags_p != flags_r. */
+int sb200_mlp_flags_compose(void* handle, const sb200_grid* grid, const uint8_t* flags_p,
+                            uint8_t* flags_r, void* stream);
 /* Correction floor: a point whose 25-point star has largest magnitude below
  * `floor` gets no correction (default 0: every point with a nonzero star).  Ahead
  * of a wavefront the stencil leaves values that decay and underflow; a correction

@@ -120,6 +120,10 @@ _SIGNATURES = {
                                    C.c_void_p], C.c_int),
     "sb200_heat_step_f32": ([C.c_void_p, C.c_void_p, C.POINTER(sb200_grid), C.c_float,
                              C.c_void_p], C.c_int),
+    "sb200_mlp_flags_compose": ([C.c_void_p, C.POINTER(sb200_grid), C.c_void_p, C.c_void_p,
+                                 C.c_void_p], C.c_int),
+    "sb200_wave_prepass_f32": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                C.POINTER(sb200_grid), C.c_float, C.c_void_p], C.c_int),
     "sb200_model_layered": ([C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_uint64, C.c_int,
                              C.c_float, C.c_float, C.c_float, C.c_float,
                              C.POINTER(C.c_float)], C.c_int),
@@ -323,6 +327,13 @@ def ricker(freq: float, t0: float, dt: float, n_steps: int):
     out = np.empty(n_steps, np.float32)
     _check(lib().sb200_ricker(freq, t0, dt, n_steps, out.ctypes.data))
     return out
+
+
+def wave_prepass(p, p_prev, vel2, r, grid: Grid, beta: float = 1.0 / 16.0, stream=None) -> None:
+    """r = p + beta dt^2 v^2 lap p; p_prev += 2 beta dt^2 v^2 lap p (sb200_wave_prepass_f32):
+    a plain step of (r, p_prev) then carries the beta dt^4 L^2 p term."""
+    _check(lib().sb200_wave_prepass_f32(_ptr(p), _ptr(p_prev), _ptr(vel2), _ptr(r), _g(grid),
+                                        C.c_float(beta), _stream(stream)))
 
 
 def heat_step_exact(u, u_next, grid: Grid, alpha: float, stream=None) -> None:
@@ -750,6 +761,11 @@ class Mlp:
             self._h, _ptr(p), _ptr(p_prev_next), _ptr(vel2), _g(grid),
             None if fin is None else _ptr(fin), None if fout is None else _ptr(fout),
             None if bx is None else C.cast(bx, C.c_void_p), _stream(stream)))
+
+    def flags_compose(self, grid: Grid, flags_p, flags_r, stream=None) -> None:
+        """flags_r = activity flags of wave_prepass's r from those of p."""
+        _check(lib().sb200_mlp_flags_compose(self._h, _g(grid), _ptr(flags_p), _ptr(flags_r),
+                                             _stream(stream)))
 
     def flags_bytes(self, grid: Grid) -> int:
         """Bytes of the activity flags of learned_step on `grid`."""

@@ -415,6 +415,30 @@ int sb200_heat_step_f32(const float* u, float* u_next, const sb200_grid* grid, f
     return finish_launch(launch_heat_naive(u, u_next, g, alpha_dt, st), "sb200_heat_step_f32");
 }
 
+int sb200_wave_prepass_f32(const float* p, float* p_prev, const float* vel2, float* r,
+                           const sb200_grid* grid, float beta, void* stream) {
+    const char* where = "sb200_wave_prepass_f32";
+    GridDesc g;
+    if (int rc = to_desc(grid, &g)) return rc;
+    if (!p || !p_prev || !vel2 || !r)
+        return fail(SB200_ERR_INVALID, std::string(where) + ": NULL field pointer");
+    if (r == p || r == p_prev || p == p_prev)
+        return fail(SB200_ERR_INVALID, std::string(where) + ": r, p and p_prev must be distinct");
+    if (!std::isfinite(beta))
+        return fail(SB200_ERR_INVALID, std::string(where) + ": beta must be finite");
+    if (!g.has_interior()) return SB200_OK;
+    if (!pencil_ok(g, {p, p_prev, vel2, r}))
+        return fail(SB200_ERR_UNSUPPORTED,
+                    std::string(where) + ": needs nx % 4 == 0 and 16-byte aligned fields");
+    const PencilConfig cfg = choose(SB200_KIND_WAVE_F32, g);
+    PencilMaps maps;
+    if (int rc = pencil_maps(false, cfg.variant, g, p, p_prev, vel2, &maps, where)) return rc;
+    return finish_launch(launch_prepass_pencil_f32(maps, p_prev, vel2, r, g, beta, cfg,
+                                                   device_error_ptr(),
+                                                   static_cast<cudaStream_t>(stream)),
+                         where);
+}
+
 int sb200_f16_pack(const float* src, uint16_t* dst, int64_t n, float scale, void* stream) {
     if (!src || !dst || n < 0) return fail(SB200_ERR_INVALID, "sb200_f16_pack: bad arguments");
     if (!(scale > 0.f) || !std::isfinite(scale))

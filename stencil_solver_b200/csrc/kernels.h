@@ -90,6 +90,10 @@ struct LearnedChunks {
     int tiles_x = 0, tiles_y = 0, zchunks = 0, zlen = 0;
 };
 LearnedChunks learned_step_chunks(const GridDesc& g, int sms, bool flagged);
+// Activity flags of r = p + c L p from those of p (same chunk layout): every
+// chunk a star of p reaches gets all bits, the others none.
+cudaError_t launch_flags_compose(const uint8_t* in, uint8_t* out, const GridDesc& g, int sms,
+                                 cudaStream_t stream);
 // flags_in: per chunk, whether p may hold a value at or above the floor (NULL:
 // all may); box (x0, x1, y0, y1, z0, z1 cells, or NULL) counts as flagged;
 // flags_out receives the flags of p_next (NULL: none).
@@ -108,6 +112,12 @@ cudaError_t launch_wave_pencil_f32(const PencilMaps& maps, const float* prev, co
 cudaError_t launch_heat_pencil_f32(const PencilMaps& maps, float* u_next, const GridDesc& g,
                                    float alpha_dt, const PencilConfig& cfg, int* err,
                                    cudaStream_t stream);
+// The acoustic tile `cfg.variant` in prepass mode: r = p + beta dt^2 v^2 lap p,
+// prev += 2 beta dt^2 v^2 lap p (maps as for the acoustic step, prev read and
+// written in place).
+cudaError_t launch_prepass_pencil_f32(const PencilMaps& maps, float* prev, const float* vel2,
+                                      float* r, const GridDesc& g, float beta,
+                                      const PencilConfig& cfg, int* err, cudaStream_t stream);
 // Resident CTAs per SM of a variant (occupancy query; analytic if that fails).
 // The first call per device also sets the variant's shared-memory attribute.
 int pencil_f32_resident(bool heat, int v);

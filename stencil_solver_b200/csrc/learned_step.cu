@@ -30,8 +30,8 @@
 // warps the epilogues, and a plane-tile with none skips the network.
 //
 // Activity flags (optional): one byte per tile and z chunk says whether the
-// chunk of p may hold a value at or above the floor; the kernel writes the same
-// for p_next.  A CTA with no flagged chunk among its 26 neighbours can have no
+// chunk of p may hold a value at or above half the floor; the kernel writes the
+// same for p_next.  A CTA with no flagged chunk among its 26 neighbours can have no
 // active star and takes a plain path: the same stencil with the queue in
 // compile-time slots (unrolled by 9), 12-stage rings in the shared memory the
 // network would use, no TMEM -- after giving up the TMEM allocation permit, which
@@ -87,13 +87,17 @@ struct LearnedArgs {
     float out_scale;   // c
     float min_scale;   // correction floor: stars whose largest magnitude is below it
                        // get no correction (0: every nonzero star)
+    float flag_floor;  // activity-flag threshold: min_scale / 2, so the flags also
+                       // bound r = p + c L p of the composition pre-pass, whose
+                       // stars exceed p's by at most 1 + 19.5 c v^2 / dx^2
+                       // (c = dt^2 / 16: below 1.3 at every stable Courant number)
     const uint16_t* w1b;  // BF16 W1, W2 (out x in)
     const uint16_t* w2b;
     float b1[H], b2[H], w3[H];
     float b3;
     int* err;
     // Activity flags (one byte per tile and z chunk; zchunks chunks of zlen):
-    // flags_in[c] != 0 when chunk c of p may hold a value at or above the floor
+    // flags_in[c] != 0 when chunk c of p may hold a value at or above half the floor
     // (NULL: every chunk may), box [x0, x1) x [y0, y1) x [z0, z1) cells counts as
     // flagged too (a source added after the previous step); flags_out[c] receives
     // the same for p_next (NULL: not written).
@@ -103,8 +107,8 @@ struct LearnedArgs {
     int box[6];
 };
 
-// Activity flag bits of a chunk: any value at or above the floor (kAny), and
-// such a value within R cells of its -x, +x, -y, +y, -z, +z face.
+// Activity flag bits of a chunk: any value at or above half the floor (kAny),
+// and such a value within R cells of its -x, +x, -y, +y, -z, +z face.
 constexpr uint32_t kAny = 1u, kXlo = 2u, kXhi = 4u, kYlo = 8u, kYhi = 16u, kZlo = 32u, kZhi = 64u;
 
 // Whether some star of chunk (tx, ty, zc) may be active.  A 25-point star reaches
@@ -284,7 +288,7 @@ __device__ __forceinline__ void plain_chunk(const CUtensorMap& pmap, const CUten
                 if (!bad && rin) {
                     stg_stream(a.next + goff, o);
                     const float m = fmaxf(fmaxf(fabsf(o.x), fabsf(o.y)), fmaxf(fabsf(o.z), fabsf(o.w)));
-                    if (m > 0.f && m >= a.min_scale) bits |= face_bits(lx, ly, i, nint);
+                    if (m > 0.f && m >= a.flag_floor) bits |= face_bits(lx, ly, i, nint);
                 }
                 goff += a.sz;
                 abort_run = __syncthreads_or(bad) != 0;
@@ -670,7 +674,7 @@ __global__ void __launch_bounds__(LNT, 3)
         if (!bad && rin) {
             stg_stream(a.next + goff, o);
             const float m = fmaxf(fmaxf(fabsf(o.x), fabsf(o.y)), fmaxf(fabsf(o.z), fabsf(o.w)));
-            if (m > 0.f && m >= a.min_scale) bits |= face_bits(lx, ly, i, nint);
+            if (m > 0.f && m >= a.flag_floor) bits |= face_bits(lx, ly, i, nint);
         }
         goff += a.sz;
 #pragma unroll
@@ -742,6 +746,43 @@ PencilBoxes learned_step_boxes() {
     return b;
 }
 
+namespace {
+
+// Flags of r = p + c L p (the composition pre-pass) from the flags of p: r can
+// hold a value at or above the flag threshold in a chunk only where a star of p
+// reaches one, i.e. where chunk_active holds for p's flags (L is a 25-point
+// star); such chunks get every bit (their face slabs are not resolved further).
+__global__ void flags_compose_kernel(const uint8_t* __restrict__ in, uint8_t* __restrict__ out,
+                                     int tiles_x, int tiles_y, int zchunks) {
+    const int64_t n = int64_t(tiles_x) * tiles_y * zchunks;
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int tx = static_cast<int>(i % tiles_x);
+    const int ty = static_cast<int>((i / tiles_x) % tiles_y);
+    const int zc = static_cast<int>(i / (int64_t(tiles_x) * tiles_y));
+    auto flag = [&](int x, int y, int z) -> uint32_t {
+        if (x < 0 || x >= tiles_x || y < 0 || y >= tiles_y || z < 0 || z >= zchunks) return 0u;
+        return in[(int64_t(z) * tiles_y + y) * tiles_x + x];
+    };
+    const bool act = (flag(tx, ty, zc) & kAny) || (flag(tx - 1, ty, zc) & kXhi) ||
+                     (flag(tx + 1, ty, zc) & kXlo) || (flag(tx, ty - 1, zc) & kYhi) ||
+                     (flag(tx, ty + 1, zc) & kYlo) || (flag(tx, ty, zc - 1) & kZhi) ||
+                     (flag(tx, ty, zc + 1) & kZlo);
+    out[i] = act ? uint8_t(kAny | kXlo | kXhi | kYlo | kYhi | kZlo | kZhi) : uint8_t(0);
+}
+
+}  // namespace
+
+cudaError_t launch_flags_compose(const uint8_t* in, uint8_t* out, const GridDesc& g, int sms,
+                                 cudaStream_t stream) {
+    const LearnedChunks c = learned_step_chunks(g, sms, true);
+    const int64_t n = int64_t(c.tiles_x) * c.tiles_y * c.zchunks;
+    if (n == 0) return cudaSuccess;
+    flags_compose_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, stream>>>(
+        in, out, c.tiles_x, c.tiles_y, c.zchunks);
+    return cudaGetLastError();
+}
+
 LearnedChunks learned_step_chunks(const GridDesc& g, int sms, bool flagged) {
     LearnedChunks c;
     if (!g.has_interior()) return c;
@@ -795,6 +836,7 @@ cudaError_t launch_learned_step(const PencilMaps& maps, float* next, const GridD
     a.dt_over_dx = g.dt / std::min(g.dx, std::min(g.dy, g.dz));
     a.out_scale = net.out_scale;
     a.min_scale = net.min_scale;
+    a.flag_floor = net.min_scale * 0.5f;
     a.w1b = net.w1b;
     a.w2b = net.w2b;
     for (int k = 0; k < H; ++k) {

@@ -1014,6 +1014,16 @@ int sb200_mlp_learned_step_flags(void* h, const float* p, float* p_prev_next, co
                              "sb200_mlp_learned_step_flags");
 }
 
+int sb200_mlp_flags_compose(void* h, const sb200_grid* grid, const uint8_t* flags_p,
+                            uint8_t* flags_r, void* stream) {
+    Mlp* m = static_cast<Mlp*>(h);
+    if (!m || !grid || !flags_p || !flags_r || flags_p == flags_r)
+        return set_error(SB200_ERR_INVALID, "sb200_mlp_flags_compose: bad arguments");
+    return cuda_err(launch_flags_compose(flags_p, flags_r, grid_desc(*grid), m->sms,
+                                         static_cast<cudaStream_t>(stream)),
+                    "sb200_mlp_flags_compose");
+}
+
 int sb200_mlp_set_kernel(void* h, int kernel) {
     Mlp* m = static_cast<Mlp*>(h);
     if (!m || kernel < 0 || kernel > 1)

@@ -25,7 +25,9 @@
 //     slot is a compile-time register and nothing is shifted.
 //   * arithmetic on point pairs uses the packed f32x2 instructions; the
 //     Laplacian is two FMA chains (x and y from the combined centre term, z from
-//     its first pair) added once.
+//     its first pair) added once; p_prev enters the update through the mixed
+//     subtract (no separate conversion).
+// Ring stages pass between the warps without a CTA barrier per plane (HandoffH).
 //
 // Renormalisation (driven by the FP64 statistics every few dozen steps): a
 // renorm step (PHASE 1) scales its output by r = a_new / a_old; the step after
@@ -107,6 +109,16 @@ __device__ __forceinline__ void stg_stream_u2(void* p, uint2 v) {
     asm volatile("st.global.cs.v2.u32 [%0], {%1, %2};" ::"l"(p), "r"(v.x), "r"(v.y) : "memory");
 }
 
+// f32(half) - b for both halves of a word (the sm_100 mixed-precision subtract).
+__device__ __forceinline__ float2 subhf2(uint32_t w, float2 b) {
+    float x, y;
+    asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\t"
+        "sub.rn.f32.f16 %0, lo, %3;\n\tsub.rn.f32.f16 %1, hi, %4;\n\t}"
+        : "=f"(x), "=f"(y)
+        : "r"(w), "f"(b.x), "f"(b.y));
+    return make_float2(x, y);
+}
+
 // f32(half `hi` of word w) + c (the mixed add on one point).
 __device__ __forceinline__ float addhf(uint32_t w, int hi, float c) {
     float d;
@@ -139,18 +151,73 @@ __device__ __forceinline__ float xsum1(const float (&c)[8], uint2 lf, uint2 rt, 
     return c[up] + c[dn];
 }
 
+// Shared-memory hand-off of ring stages between the warps of a CTA, in place of
+// a CTA barrier per plane: a warp that has read the last it needs of a stage
+// counts itself done (acquire-release atomic), and the warp that completes the
+// count refills the stage by TMA.  No warp waits for another; a warp at plane
+// iteration k needs only refills released at iterations <= k - 4, which every
+// warp, the slowest included, has passed.
+template <int S, int AUX>
+struct HandoffH {
+    uint32_t done_p[S];    // warps done with the plane in each p stage
+    uint32_t done_a[AUX];  // warps done with each aux stage
+    int issued_p;          // highest plane index of this tile handed to TMA
+    int issued_a;          // highest aux iteration of this tile handed to TMA
+    int abort;             // a bounded wait gave up somewhere in the CTA
+};
+
+template <int S, int AUX>
+__device__ __forceinline__ void init_handoff(HandoffH<S, AUX>* hs) {
+#pragma unroll
+    for (int s = 0; s < S; ++s) hs->done_p[s] = 0u;
+#pragma unroll
+    for (int s = 0; s < AUX; ++s) hs->done_a[s] = 0u;
+    hs->issued_p = hs->issued_a = -1;
+    hs->abort = 0;
+}
+
+__device__ __forceinline__ uint32_t atom_add_acq_rel_shared(uint32_t* p, uint32_t v) {
+    uint32_t old;
+    asm volatile("atom.acq_rel.cta.shared::cta.add.u32 %0, [%1], %2;"
+                 : "=r"(old)
+                 : "r"(smem_u32(p)), "r"(v)
+                 : "memory");
+    return old;
+}
+
+// Orders the stage reads acquired through the hand-off counter before the
+// async-proxy (TMA) write that refills the stage.
+__device__ __forceinline__ void fence_proxy_async_shared() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Ring position a CTA carries from one tile to the next: the sequence numbers of
+// the next p plane and the next aux iteration.  Stage = seq % ring size, phase
+// parity = (seq / ring size) & 1, so a persistent CTA initialises its mbarriers
+// once and their phases continue across the tiles it sweeps.
+struct RingH {
+    uint32_t p = 0;
+    uint32_t aux = 0;
+};
+
 // One tile: columns [tx TX, tx TX + TX) x rows [4 + ty TY, ...) of the interior,
 // marched over z chunk zc.  All threads of the CTA call it; `sm`, `full` and
-// `auxf` are the CTA's rings, their mbarriers freshly initialised by the caller
-// (phase 0 on every stage).  Every copy it issues has landed when it returns;
-// false means a bounded wait gave up (the error is recorded).
+// `auxf` are the CTA's rings, initialised by the caller, `ring` the position in
+// them (advanced on return) and `hs` the stage hand-off (counters at zero, abort
+// clear).  Every copy it issues has landed when it returns; false means a
+// bounded wait gave up (the error is recorded).
 template <int TX, int TY, int S, int AUX, int PHASE, int UNR>
 __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const CUtensorMap* qmap,
                                                 const CUtensorMap* kmap, const F16Args& a,
                                                 int tx, int ty, int zc, uint16_t* sm,
-                                                uint64_t* full, uint64_t* auxf) {
+                                                uint64_t* full, uint64_t* auxf, RingH& ring,
+                                                HandoffH<S, AUX>* hs) {
     using P = ShapeH<TX, TY, S, AUX>;
+    static_assert(P::NT % 32 == 0, "whole warps");
+    constexpr uint32_t kWarps = P::NT / 32;
     uint16_t* aux = sm + S * P::PLANE;  // AUX stages of [p_prev tile | K tile]
+    const uint32_t pb = ring.p;         // sequence number of plane 0
+    const uint32_t ab = ring.aux;       // sequence number of aux iteration 0
 
     const int tid = threadIdx.x;
     const int lx = tid % P::TPR;
@@ -167,20 +234,56 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
         prefetch_tmap(qmap);
         prefetch_tmap(kmap);
     }
-    int issued_hi = -1, aux_issued_hi = -1;
-    auto issue_plane = [&](int j) {  // thread 0 only
-        mbar_arrive_expect_tx(&full[j % S], P::PLANE_BYTES);
-        tma_load_3d(sm + (j % S) * P::PLANE, pmap, &full[j % S], xa - 8, y0 - R, zb - R + j);
-        issued_hi = j;
+    // Refills are issued by one thread at a time per stage (thread 0 at the
+    // start, then whichever warp completes a stage's hand-off count).
+    auto issue_plane = [&](int j) {
+        const uint32_t st = (pb + j) % S;
+        mbar_arrive_expect_tx(&full[st], P::PLANE_BYTES);
+        tma_load_3d(sm + st * P::PLANE, pmap, &full[st], xa - 8, y0 - R, zb - R + j);
+        atomicMax(&hs->issued_p, j);
     };
-    auto issue_aux = [&](int it) {  // thread 0 only
-        uint16_t* st = aux + (it % AUX) * 2 * P::TILE;
-        mbar_arrive_expect_tx(&auxf[it % AUX], 2 * P::TILE_BYTES);
-        tma_load_3d(st, qmap, &auxf[it % AUX], xa, y0, zb + it);
-        tma_load_3d(st + P::TILE, kmap, &auxf[it % AUX], xa, y0, zb + it);
-        aux_issued_hi = it;
+    auto issue_aux = [&](int it) {
+        const uint32_t sa = (ab + it) % AUX;
+        uint16_t* st = aux + sa * 2 * P::TILE;
+        mbar_arrive_expect_tx(&auxf[sa], 2 * P::TILE_BYTES);
+        tma_load_3d(st, qmap, &auxf[sa], xa, y0, zb + it);
+        tma_load_3d(st + P::TILE, kmap, &auxf[sa], xa, y0, zb + it);
+        atomicMax(&hs->issued_a, it);
+    };
+    auto wait_plane = [&](int j) { return mbar_wait(&full[(pb + j) % S], ((pb + j) / S) & 1u); };
+    auto wait_aux = [&](int it) {
+        return mbar_wait(&auxf[(ab + it) % AUX], ((ab + it) / AUX) & 1u);
+    };
+    // This warp is done with plane j's stage / aux iteration it's stage; the
+    // warp that completes the count refills it S planes / AUX iterations on.
+    const bool lane0 = (tid & 31) == 0;
+    auto release_plane = [&](int j) {
+        if (j + S >= nplanes) return;  // no refill: nothing to hand off
+        __syncwarp();
+        if (lane0) {
+            uint32_t* c = &hs->done_p[(pb + j) % S];
+            if (atom_add_acq_rel_shared(c, 1u) == kWarps - 1) {
+                atomicExch(c, 0u);
+                fence_proxy_async_shared();
+                issue_plane(j + S);
+            }
+        }
+    };
+    auto release_aux = [&](int it) {
+        if (it + AUX >= nint) return;
+        __syncwarp();
+        if (lane0) {
+            uint32_t* c = &hs->done_a[(ab + it) % AUX];
+            if (atom_add_acq_rel_shared(c, 1u) == kWarps - 1) {
+                atomicExch(c, 0u);
+                fence_proxy_async_shared();
+                issue_aux(it + AUX);
+            }
+        }
     };
     if (tid == 0) {
+        hs->issued_p = -1;
+        hs->issued_a = -1;
         for (int s = 0; s < S && s < nplanes; ++s) issue_plane(s);
         for (int it = 0; it < AUX && it < nint; ++it) issue_aux(it);
     }
@@ -215,7 +318,7 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
     float m_out = 1.f, m_q = 1.f;
     if (PHASE == 1) m_out = a.scale->r;
     if (PHASE == 2) m_q = a.scale->r;
-    const float2 nmq2 = dup2(-m_q), mout2 = dup2(m_out);
+    const float2 nmq2 = dup2(-m_q), nmout2 = dup2(-m_out);
 
     // Plane index p (z = zb - 4 + p) lives in slot p % 4 of both rings.
     uint4 hq[4];      // FP16: centre and the planes above it
@@ -223,8 +326,8 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
     bool bad = false;
 #pragma unroll
     for (int p = 0; p < 8; ++p) {
-        if (!mbar_wait(&full[p % S], (p / S) & 1)) bad = true;
-        const uint4 v = lds128h(sm + (p % S) * P::PLANE + soff);
+        if (!wait_plane(p)) bad = true;
+        const uint4 v = lds128h(sm + ((pb + p) % S) * P::PLANE + soff);
         if (p < R) {
 #pragma unroll
             for (int h = 0; h < 4; ++h) dq[p][h] = h2f2(get_word(v, h));
@@ -233,28 +336,25 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
         }
     }
     bool abort_run = __syncthreads_or(bad) != 0;
+    if (abort_run && tid == 0) hs->abort = 1;
     if (!abort_run && tid == 0) {
 #pragma unroll
         for (int p = 0; p < R; ++p)  // planes 0..3 are consumed: refill their stages
             if (p + S < nplanes) issue_plane(p + S);
     }
 
-    // The plane loop is unrolled by UNR (4 or 8).  i0 is a multiple of 4 and so
-    // is S: the fed plane's stage is a block base + u, wrapping at most once
-    // (UNR = 8), and its phase is a block constant or flips with the wrap; the aux
-    // ring (AUX | 4) has compile-time stages and a block-constant phase.
+    // The plane loop is unrolled by UNR (4 or 8); the register rings' slots are
+    // compile-time (i0 is a multiple of 4).  Shared-memory stages and phases
+    // follow the sequence numbers.
     static_assert(UNR == 4 || UNR == 8, "unroll");
     static_assert(UNR == 4 || S == 8, "an unroll of 8 needs an 8-stage ring");
     for (int i0 = 0; i0 < nint && !abort_run; i0 += UNR) {
-        const int cbase = (i0 + 4) % S, fbase = (i0 + 8) % S;
-        const uint32_t fpar = ((i0 + 8) / S) & 1u, apar = (i0 / AUX) & 1u;
 #pragma unroll
         for (int u = 0; u < UNR; ++u) {
             const int i = i0 + u;
             if (i < nint && !abort_run) {
                 // Centre plane i + 4 (slot u); it was waited for when it was fed.
-                const int cst = (cbase + u) % S, fst = (fbase + u) % S;
-                const uint32_t fph = fpar ^ (fbase + u >= S ? 1u : 0u);
+                const uint32_t cst = (pb + i + 4) % S, fst = (pb + i + 8) % S;
                 const uint16_t* pc = sm + cst * P::PLANE + soff;
                 // x window: 4 halves left and right of the chunk stay FP16; the
                 // own 8 points (the centre) are converted once.
@@ -266,7 +366,7 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                 const float cf[8] = {cv[0].x, cv[0].y, cv[1].x, cv[1].y,
                                      cv[2].x, cv[2].y, cv[3].x, cv[3].y};
                 // feed: plane i + 8 (z + 4) replaces the centre in slot u
-                if (!mbar_wait(&full[fst], fph)) bad = true;
+                if (!wait_plane(i + 8)) bad = true;
                 hq[u % 4] = lds128h(sm + fst * P::PLANE + soff);
                 uint4 yu[R], yd[R];  // staged rows y +- d of the centre plane
 #pragma unroll
@@ -274,6 +374,7 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                     yu[d - 1] = lds128h(pc + d * P::SX);
                     yd[d - 1] = lds128h(pc - d * P::SX);
                 }
+                release_plane(i + 4);  // the centre plane's last reads
                 // lap = [c (cx+cy+cz) + sum_r (ax_r sx_r + ay_r sy_r)] + sum_r az_r sz_r,
                 // pair sums s = p[+r] + p[-r]; up operands of y and z enter FP16.
                 float2 lap[4];
@@ -307,21 +408,33 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
 #pragma unroll
                 for (int h = 0; h < 4; ++h) dq[u % 4][h] = cv[h];
 
-                if (!mbar_wait(&auxf[u % AUX], apar ^ ((u / AUX) & 1u))) bad = true;
-                const uint16_t* st = aux + (u % AUX) * 2 * P::TILE + aoff;
+                if (!wait_aux(i)) bad = true;
+                const uint16_t* st = aux + ((ab + i) % AUX) * 2 * P::TILE + aoff;
                 const uint4 qv = lds128h(st);
                 const uint4 kv = lds128h(st + P::TILE);
+                release_aux(i);
+                // o holds p_next (PHASE 2) or, in the other phases, -p_next
+                // before the PHASE 1 rescale: u = K lap + 2c (2c is exact), then
+                // the mixed subtract q - u converts p_prev on the way; the sign
+                // is restored by the rescale factor -m_out (PHASE 1) or by the
+                // sign bits of the packed halves (PHASE 0).
+                constexpr bool kNeg = PHASE == 0;
                 float o[8];
 #pragma unroll
                 for (int h = 0; h < 4; ++h) {
                     const float2 c = cv[h];
-                    const float2 pq = h2f2(get_word(qv, h));
                     const uint32_t kw = get_word(kv, h);
                     const float2 kk = make_float2(__uint_as_float(kw << 16),
                                                   __uint_as_float(kw & 0xffff0000u));
-                    // 2c - m_q pq in one rounding (2c is exact), then + K lap
-                    float2 ov = fma2(kk, lap[h], fma2(nmq2, pq, add2(c, c)));
-                    if (PHASE == 1) ov = mul2(ov, mout2);
+                    float2 ov;
+                    if (PHASE == 2) {
+                        // 2c - m_q pq in one rounding, then + K lap
+                        const float2 pq = h2f2(get_word(qv, h));
+                        ov = fma2(kk, lap[h], fma2(nmq2, pq, add2(c, c)));
+                    } else {
+                        ov = subhf2(get_word(qv, h), fma2(kk, lap[h], add2(c, c)));
+                        if (PHASE == 1) ov = mul2(ov, nmout2);
+                    }
                     o[2 * h] = ov.x;
                     o[2 * h + 1] = ov.y;
                 }
@@ -335,10 +448,10 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
 #pragma unroll
                         for (int e = 0; e < 8; ++e)
                             if (e == src_e) {
-                                o[e] += add;
+                                o[e] = kNeg ? o[e] - add : o[e] + add;
                                 if (a.trace)
                                     a.trace[(a.src_step ? *a.src_step : 0) + a.src_off] =
-                                        __half2float(__float2half_rn(o[e])) / sa;
+                                        __half2float(__float2half_rn(kNeg ? -o[e] : o[e])) / sa;
                             }
                     }
                 }
@@ -349,6 +462,12 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                     pk.y = pack_h2(o[2], o[3]);
                     pk.z = pack_h2(o[4], o[5]);
                     pk.w = pack_h2(o[6], o[7]);
+                    if (kNeg) {  // -(-p_next): flip the sign bits (exact)
+                        pk.x ^= 0x80008000u;
+                        pk.y ^= 0x80008000u;
+                        pk.z ^= 0x80008000u;
+                        pk.w ^= 0x80008000u;
+                    }
                     if (xfull)
                         stg_stream_u4(dst, pk);
                     else if (gx < R)  // x = 4..7 of the first chunk
@@ -357,40 +476,36 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                         stg_stream_u2(dst, make_uint2(pk.x, pk.y));
                 }
                 goff += a.sz;
-                abort_run = __syncthreads_or(bad) != 0;
-                if (!abort_run && tid == 0) {
-                    if (i + 4 + S < nplanes) issue_plane(i + 4 + S);  // the centre's stage
-                    if (i + AUX < nint) issue_aux(i + AUX);
-                }
+                if (bad) *reinterpret_cast<volatile int*>(&hs->abort) = 1;
+                abort_run = *reinterpret_cast<volatile int*>(&hs->abort) != 0;
             }
         }
     }
 
-    if (abort_run && tid == 0) {
-        record_error(a.err, kDevWaitTimeout);
-        for (int jj = max(0, issued_hi - S + 1); jj <= issued_hi; ++jj)
-            (void)mbar_wait(&full[jj % S], (jj / S) & 1);
-        for (int it = max(0, aux_issued_hi - AUX + 1); it <= aux_issued_hi; ++it)
-            (void)mbar_wait(&auxf[it % AUX], (it / AUX) & 1);
+    __syncthreads();  // every warp has left the plane loop
+    if (hs->abort != 0) {
+        if (tid == 0) {
+            record_error(a.err, kDevWaitTimeout);
+            // Let every copy still in flight land before the shared memory is
+            // released or reused (a stage has at most one fill outstanding).
+            const int ip = hs->issued_p, ia = hs->issued_a;
+            for (int jj = max(0, ip - S + 1); jj <= ip; ++jj) (void)wait_plane(jj);
+            for (int it = max(0, ia - AUX + 1); it <= ia; ++it) (void)wait_aux(it);
+        }
+        return false;
     }
-    return !abort_run;
+    ring.p = pb + nplanes;
+    ring.aux = ab + nint;
+    return true;
 }
 
-// (Re)initialises the CTA's ring barriers (thread 0); the caller synchronises.
-// A barrier is invalidated before it is initialised again: by then every copy
-// that completed on it has been waited for.
+// Initialises the CTA's ring barriers (thread 0); the caller synchronises.
 template <int S, int AUX>
-__device__ __forceinline__ void init_rings_f16(uint64_t* full, uint64_t* auxf, bool again) {
+__device__ __forceinline__ void init_rings_f16(uint64_t* full, uint64_t* auxf) {
 #pragma unroll
-    for (int s = 0; s < S; ++s) {
-        if (again) mbar_inval(&full[s]);
-        mbar_init(&full[s], 1);
-    }
+    for (int s = 0; s < S; ++s) mbar_init(&full[s], 1);
 #pragma unroll
-    for (int s = 0; s < AUX; ++s) {
-        if (again) mbar_inval(&auxf[s]);
-        mbar_init(&auxf[s], 1);
-    }
+    for (int s = 0; s < AUX; ++s) mbar_init(&auxf[s], 1);
     fence_barrier_init();
 }
 
@@ -404,22 +519,27 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
     extern __shared__ unsigned char dsmem[];
     __shared__ __align__(8) uint64_t full[S];
     __shared__ __align__(8) uint64_t auxf[AUX];
+    __shared__ HandoffH<S, AUX> hs;
     uint16_t* sm = reinterpret_cast<uint16_t*>(smem_align<128>(dsmem));
-    if (threadIdx.x == 0) init_rings_f16<S, AUX>(full, auxf, false);
+    if (threadIdx.x == 0) {
+        init_rings_f16<S, AUX>(full, auxf);
+        init_handoff(&hs);
+    }
     __syncthreads();
     int b = blockIdx.x;
     const int tx = b % a.tiles_x;
     b /= a.tiles_x;
     const int ty = b % a.tiles_y;
     b /= a.tiles_y;
+    RingH ring;
     (void)pencil_f16_tile<TX, TY, S, AUX, PHASE, UNR>(&pmap, &qmap, &kmap, a, tx, ty, b, sm, full,
-                                                      auxf);
+                                                      auxf, ring, &hs);
 }
 
 // Many grids (shots) in one persistent launch, as batch_f32_kernel: CTAs take
 // (shot, tile x, tile y, z chunk) items from the queue; the rings' barriers are
-// re-initialised for every item; the last CTA to finish resets the queue and
-// advances the step counter the sources read.
+// initialised once and their phases carried from item to item; the last CTA to
+// finish resets the queue and advances the step counter the sources read.
 template <int TX, int TY, int S, int AUX, int PHASE, int UNR>
 __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, AUX>::MINB)
     batch_f16_kernel(const ShotF16* __restrict__ shots, const int4* __restrict__ items,
@@ -428,14 +548,15 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
     __shared__ __align__(8) uint64_t full[S];
     __shared__ __align__(8) uint64_t auxf[AUX];
     __shared__ int s_item;
+    __shared__ HandoffH<S, AUX> hs;
     uint16_t* sm = reinterpret_cast<uint16_t*>(smem_align<128>(dsmem));
-    bool first = true;
+    if (threadIdx.x == 0) {
+        init_rings_f16<S, AUX>(full, auxf);
+        init_handoff(&hs);
+    }
+    RingH ring;
     for (;;) {
-        if (threadIdx.x == 0) {
-            s_item = atomicAdd(&queue->next, 1);
-            init_rings_f16<S, AUX>(full, auxf, !first);
-        }
-        first = false;
+        if (threadIdx.x == 0) s_item = atomicAdd(&queue->next, 1);
         __syncthreads();
         const int it = s_item;
         __syncthreads();  // every thread has read s_item before it is replaced
@@ -444,7 +565,7 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
         const ShotF16* sh = shots + w.x;
         const F16Args a = sh->args;
         if (!pencil_f16_tile<TX, TY, S, AUX, PHASE, UNR>(&sh->p, &sh->prev, &sh->k, a, w.y, w.z,
-                                                         w.w, sm, full, auxf))
+                                                         w.w, sm, full, auxf, ring, &hs))
             break;
     }
     if (threadIdx.x == 0) {
@@ -527,6 +648,8 @@ const VariantH kF16[] = {
     SB200_VARIANT_H(64, 16, 8, 4, 8, "h64x16_s8_a4_u8"),
     SB200_VARIANT_H(64, 32, 8, 4, 8, "h64x32_s8_a4_u8"),
     SB200_VARIANT_H(128, 16, 8, 4, 8, "h128x16_s8_a4_u8"),
+    SB200_VARIANT_H(64, 16, 12, 4, 4, "h64x16_s12_a4"),
+    SB200_VARIANT_H(64, 32, 12, 4, 4, "h64x32_s12_a4"),
 };
 constexpr int kNumF16 = sizeof(kF16) / sizeof(kF16[0]);
 

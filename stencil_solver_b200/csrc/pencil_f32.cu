@@ -21,9 +21,16 @@
 //     leapfrog: each element of p_prev is read once, before its own update).
 // Arithmetic per point: each axis' centre term is cancelled against its r = 1 pair
 // in one FMA and the axes are combined as (x + y) + z, which keeps the rounding
-// close to the reference's per-axis evaluation.
+// close to the reference's per-axis evaluation.  Heat takes u + lap in two FMA
+// chains whose sum meets the centre in one FMA with weight 1 + (cx + cy + cz).
+// Modes: acoustic (the leapfrog step), heat (u + alpha dt lap u) and prepass,
+// the first half of the coarse step with the two-step composition term
+// (sb200_wave_prepass_f32): r = p + beta dt^2 v^2 lap p into `next`, and
+// p_prev + 2 beta dt^2 v^2 lap p written over p_prev, so that the plain step of
+// (r, p_prev) is 2p - p_prev + dt^2 L p + beta dt^4 L^2 p (L = v^2 lap).
 // Algorithmic DRAM traffic: acoustic 16 B / interior point (read p, p_prev, vel2;
-// write p_next), heat 8 B (read u, write u_next).
+// write p_next), heat 8 B (read u, write u_next), prepass 20 B (read p, p_prev,
+// vel2; write r, p_prev).
 #include <algorithm>
 #include <mutex>
 
@@ -34,6 +41,8 @@
 namespace sb200 {
 
 namespace {
+
+enum Mode : int { kModeAcoustic = 0, kModeHeat = 1, kModePrepass = 2 };
 
 template <int TX, int TY, int RPT, int S, int AUX>
 struct Shape {
@@ -66,12 +75,14 @@ struct Ring {
 // z chunk zc.  All threads of the CTA call it; `sm`, `full` and `auxf` are the
 // CTA's rings, initialised by the caller.  Returns false when a bounded wait gave
 // up: the error is recorded and every copy in flight has landed.
-template <int TX, int TY, int RPT, int S, int AUX, bool HEAT>
+template <int TX, int TY, int RPT, int S, int AUX, int MODE>
 __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUtensorMap* qmap,
                                             const CUtensorMap* vmap, const PencilArgs& a,
                                             int tile_x, int tile_y, int zc, float* sm,
                                             uint64_t* full, uint64_t* auxf, Ring& ring) {
     using P = Shape<TX, TY, RPT, S, AUX>;
+    constexpr bool HEAT = MODE == kModeHeat;
+    constexpr bool PRE = MODE == kModePrepass;
     constexpr bool kAuxTma = !HEAT && AUX > 0;
     constexpr int NAUX = AUX > 0 ? AUX : 1;
     float* aux = sm + S * P::PLANE;  // AUX stages of [p_prev tile | vel2 tile]
@@ -135,7 +146,7 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
 
     // Source ownership: which (row, lane element) of this thread, if any.
     int src_j = -1, src_i = -1;
-    if (!HEAT && a.src_z >= 0 && a.src_x >= gx && a.src_x < gx + 4 && a.src_y >= gy &&
+    if (MODE == kModeAcoustic && a.src_z >= 0 && a.src_x >= gx && a.src_x < gx + 4 && a.src_y >= gy &&
         a.src_y < gy + RPT && xin) {
         src_j = a.src_y - gy;
         src_i = a.src_x - gx;
@@ -149,6 +160,7 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
         az2[r] = dup2(a.w.az[r]);
     }
     const float2 cx2 = dup2(a.w.cx), cy2 = dup2(a.w.cy), cz2 = dup2(a.w.cz), neg1 = dup2(-1.f);
+    const float2 hc2 = dup2(a.heat_c);
 
     float4 q[9][RPT];
     bool bad = false;
@@ -215,6 +227,11 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
                         }
                     }
                 }
+                // Acoustic / prepass: lap per axis (centre cancelled against the
+                // r = 1 pair first), combined as (x + y) + z.  Heat: u + lap in two
+                // chains -- the y rows plus the x pairs, and the z pairs -- whose
+                // sum takes the centre through one FMA with heat_c, so `lap` holds
+                // the new value itself.
                 float2 lap[RPT][2];
 #pragma unroll
                 for (int j = 0; j < RPT; ++j) {
@@ -226,20 +243,36 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
                         const float2 ce = pair_of(c, h);
-                        float2 tz = mul2(cz2, ce);
-                        float2 tx = mul2(cx2, ce);
+                        const int e = 4 + 2 * h;  // window index of the pair's first lane
+                        if (HEAT) {
+                            float2 txy = ya[j][h];
+                            float2 tz = make_float2(0.f, 0.f);
 #pragma unroll
-                        for (int r = 1; r <= R; ++r) {
-                            const float2 up = pair_of(q[(u + 4 + r) % 9][j], h);
-                            const float2 dn = pair_of(q[(u + 4 - r + 9) % 9][j], h);
-                            tz = fma2(az2[r - 1], add2(up, dn), tz);
-                            const int e = 4 + 2 * h;  // window index of the pair's first lane
-                            const float2 s = make_float2(win[e + r] + win[e - r],
-                                                         win[e + 1 + r] + win[e + 1 - r]);
-                            tx = fma2(ax2[r - 1], s, tx);
+                            for (int r = 1; r <= R; ++r) {
+                                const float2 up = pair_of(q[(u + 4 + r) % 9][j], h);
+                                const float2 dn = pair_of(q[(u + 4 - r + 9) % 9][j], h);
+                                tz = r == 1 ? mul2(az2[0], add2(up, dn))
+                                            : fma2(az2[r - 1], add2(up, dn), tz);
+                                const float2 s = make_float2(win[e + r] + win[e - r],
+                                                             win[e + 1 + r] + win[e + 1 - r]);
+                                txy = fma2(ax2[r - 1], s, txy);
+                            }
+                            lap[j][h] = fma2(hc2, ce, add2(txy, tz));
+                        } else {
+                            float2 tz = mul2(cz2, ce);
+                            float2 tx = mul2(cx2, ce);
+#pragma unroll
+                            for (int r = 1; r <= R; ++r) {
+                                const float2 up = pair_of(q[(u + 4 + r) % 9][j], h);
+                                const float2 dn = pair_of(q[(u + 4 - r + 9) % 9][j], h);
+                                tz = fma2(az2[r - 1], add2(up, dn), tz);
+                                const float2 s = make_float2(win[e + r] + win[e - r],
+                                                             win[e + 1 + r] + win[e + 1 - r]);
+                                tx = fma2(ax2[r - 1], s, tx);
+                            }
+                            const float2 ty = fma2(cy2, ce, ya[j][h]);
+                            lap[j][h] = add2(add2(tx, ty), tz);
                         }
-                        const float2 ty = fma2(cy2, ce, ya[j][h]);
-                        lap[j][h] = add2(add2(tx, ty), tz);
                     }
                 }
                 if (kAuxTma) {
@@ -258,9 +291,18 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
                     const float4 c = q[cs][j];
                     float4 o;
                     if (HEAT) {
-                        const float2 o0 = add2(pair_of(c, 0), lap[j][0]);
-                        const float2 o1 = add2(pair_of(c, 1), lap[j][1]);
-                        o = make_float4(o0.x, o0.y, o1.x, o1.y);
+                        o = make_float4(lap[j][0].x, lap[j][0].y, lap[j][1].x, lap[j][1].y);
+                    } else if (PRE) {
+                        // weights carry beta dt^2: r = c + vv lap, p_prev += 2 vv lap
+                        const float2 v0 = pair_of(vv[j], 0), v1 = pair_of(vv[j], 1);
+                        const float2 r0 = fma2(v0, lap[j][0], pair_of(c, 0));
+                        const float2 r1 = fma2(v1, lap[j][1], pair_of(c, 1));
+                        const float2 q0 = fma2(add2(v0, v0), lap[j][0], pair_of(pv[j], 0));
+                        const float2 q1 = fma2(add2(v1, v1), lap[j][1], pair_of(pv[j], 1));
+                        o = make_float4(r0.x, r0.y, r1.x, r1.y);
+                        if (rin[j])
+                            stg_stream(a.prev_out + goff + j * a.sy,
+                                       make_float4(q0.x, q0.y, q1.x, q1.y));
                     } else {
                         // fmaf(vv, lap, fmaf(2, c, -pv)): 2c - pv is rounded once (2c is
                         // exact), as fma(-1, pv, c + c)
@@ -334,7 +376,7 @@ __device__ __forceinline__ float* setup_rings(unsigned char* dsmem, uint64_t* fu
 
 // One grid: CTA b owns tile (b % tiles_x, (b / tiles_x) % tiles_y) and z chunk
 // b / (tiles_x * tiles_y).
-template <int TX, int TY, int RPT, int S, int AUX, bool HEAT>
+template <int TX, int TY, int RPT, int S, int AUX, int MODE>
 __global__ void __launch_bounds__(Shape<TX, TY, RPT, S, AUX>::NT, Shape<TX, TY, RPT, S, AUX>::MINB)
     pencil_f32_kernel(const __grid_constant__ CUtensorMap pmap,
                       const __grid_constant__ CUtensorMap qmap,
@@ -350,7 +392,7 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S, AUX>::NT, Shape<TX, TY, 
     const int ty = b % a.tiles_y;
     b /= a.tiles_y;
     Ring ring;
-    (void)pencil_tile<TX, TY, RPT, S, AUX, HEAT>(&pmap, &qmap, &vmap, a, tx, ty, b, sm, full,
+    (void)pencil_tile<TX, TY, RPT, S, AUX, MODE>(&pmap, &qmap, &vmap, a, tx, ty, b, sm, full,
                                                  auxf, ring);
 }
 
@@ -379,7 +421,7 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S, AUX>::NT, Shape<TX, TY, 
         const int4 w = items[it];
         const ShotF32* sh = shots + w.x;
         const PencilArgs a = sh->args;
-        if (!pencil_tile<TX, TY, RPT, S, AUX, false>(&sh->p, &sh->prev, &sh->vel2, a, w.y, w.z,
+        if (!pencil_tile<TX, TY, RPT, S, AUX, kModeAcoustic>(&sh->p, &sh->prev, &sh->vel2, a, w.y, w.z,
                                                      w.w, sm, full, auxf, ring))
             break;
     }
@@ -401,14 +443,14 @@ using ResidentFn = int (*)();
 
 // CTAs of a variant that fit on one SM: the occupancy calculator when a device
 // is present, else the shared-memory / register limits computed here.
-template <int TX, int TY, int RPT, int S, int AUX, bool HEAT>
+template <int TX, int TY, int RPT, int S, int AUX, int MODE>
 int resident_variant() {
     using P = Shape<TX, TY, RPT, S, AUX>;
     static int cached[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (cached[dev & 63] > 0) return cached[dev & 63];
-    auto kern = pencil_f32_kernel<TX, TY, RPT, S, AUX, HEAT>;
+    auto kern = pencil_f32_kernel<TX, TY, RPT, S, AUX, MODE>;
     int n = 0;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(P::SMEM)) == cudaSuccess &&
@@ -423,13 +465,13 @@ int resident_variant() {
     return std::max(1, std::min(by_smem, by_regs));
 }
 
-template <int TX, int TY, int RPT, int S, int AUX, bool HEAT>
+template <int TX, int TY, int RPT, int S, int AUX, int MODE>
 cudaError_t launch_variant(const PencilMaps& m, const PencilArgs& a, unsigned ctas,
                            cudaStream_t stream) {
     using P = Shape<TX, TY, RPT, S, AUX>;
     // Sets the shared-memory attribute on the first call per device (cached).
-    resident_variant<TX, TY, RPT, S, AUX, HEAT>();
-    pencil_f32_kernel<TX, TY, RPT, S, AUX, HEAT><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
+    resident_variant<TX, TY, RPT, S, AUX, MODE>();
+    pencil_f32_kernel<TX, TY, RPT, S, AUX, MODE><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
                                                                                  m.vel2, a);
     return cudaGetLastError();
 }
@@ -439,12 +481,15 @@ struct Variant {
     const char* name;
     LaunchFn launch;
     ResidentFn resident;
+    LaunchFn launch_prepass;  // acoustic tiles only: the same shape in prepass mode
 };
 
-#define SB200_VARIANT(TX, TY, RPT, S, AUX, HEAT, NAME)                              \
-    Variant {                                                                       \
-        TX, TY, RPT, S, AUX, NAME, &launch_variant<TX, TY, RPT, S, AUX, HEAT>,     \
-            &resident_variant<TX, TY, RPT, S, AUX, HEAT>                           \
+#define SB200_VARIANT(TX, TY, RPT, S, AUX, HEAT, NAME)                                       \
+    Variant {                                                                                \
+        TX, TY, RPT, S, AUX, NAME,                                                           \
+            &launch_variant<TX, TY, RPT, S, AUX, HEAT ? kModeHeat : kModeAcoustic>,          \
+            &resident_variant<TX, TY, RPT, S, AUX, HEAT ? kModeHeat : kModeAcoustic>,        \
+            HEAT ? nullptr : &launch_variant<TX, TY, RPT, S, AUX, kModePrepass>              \
     }
 
 // Index 0 of each table is the default when no tuned choice exists.
@@ -463,6 +508,10 @@ const Variant kHeat[] = {
     SB200_VARIANT(32, 16, 1, 8, 0, true, "t32x16_r1_s8"),
     SB200_VARIANT(64, 32, 2, 8, 0, true, "t64x32_r2_s8"),
     SB200_VARIANT(32, 64, 2, 8, 0, true, "t32x64_r2_s8"),
+    SB200_VARIANT(64, 24, 2, 8, 0, true, "t64x24_r2_s8"),
+    SB200_VARIANT(128, 16, 2, 8, 0, true, "t128x16_r2_s8"),
+    SB200_VARIANT(64, 8, 2, 8, 0, true, "t64x8_r2_s8"),
+    SB200_VARIANT(64, 16, 2, 12, 0, true, "t64x16_r2_s12"),
 };
 constexpr int kNumWave = sizeof(kWave) / sizeof(kWave[0]);
 constexpr int kNumHeat = sizeof(kHeat) / sizeof(kHeat[0]);
@@ -564,6 +613,20 @@ cudaError_t launch_wave_pencil_f32(const PencilMaps& maps, const float* prev, co
     return v.launch(maps, a, ctas_of(a, g), stream);
 }
 
+cudaError_t launch_prepass_pencil_f32(const PencilMaps& maps, float* prev, const float* vel2,
+                                      float* r, const GridDesc& g, float beta,
+                                      const PencilConfig& cfg, int* err, cudaStream_t stream) {
+    if (!g.has_interior()) return cudaSuccess;
+    const Variant& v = kWave[cfg.variant];
+    PencilArgs a = base_args(v.tx, v.ty, g, cfg.zchunks, err);
+    a.prev = prev;
+    a.prev_out = prev;
+    a.vel2 = vel2;
+    a.next = r;
+    a.w = fold_weights(g, beta * g.dt * g.dt);
+    return v.launch_prepass(maps, a, ctas_of(a, g), stream);
+}
+
 cudaError_t launch_heat_pencil_f32(const PencilMaps& maps, float* u_next, const GridDesc& g,
                                    float alpha_dt, const PencilConfig& cfg, int* err,
                                    cudaStream_t stream) {
@@ -572,6 +635,10 @@ cudaError_t launch_heat_pencil_f32(const PencilMaps& maps, float* u_next, const 
     PencilArgs a = base_args(v.tx, v.ty, g, cfg.zchunks, err);
     a.next = u_next;
     a.w = fold_weights(g, alpha_dt);
+    a.heat_c = static_cast<float>(
+        1.0 + double(C0) * alpha_dt *
+                  (1.0 / (double(g.dx) * g.dx) + 1.0 / (double(g.dy) * g.dy) +
+                   1.0 / (double(g.dz) * g.dz)));
     return v.launch(maps, a, ctas_of(a, g), stream);
 }
 

@@ -48,7 +48,8 @@ from typing import NamedTuple
 
 import numpy as np
 
-from . import Grid, Mlp, _check, add_box, lib, mlp_samples, restrict2, smooth3, wave_step
+from . import (Grid, Mlp, _check, add_box, lib, mlp_samples, restrict2, smooth3, wave_prepass,
+               wave_step)
 
 OFFSET = -4  # coarse cell i <-> fine cell 2 i + OFFSET
 # Correction floor of a trained network (Mlp.min_scale).  A Problem's source is
@@ -117,6 +118,7 @@ class Problem:
     corr_cells: float = 20.0
     vel2_window: object = None  # device fine model to use instead of generating one
     compose_source: bool = True  # the coarse source's h^4 L S term (see the module doc)
+    compose_state: bool = False  # the coarse step's h^4 L^2 p term (coarse_step)
 
     def __post_init__(self):
         if self.src_c is None:
@@ -279,30 +281,60 @@ def fine_solve(pb: Problem, vf, steps: int, on_even=None):
 
 
 def coarse_step(pb: Problem, vc, p, q, src, w, m, mlp: Mlp | None = None,
-                fused: bool = True, flags=None) -> None:
+                fused: bool = True, flags=None, r=None):
     """One coarse step from level m (p) over level m-1 (q, overwritten with m+1):
     the acoustic step, the learned correction (mlp given; one fused launch unless
     fused is False), then the source.  flags = (flags of p, flags for q): the
     fused step's activity flags (chunks far from any value at the correction
-    floor skip the network; the source box counts as active)."""
+    floor skip the network; the source box counts as active); with
+    pb.compose_state a third buffer, the scratch for the flags of r.
+
+    With pb.compose_state the step first runs the pre-pass
+    (sb200_wave_prepass_f32, beta = 1/16) into the scratch field r (zero halo):
+    r = p + (dt^2 / 16) L p and q += (dt^2 / 8) L p, and then steps (r, q), which
+    adds the composition term h^4 L^2 p of two fine steps (h = dt / 2).  The
+    network then sees the stars of r.  Returns the field that was stepped."""
     g = pb.coarse
+    cur = p
+    box = None if flags is None else src.box()
+    if pb.compose_state:
+        if r is None:
+            raise ValueError("coarse_step: compose_state needs the scratch field r")
+        wave_prepass(p, q, vc, r, g, 1.0 / 16.0)
+        cur = r
+        if flags is not None and mlp is not None and fused:
+            # flags = (flags of p, flags for q, scratch for the flags of r)
+            mlp.flags_compose(g, flags[0], flags[2])
+            flags = (flags[2], flags[1])
+            box = tuple(b + (4 if k % 2 else -4) for k, b in enumerate(box))
     if mlp is None:
-        wave_step(p, q, vc, q, g)
+        wave_step(cur, q, vc, q, g)
     elif fused:
-        mlp.learned_step(p, q, vc, g, flags=flags, box=None if flags is None else src.box())
+        mlp.learned_step(cur, q, vc, g, flags=flags, box=box)
     else:
-        wave_step(p, q, vc, q, g)
-        mlp.correct(p, vc, q, g)
+        wave_step(cur, q, vc, q, g)
+        mlp.correct(cur, vc, q, g)
     _inject(pb, False, q, src, w, m)
+    return cur
 
 
-def new_flags(mlp: Mlp, g: Grid):
-    """A pair of activity-flag buffers for the fused step on g, every bit set
-    (every chunk and face active)."""
+def new_flags(mlp: Mlp, g: Grid, compose: bool = False):
+    """Activity-flag buffers for the fused step on g, every bit set (every chunk
+    and face active): the pair that alternates between p and q, and with
+    `compose` a third, the scratch for the flags of the pre-pass field r."""
     torch = _torch()
     n = mlp.flags_bytes(g)
-    return [torch.full((n,), 255, dtype=torch.uint8, device="cuda"),
-            torch.full((n,), 255, dtype=torch.uint8, device="cuda")]
+    return [torch.full((n,), 255, dtype=torch.uint8, device="cuda")
+            for _ in range(3 if compose else 2)]
+
+
+def _flag_args(fl):
+    return None if fl is None else tuple(fl)
+
+
+def _rotate(fl):
+    if fl is not None:
+        fl[0], fl[1] = fl[1], fl[0]
 
 
 def coarse_solve(pb: Problem, vc, steps: int, mlp: Mlp | None = None, use_flags: bool = True):
@@ -312,14 +344,14 @@ def coarse_solve(pb: Problem, vc, steps: int, mlp: Mlp | None = None, use_flags:
     g = pb.coarse
     p = torch.zeros(g.shape, device="cuda")
     q = torch.zeros(g.shape, device="cuda")
+    r = torch.zeros(g.shape, device="cuda") if pb.compose_state else None
     w = pb.wavelet(False, steps)
     src = pb.source(False)
-    fl = new_flags(mlp, g) if mlp is not None and use_flags else None
+    fl = new_flags(mlp, g, pb.compose_state) if mlp is not None and use_flags else None
     for m in range(steps):
-        coarse_step(pb, vc, p, q, src, w, m, mlp, flags=None if fl is None else (fl[0], fl[1]))
+        coarse_step(pb, vc, p, q, src, w, m, mlp, flags=_flag_args(fl), r=r)
         p, q = q, p
-        if fl is not None:
-            fl.reverse()
+        _rotate(fl)
     return p
 
 
@@ -357,6 +389,7 @@ def make_pairs(problems, fine_steps: int, samples_per_pair: int = 4096, every: i
         src_c = pb.source(False)
         ring = {}
         plain = torch.empty(gc.shape, device="cuda")
+        rbuf = torch.zeros(gc.shape, device="cuda") if pb.compose_state else None
         nz, ny, nx = gc.shape
         box = torch.zeros(gc.shape, dtype=torch.bool, device="cuda")
         box[wall:nz - wall, wall:ny - wall, wall:nx - wall] = True
@@ -376,8 +409,8 @@ def make_pairs(problems, fine_steps: int, samples_per_pair: int = 4096, every: i
             if m >= max(first, 2) and (m - first) % every == 0:
                 cm2, cm1, cm = ring[m - 2], ring[m - 1], ring[m]
                 plain.copy_(cm2)  # in-place leapfrog writes over the older level
-                coarse_step(pb, vc, cm1, plain, src_c, w_c, m - 1)
-                sample_rows(cm1, cm, m)
+                stepped = coarse_step(pb, vc, cm1, plain, src_c, w_c, m - 1, r=rbuf)
+                sample_rows(stepped, cm, m)
 
         def sample_rows(state, target, m):
             """Rows at random cells of `state` (level m - 1); `plain` holds its plain step."""
@@ -478,7 +511,8 @@ def proxy_of(pb: Problem, nc_proxy: int = 64) -> Problem:
     win = vf[z0:z0 + nfp, y0:y0 + nfp, x0:x0 + nfp].contiguous()
     src = (pb.src_c[0] - x0 // 2, pb.src_c[1] - y0 // 2, pb.src_c[2] - z0 // 2)
     return Problem(nc_proxy, pb.h, pb.dt, pb.seed, freq=pb.freq, src_c=src,
-                   sigma_cells=pb.sigma_cells, vel2_window=win, compose_source=pb.compose_source)
+                   sigma_cells=pb.sigma_cells, vel2_window=win, compose_source=pb.compose_source,
+                   compose_state=pb.compose_state)
 
 
 @dataclass
@@ -515,19 +549,21 @@ def learned_solve(pb: Problem, coarse_steps: int, mlp: Mlp, bound: float = 1e-3,
     fp = torch.zeros(gpf.shape, device="cuda")
     fq = torch.zeros(gpf.shape, device="cuda")
     judge = torch.empty(gp.shape, device="cuda")
+    r = torch.zeros(g.shape, device="cuda") if pb.compose_state else None
+    pr = torch.zeros(gp.shape, device="cuda") if pb.compose_state else None
     w = pb.wavelet(False, coarse_steps)
     wp = px.wavelet(False, coarse_steps)
     wf = px.wavelet(True, 2 * coarse_steps)
     src, psrc, pfsrc = pb.source(False), px.source(False), px.source(True)
-    fl, pfl = new_flags(mlp, g), new_flags(mlp, gp)
+    fl, pfl = new_flags(mlp, g, pb.compose_state), new_flags(mlp, gp, pb.compose_state)
     checks, fallback = [], None
     for m in range(coarse_steps):
-        coarse_step(pb, vc, p, q, src, w, m, mlp, flags=(fl[0], fl[1]))
+        coarse_step(pb, vc, p, q, src, w, m, mlp, flags=_flag_args(fl), r=r)
         p, q = q, p
-        fl.reverse()
-        coarse_step(px, pvc, pp, pq, psrc, wp, m, mlp, flags=(pfl[0], pfl[1]))
+        _rotate(fl)
+        coarse_step(px, pvc, pp, pq, psrc, wp, m, mlp, flags=_flag_args(pfl), r=pr)
         pp, pq = pq, pp
-        pfl.reverse()
+        _rotate(pfl)
         for k in (2 * m, 2 * m + 1):
             wave_step(fp, fq, pvf, fq, gpf)
             _inject(px, True, fq, pfsrc, wf, k)

@@ -382,3 +382,53 @@ def test_learned_step_flags_keep_the_bits(torch_cuda, floor):
                 assert torch.equal(a, b), (k, float((a - b).abs().max()))
         assert idle > 0 and active > 0, (idle, active)
         assert not torch.equal(states["ref"][0], dev(torch, p0))
+
+
+def test_composed_flags_keep_the_bits(torch_cuda):
+    """The composition pre-pass (r = p + c L p, p_prev += 2 c L p) followed by the
+    fused step on r: with the flags of r composed from those of p
+    (sb200_mlp_flags_compose) and the source box grown by the stencil radius, 14
+    steps of a sparse field with a source box give the same bits as the same
+    steps without flags, and some chunks take the plain path."""
+    torch = torch_cuda
+    nz, ny, nx = 100, 64, 96
+    rng = np.random.default_rng(37)
+    p0 = np.zeros((nz, ny, nx), np.float32)
+    p0[10:18, 8:14, 10:20] = rng.standard_normal((8, 6, 10))
+    v2 = rng.uniform(1500, 4500, (nz, ny, nx)).astype(np.float32) ** 2
+    g = sb.Grid(nx, ny, nz, 10.0, 10.0, 10.0, 8e-4)
+    w, _, _ = net_and_rows(15, 1)
+    origin, dims = (60, 40, 70), (5, 4, 3)
+    pat = torch.from_numpy(rng.uniform(0.5, 1.0, dims[::-1]).astype(np.float32)).cuda()
+    box = (origin[0] - 4, origin[0] + dims[0] + 4, origin[1] - 4, origin[1] + dims[1] + 4,
+           origin[2] - 4, origin[2] + dims[2] + 4)
+    V = dev(torch, v2)
+    with sb.Mlp() as m:
+        m.set_params(w)
+        m.output_scale = 0.3
+        m.min_scale = 2.0 ** -20
+        m.set_kernel("tcgen05")
+        n = m.flags_bytes(g)
+        states = {k: [dev(torch, p0), dev(torch, p0)] for k in ("plain", "flags")}
+        r = {k: torch.zeros_like(states[k][0]) for k in states}
+        fl = [torch.full((n,), 255, dtype=torch.uint8, device="cuda"),
+              torch.zeros(n, dtype=torch.uint8, device="cuda"),
+              torch.zeros(n, dtype=torch.uint8, device="cuda")]
+        idle = 0
+        for step in range(14):
+            for k, (p, q) in states.items():
+                sb.wave_prepass(p, q, V, r[k], g, 1.0 / 16.0)
+                if k == "plain":
+                    m.learned_step(r[k], q, V, g)
+                else:
+                    m.flags_compose(g, fl[0], fl[2])
+                    idle += int((fl[2].cpu().numpy() == 0).sum())
+                    m.learned_step(r[k], q, V, g, flags=(fl[2], fl[1]), box=box)
+                sb.add_box(q, g, origin, dims, pat, 0.25 * (step % 3 + 1))
+                states[k] = [q, p]
+            fl[0], fl[1] = fl[1], fl[0]
+        torch.cuda.synchronize()
+        for a, b in zip(states["flags"], states["plain"]):
+            assert torch.equal(a, b), float((a - b).abs().max())
+        assert idle > 0
+        assert sb.device_error() == 0
