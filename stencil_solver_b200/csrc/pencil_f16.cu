@@ -153,10 +153,15 @@ __device__ __forceinline__ float xsum1(const float (&c)[8], uint2 lf, uint2 rt, 
 
 // Shared-memory hand-off of ring stages between the warps of a CTA, in place of
 // a CTA barrier per plane: a warp that has read the last it needs of a stage
-// counts itself done (acquire-release atomic), and the warp that completes the
-// count refills the stage by TMA.  No warp waits for another; a warp at plane
-// iteration k needs only refills released at iterations <= k - 4, which every
-// warp, the slowest included, has passed.
+// counts itself done (a shared-memory atomic after __syncwarp), and the warp that
+// completes the count refills the stage by TMA.  No warp waits for another; a
+// warp at plane iteration k needs only refills released at iterations <= k - 4,
+// which every warp, the slowest included, has passed.  The count is a relaxed
+// atomic: an acquire-release one also orders the warp's outstanding global
+// stores (a fence per plane that waited on DRAM writes: 2.24 ms per 1024^3 step
+// against 1.62), while the stage reads it must follow are shared-memory loads,
+// which the shared-memory pipe completes in issue order before the warp's later
+// atomic on the counter.
 template <int S, int AUX>
 struct HandoffH {
     uint32_t done_p[S];    // warps done with the plane in each p stage
@@ -176,17 +181,17 @@ __device__ __forceinline__ void init_handoff(HandoffH<S, AUX>* hs) {
     hs->abort = 0;
 }
 
-__device__ __forceinline__ uint32_t atom_add_acq_rel_shared(uint32_t* p, uint32_t v) {
+__device__ __forceinline__ uint32_t atom_add_relaxed_shared(uint32_t* p, uint32_t v) {
     uint32_t old;
-    asm volatile("atom.acq_rel.cta.shared::cta.add.u32 %0, [%1], %2;"
+    asm volatile("atom.relaxed.cta.shared::cta.add.u32 %0, [%1], %2;"
                  : "=r"(old)
                  : "r"(smem_u32(p)), "r"(v)
                  : "memory");
     return old;
 }
 
-// Orders the stage reads acquired through the hand-off counter before the
-// async-proxy (TMA) write that refills the stage.
+// Orders the generic-proxy view of shared memory before the async-proxy (TMA)
+// write that refills a stage.
 __device__ __forceinline__ void fence_proxy_async_shared() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
@@ -206,7 +211,7 @@ struct RingH {
 // them (advanced on return) and `hs` the stage hand-off (counters at zero, abort
 // clear).  Every copy it issues has landed when it returns; false means a
 // bounded wait gave up (the error is recorded).
-template <int TX, int TY, int S, int AUX, int PHASE, int UNR>
+template <int TX, int TY, int S, int AUX, int PHASE, int UNR, int SYNC>
 __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const CUtensorMap* qmap,
                                                 const CUtensorMap* kmap, const F16Args& a,
                                                 int tx, int ty, int zc, uint16_t* sm,
@@ -258,11 +263,11 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
     // warp that completes the count refills it S planes / AUX iterations on.
     const bool lane0 = (tid & 31) == 0;
     auto release_plane = [&](int j) {
-        if (j + S >= nplanes) return;  // no refill: nothing to hand off
+        if (!SYNC || j + S >= nplanes) return;  // barrier mode / no refill
         __syncwarp();
         if (lane0) {
             uint32_t* c = &hs->done_p[(pb + j) % S];
-            if (atom_add_acq_rel_shared(c, 1u) == kWarps - 1) {
+            if (atom_add_relaxed_shared(c, 1u) == kWarps - 1) {
                 atomicExch(c, 0u);
                 fence_proxy_async_shared();
                 issue_plane(j + S);
@@ -270,11 +275,11 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
         }
     };
     auto release_aux = [&](int it) {
-        if (it + AUX >= nint) return;
+        if (!SYNC || it + AUX >= nint) return;
         __syncwarp();
         if (lane0) {
             uint32_t* c = &hs->done_a[(ab + it) % AUX];
-            if (atom_add_acq_rel_shared(c, 1u) == kWarps - 1) {
+            if (atom_add_relaxed_shared(c, 1u) == kWarps - 1) {
                 atomicExch(c, 0u);
                 fence_proxy_async_shared();
                 issue_aux(it + AUX);
@@ -476,8 +481,19 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                         stg_stream_u2(dst, make_uint2(pk.x, pk.y));
                 }
                 goff += a.sz;
-                if (bad) *reinterpret_cast<volatile int*>(&hs->abort) = 1;
-                abort_run = *reinterpret_cast<volatile int*>(&hs->abort) != 0;
+                if (SYNC) {
+                    if (bad) *reinterpret_cast<volatile int*>(&hs->abort) = 1;
+                    abort_run = *reinterpret_cast<volatile int*>(&hs->abort) != 0;
+                } else {
+                    // the CTA barrier per plane: the centre's stage and this
+                    // plane's aux stage are free once every thread is past it
+                    abort_run = __syncthreads_or(bad) != 0;
+                    if (abort_run && tid == 0) hs->abort = 1;
+                    if (!abort_run && tid == 0) {
+                        if (i + 4 + S < nplanes) issue_plane(i + 4 + S);
+                        if (i + AUX < nint) issue_aux(i + AUX);
+                    }
+                }
             }
         }
     }
@@ -511,7 +527,7 @@ __device__ __forceinline__ void init_rings_f16(uint64_t* full, uint64_t* auxf) {
 
 // One grid: CTA b owns tile (b % tiles_x, (b / tiles_x) % tiles_y) and z chunk
 // b / (tiles_x * tiles_y).
-template <int TX, int TY, int S, int AUX, int PHASE, int UNR>
+template <int TX, int TY, int S, int AUX, int PHASE, int UNR, int SYNC>
 __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, AUX>::MINB)
     pencil_f16_kernel(const __grid_constant__ CUtensorMap pmap,
                       const __grid_constant__ CUtensorMap qmap,
@@ -532,7 +548,7 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
     const int ty = b % a.tiles_y;
     b /= a.tiles_y;
     RingH ring;
-    (void)pencil_f16_tile<TX, TY, S, AUX, PHASE, UNR>(&pmap, &qmap, &kmap, a, tx, ty, b, sm, full,
+    (void)pencil_f16_tile<TX, TY, S, AUX, PHASE, UNR, SYNC>(&pmap, &qmap, &kmap, a, tx, ty, b, sm, full,
                                                       auxf, ring, &hs);
 }
 
@@ -540,7 +556,7 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
 // (shot, tile x, tile y, z chunk) items from the queue; the rings' barriers are
 // initialised once and their phases carried from item to item; the last CTA to
 // finish resets the queue and advances the step counter the sources read.
-template <int TX, int TY, int S, int AUX, int PHASE, int UNR>
+template <int TX, int TY, int S, int AUX, int PHASE, int UNR, int SYNC>
 __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, AUX>::MINB)
     batch_f16_kernel(const ShotF16* __restrict__ shots, const int4* __restrict__ items,
                      int n_items, BatchQueue* queue) {
@@ -564,7 +580,7 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
         const int4 w = items[it];
         const ShotF16* sh = shots + w.x;
         const F16Args a = sh->args;
-        if (!pencil_f16_tile<TX, TY, S, AUX, PHASE, UNR>(&sh->p, &sh->prev, &sh->k, a, w.y, w.z,
+        if (!pencil_f16_tile<TX, TY, S, AUX, PHASE, UNR, SYNC>(&sh->p, &sh->prev, &sh->k, a, w.y, w.z,
                                                          w.w, sm, full, auxf, ring, &hs))
             break;
     }
@@ -583,21 +599,21 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
 using LaunchFnH = cudaError_t (*)(const PencilMaps&, const F16Args&, unsigned, int, cudaStream_t);
 using ResidentFnH = int (*)();
 
-template <int TX, int TY, int S, int AUX, int UNR>
+template <int TX, int TY, int S, int AUX, int UNR, int SYNC>
 int resident_f16() {
     using P = ShapeH<TX, TY, S, AUX>;
     static int cached[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (cached[dev & 63] > 0) return cached[dev & 63];
-    auto kern = pencil_f16_kernel<TX, TY, S, AUX, 0, UNR>;
+    auto kern = pencil_f16_kernel<TX, TY, S, AUX, 0, UNR, SYNC>;
     const int smem = static_cast<int>(P::SMEM);
     int n = 0;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) ==
             cudaSuccess &&
-        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, S, AUX, 1, UNR>,
+        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, S, AUX, 1, UNR, SYNC>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
-        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, S, AUX, 2, UNR>,
+        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, S, AUX, 2, UNR, SYNC>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, P::NT, P::SMEM) == cudaSuccess &&
         n > 0) {
@@ -608,19 +624,19 @@ int resident_f16() {
     return std::max(1, std::min(int((228u * 1024u) / (P::SMEM + 1024u)), 65536 / (P::NT * 128)));
 }
 
-template <int TX, int TY, int S, int AUX, int UNR>
+template <int TX, int TY, int S, int AUX, int UNR, int SYNC>
 cudaError_t launch_f16(const PencilMaps& m, const F16Args& a, unsigned ctas, int phase,
                        cudaStream_t stream) {
     using P = ShapeH<TX, TY, S, AUX>;
-    resident_f16<TX, TY, S, AUX, UNR>();  // sets the attributes once per device
+    resident_f16<TX, TY, S, AUX, UNR, SYNC>();  // sets the attributes once per device
     if (phase == 1)
-        pencil_f16_kernel<TX, TY, S, AUX, 1, UNR><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
+        pencil_f16_kernel<TX, TY, S, AUX, 1, UNR, SYNC><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
                                                                                      m.vel2, a);
     else if (phase == 2)
-        pencil_f16_kernel<TX, TY, S, AUX, 2, UNR><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
+        pencil_f16_kernel<TX, TY, S, AUX, 2, UNR, SYNC><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
                                                                                      m.vel2, a);
     else
-        pencil_f16_kernel<TX, TY, S, AUX, 0, UNR><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
+        pencil_f16_kernel<TX, TY, S, AUX, 0, UNR, SYNC><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
                                                                                      m.vel2, a);
     return cudaGetLastError();
 }
@@ -632,24 +648,25 @@ struct VariantH {
     ResidentFnH resident;
 };
 
-#define SB200_VARIANT_H(TX, TY, S, AUX, UNR, NAME)                                         \
+#define SB200_VARIANT_H(TX, TY, S, AUX, UNR, SYNC, NAME)                                   \
     VariantH {                                                                               \
-        TX, TY, S, AUX, NAME, &launch_f16<TX, TY, S, AUX, UNR>,                             \
-            &resident_f16<TX, TY, S, AUX, UNR>                                               \
+        TX, TY, S, AUX, NAME, &launch_f16<TX, TY, S, AUX, UNR, SYNC>,                       \
+            &resident_f16<TX, TY, S, AUX, UNR, SYNC>                                         \
     }
 
-// "_u8": the plane loop unrolled by 8 instead of 4.
+// SYNC 1: ring stages handed between warps (HandoffH); 0: a CTA barrier per
+// plane ("_b").  "_u8" would unroll the plane loop by 8 (none listed: slower).
 const VariantH kF16[] = {
-    SB200_VARIANT_H(64, 16, 8, 4, 4, "h64x16_s8_a4"),
-    SB200_VARIANT_H(64, 32, 8, 4, 4, "h64x32_s8_a4"),
-    SB200_VARIANT_H(128, 16, 8, 4, 4, "h128x16_s8_a4"),
-    SB200_VARIANT_H(64, 8, 8, 4, 4, "h64x8_s8_a4"),
-    SB200_VARIANT_H(32, 16, 8, 4, 4, "h32x16_s8_a4"),
-    SB200_VARIANT_H(64, 16, 8, 4, 8, "h64x16_s8_a4_u8"),
-    SB200_VARIANT_H(64, 32, 8, 4, 8, "h64x32_s8_a4_u8"),
-    SB200_VARIANT_H(128, 16, 8, 4, 8, "h128x16_s8_a4_u8"),
-    SB200_VARIANT_H(64, 16, 12, 4, 4, "h64x16_s12_a4"),
-    SB200_VARIANT_H(64, 32, 12, 4, 4, "h64x32_s12_a4"),
+    SB200_VARIANT_H(64, 16, 8, 4, 4, 1, "h64x16_s8_a4"),
+    SB200_VARIANT_H(64, 32, 8, 4, 4, 1, "h64x32_s8_a4"),
+    SB200_VARIANT_H(128, 16, 8, 4, 4, 1, "h128x16_s8_a4"),
+    SB200_VARIANT_H(64, 8, 8, 4, 4, 1, "h64x8_s8_a4"),
+    SB200_VARIANT_H(32, 16, 8, 4, 4, 1, "h32x16_s8_a4"),
+    SB200_VARIANT_H(64, 32, 12, 4, 4, 1, "h64x32_s12_a4"),
+    SB200_VARIANT_H(64, 16, 8, 4, 4, 0, "h64x16_s8_a4_b"),
+    SB200_VARIANT_H(64, 32, 8, 4, 4, 0, "h64x32_s8_a4_b"),
+    SB200_VARIANT_H(128, 16, 8, 4, 4, 0, "h128x16_s8_a4_b"),
+    SB200_VARIANT_H(64, 32, 12, 4, 4, 0, "h64x32_s12_a4_b"),
 };
 constexpr int kNumF16 = sizeof(kF16) / sizeof(kF16[0]);
 
@@ -733,7 +750,7 @@ F16Args make_f16_args(int TX, int TY, const GridDesc& g, int zchunks, uint16_t* 
 using LaunchFnB16 = cudaError_t (*)(const ShotF16*, const int4*, int, BatchQueue*, unsigned, int,
                                     cudaStream_t);
 
-template <int TX, int TY, int S, int AUX, int UNR>
+template <int TX, int TY, int S, int AUX, int UNR, int SYNC>
 int resident_batch_f16() {
     using P = ShapeH<TX, TY, S, AUX>;
     static int cached[64] = {};
@@ -742,13 +759,13 @@ int resident_batch_f16() {
     if (cached[dev & 63] > 0) return cached[dev & 63];
     const int smem = static_cast<int>(P::SMEM);
     int n = 0;
-    if (cudaFuncSetAttribute(batch_f16_kernel<TX, TY, S, AUX, 0, UNR>,
+    if (cudaFuncSetAttribute(batch_f16_kernel<TX, TY, S, AUX, 0, UNR, SYNC>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
-        cudaFuncSetAttribute(batch_f16_kernel<TX, TY, S, AUX, 1, UNR>,
+        cudaFuncSetAttribute(batch_f16_kernel<TX, TY, S, AUX, 1, UNR, SYNC>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
-        cudaFuncSetAttribute(batch_f16_kernel<TX, TY, S, AUX, 2, UNR>,
+        cudaFuncSetAttribute(batch_f16_kernel<TX, TY, S, AUX, 2, UNR, SYNC>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_f16_kernel<TX, TY, S, AUX, 0, UNR>,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_f16_kernel<TX, TY, S, AUX, 0, UNR, SYNC>,
                                                       P::NT, P::SMEM) == cudaSuccess &&
         n > 0) {
         cached[dev & 63] = n;
@@ -758,19 +775,19 @@ int resident_batch_f16() {
     return std::max(1, std::min(int((228u * 1024u) / (P::SMEM + 1024u)), 65536 / (P::NT * 128)));
 }
 
-template <int TX, int TY, int S, int AUX, int UNR>
+template <int TX, int TY, int S, int AUX, int UNR, int SYNC>
 cudaError_t launch_batch_f16_t(const ShotF16* shots, const int4* items, int n_items,
                                BatchQueue* queue, unsigned ctas, int phase, cudaStream_t stream) {
     using P = ShapeH<TX, TY, S, AUX>;
-    resident_batch_f16<TX, TY, S, AUX, UNR>();  // sets the attributes once per device
+    resident_batch_f16<TX, TY, S, AUX, UNR, SYNC>();  // sets the attributes once per device
     if (phase == 1)
-        batch_f16_kernel<TX, TY, S, AUX, 1, UNR><<<ctas, P::NT, P::SMEM, stream>>>(shots, items,
+        batch_f16_kernel<TX, TY, S, AUX, 1, UNR, SYNC><<<ctas, P::NT, P::SMEM, stream>>>(shots, items,
                                                                                     n_items, queue);
     else if (phase == 2)
-        batch_f16_kernel<TX, TY, S, AUX, 2, UNR><<<ctas, P::NT, P::SMEM, stream>>>(shots, items,
+        batch_f16_kernel<TX, TY, S, AUX, 2, UNR, SYNC><<<ctas, P::NT, P::SMEM, stream>>>(shots, items,
                                                                                     n_items, queue);
     else
-        batch_f16_kernel<TX, TY, S, AUX, 0, UNR><<<ctas, P::NT, P::SMEM, stream>>>(shots, items,
+        batch_f16_kernel<TX, TY, S, AUX, 0, UNR, SYNC><<<ctas, P::NT, P::SMEM, stream>>>(shots, items,
                                                                                     n_items, queue);
     return cudaGetLastError();
 }
@@ -783,12 +800,14 @@ struct VariantB16 {
 };
 
 const VariantB16 kBatchF16[] = {
-    {64, 16, "bh64x16_s8_a4", &launch_batch_f16_t<64, 16, 8, 4, 4>,
-     &resident_batch_f16<64, 16, 8, 4, 4>},
-    {32, 16, "bh32x16_s8_a4", &launch_batch_f16_t<32, 16, 8, 4, 4>,
-     &resident_batch_f16<32, 16, 8, 4, 4>},
-    {64, 8, "bh64x8_s8_a4", &launch_batch_f16_t<64, 8, 8, 4, 4>,
-     &resident_batch_f16<64, 8, 8, 4, 4>},
+    {64, 16, "bh64x16_s8_a4", &launch_batch_f16_t<64, 16, 8, 4, 4, 1>,
+     &resident_batch_f16<64, 16, 8, 4, 4, 1>},
+    {32, 16, "bh32x16_s8_a4", &launch_batch_f16_t<32, 16, 8, 4, 4, 1>,
+     &resident_batch_f16<32, 16, 8, 4, 4, 1>},
+    {64, 8, "bh64x8_s8_a4", &launch_batch_f16_t<64, 8, 8, 4, 4, 1>,
+     &resident_batch_f16<64, 8, 8, 4, 4, 1>},
+    {64, 16, "bh64x16_s8_a4_b", &launch_batch_f16_t<64, 16, 8, 4, 4, 0>,
+     &resident_batch_f16<64, 16, 8, 4, 4, 0>},
 };
 constexpr int kNumBatchF16 = sizeof(kBatchF16) / sizeof(kBatchF16[0]);
 
