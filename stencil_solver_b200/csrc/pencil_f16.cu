@@ -27,7 +27,7 @@
 //     Laplacian is two FMA chains (x and y from the combined centre term, z from
 //     its first pair) added once; p_prev enters the update through the mixed
 //     subtract (no separate conversion).
-// Ring stages pass between the warps without a CTA barrier per plane (HandoffH).
+// Ring stages pass between the warps without a CTA barrier per plane (StageHandoff).
 //
 // Renormalisation (driven by the FP64 statistics every few dozen steps): a
 // renorm step (PHASE 1) scales its output by r = a_new / a_old; the step after
@@ -151,51 +151,6 @@ __device__ __forceinline__ float xsum1(const float (&c)[8], uint2 lf, uint2 rt, 
     return c[up] + c[dn];
 }
 
-// Shared-memory hand-off of ring stages between the warps of a CTA, in place of
-// a CTA barrier per plane: a warp that has read the last it needs of a stage
-// counts itself done (a shared-memory atomic after __syncwarp), and the warp that
-// completes the count refills the stage by TMA.  No warp waits for another; a
-// warp at plane iteration k needs only refills released at iterations <= k - 4,
-// which every warp, the slowest included, has passed.  The count is a relaxed
-// atomic: an acquire-release one also orders the warp's outstanding global
-// stores (a fence per plane that waited on DRAM writes: 2.24 ms per 1024^3 step
-// against 1.62), while the stage reads it must follow are shared-memory loads,
-// which the shared-memory pipe completes in issue order before the warp's later
-// atomic on the counter.
-template <int S, int AUX>
-struct HandoffH {
-    uint32_t done_p[S];    // warps done with the plane in each p stage
-    uint32_t done_a[AUX];  // warps done with each aux stage
-    int issued_p;          // highest plane index of this tile handed to TMA
-    int issued_a;          // highest aux iteration of this tile handed to TMA
-    int abort;             // a bounded wait gave up somewhere in the CTA
-};
-
-template <int S, int AUX>
-__device__ __forceinline__ void init_handoff(HandoffH<S, AUX>* hs) {
-#pragma unroll
-    for (int s = 0; s < S; ++s) hs->done_p[s] = 0u;
-#pragma unroll
-    for (int s = 0; s < AUX; ++s) hs->done_a[s] = 0u;
-    hs->issued_p = hs->issued_a = -1;
-    hs->abort = 0;
-}
-
-__device__ __forceinline__ uint32_t atom_add_relaxed_shared(uint32_t* p, uint32_t v) {
-    uint32_t old;
-    asm volatile("atom.relaxed.cta.shared::cta.add.u32 %0, [%1], %2;"
-                 : "=r"(old)
-                 : "r"(smem_u32(p)), "r"(v)
-                 : "memory");
-    return old;
-}
-
-// Orders the generic-proxy view of shared memory before the async-proxy (TMA)
-// write that refills a stage.
-__device__ __forceinline__ void fence_proxy_async_shared() {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
 // Ring position a CTA carries from one tile to the next: the sequence numbers of
 // the next p plane and the next aux iteration.  Stage = seq % ring size, phase
 // parity = (seq / ring size) & 1, so a persistent CTA initialises its mbarriers
@@ -216,7 +171,7 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                                                 const CUtensorMap* kmap, const F16Args& a,
                                                 int tx, int ty, int zc, uint16_t* sm,
                                                 uint64_t* full, uint64_t* auxf, RingH& ring,
-                                                HandoffH<S, AUX>* hs) {
+                                                StageHandoff<S, AUX>* hs) {
     using P = ShapeH<TX, TY, S, AUX>;
     static_assert(P::NT % 32 == 0, "whole warps");
     constexpr uint32_t kWarps = P::NT / 32;
@@ -535,7 +490,7 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
     extern __shared__ unsigned char dsmem[];
     __shared__ __align__(8) uint64_t full[S];
     __shared__ __align__(8) uint64_t auxf[AUX];
-    __shared__ HandoffH<S, AUX> hs;
+    __shared__ StageHandoff<S, AUX> hs;
     uint16_t* sm = reinterpret_cast<uint16_t*>(smem_align<128>(dsmem));
     if (threadIdx.x == 0) {
         init_rings_f16<S, AUX>(full, auxf);
@@ -564,7 +519,7 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
     __shared__ __align__(8) uint64_t full[S];
     __shared__ __align__(8) uint64_t auxf[AUX];
     __shared__ int s_item;
-    __shared__ HandoffH<S, AUX> hs;
+    __shared__ StageHandoff<S, AUX> hs;
     uint16_t* sm = reinterpret_cast<uint16_t*>(smem_align<128>(dsmem));
     if (threadIdx.x == 0) {
         init_rings_f16<S, AUX>(full, auxf);
@@ -654,7 +609,7 @@ struct VariantH {
             &resident_f16<TX, TY, S, AUX, UNR, SYNC>                                         \
     }
 
-// SYNC 1: ring stages handed between warps (HandoffH); 0: a CTA barrier per
+// SYNC 1: ring stages handed between warps (StageHandoff); 0: a CTA barrier per
 // plane ("_b").  "_u8" would unroll the plane loop by 8 (none listed: slower).
 const VariantH kF16[] = {
     SB200_VARIANT_H(64, 16, 8, 4, 4, 1, "h64x16_s8_a4"),

@@ -55,12 +55,15 @@ def test_time_to_solution_summary():
     sec = {"fp16_storage": {"ms_per_step": 1.62,
                             "accuracy_256^3_500_steps": {"field_rel_l2_vs_fp32": 0.018,
                                                          "trace_rel_l2_vs_fp32": 7e-4}},
-           "learned": {"within_bound": {"coarse_steps": 80, "judged_ms": 44.0, "fine_ms": 440.0,
-                                        "fallback_at_step": None, "rel_l2_judged": 6.6e-4,
-                                        "time_to_solution_speedup_vs_fine": 10.0}}}
+           "learned": {"coarse_steps": 200, "fine_ms": 1100.0,
+                       "judged": {"ms": 110.0, "fallback_at_step": None, "rel_l2": 3e-4,
+                                  "speedup_vs_fine": 10.0}}}
     s = bench.time_to_solution_summary(2.72, sec)
     assert s["plain_fp32_1024^3_1000_steps_ms"] == pytest.approx(2720.0)
     assert s["fp16_1024^3_1000_steps_ms"] == pytest.approx(1620.0)
     assert not s["fp16_field_within_1e-3"] and s["fp16_trace_within_1e-3"]
     assert s["learned_within_1e-3"] and s["learned_speedup_vs_fine"] == 10.0
+    assert s["learned_coarse_steps"] == 200 and s["learned_judged_ms"] == 110.0
+    sec["learned"]["judged"]["fallback_at_step"] = 100  # the judge fell back
+    assert not bench.time_to_solution_summary(2.72, sec)["learned_within_1e-3"]
     assert bench.time_to_solution_summary(2.72, {}) == {"plain_fp32_1024^3_1000_steps_ms": 2720.0}
