@@ -25,9 +25,7 @@
 //     slot is a compile-time register and nothing is shifted.
 //   * arithmetic on point pairs uses the packed f32x2 instructions; the
 //     Laplacian is two FMA chains (x and y from the combined centre term, z from
-//     its first pair) added once; p_prev enters the update through the mixed
-//     subtract (no separate conversion).
-// Ring stages pass between the warps without a CTA barrier per plane (StageHandoff).
+//     its first pair) added once.
 //
 // Renormalisation (driven by the FP64 statistics every few dozen steps): a
 // renorm step (PHASE 1) scales its output by r = a_new / a_old; the step after
@@ -151,33 +149,39 @@ __device__ __forceinline__ float xsum1(const float (&c)[8], uint2 lf, uint2 rt, 
     return c[up] + c[dn];
 }
 
-// Ring position a CTA carries from one tile to the next: the sequence numbers of
-// the next p plane and the next aux iteration.  Stage = seq % ring size, phase
-// parity = (seq / ring size) & 1, so a persistent CTA initialises its mbarriers
-// once and their phases continue across the tiles it sweeps.
+// Ring position a persistent CTA carries from one tile to the next: the
+// sequence numbers of the next p plane and the next aux iteration.  Stage =
+// seq % ring size, phase parity = (seq / ring size) & 1, so its mbarriers are
+// initialised once and their phases continue across the tiles it sweeps.
 struct RingH {
     uint32_t p = 0;
     uint32_t aux = 0;
 };
 
+// Update formulas of the step (template parameter UPD):
+//   kUpdConvert:  p_prev converted to FP32, then fma(K, lap, fma(-m_q, pq, 2c));
+//   kUpdMixedSub: u = fma(K, lap, 2c), then the mixed subtract pq - u converts p_prev
+//                 on the way and gives -p_next, whose sign the rescale factor
+//                 (PHASE 1) or the packed halves' sign bits (PHASE 0) restore;
+//                 PHASE 2 (p_prev rescaled) uses kUpdConvert.
+constexpr int kUpdConvert = 0, kUpdMixedSub = 1;
+
 // One tile: columns [tx TX, tx TX + TX) x rows [4 + ty TY, ...) of the interior,
 // marched over z chunk zc.  All threads of the CTA call it; `sm`, `full` and
-// `auxf` are the CTA's rings, initialised by the caller, `ring` the position in
-// them (advanced on return) and `hs` the stage hand-off (counters at zero, abort
-// clear).  Every copy it issues has landed when it returns; false means a
-// bounded wait gave up (the error is recorded).
-template <int TX, int TY, int S, int AUX, int PHASE, int UNR, int SYNC>
+// `auxf` are the CTA's rings.  CARRY false: their mbarriers are freshly
+// initialised (phase 0 on every stage) and the ring positions are compile-time;
+// CARRY true: `ring` gives the positions (advanced on return).  Every copy it
+// issues has landed when it returns; false means a bounded wait gave up (the
+// error is recorded).
+template <int TX, int TY, int S, int AUX, int PHASE, int UNR, bool CARRY, int UPD>
 __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const CUtensorMap* qmap,
                                                 const CUtensorMap* kmap, const F16Args& a,
                                                 int tx, int ty, int zc, uint16_t* sm,
-                                                uint64_t* full, uint64_t* auxf, RingH& ring,
-                                                StageHandoff<S, AUX>* hs) {
+                                                uint64_t* full, uint64_t* auxf, RingH& ring) {
     using P = ShapeH<TX, TY, S, AUX>;
-    static_assert(P::NT % 32 == 0, "whole warps");
-    constexpr uint32_t kWarps = P::NT / 32;
+    const uint32_t pb = CARRY ? ring.p : 0u;    // sequence number of plane 0
+    const uint32_t ab = CARRY ? ring.aux : 0u;  // sequence number of aux iteration 0
     uint16_t* aux = sm + S * P::PLANE;  // AUX stages of [p_prev tile | K tile]
-    const uint32_t pb = ring.p;         // sequence number of plane 0
-    const uint32_t ab = ring.aux;       // sequence number of aux iteration 0
 
     const int tid = threadIdx.x;
     const int lx = tid % P::TPR;
@@ -194,56 +198,26 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
         prefetch_tmap(qmap);
         prefetch_tmap(kmap);
     }
-    // Refills are issued by one thread at a time per stage (thread 0 at the
-    // start, then whichever warp completes a stage's hand-off count).
-    auto issue_plane = [&](int j) {
+    int issued_hi = -1, aux_issued_hi = -1;
+    auto issue_plane = [&](int j) {  // thread 0 only
         const uint32_t st = (pb + j) % S;
         mbar_arrive_expect_tx(&full[st], P::PLANE_BYTES);
         tma_load_3d(sm + st * P::PLANE, pmap, &full[st], xa - 8, y0 - R, zb - R + j);
-        atomicMax(&hs->issued_p, j);
+        issued_hi = j;
     };
-    auto issue_aux = [&](int it) {
+    auto issue_aux = [&](int it) {  // thread 0 only
         const uint32_t sa = (ab + it) % AUX;
         uint16_t* st = aux + sa * 2 * P::TILE;
         mbar_arrive_expect_tx(&auxf[sa], 2 * P::TILE_BYTES);
         tma_load_3d(st, qmap, &auxf[sa], xa, y0, zb + it);
         tma_load_3d(st + P::TILE, kmap, &auxf[sa], xa, y0, zb + it);
-        atomicMax(&hs->issued_a, it);
+        aux_issued_hi = it;
     };
     auto wait_plane = [&](int j) { return mbar_wait(&full[(pb + j) % S], ((pb + j) / S) & 1u); };
     auto wait_aux = [&](int it) {
         return mbar_wait(&auxf[(ab + it) % AUX], ((ab + it) / AUX) & 1u);
     };
-    // This warp is done with plane j's stage / aux iteration it's stage; the
-    // warp that completes the count refills it S planes / AUX iterations on.
-    const bool lane0 = (tid & 31) == 0;
-    auto release_plane = [&](int j) {
-        if (!SYNC || j + S >= nplanes) return;  // barrier mode / no refill
-        __syncwarp();
-        if (lane0) {
-            uint32_t* c = &hs->done_p[(pb + j) % S];
-            if (atom_add_relaxed_shared(c, 1u) == kWarps - 1) {
-                atomicExch(c, 0u);
-                fence_proxy_async_shared();
-                issue_plane(j + S);
-            }
-        }
-    };
-    auto release_aux = [&](int it) {
-        if (!SYNC || it + AUX >= nint) return;
-        __syncwarp();
-        if (lane0) {
-            uint32_t* c = &hs->done_a[(ab + it) % AUX];
-            if (atom_add_relaxed_shared(c, 1u) == kWarps - 1) {
-                atomicExch(c, 0u);
-                fence_proxy_async_shared();
-                issue_aux(it + AUX);
-            }
-        }
-    };
     if (tid == 0) {
-        hs->issued_p = -1;
-        hs->issued_a = -1;
         for (int s = 0; s < S && s < nplanes; ++s) issue_plane(s);
         for (int it = 0; it < AUX && it < nint; ++it) issue_aux(it);
     }
@@ -278,7 +252,7 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
     float m_out = 1.f, m_q = 1.f;
     if (PHASE == 1) m_out = a.scale->r;
     if (PHASE == 2) m_q = a.scale->r;
-    const float2 nmq2 = dup2(-m_q), nmout2 = dup2(-m_out);
+    const float2 nmq2 = dup2(-m_q), mout2 = dup2(m_out), nmout2 = dup2(-m_out);
 
     // Plane index p (z = zb - 4 + p) lives in slot p % 4 of both rings.
     uint4 hq[4];      // FP16: centre and the planes above it
@@ -296,25 +270,29 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
         }
     }
     bool abort_run = __syncthreads_or(bad) != 0;
-    if (abort_run && tid == 0) hs->abort = 1;
     if (!abort_run && tid == 0) {
 #pragma unroll
         for (int p = 0; p < R; ++p)  // planes 0..3 are consumed: refill their stages
             if (p + S < nplanes) issue_plane(p + S);
     }
 
-    // The plane loop is unrolled by UNR (4 or 8); the register rings' slots are
-    // compile-time (i0 is a multiple of 4).  Shared-memory stages and phases
-    // follow the sequence numbers.
+    // The plane loop is unrolled by UNR (4 or 8).  i0 is a multiple of 4 and so
+    // is S: the fed plane's stage is a block base + u, wrapping at most once
+    // (UNR = 8), and its phase is a block constant or flips with the wrap; the aux
+    // ring (AUX | 4) has compile-time stages and a block-constant phase.
     static_assert(UNR == 4 || UNR == 8, "unroll");
     static_assert(UNR == 4 || S == 8, "an unroll of 8 needs an 8-stage ring");
     for (int i0 = 0; i0 < nint && !abort_run; i0 += UNR) {
+        // (CARRY: the same block bases offset by the carried sequence numbers)
+        const int cbase = (pb + i0 + 4) % S, fbase = (pb + i0 + 8) % S;
+        const uint32_t fpar = ((pb + i0 + 8) / S) & 1u, apar = (i0 / AUX) & 1u;
 #pragma unroll
         for (int u = 0; u < UNR; ++u) {
             const int i = i0 + u;
             if (i < nint && !abort_run) {
                 // Centre plane i + 4 (slot u); it was waited for when it was fed.
-                const uint32_t cst = (pb + i + 4) % S, fst = (pb + i + 8) % S;
+                const int cst = (cbase + u) % S, fst = (fbase + u) % S;
+                const uint32_t fph = fpar ^ (fbase + u >= S ? 1u : 0u);
                 const uint16_t* pc = sm + cst * P::PLANE + soff;
                 // x window: 4 halves left and right of the chunk stay FP16; the
                 // own 8 points (the centre) are converted once.
@@ -326,7 +304,7 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                 const float cf[8] = {cv[0].x, cv[0].y, cv[1].x, cv[1].y,
                                      cv[2].x, cv[2].y, cv[3].x, cv[3].y};
                 // feed: plane i + 8 (z + 4) replaces the centre in slot u
-                if (!wait_plane(i + 8)) bad = true;
+                if (!mbar_wait(&full[fst], fph)) bad = true;
                 hq[u % 4] = lds128h(sm + fst * P::PLANE + soff);
                 uint4 yu[R], yd[R];  // staged rows y +- d of the centre plane
 #pragma unroll
@@ -334,7 +312,6 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                     yu[d - 1] = lds128h(pc + d * P::SX);
                     yd[d - 1] = lds128h(pc - d * P::SX);
                 }
-                release_plane(i + 4);  // the centre plane's last reads
                 // lap = [c (cx+cy+cz) + sum_r (ax_r sx_r + ay_r sy_r)] + sum_r az_r sz_r,
                 // pair sums s = p[+r] + p[-r]; up operands of y and z enter FP16.
                 float2 lap[4];
@@ -368,17 +345,21 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
 #pragma unroll
                 for (int h = 0; h < 4; ++h) dq[u % 4][h] = cv[h];
 
-                if (!wait_aux(i)) bad = true;
-                const uint16_t* st = aux + ((ab + i) % AUX) * 2 * P::TILE + aoff;
+                bool aok;
+                const uint16_t* st;
+                if (CARRY) {
+                    aok = wait_aux(i);
+                    st = aux + ((ab + i) % AUX) * 2 * P::TILE + aoff;
+                } else {  // compile-time stage, block-constant phase
+                    aok = mbar_wait(&auxf[u % AUX], apar ^ ((u / AUX) & 1u));
+                    st = aux + (u % AUX) * 2 * P::TILE + aoff;
+                }
+                if (!aok) bad = true;
                 const uint4 qv = lds128h(st);
                 const uint4 kv = lds128h(st + P::TILE);
-                release_aux(i);
-                // o holds p_next (PHASE 2) or, in the other phases, -p_next
-                // before the PHASE 1 rescale: u = K lap + 2c (2c is exact), then
-                // the mixed subtract q - u converts p_prev on the way; the sign
-                // is restored by the rescale factor -m_out (PHASE 1) or by the
-                // sign bits of the packed halves (PHASE 0).
-                constexpr bool kNeg = PHASE == 0;
+                // kNeg: o holds -p_next (see kUpdMixedSub)
+                constexpr bool kMixed = UPD == kUpdMixedSub && PHASE != 2;
+                constexpr bool kNeg = kMixed && PHASE == 0;
                 float o[8];
 #pragma unroll
                 for (int h = 0; h < 4; ++h) {
@@ -387,13 +368,14 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                     const float2 kk = make_float2(__uint_as_float(kw << 16),
                                                   __uint_as_float(kw & 0xffff0000u));
                     float2 ov;
-                    if (PHASE == 2) {
-                        // 2c - m_q pq in one rounding, then + K lap
-                        const float2 pq = h2f2(get_word(qv, h));
-                        ov = fma2(kk, lap[h], fma2(nmq2, pq, add2(c, c)));
-                    } else {
+                    if (kMixed) {
                         ov = subhf2(get_word(qv, h), fma2(kk, lap[h], add2(c, c)));
                         if (PHASE == 1) ov = mul2(ov, nmout2);
+                    } else {
+                        // 2c - m_q pq in one rounding (2c is exact), then + K lap
+                        const float2 pq = h2f2(get_word(qv, h));
+                        ov = fma2(kk, lap[h], fma2(nmq2, pq, add2(c, c)));
+                        if (PHASE == 1) ov = mul2(ov, mout2);
                     }
                     o[2 * h] = ov.x;
                     o[2 * h + 1] = ov.y;
@@ -436,37 +418,28 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                         stg_stream_u2(dst, make_uint2(pk.x, pk.y));
                 }
                 goff += a.sz;
-                if (SYNC) {
-                    if (bad) *reinterpret_cast<volatile int*>(&hs->abort) = 1;
-                    abort_run = *reinterpret_cast<volatile int*>(&hs->abort) != 0;
-                } else {
-                    // the CTA barrier per plane: the centre's stage and this
-                    // plane's aux stage are free once every thread is past it
-                    abort_run = __syncthreads_or(bad) != 0;
-                    if (abort_run && tid == 0) hs->abort = 1;
-                    if (!abort_run && tid == 0) {
-                        if (i + 4 + S < nplanes) issue_plane(i + 4 + S);
-                        if (i + AUX < nint) issue_aux(i + AUX);
-                    }
+                abort_run = __syncthreads_or(bad) != 0;
+                if (!abort_run && tid == 0) {
+                    if (i + 4 + S < nplanes) issue_plane(i + 4 + S);  // the centre's stage
+                    if (i + AUX < nint) issue_aux(i + AUX);
                 }
             }
         }
     }
 
-    __syncthreads();  // every warp has left the plane loop
-    if (hs->abort != 0) {
+    if (abort_run) {
         if (tid == 0) {
             record_error(a.err, kDevWaitTimeout);
-            // Let every copy still in flight land before the shared memory is
-            // released or reused (a stage has at most one fill outstanding).
-            const int ip = hs->issued_p, ia = hs->issued_a;
-            for (int jj = max(0, ip - S + 1); jj <= ip; ++jj) (void)wait_plane(jj);
-            for (int it = max(0, ia - AUX + 1); it <= ia; ++it) (void)wait_aux(it);
+            for (int jj = max(0, issued_hi - S + 1); jj <= issued_hi; ++jj) (void)wait_plane(jj);
+            for (int it = max(0, aux_issued_hi - AUX + 1); it <= aux_issued_hi; ++it)
+                (void)wait_aux(it);
         }
         return false;
     }
-    ring.p = pb + nplanes;
-    ring.aux = ab + nint;
+    if (CARRY) {
+        ring.p = pb + nplanes;
+        ring.aux = ab + nint;
+    }
     return true;
 }
 
@@ -482,7 +455,7 @@ __device__ __forceinline__ void init_rings_f16(uint64_t* full, uint64_t* auxf) {
 
 // One grid: CTA b owns tile (b % tiles_x, (b / tiles_x) % tiles_y) and z chunk
 // b / (tiles_x * tiles_y).
-template <int TX, int TY, int S, int AUX, int PHASE, int UNR, int SYNC>
+template <int TX, int TY, int S, int AUX, int PHASE, int UNR, int UPD>
 __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, AUX>::MINB)
     pencil_f16_kernel(const __grid_constant__ CUtensorMap pmap,
                       const __grid_constant__ CUtensorMap qmap,
@@ -490,12 +463,8 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
     extern __shared__ unsigned char dsmem[];
     __shared__ __align__(8) uint64_t full[S];
     __shared__ __align__(8) uint64_t auxf[AUX];
-    __shared__ StageHandoff<S, AUX> hs;
     uint16_t* sm = reinterpret_cast<uint16_t*>(smem_align<128>(dsmem));
-    if (threadIdx.x == 0) {
-        init_rings_f16<S, AUX>(full, auxf);
-        init_handoff(&hs);
-    }
+    if (threadIdx.x == 0) init_rings_f16<S, AUX>(full, auxf);
     __syncthreads();
     int b = blockIdx.x;
     const int tx = b % a.tiles_x;
@@ -503,15 +472,15 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
     const int ty = b % a.tiles_y;
     b /= a.tiles_y;
     RingH ring;
-    (void)pencil_f16_tile<TX, TY, S, AUX, PHASE, UNR, SYNC>(&pmap, &qmap, &kmap, a, tx, ty, b, sm, full,
-                                                      auxf, ring, &hs);
+    (void)pencil_f16_tile<TX, TY, S, AUX, PHASE, UNR, false, UPD>(&pmap, &qmap, &kmap, a, tx, ty,
+                                                                  b, sm, full, auxf, ring);
 }
 
 // Many grids (shots) in one persistent launch, as batch_f32_kernel: CTAs take
 // (shot, tile x, tile y, z chunk) items from the queue; the rings' barriers are
-// initialised once and their phases carried from item to item; the last CTA to
-// finish resets the queue and advances the step counter the sources read.
-template <int TX, int TY, int S, int AUX, int PHASE, int UNR, int SYNC>
+// initialised once and their phases carried from item to item (RingH); the last
+// CTA to finish resets the queue and advances the step counter the sources read.
+template <int TX, int TY, int S, int AUX, int PHASE, int UNR, int UPD>
 __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, AUX>::MINB)
     batch_f16_kernel(const ShotF16* __restrict__ shots, const int4* __restrict__ items,
                      int n_items, BatchQueue* queue) {
@@ -519,12 +488,8 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
     __shared__ __align__(8) uint64_t full[S];
     __shared__ __align__(8) uint64_t auxf[AUX];
     __shared__ int s_item;
-    __shared__ StageHandoff<S, AUX> hs;
     uint16_t* sm = reinterpret_cast<uint16_t*>(smem_align<128>(dsmem));
-    if (threadIdx.x == 0) {
-        init_rings_f16<S, AUX>(full, auxf);
-        init_handoff(&hs);
-    }
+    if (threadIdx.x == 0) init_rings_f16<S, AUX>(full, auxf);
     RingH ring;
     for (;;) {
         if (threadIdx.x == 0) s_item = atomicAdd(&queue->next, 1);
@@ -535,8 +500,9 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
         const int4 w = items[it];
         const ShotF16* sh = shots + w.x;
         const F16Args a = sh->args;
-        if (!pencil_f16_tile<TX, TY, S, AUX, PHASE, UNR, SYNC>(&sh->p, &sh->prev, &sh->k, a, w.y, w.z,
-                                                         w.w, sm, full, auxf, ring, &hs))
+        if (!pencil_f16_tile<TX, TY, S, AUX, PHASE, UNR, true, UPD>(&sh->p, &sh->prev, &sh->k, a,
+                                                                    w.y, w.z, w.w, sm, full, auxf,
+                                                                    ring))
             break;
     }
     if (threadIdx.x == 0) {
@@ -554,21 +520,21 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
 using LaunchFnH = cudaError_t (*)(const PencilMaps&, const F16Args&, unsigned, int, cudaStream_t);
 using ResidentFnH = int (*)();
 
-template <int TX, int TY, int S, int AUX, int UNR, int SYNC>
+template <int TX, int TY, int S, int AUX, int UNR, int UPD>
 int resident_f16() {
     using P = ShapeH<TX, TY, S, AUX>;
     static int cached[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (cached[dev & 63] > 0) return cached[dev & 63];
-    auto kern = pencil_f16_kernel<TX, TY, S, AUX, 0, UNR, SYNC>;
+    auto kern = pencil_f16_kernel<TX, TY, S, AUX, 0, UNR, UPD>;
     const int smem = static_cast<int>(P::SMEM);
     int n = 0;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) ==
             cudaSuccess &&
-        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, S, AUX, 1, UNR, SYNC>,
+        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, S, AUX, 1, UNR, UPD>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
-        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, S, AUX, 2, UNR, SYNC>,
+        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, S, AUX, 2, UNR, UPD>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, P::NT, P::SMEM) == cudaSuccess &&
         n > 0) {
@@ -579,19 +545,19 @@ int resident_f16() {
     return std::max(1, std::min(int((228u * 1024u) / (P::SMEM + 1024u)), 65536 / (P::NT * 128)));
 }
 
-template <int TX, int TY, int S, int AUX, int UNR, int SYNC>
+template <int TX, int TY, int S, int AUX, int UNR, int UPD>
 cudaError_t launch_f16(const PencilMaps& m, const F16Args& a, unsigned ctas, int phase,
                        cudaStream_t stream) {
     using P = ShapeH<TX, TY, S, AUX>;
-    resident_f16<TX, TY, S, AUX, UNR, SYNC>();  // sets the attributes once per device
+    resident_f16<TX, TY, S, AUX, UNR, UPD>();  // sets the attributes once per device
     if (phase == 1)
-        pencil_f16_kernel<TX, TY, S, AUX, 1, UNR, SYNC><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
+        pencil_f16_kernel<TX, TY, S, AUX, 1, UNR, UPD><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
                                                                                      m.vel2, a);
     else if (phase == 2)
-        pencil_f16_kernel<TX, TY, S, AUX, 2, UNR, SYNC><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
+        pencil_f16_kernel<TX, TY, S, AUX, 2, UNR, UPD><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
                                                                                      m.vel2, a);
     else
-        pencil_f16_kernel<TX, TY, S, AUX, 0, UNR, SYNC><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
+        pencil_f16_kernel<TX, TY, S, AUX, 0, UNR, UPD><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
                                                                                      m.vel2, a);
     return cudaGetLastError();
 }
@@ -603,25 +569,25 @@ struct VariantH {
     ResidentFnH resident;
 };
 
-#define SB200_VARIANT_H(TX, TY, S, AUX, UNR, SYNC, NAME)                                   \
+#define SB200_VARIANT_H(TX, TY, S, AUX, UNR, UPD, NAME)                                    \
     VariantH {                                                                               \
-        TX, TY, S, AUX, NAME, &launch_f16<TX, TY, S, AUX, UNR, SYNC>,                       \
-            &resident_f16<TX, TY, S, AUX, UNR, SYNC>                                         \
+        TX, TY, S, AUX, NAME, &launch_f16<TX, TY, S, AUX, UNR, UPD>,                        \
+            &resident_f16<TX, TY, S, AUX, UNR, UPD>                                          \
     }
 
-// SYNC 1: ring stages handed between warps (StageHandoff); 0: a CTA barrier per
-// plane ("_b").  "_u8" would unroll the plane loop by 8 (none listed: slower).
+// "_u8": the plane loop unrolled by 8 instead of 4; "_ms": the kUpdMixedSub update.
 const VariantH kF16[] = {
-    SB200_VARIANT_H(64, 16, 8, 4, 4, 1, "h64x16_s8_a4"),
-    SB200_VARIANT_H(64, 32, 8, 4, 4, 1, "h64x32_s8_a4"),
-    SB200_VARIANT_H(128, 16, 8, 4, 4, 1, "h128x16_s8_a4"),
-    SB200_VARIANT_H(64, 8, 8, 4, 4, 1, "h64x8_s8_a4"),
-    SB200_VARIANT_H(32, 16, 8, 4, 4, 1, "h32x16_s8_a4"),
-    SB200_VARIANT_H(64, 32, 12, 4, 4, 1, "h64x32_s12_a4"),
-    SB200_VARIANT_H(64, 16, 8, 4, 4, 0, "h64x16_s8_a4_b"),
-    SB200_VARIANT_H(64, 32, 8, 4, 4, 0, "h64x32_s8_a4_b"),
-    SB200_VARIANT_H(128, 16, 8, 4, 4, 0, "h128x16_s8_a4_b"),
-    SB200_VARIANT_H(64, 32, 12, 4, 4, 0, "h64x32_s12_a4_b"),
+    SB200_VARIANT_H(64, 16, 8, 4, 4, kUpdConvert, "h64x16_s8_a4"),
+    SB200_VARIANT_H(64, 32, 8, 4, 4, kUpdConvert, "h64x32_s8_a4"),
+    SB200_VARIANT_H(128, 16, 8, 4, 4, kUpdConvert, "h128x16_s8_a4"),
+    SB200_VARIANT_H(64, 8, 8, 4, 4, kUpdConvert, "h64x8_s8_a4"),
+    SB200_VARIANT_H(32, 16, 8, 4, 4, kUpdConvert, "h32x16_s8_a4"),
+    SB200_VARIANT_H(64, 16, 8, 4, 8, kUpdConvert, "h64x16_s8_a4_u8"),
+    SB200_VARIANT_H(64, 32, 8, 4, 8, kUpdConvert, "h64x32_s8_a4_u8"),
+    SB200_VARIANT_H(128, 16, 8, 4, 8, kUpdConvert, "h128x16_s8_a4_u8"),
+    SB200_VARIANT_H(64, 16, 8, 4, 4, kUpdMixedSub, "h64x16_s8_a4_ms"),
+    SB200_VARIANT_H(64, 32, 8, 4, 4, kUpdMixedSub, "h64x32_s8_a4_ms"),
+    SB200_VARIANT_H(128, 16, 8, 4, 4, kUpdMixedSub, "h128x16_s8_a4_ms"),
 };
 constexpr int kNumF16 = sizeof(kF16) / sizeof(kF16[0]);
 
@@ -705,7 +671,7 @@ F16Args make_f16_args(int TX, int TY, const GridDesc& g, int zchunks, uint16_t* 
 using LaunchFnB16 = cudaError_t (*)(const ShotF16*, const int4*, int, BatchQueue*, unsigned, int,
                                     cudaStream_t);
 
-template <int TX, int TY, int S, int AUX, int UNR, int SYNC>
+template <int TX, int TY, int S, int AUX, int UNR, int UPD>
 int resident_batch_f16() {
     using P = ShapeH<TX, TY, S, AUX>;
     static int cached[64] = {};
@@ -714,13 +680,13 @@ int resident_batch_f16() {
     if (cached[dev & 63] > 0) return cached[dev & 63];
     const int smem = static_cast<int>(P::SMEM);
     int n = 0;
-    if (cudaFuncSetAttribute(batch_f16_kernel<TX, TY, S, AUX, 0, UNR, SYNC>,
+    if (cudaFuncSetAttribute(batch_f16_kernel<TX, TY, S, AUX, 0, UNR, UPD>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
-        cudaFuncSetAttribute(batch_f16_kernel<TX, TY, S, AUX, 1, UNR, SYNC>,
+        cudaFuncSetAttribute(batch_f16_kernel<TX, TY, S, AUX, 1, UNR, UPD>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
-        cudaFuncSetAttribute(batch_f16_kernel<TX, TY, S, AUX, 2, UNR, SYNC>,
+        cudaFuncSetAttribute(batch_f16_kernel<TX, TY, S, AUX, 2, UNR, UPD>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_f16_kernel<TX, TY, S, AUX, 0, UNR, SYNC>,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_f16_kernel<TX, TY, S, AUX, 0, UNR, UPD>,
                                                       P::NT, P::SMEM) == cudaSuccess &&
         n > 0) {
         cached[dev & 63] = n;
@@ -730,19 +696,19 @@ int resident_batch_f16() {
     return std::max(1, std::min(int((228u * 1024u) / (P::SMEM + 1024u)), 65536 / (P::NT * 128)));
 }
 
-template <int TX, int TY, int S, int AUX, int UNR, int SYNC>
+template <int TX, int TY, int S, int AUX, int UNR, int UPD>
 cudaError_t launch_batch_f16_t(const ShotF16* shots, const int4* items, int n_items,
                                BatchQueue* queue, unsigned ctas, int phase, cudaStream_t stream) {
     using P = ShapeH<TX, TY, S, AUX>;
-    resident_batch_f16<TX, TY, S, AUX, UNR, SYNC>();  // sets the attributes once per device
+    resident_batch_f16<TX, TY, S, AUX, UNR, UPD>();  // sets the attributes once per device
     if (phase == 1)
-        batch_f16_kernel<TX, TY, S, AUX, 1, UNR, SYNC><<<ctas, P::NT, P::SMEM, stream>>>(shots, items,
+        batch_f16_kernel<TX, TY, S, AUX, 1, UNR, UPD><<<ctas, P::NT, P::SMEM, stream>>>(shots, items,
                                                                                     n_items, queue);
     else if (phase == 2)
-        batch_f16_kernel<TX, TY, S, AUX, 2, UNR, SYNC><<<ctas, P::NT, P::SMEM, stream>>>(shots, items,
+        batch_f16_kernel<TX, TY, S, AUX, 2, UNR, UPD><<<ctas, P::NT, P::SMEM, stream>>>(shots, items,
                                                                                     n_items, queue);
     else
-        batch_f16_kernel<TX, TY, S, AUX, 0, UNR, SYNC><<<ctas, P::NT, P::SMEM, stream>>>(shots, items,
+        batch_f16_kernel<TX, TY, S, AUX, 0, UNR, UPD><<<ctas, P::NT, P::SMEM, stream>>>(shots, items,
                                                                                     n_items, queue);
     return cudaGetLastError();
 }
@@ -755,14 +721,12 @@ struct VariantB16 {
 };
 
 const VariantB16 kBatchF16[] = {
-    {64, 16, "bh64x16_s8_a4", &launch_batch_f16_t<64, 16, 8, 4, 4, 1>,
-     &resident_batch_f16<64, 16, 8, 4, 4, 1>},
-    {32, 16, "bh32x16_s8_a4", &launch_batch_f16_t<32, 16, 8, 4, 4, 1>,
-     &resident_batch_f16<32, 16, 8, 4, 4, 1>},
-    {64, 8, "bh64x8_s8_a4", &launch_batch_f16_t<64, 8, 8, 4, 4, 1>,
-     &resident_batch_f16<64, 8, 8, 4, 4, 1>},
-    {64, 16, "bh64x16_s8_a4_b", &launch_batch_f16_t<64, 16, 8, 4, 4, 0>,
-     &resident_batch_f16<64, 16, 8, 4, 4, 0>},
+    {64, 16, "bh64x16_s8_a4", &launch_batch_f16_t<64, 16, 8, 4, 4, kUpdConvert>,
+     &resident_batch_f16<64, 16, 8, 4, 4, kUpdConvert>},
+    {32, 16, "bh32x16_s8_a4", &launch_batch_f16_t<32, 16, 8, 4, 4, kUpdConvert>,
+     &resident_batch_f16<32, 16, 8, 4, 4, kUpdConvert>},
+    {64, 8, "bh64x8_s8_a4", &launch_batch_f16_t<64, 8, 8, 4, 4, kUpdConvert>,
+     &resident_batch_f16<64, 8, 8, 4, 4, kUpdConvert>},
 };
 constexpr int kNumBatchF16 = sizeof(kBatchF16) / sizeof(kBatchF16[0]);
 

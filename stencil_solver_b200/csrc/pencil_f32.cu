@@ -42,10 +42,7 @@ namespace sb200 {
 
 namespace {
 
-// The kind of a sweep (low two bits) and, as a flag, how ring stages pass
-// between warps: kModeHandoff = by StageHandoff (no CTA barrier per plane),
-// else a CTA barrier per plane.
-enum Mode : int { kModeAcoustic = 0, kModeHeat = 1, kModePrepass = 2, kModeHandoff = 4 };
+enum Mode : int { kModeAcoustic = 0, kModeHeat = 1, kModePrepass = 2 };
 
 template <int TX, int TY, int RPT, int S, int AUX>
 struct Shape {
@@ -82,15 +79,10 @@ template <int TX, int TY, int RPT, int S, int AUX, int MODE>
 __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUtensorMap* qmap,
                                             const CUtensorMap* vmap, const PencilArgs& a,
                                             int tile_x, int tile_y, int zc, float* sm,
-                                            uint64_t* full, uint64_t* auxf, Ring& ring,
-                                            StageHandoff<S, (AUX > 0 ? AUX : 1)>* hs) {
+                                            uint64_t* full, uint64_t* auxf, Ring& ring) {
     using P = Shape<TX, TY, RPT, S, AUX>;
-    constexpr int KIND = MODE & 3;
-    constexpr bool HO = (MODE & kModeHandoff) != 0;
-    constexpr bool HEAT = KIND == kModeHeat;
-    constexpr bool PRE = KIND == kModePrepass;
-    static_assert(P::NT % 32 == 0, "whole warps");
-    constexpr uint32_t kWarps = P::NT / 32;
+    constexpr bool HEAT = MODE == kModeHeat;
+    constexpr bool PRE = MODE == kModePrepass;
     constexpr bool kAuxTma = !HEAT && AUX > 0;
     constexpr int NAUX = AUX > 0 ? AUX : 1;
     float* aux = sm + S * P::PLANE;  // AUX stages of [p_prev tile | vel2 tile]
@@ -107,55 +99,21 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
     const uint32_t pb = ring.p;        // sequence number of plane 0
     const uint32_t ab = ring.aux;      // sequence number of aux iteration 0
 
-    // Barrier mode: thread 0 issues every copy and tracks the highest one.
-    // Hand-off mode: the warp that completes a stage's count issues its refill,
-    // and the highest issued indices live in `hs`.
-    int issued_hi = -1;      // barrier mode: highest p plane handed to TMA
-    int aux_issued_hi = -1;  // barrier mode: highest aux iteration handed to TMA
-    auto issue_plane = [&](int j) {
+    int issued_hi = -1;      // thread 0: highest p plane handed to TMA
+    int aux_issued_hi = -1;  // thread 0: highest aux iteration handed to TMA
+    auto issue_plane = [&](int j) {  // thread 0 only
         const uint32_t s = (pb + j) % S;
         mbar_arrive_expect_tx(&full[s], P::PLANE_BYTES);
         tma_load_3d(sm + s * P::PLANE, pmap, &full[s], x0 - R, y0 - R, zb - R + j);
-        if (HO)
-            atomicMax(&hs->issued_p, j);
-        else
-            issued_hi = j;
+        issued_hi = j;
     };
-    auto issue_aux = [&](int it) {
+    auto issue_aux = [&](int it) {  // thread 0 only
         const uint32_t s = (ab + it) % NAUX;
         float* st = aux + s * 2 * P::TILE;
         mbar_arrive_expect_tx(&auxf[s], 2 * P::TILE_BYTES);
         tma_load_3d(st, qmap, &auxf[s], x0, y0, zb + it);
         tma_load_3d(st + P::TILE, vmap, &auxf[s], x0, y0, zb + it);
-        if (HO)
-            atomicMax(&hs->issued_a, it);
-        else
-            aux_issued_hi = it;
-    };
-    const bool lane0 = (threadIdx.x & 31) == 0;
-    auto release_plane = [&](int j) {  // hand-off mode: this warp is done with plane j
-        if (!HO || j + S >= nplanes) return;
-        __syncwarp();
-        if (lane0) {
-            uint32_t* c = &hs->done_p[(pb + j) % S];
-            if (atom_add_relaxed_shared(c, 1u) == kWarps - 1) {
-                atomicExch(c, 0u);
-                fence_proxy_async_shared();
-                issue_plane(j + S);
-            }
-        }
-    };
-    auto release_aux = [&](int it) {  // hand-off mode: this warp is done with aux `it`
-        if (!HO || !kAuxTma || it + NAUX >= nint) return;
-        __syncwarp();
-        if (lane0) {
-            uint32_t* c = &hs->done_a[(ab + it) % NAUX];
-            if (atom_add_relaxed_shared(c, 1u) == kWarps - 1) {
-                atomicExch(c, 0u);
-                fence_proxy_async_shared();
-                issue_aux(it + NAUX);
-            }
-        }
+        aux_issued_hi = it;
     };
     auto wait_plane = [&](int j) {
         return mbar_wait(&full[(pb + j) % S], ((pb + j) / S) & 1);
@@ -171,7 +129,6 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
             prefetch_tmap(qmap);
             prefetch_tmap(vmap);
         }
-        if (HO) hs->issued_p = hs->issued_a = -1;
         for (int s = 0; s < S && s < nplanes; ++s) issue_plane(s);
         if (kAuxTma)
             for (int it = 0; it < NAUX && it < nint; ++it) issue_aux(it);
@@ -189,7 +146,7 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
 
     // Source ownership: which (row, lane element) of this thread, if any.
     int src_j = -1, src_i = -1;
-    if (KIND == kModeAcoustic && a.src_z >= 0 && a.src_x >= gx && a.src_x < gx + 4 && a.src_y >= gy &&
+    if (MODE == kModeAcoustic && a.src_z >= 0 && a.src_x >= gx && a.src_x < gx + 4 && a.src_y >= gy &&
         a.src_y < gy + RPT && xin) {
         src_j = a.src_y - gy;
         src_i = a.src_x - gx;
@@ -216,7 +173,6 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
         for (int j = 0; j < RPT; ++j) q[jj][j] = lds128(pl + j * P::SX);
     }
     bool abort_run = __syncthreads_or(bad) != 0;
-    if (HO && abort_run && tid == 0) hs->abort = 1;
     if (!abort_run && tid == 0) {
         // Planes 0..3 are only queue feed: their stages are free again.
 #pragma unroll
@@ -319,7 +275,6 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
                         }
                     }
                 }
-                release_plane(i + 4);  // the centre plane's last reads are done
                 if (kAuxTma) {
                     if (!wait_aux(i)) bad = true;
                     const float* st = aux + ((ab + i) % NAUX) * 2 * P::TILE + aoff;
@@ -328,7 +283,6 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
                         pv[j] = lds128(st + j * TX);
                         vv[j] = lds128(st + P::TILE + j * TX);
                     }
-                    release_aux(i);
                 }
                 // Update and store.
                 const int z = zb + i;
@@ -375,28 +329,17 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
                     if (rin[j]) stg_stream(a.next + goff + j * a.sy, o);
                 }
                 goff += a.sz;
-                if (HO) {
-                    if (bad) *reinterpret_cast<volatile int*>(&hs->abort) = 1;
-                    abort_run = *reinterpret_cast<volatile int*>(&hs->abort) != 0;
-                } else {
-                    // The stages of plane z (p) and of iteration i (aux) are free
-                    // now: refill them S planes / AUX iterations ahead.
-                    abort_run = __syncthreads_or(bad) != 0;
-                    if (!abort_run && tid == 0) {
-                        if (i + 4 + S < nplanes) issue_plane(i + 4 + S);
-                        if (kAuxTma && i + NAUX < nint) issue_aux(i + NAUX);
-                    }
+                // The stages of plane z (p) and of iteration i (aux) are free now:
+                // refill them S planes / AUX iterations ahead.
+                abort_run = __syncthreads_or(bad) != 0;
+                if (!abort_run && tid == 0) {
+                    if (i + 4 + S < nplanes) issue_plane(i + 4 + S);
+                    if (kAuxTma && i + NAUX < nint) issue_aux(i + NAUX);
                 }
             }
         }
     }
 
-    if (HO) {
-        __syncthreads();  // every warp has left the plane loop
-        abort_run = hs->abort != 0;
-        issued_hi = hs->issued_p;
-        aux_issued_hi = hs->issued_a;
-    }
     if (abort_run) {
         if (tid == 0) {
             record_error(a.err, kDevWaitTimeout);
@@ -442,8 +385,6 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S, AUX>::NT, Shape<TX, TY, 
     extern __shared__ unsigned char dsmem[];
     __shared__ __align__(8) uint64_t full[S];
     __shared__ __align__(8) uint64_t auxf[NAUX];
-    __shared__ StageHandoff<S, NAUX> hs;
-    if ((MODE & kModeHandoff) && threadIdx.x == 0) init_handoff(&hs);
     float* sm = setup_rings<TX, TY, RPT, S, AUX>(dsmem, full, auxf);
     int b = blockIdx.x;
     const int tx = b % a.tiles_x;
@@ -452,7 +393,7 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S, AUX>::NT, Shape<TX, TY, 
     b /= a.tiles_y;
     Ring ring;
     (void)pencil_tile<TX, TY, RPT, S, AUX, MODE>(&pmap, &qmap, &vmap, a, tx, ty, b, sm, full,
-                                                 auxf, ring, &hs);
+                                                 auxf, ring);
 }
 
 // Many grids (shots) in one persistent launch.  Each CTA takes work items --
@@ -481,7 +422,7 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S, AUX>::NT, Shape<TX, TY, 
         const ShotF32* sh = shots + w.x;
         const PencilArgs a = sh->args;
         if (!pencil_tile<TX, TY, RPT, S, AUX, kModeAcoustic>(&sh->p, &sh->prev, &sh->vel2, a, w.y, w.z,
-                                                     w.w, sm, full, auxf, ring, nullptr))
+                                                     w.w, sm, full, auxf, ring))
             break;
     }
     if (threadIdx.x == 0) {
@@ -544,24 +485,21 @@ struct Variant {
 };
 
 // The prepass launcher of an acoustic tile (heat tiles have none).
-template <int TX, int TY, int RPT, int S, int AUX, bool HEAT, int FLAGS>
+template <int TX, int TY, int RPT, int S, int AUX, bool HEAT>
 constexpr LaunchFn prepass_launcher() {
     if constexpr (HEAT)
         return nullptr;
     else
-        return &launch_variant<TX, TY, RPT, S, AUX, kModePrepass | FLAGS>;
+        return &launch_variant<TX, TY, RPT, S, AUX, kModePrepass>;
 }
 
-// FLAGS: kModeHandoff for tiles whose warps hand ring stages to each other.
-#define SB200_VARIANT_F(TX, TY, RPT, S, AUX, HEAT, FLAGS, NAME)                              \
+#define SB200_VARIANT(TX, TY, RPT, S, AUX, HEAT, NAME)                                       \
     Variant {                                                                                \
         TX, TY, RPT, S, AUX, NAME,                                                           \
-            &launch_variant<TX, TY, RPT, S, AUX, (HEAT ? kModeHeat : kModeAcoustic) | FLAGS>, \
-            &resident_variant<TX, TY, RPT, S, AUX, (HEAT ? kModeHeat : kModeAcoustic) | FLAGS>, \
-            prepass_launcher<TX, TY, RPT, S, AUX, HEAT, FLAGS>()                             \
+            &launch_variant<TX, TY, RPT, S, AUX, HEAT ? kModeHeat : kModeAcoustic>,          \
+            &resident_variant<TX, TY, RPT, S, AUX, HEAT ? kModeHeat : kModeAcoustic>,        \
+            prepass_launcher<TX, TY, RPT, S, AUX, HEAT>()                                    \
     }
-#define SB200_VARIANT(TX, TY, RPT, S, AUX, HEAT, NAME) \
-    SB200_VARIANT_F(TX, TY, RPT, S, AUX, HEAT, 0, NAME)
 
 // Index 0 of each table is the default when no tuned choice exists.
 const Variant kWave[] = {
@@ -572,8 +510,6 @@ const Variant kWave[] = {
     SB200_VARIANT(32, 16, 1, 8, 4, false, "t32x16_r1_s8_a4"),
     SB200_VARIANT(64, 32, 2, 8, 3, false, "t64x32_r2_s8_a3"),
     SB200_VARIANT(32, 64, 2, 8, 3, false, "t32x64_r2_s8_a3"),
-    SB200_VARIANT_F(64, 32, 2, 8, 3, false, kModeHandoff, "t64x32_r2_s8_a3_h"),
-    SB200_VARIANT_F(64, 16, 2, 8, 3, false, kModeHandoff, "t64x16_r2_s8_a3_h"),
 };
 const Variant kHeat[] = {
     SB200_VARIANT(32, 32, 2, 8, 0, true, "t32x32_r2_s8"),
@@ -581,13 +517,7 @@ const Variant kHeat[] = {
     SB200_VARIANT(32, 16, 1, 8, 0, true, "t32x16_r1_s8"),
     SB200_VARIANT(64, 32, 2, 8, 0, true, "t64x32_r2_s8"),
     SB200_VARIANT(32, 64, 2, 8, 0, true, "t32x64_r2_s8"),
-    SB200_VARIANT(64, 24, 2, 8, 0, true, "t64x24_r2_s8"),
     SB200_VARIANT(128, 16, 2, 8, 0, true, "t128x16_r2_s8"),
-    SB200_VARIANT(64, 8, 2, 8, 0, true, "t64x8_r2_s8"),
-    SB200_VARIANT(64, 16, 2, 12, 0, true, "t64x16_r2_s12"),
-    SB200_VARIANT_F(64, 16, 2, 8, 0, true, kModeHandoff, "t64x16_r2_s8_h"),
-    SB200_VARIANT_F(128, 16, 2, 8, 0, true, kModeHandoff, "t128x16_r2_s8_h"),
-    SB200_VARIANT_F(64, 32, 2, 8, 0, true, kModeHandoff, "t64x32_r2_s8_h"),
 };
 constexpr int kNumWave = sizeof(kWave) / sizeof(kWave[0]);
 constexpr int kNumHeat = sizeof(kHeat) / sizeof(kHeat[0]);

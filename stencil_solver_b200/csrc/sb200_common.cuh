@@ -213,49 +213,4 @@ __device__ __forceinline__ float2 pair_of(const float4& v, int h) {
     return h == 0 ? make_float2(v.x, v.y) : make_float2(v.z, v.w);
 }
 
-// Shared-memory hand-off of ring stages between the warps of a CTA, in place of
-// a CTA barrier per plane: a warp that has read the last it needs of a stage
-// counts itself done (a shared-memory atomic after __syncwarp), and the warp that
-// completes the count refills the stage by TMA.  No warp waits for another; a
-// warp at plane iteration k needs only refills released at iterations <= k - 4,
-// which every warp, the slowest included, has passed.  The count is a relaxed
-// atomic: an acquire-release one also orders the warp's outstanding global
-// stores (a fence per plane that waited on DRAM writes: 2.24 ms per 1024^3 step
-// against 1.62), while the stage reads it must follow are shared-memory loads,
-// which the shared-memory pipe completes in issue order before the warp's later
-// atomic on the counter.
-template <int S, int AUX>
-struct StageHandoff {
-    uint32_t done_p[S];    // warps done with the plane in each p stage
-    uint32_t done_a[AUX];  // warps done with each aux stage
-    int issued_p;          // highest plane index of this tile handed to TMA
-    int issued_a;          // highest aux iteration of this tile handed to TMA
-    int abort;             // a bounded wait gave up somewhere in the CTA
-};
-
-template <int S, int AUX>
-__device__ __forceinline__ void init_handoff(StageHandoff<S, AUX>* hs) {
-#pragma unroll
-    for (int s = 0; s < S; ++s) hs->done_p[s] = 0u;
-#pragma unroll
-    for (int s = 0; s < AUX; ++s) hs->done_a[s] = 0u;
-    hs->issued_p = hs->issued_a = -1;
-    hs->abort = 0;
-}
-
-__device__ __forceinline__ uint32_t atom_add_relaxed_shared(uint32_t* p, uint32_t v) {
-    uint32_t old;
-    asm volatile("atom.relaxed.cta.shared::cta.add.u32 %0, [%1], %2;"
-                 : "=r"(old)
-                 : "r"(smem_u32(p)), "r"(v)
-                 : "memory");
-    return old;
-}
-
-// Orders the generic-proxy view of shared memory before the async-proxy (TMA)
-// write that refills a stage.
-__device__ __forceinline__ void fence_proxy_async_shared() {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
 }  // namespace sb200
