@@ -605,7 +605,8 @@ def secondary_learned(train_models: int = 16, nc_eval: int = 516, coarse_steps: 
         "fine_ms": ms_fine, "plain_coarse_ms": ms_plain, "learned_coarse_ms": ms_learned,
         "rel_l2_plain_coarse": err_plain, "rel_l2_learned_coarse": err_learned,
         "judged": {"bound": 1e-3, "ms": rep.ms, "fallback_at_step": rep.fallback_at,
-                   "proxy_checks": rep.checks, "rel_l2": err_judged,
+                   "network_off_at_step": rep.network_off_at,
+                   "proxy_checks_step_corrected_uncorrected": rep.checks, "rel_l2": err_judged,
                    "speedup_vs_fine": ms_fine / rep.ms},
         "velocity": f"layered, smoothed over {smooth} coarse cells",
         "source": f"25 Hz Ricker on a Gaussian of {sigma} coarse cells",

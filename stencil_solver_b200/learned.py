@@ -519,21 +519,25 @@ def proxy_of(pb: Problem, nc_proxy: int = 64) -> Problem:
 class SolveReport:
     steps: int                # coarse steps asked for
     fallback_at: object       # coarse step at which the judge tripped, or None
-    checks: list              # (coarse step, the proxy's relative L2 error)
+    checks: list              # (coarse step, proxy rel L2 of the corrected solve, of the plain one)
     ms: float                 # device time of the whole solve
     field: object             # result on the coarse grid (restricted fine solve after a fallback)
+    network_off_at: object = None  # coarse step after which the network was switched off, or None
 
 
 def learned_solve(pb: Problem, coarse_steps: int, mlp: Mlp, bound: float = 1e-3,
-                  check_every: int = 20, nc_proxy: int = 64) -> SolveReport:
+                  check_every: int = 20, nc_proxy: int = 64, rival: bool = True) -> SolveReport:
     """Corrected coarse solve with the plain fine solver as judge and fallback.
 
     A proxy pair (proxy_of) is advanced alongside the main coarse solve: its
-    plain fine solve (2 steps per coarse step) and its corrected coarse solve.
-    Every check_every coarse steps the proxy's corrected field is compared with
-    its restricted fine field; when the relative L2 error exceeds `bound` the
-    corrected solve is abandoned and the plain fine solve computes the answer.
-    Device time (CUDA events) covers everything, fallback included."""
+    plain fine solve (2 steps per coarse step), its corrected coarse solve and,
+    with `rival`, its coarse solve without the network.  Every check_every
+    coarse steps the proxy's coarse fields are compared with its restricted fine
+    field.  When the corrected proxy is further from the fine one than the
+    uncorrected one, the network is switched off for the rest of the solve (main
+    and proxy); when the proxy of the method in use exceeds `bound`, the coarse
+    solve is abandoned and the plain fine solve computes the answer.  Device time
+    (CUDA events) covers everything, fallback included."""
     torch = _torch()
     vf, vc = pb.device_models()
     px = proxy_of(pb, nc_proxy)
@@ -546,6 +550,8 @@ def learned_solve(pb: Problem, coarse_steps: int, mlp: Mlp, bound: float = 1e-3,
     q = torch.zeros(g.shape, device="cuda")
     pp = torch.zeros(gp.shape, device="cuda")
     pq = torch.zeros(gp.shape, device="cuda")
+    rp = torch.zeros(gp.shape, device="cuda") if rival else None  # proxy without the network
+    rq = torch.zeros(gp.shape, device="cuda") if rival else None
     fp = torch.zeros(gpf.shape, device="cuda")
     fq = torch.zeros(gpf.shape, device="cuda")
     judge = torch.empty(gp.shape, device="cuda")
@@ -556,14 +562,18 @@ def learned_solve(pb: Problem, coarse_steps: int, mlp: Mlp, bound: float = 1e-3,
     wf = px.wavelet(True, 2 * coarse_steps)
     src, psrc, pfsrc = pb.source(False), px.source(False), px.source(True)
     fl, pfl = new_flags(mlp, g, pb.compose_state), new_flags(mlp, gp, pb.compose_state)
-    checks, fallback = [], None
+    net = mlp
+    checks, fallback, off_at = [], None, None
     for m in range(coarse_steps):
-        coarse_step(pb, vc, p, q, src, w, m, mlp, flags=_flag_args(fl), r=r)
+        coarse_step(pb, vc, p, q, src, w, m, net, flags=_flag_args(fl) if net else None, r=r)
         p, q = q, p
         _rotate(fl)
-        coarse_step(px, pvc, pp, pq, psrc, wp, m, mlp, flags=_flag_args(pfl), r=pr)
+        coarse_step(px, pvc, pp, pq, psrc, wp, m, net, flags=_flag_args(pfl) if net else None, r=pr)
         pp, pq = pq, pp
         _rotate(pfl)
+        if rival and net is not None:
+            coarse_step(px, pvc, rp, rq, psrc, wp, m, None, r=pr)
+            rp, rq = rq, rp
         for k in (2 * m, 2 * m + 1):
             wave_step(fp, fq, pvf, fq, gpf)
             _inject(px, True, fq, pfsrc, wf, k)
@@ -571,7 +581,15 @@ def learned_solve(pb: Problem, coarse_steps: int, mlp: Mlp, bound: float = 1e-3,
         if (m + 1) % check_every == 0 or m + 1 == coarse_steps:
             restrict2(fp, gpf, judge, gp, OFFSET)
             err = rel_l2(pp, judge)
-            checks.append((m + 1, err))
+            err_rival = rel_l2(rp, judge) if rival and net is not None else None
+            checks.append((m + 1, err, err_rival))
+            if err_rival is not None and err_rival < err:
+                # the network loses on the proxy: carry on without it from the
+                # uncorrected proxy state (its history is the uncorrected one)
+                net, off_at = None, m + 1
+                pp.copy_(rp)
+                pq.copy_(rq)
+                err = err_rival
             if err > bound:
                 fallback = m + 1
                 break
@@ -583,7 +601,7 @@ def learned_solve(pb: Problem, coarse_steps: int, mlp: Mlp, bound: float = 1e-3,
         del ff
     e1.record()
     torch.cuda.synchronize()
-    return SolveReport(coarse_steps, fallback, checks, e0.elapsed_time(e1), p)
+    return SolveReport(coarse_steps, fallback, checks, e0.elapsed_time(e1), p, off_at)
 
 
 def time_fine_solve(pb: Problem, fine_steps: int):

@@ -114,7 +114,7 @@ def test_source_composition_lowers_the_early_corrected_error(trained):
 def test_judged_solve_without_fallback_is_the_corrected_solve(trained):
     mlp, _ = trained
     pb = mk80(77)
-    rep = learned.learned_solve(pb, 60, mlp, bound=1.0, check_every=20)
+    rep = learned.learned_solve(pb, 60, mlp, bound=1.0, check_every=20, rival=False)
     assert rep.fallback_at is None and [c[0] for c in rep.checks] == [20, 40, 60]
     _, vc = pb.device_models()
     ref = learned.coarse_solve(pb, vc, 60, mlp)
@@ -128,3 +128,28 @@ def test_judged_solve_falls_back_to_the_fine_solve(trained):
     assert rep.fallback_at == 10 and len(rep.checks) == 1 and rep.checks[0][1] > 1e-12
     _, ref = learned.time_fine_solve(pb, 80)
     assert bool((rep.field == ref).all())
+
+
+def test_composition_prepass_beats_the_plain_coarse_step(torch_cuda):
+    """The coarse step with the two-step composition term (sb200_wave_prepass_f32:
+    h^4 L^2 p, h = dt / 2) against the plain coarse step, both against the
+    restricted plain fine solve of an unseen smoothed layered model."""
+    errs = {comp: learned.evaluate(mk80(97, compose_state=comp), 120, None)["plain"]
+            for comp in (False, True)}
+    print("composition pre-pass", errs)
+    assert errs[True] < 0.2 * errs[False], errs
+
+
+def test_judge_switches_off_a_network_that_loses(trained):
+    """The judge runs the proxy with and without the network: a network that
+    gains stays on; one that loses is switched off at the first check and the
+    solve carries on without it.  The network trained on the plain step's
+    residual double-counts the L^2 term on a pre-passed step, so it loses there."""
+    mlp, _ = trained
+    rep = learned.learned_solve(mk80(76), 40, mlp, bound=1.0, check_every=20)
+    assert rep.network_off_at is None and rep.checks[0][1] < rep.checks[0][2], rep.checks
+    pbc = mk80(76, compose_state=True)
+    rep = learned.learned_solve(pbc, 40, mlp, bound=1.0, check_every=20)
+    assert rep.network_off_at == 20 and rep.fallback_at is None, rep.checks
+    assert rep.checks[0][1] > rep.checks[0][2]
+    assert rep.checks[1][2] is None  # no rival once the network is off
