@@ -117,6 +117,32 @@ __device__ __forceinline__ float2 subhf2(uint32_t w, float2 b) {
     return make_float2(x, y);
 }
 
+// c + f32(half `hi` of word w) * f32(half m): the sm_100 mixed-precision FMA (the
+// product of two halves is exact in FP32, so one rounding, as an FP32 FMA of the
+// same values).
+__device__ __forceinline__ float fmahf(uint32_t w, int hi, uint16_t m, float c) {
+    float d;
+    if (hi)
+        asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %1;\n\t"
+            "fma.rn.f32.f16 %0, hi, %2, %3;\n\t}"
+            : "=f"(d)
+            : "r"(w), "h"(m), "f"(c));
+    else
+        asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %1;\n\t"
+            "fma.rn.f32.f16 %0, lo, %2, %3;\n\t}"
+            : "=f"(d)
+            : "r"(w), "h"(m), "f"(c));
+    return d;
+}
+
+// The y weights of an isotropic x-y grid scaled by 5040, the least common
+// multiple of the coefficients' denominators: 8064, -1008, 128, -9, all exact
+// halves (FDCoeffs<4> c_1..c_4 = 8/5, -1/5, 8/315, -1/560).
+__host__ __device__ constexpr uint16_t y_weight5040(int r) {  // r = 1..4
+    return r == 1 ? 0x6FE0u : r == 2 ? 0xE3E0u : r == 3 ? 0x5800u : 0xC880u;
+}
+constexpr float kInv5040 = 1.0f / 5040.0f;
+
 // f32(half `hi` of word w) + c (the mixed add on one point).
 __device__ __forceinline__ float addhf(uint32_t w, int hi, float c) {
     float d;
@@ -164,7 +190,12 @@ struct RingH {
 //                 on the way and gives -p_next, whose sign the rescale factor
 //                 (PHASE 1) or the packed halves' sign bits (PHASE 0) restore;
 //                 PHASE 2 (p_prev rescaled) uses kUpdConvert.
-constexpr int kUpdConvert = 0, kUpdMixedSub = 1;
+// and, as a flag, the y pairs:
+//   kUpdExactY:   on a grid with dx == dy each y neighbour enters through one
+//                 mixed-precision FMA with the 5040-scaled weights (no conversion,
+//                 no pair add), accumulated apart and scaled by 1/5040 once;
+//                 without it a y pair costs a conversion, a mixed add and an FMA.
+constexpr int kUpdConvert = 0, kUpdMixedSub = 1, kUpdExactY = 2;
 
 // One tile: columns [tx TX, tx TX + TX) x rows [4 + ty TY, ...) of the interior,
 // marched over z chunk zc.  All threads of the CTA call it; `sm`, `full` and
@@ -319,6 +350,7 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                 for (int h = 0; h < 4; ++h) {
                     const float2 c = cv[h];
                     float2 txy = mul2(cxy2, c);
+                    float2 ty = make_float2(0.f, 0.f);  // kUpdExactY: 5040 x the y pairs
                     float2 tz = mul2(az2[0], addhf2(get_word(hq[(u + 1) % 4], h),
                                                     dq[(u + 3) % 4][h]));
 #pragma unroll
@@ -329,9 +361,17 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                                                : make_float2(xsum1(cf, lf, rt, 2 * h, r),
                                                              xsum1(cf, lf, rt, 2 * h + 1, r));
                         txy = fma2(ax2[r - 1], sx, txy);
-                        txy = fma2(ay2[r - 1],
-                                   addhf2(get_word(yu[r - 1], h), h2f2(get_word(yd[r - 1], h))),
-                                   txy);
+                        if (UPD & kUpdExactY) {
+                            const uint16_t wy = y_weight5040(r);
+                            ty.x = fmahf(get_word(yu[r - 1], h), 0, wy, ty.x);
+                            ty.y = fmahf(get_word(yu[r - 1], h), 1, wy, ty.y);
+                            ty.x = fmahf(get_word(yd[r - 1], h), 0, wy, ty.x);
+                            ty.y = fmahf(get_word(yd[r - 1], h), 1, wy, ty.y);
+                        } else {
+                            txy = fma2(ay2[r - 1],
+                                       addhf2(get_word(yu[r - 1], h), h2f2(get_word(yd[r - 1], h))),
+                                       txy);
+                        }
                         // up: plane z + r (FP16, slot (u + r) % 4; r = 4 is the plane
                         // just fed); down: plane z - r (FP32, slot (u + 4 - r) % 4)
                         if (r > 1)
@@ -339,6 +379,7 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                                                          dq[(u + 4 - r) % 4][h]),
                                       tz);
                     }
+                    if (UPD & kUpdExactY) txy = fma2(dup2(kInv5040), ty, txy);
                     lap[h] = add2(txy, tz);
                 }
                 // plane z - 4 is no longer needed: its slot takes the centre (z).
@@ -358,7 +399,7 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                 const uint4 qv = lds128h(st);
                 const uint4 kv = lds128h(st + P::TILE);
                 // kNeg: o holds -p_next (see kUpdMixedSub)
-                constexpr bool kMixed = UPD == kUpdMixedSub && PHASE != 2;
+                constexpr bool kMixed = (UPD & kUpdMixedSub) && PHASE != 2;
                 constexpr bool kNeg = kMixed && PHASE == 0;
                 float o[8];
 #pragma unroll
@@ -563,7 +604,7 @@ cudaError_t launch_f16(const PencilMaps& m, const F16Args& a, unsigned ctas, int
 }
 
 struct VariantH {
-    int tx, ty, stages, aux;
+    int tx, ty, stages, aux, unr, upd;
     const char* name;
     LaunchFnH launch;
     ResidentFnH resident;
@@ -571,11 +612,12 @@ struct VariantH {
 
 #define SB200_VARIANT_H(TX, TY, S, AUX, UNR, UPD, NAME)                                    \
     VariantH {                                                                               \
-        TX, TY, S, AUX, NAME, &launch_f16<TX, TY, S, AUX, UNR, UPD>,                        \
+        TX, TY, S, AUX, UNR, UPD, NAME, &launch_f16<TX, TY, S, AUX, UNR, UPD>,              \
             &resident_f16<TX, TY, S, AUX, UNR, UPD>                                          \
     }
 
-// "_u8": the plane loop unrolled by 8 instead of 4; "_ms": the kUpdMixedSub update.
+// "_u8": the plane loop unrolled by 8 instead of 4; "_ms": the kUpdMixedSub update;
+// "_ye": kUpdExactY (on grids with dx != dy the same tile without it runs).
 const VariantH kF16[] = {
     SB200_VARIANT_H(64, 16, 8, 4, 4, kUpdConvert, "h64x16_s8_a4"),
     SB200_VARIANT_H(64, 32, 8, 4, 4, kUpdConvert, "h64x32_s8_a4"),
@@ -588,6 +630,10 @@ const VariantH kF16[] = {
     SB200_VARIANT_H(64, 16, 8, 4, 4, kUpdMixedSub, "h64x16_s8_a4_ms"),
     SB200_VARIANT_H(64, 32, 8, 4, 4, kUpdMixedSub, "h64x32_s8_a4_ms"),
     SB200_VARIANT_H(128, 16, 8, 4, 4, kUpdMixedSub, "h128x16_s8_a4_ms"),
+    SB200_VARIANT_H(64, 16, 8, 4, 4, kUpdExactY, "h64x16_s8_a4_ye"),
+    SB200_VARIANT_H(64, 32, 8, 4, 4, kUpdExactY, "h64x32_s8_a4_ye"),
+    SB200_VARIANT_H(64, 16, 8, 4, 4, kUpdMixedSub | kUpdExactY, "h64x16_s8_a4_ms_ye"),
+    SB200_VARIANT_H(64, 32, 8, 4, 4, kUpdMixedSub | kUpdExactY, "h64x32_s8_a4_ms_ye"),
 };
 constexpr int kNumF16 = sizeof(kF16) / sizeof(kF16[0]);
 
@@ -736,7 +782,19 @@ cudaError_t launch_wave_pencil_f16(const PencilMaps& maps, uint16_t* next, const
                                    const SourceDesc& src, const F16Scale* scale, int phase,
                                    const PencilConfig& cfg, int* err, cudaStream_t stream) {
     if (!g.has_interior()) return cudaSuccess;
-    const VariantH& v = kF16[cfg.variant];
+    int vi = cfg.variant;
+    if ((kF16[vi].upd & kUpdExactY) && !(g.dx == g.dy)) {
+        // the 5040-scaled weights are exact halves only for dx == dy: run the same
+        // tile shape (same tensor-map boxes) without the exact-y form
+        for (int k = 0; k < kNumF16; ++k)
+            if (kF16[k].tx == kF16[vi].tx && kF16[k].ty == kF16[vi].ty &&
+                kF16[k].stages == kF16[vi].stages && kF16[k].aux == kF16[vi].aux &&
+                kF16[k].unr == kF16[vi].unr && kF16[k].upd == (kF16[vi].upd & ~kUpdExactY)) {
+                vi = k;
+                break;
+            }
+    }
+    const VariantH& v = kF16[vi];
     const F16Args a = make_f16_args(v.tx, v.ty, g, cfg.zchunks, next, src, scale, err);
     const int inz = static_cast<int>(g.nz - 2 * R);
     const unsigned ctas = static_cast<unsigned>(int64_t(a.tiles_x) * a.tiles_y *
