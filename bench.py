@@ -570,6 +570,7 @@ def secondary_learned(train_models: int = 16, nc_eval: int = 516, coarse_steps: 
         sb.tune(sb.KIND_WAVE_F32, gg, f1, f2, vv, f3, reps=3)
         del f1, f2, f3
     torch.cuda.empty_cache()
+    vmax_c = float(vc.max().sqrt())
     ms_fine, judge = learned.time_fine_solve(pb, 2 * coarse_steps)
     # untimed: the network's parameter copy to the host after training
     learned.coarse_solve(pb, vc, 2)
@@ -605,6 +606,7 @@ def secondary_learned(train_models: int = 16, nc_eval: int = 516, coarse_steps: 
         "fine_ms": ms_fine, "plain_coarse_ms": ms_plain, "learned_coarse_ms": ms_learned,
         "rel_l2_plain_coarse": err_plain, "rel_l2_learned_coarse": err_learned,
         "judged": {"bound": 1e-3, "ms": rep.ms, "fallback_at_step": rep.fallback_at,
+                   "proxy_extent": learned.proxy_extent(pb, coarse_steps, vmax_c),
                    "network_off_at_step": rep.network_off_at,
                    "proxy_checks_step_corrected_uncorrected": rep.checks, "rel_l2": err_judged,
                    "speedup_vs_fine": ms_fine / rep.ms},

@@ -525,8 +525,20 @@ class SolveReport:
     network_off_at: object = None  # coarse step after which the network was switched off, or None
 
 
+def proxy_extent(pb: Problem, coarse_steps: int, vmax: float) -> int:
+    """Coarse extent of a proxy window that the waves from the source do not cross
+    within coarse_steps steps at speed vmax (the source's reach plus 8 cells of
+    margin on each side), a multiple of 8, at most the problem's own extent.  Its
+    walls must stay out of reach: the coarse and fine grids' near walls sit half a
+    coarse cell apart, so reflections there differ between them."""
+    reach = coarse_steps * vmax * pb.dt / pb.h + 3.5 * pb.sigma_cells + 8.0
+    n = int(math.ceil((2.0 * reach + 8.0) / 8.0)) * 8
+    return max(32, min(n, pb.nc))
+
+
 def learned_solve(pb: Problem, coarse_steps: int, mlp: Mlp, bound: float = 1e-3,
-                  check_every: int = 20, nc_proxy: int = 64, rival: bool = True) -> SolveReport:
+                  check_every: int = 20, nc_proxy: int | None = None,
+                  rival: bool = True) -> SolveReport:
     """Corrected coarse solve with the plain fine solver as judge and fallback.
 
     A proxy pair (proxy_of) is advanced alongside the main coarse solve: its
@@ -537,9 +549,12 @@ def learned_solve(pb: Problem, coarse_steps: int, mlp: Mlp, bound: float = 1e-3,
     uncorrected one, the network is switched off for the rest of the solve (main
     and proxy); when the proxy of the method in use exceeds `bound`, the coarse
     solve is abandoned and the plain fine solve computes the answer.  Device time
-    (CUDA events) covers everything, fallback included."""
+    (CUDA events) covers everything, fallback included.  nc_proxy None: the
+    proxy_extent of the solve."""
     torch = _torch()
     vf, vc = pb.device_models()
+    if nc_proxy is None:
+        nc_proxy = proxy_extent(pb, coarse_steps, float(vc.max().sqrt()))
     px = proxy_of(pb, nc_proxy)
     pvf, pvc = px.device_models()
     e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
