@@ -547,10 +547,18 @@ private:
         return cuda(cudaStreamSynchronize(st_));
     }
 
+    // FP16: the exact-y form when every shot has dx == dy (per-shot bits then
+    // equal the single-grid FP16 step's on that shot's grid).
+    bool exact_y() const {
+        for (const Shot& h : shots_)
+            if (!f16_exact_y(h.g)) return false;
+        return true;
+    }
+
     int launch(int par, int phase) {
         const cudaError_t e =
             f16_ ? launch_batch_f16(variant_, static_cast<const ShotF16*>(table_[par]), items_,
-                                    n_items_, queue_, ctas_, phase, st_)
+                                    n_items_, queue_, ctas_, phase, exact_y(), st_)
                  : launch_batch_f32(variant_, static_cast<const ShotF32*>(table_[par]), items_,
                                     n_items_, queue_, ctas_, st_);
         return cuda(e);

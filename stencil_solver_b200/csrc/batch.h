@@ -97,8 +97,13 @@ void batch_f16_prepare();
 // scale: the shot's device scale, next: its p_prev / p_next level.
 F16Args batch_f16_shot_args(int v, const GridDesc& g, int zchunks, uint16_t* next,
                             const SourceDesc& src, const F16Scale* scale, int* err);
-// phase: 0 plain, 1 renormalisation step, 2 the step after it (every shot).
+// phase: 0 plain, 1 renormalisation step, 2 the step after it (every shot);
+// exact_y: every shot has dx == dy (the FP16 step's exact-y form, as the single-grid
+// kernel takes it on such grids, so a shot gets the same bits in both).
 cudaError_t launch_batch_f16(int v, const ShotF16* shots, const int4* items, int n_items,
-                             BatchQueue* queue, unsigned ctas, int phase, cudaStream_t stream);
+                             BatchQueue* queue, unsigned ctas, int phase, bool exact_y,
+                             cudaStream_t stream);
+// Whether the FP16 step takes its exact-y form on grid g (dx == dy).
+bool f16_exact_y(const GridDesc& g);
 
 }  // namespace sb200

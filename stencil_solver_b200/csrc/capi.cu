@@ -97,8 +97,8 @@ int sm_count() {
 }
 
 // Untuned default tile of a kind: the tuner's usual pick on large grids
-// (1024^3 acoustic: t64x32_r2_s8_a3; 512^3 heat: t64x16_r2_s8), found by name so
-// the tables can be reordered.
+// (1024^3 acoustic: t64x32_r2_s8_a3; 512^3 heat: t64x16_r2_s8; FP16 1024^3:
+// h64x16_s8_a4), found by name so the tables can be reordered.
 int default_variant(int kind) {
     const char* want = kind == SB200_KIND_WAVE_F32 ? "t64x32_r2_s8_a3"
                        : kind == SB200_KIND_HEAT_F32 ? "t64x16_r2_s8"

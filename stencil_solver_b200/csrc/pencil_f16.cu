@@ -558,39 +558,54 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
 }
 
 
-using LaunchFnH = cudaError_t (*)(const PencilMaps&, const F16Args&, unsigned, int, cudaStream_t);
+using LaunchFnH = cudaError_t (*)(const PencilMaps&, const F16Args&, unsigned, int, bool,
+                                   cudaStream_t);
 using ResidentFnH = int (*)();
 
+// The two update forms every tile is compiled in: kUpdMixedSub, and with
+// kUpdExactY on grids with dx == dy (the form follows the grid, not the tile, so
+// every tile gives the same bits on a grid).
+constexpr int kFormPlain = kUpdMixedSub, kFormExactY = kUpdMixedSub | kUpdExactY;
+
 template <int TX, int TY, int S, int AUX, int UNR, int UPD>
+bool set_f16_smem(int smem) {
+    return cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, S, AUX, 0, UNR, UPD>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
+           cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, S, AUX, 1, UNR, UPD>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
+           cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, S, AUX, 2, UNR, UPD>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess;
+}
+
+template <int TX, int TY, int S, int AUX, int UNR>
 int resident_f16() {
     using P = ShapeH<TX, TY, S, AUX>;
     static int cached[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (cached[dev & 63] > 0) return cached[dev & 63];
-    auto kern = pencil_f16_kernel<TX, TY, S, AUX, 0, UNR, UPD>;
     const int smem = static_cast<int>(P::SMEM);
-    int n = 0;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) ==
+    int n = 0, n2 = 0;
+    if (set_f16_smem<TX, TY, S, AUX, UNR, kFormPlain>(smem) &&
+        set_f16_smem<TX, TY, S, AUX, UNR, kFormExactY>(smem) &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &n, pencil_f16_kernel<TX, TY, S, AUX, 0, UNR, kFormPlain>, P::NT, P::SMEM) ==
             cudaSuccess &&
-        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, S, AUX, 1, UNR, UPD>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
-        cudaFuncSetAttribute(pencil_f16_kernel<TX, TY, S, AUX, 2, UNR, UPD>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, P::NT, P::SMEM) == cudaSuccess &&
-        n > 0) {
-        cached[dev & 63] = n;
-        return n;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &n2, pencil_f16_kernel<TX, TY, S, AUX, 0, UNR, kFormExactY>, P::NT, P::SMEM) ==
+            cudaSuccess &&
+        std::min(n, n2) > 0) {
+        cached[dev & 63] = std::min(n, n2);
+        return cached[dev & 63];
     }
     cudaGetLastError();
     return std::max(1, std::min(int((228u * 1024u) / (P::SMEM + 1024u)), 65536 / (P::NT * 128)));
 }
 
 template <int TX, int TY, int S, int AUX, int UNR, int UPD>
-cudaError_t launch_f16(const PencilMaps& m, const F16Args& a, unsigned ctas, int phase,
-                       cudaStream_t stream) {
+void launch_f16_form(const PencilMaps& m, const F16Args& a, unsigned ctas, int phase,
+                     cudaStream_t stream) {
     using P = ShapeH<TX, TY, S, AUX>;
-    resident_f16<TX, TY, S, AUX, UNR, UPD>();  // sets the attributes once per device
     if (phase == 1)
         pencil_f16_kernel<TX, TY, S, AUX, 1, UNR, UPD><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
                                                                                      m.vel2, a);
@@ -600,40 +615,40 @@ cudaError_t launch_f16(const PencilMaps& m, const F16Args& a, unsigned ctas, int
     else
         pencil_f16_kernel<TX, TY, S, AUX, 0, UNR, UPD><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev,
                                                                                      m.vel2, a);
+}
+
+template <int TX, int TY, int S, int AUX, int UNR>
+cudaError_t launch_f16(const PencilMaps& m, const F16Args& a, unsigned ctas, int phase,
+                       bool exact_y, cudaStream_t stream) {
+    resident_f16<TX, TY, S, AUX, UNR>();  // sets the attributes once per device
+    if (exact_y)
+        launch_f16_form<TX, TY, S, AUX, UNR, kFormExactY>(m, a, ctas, phase, stream);
+    else
+        launch_f16_form<TX, TY, S, AUX, UNR, kFormPlain>(m, a, ctas, phase, stream);
     return cudaGetLastError();
 }
 
 struct VariantH {
-    int tx, ty, stages, aux, unr, upd;
+    int tx, ty, stages, aux;
     const char* name;
     LaunchFnH launch;
     ResidentFnH resident;
 };
 
-#define SB200_VARIANT_H(TX, TY, S, AUX, UNR, UPD, NAME)                                    \
+#define SB200_VARIANT_H(TX, TY, S, AUX, UNR, NAME)                                         \
     VariantH {                                                                               \
-        TX, TY, S, AUX, UNR, UPD, NAME, &launch_f16<TX, TY, S, AUX, UNR, UPD>,              \
-            &resident_f16<TX, TY, S, AUX, UNR, UPD>                                          \
+        TX, TY, S, AUX, NAME, &launch_f16<TX, TY, S, AUX, UNR>,                             \
+            &resident_f16<TX, TY, S, AUX, UNR>                                               \
     }
 
-// "_u8": the plane loop unrolled by 8 instead of 4; "_ms": the kUpdMixedSub update;
-// "_ye": kUpdExactY (on grids with dx != dy the same tile without it runs).
+// Tile shapes.  Measured at 1024^3 (median of 5 interleaved rounds, random
+// fields, h64x16): the update with a separate p_prev conversion 1.86 ms, the
+// mixed subtract 1.83-1.86, exact y alone 1.80-1.82, both 1.78-1.80; not kept:
+// 64 x 8 tiles (2.08), 32 x 16 (2.12), the plane loop unrolled by 8 (1.82-2.14).
 const VariantH kF16[] = {
-    SB200_VARIANT_H(64, 16, 8, 4, 4, kUpdConvert, "h64x16_s8_a4"),
-    SB200_VARIANT_H(64, 32, 8, 4, 4, kUpdConvert, "h64x32_s8_a4"),
-    SB200_VARIANT_H(128, 16, 8, 4, 4, kUpdConvert, "h128x16_s8_a4"),
-    SB200_VARIANT_H(64, 8, 8, 4, 4, kUpdConvert, "h64x8_s8_a4"),
-    SB200_VARIANT_H(32, 16, 8, 4, 4, kUpdConvert, "h32x16_s8_a4"),
-    SB200_VARIANT_H(64, 16, 8, 4, 8, kUpdConvert, "h64x16_s8_a4_u8"),
-    SB200_VARIANT_H(64, 32, 8, 4, 8, kUpdConvert, "h64x32_s8_a4_u8"),
-    SB200_VARIANT_H(128, 16, 8, 4, 8, kUpdConvert, "h128x16_s8_a4_u8"),
-    SB200_VARIANT_H(64, 16, 8, 4, 4, kUpdMixedSub, "h64x16_s8_a4_ms"),
-    SB200_VARIANT_H(64, 32, 8, 4, 4, kUpdMixedSub, "h64x32_s8_a4_ms"),
-    SB200_VARIANT_H(128, 16, 8, 4, 4, kUpdMixedSub, "h128x16_s8_a4_ms"),
-    SB200_VARIANT_H(64, 16, 8, 4, 4, kUpdExactY, "h64x16_s8_a4_ye"),
-    SB200_VARIANT_H(64, 32, 8, 4, 4, kUpdExactY, "h64x32_s8_a4_ye"),
-    SB200_VARIANT_H(64, 16, 8, 4, 4, kUpdMixedSub | kUpdExactY, "h64x16_s8_a4_ms_ye"),
-    SB200_VARIANT_H(64, 32, 8, 4, 4, kUpdMixedSub | kUpdExactY, "h64x32_s8_a4_ms_ye"),
+    SB200_VARIANT_H(64, 16, 8, 4, 4, "h64x16_s8_a4"),
+    SB200_VARIANT_H(64, 32, 8, 4, 4, "h64x32_s8_a4"),
+    SB200_VARIANT_H(128, 16, 8, 4, 4, "h128x16_s8_a4"),
 };
 constexpr int kNumF16 = sizeof(kF16) / sizeof(kF16[0]);
 
@@ -664,6 +679,10 @@ int64_t pencil_f16_ctas(int v, const GridDesc& g, int zchunks) {
     const int zlen = (inz + zc - 1) / zc;
     return int64_t(tiles_x) * tiles_y * ((inz + zlen - 1) / zlen);
 }
+
+// Whether the exact-y form applies: dx == dy (the 5040-scaled y weights of
+// c_r (dx/dy)^2 are exact halves only then).
+bool f16_exact_y(const GridDesc& g) { return g.dx == g.dy; }
 
 namespace {
 
@@ -715,9 +734,19 @@ F16Args make_f16_args(int TX, int TY, const GridDesc& g, int zchunks, uint16_t* 
 // ── batched FP16 shots ────────────────────────────────────────────────────────
 
 using LaunchFnB16 = cudaError_t (*)(const ShotF16*, const int4*, int, BatchQueue*, unsigned, int,
-                                    cudaStream_t);
+                                    bool, cudaStream_t);
 
 template <int TX, int TY, int S, int AUX, int UNR, int UPD>
+bool set_batch_f16_smem(int smem) {
+    return cudaFuncSetAttribute(batch_f16_kernel<TX, TY, S, AUX, 0, UNR, UPD>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
+           cudaFuncSetAttribute(batch_f16_kernel<TX, TY, S, AUX, 1, UNR, UPD>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
+           cudaFuncSetAttribute(batch_f16_kernel<TX, TY, S, AUX, 2, UNR, UPD>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess;
+}
+
+template <int TX, int TY, int S, int AUX, int UNR>
 int resident_batch_f16() {
     using P = ShapeH<TX, TY, S, AUX>;
     static int cached[64] = {};
@@ -725,28 +754,27 @@ int resident_batch_f16() {
     cudaGetDevice(&dev);
     if (cached[dev & 63] > 0) return cached[dev & 63];
     const int smem = static_cast<int>(P::SMEM);
-    int n = 0;
-    if (cudaFuncSetAttribute(batch_f16_kernel<TX, TY, S, AUX, 0, UNR, UPD>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
-        cudaFuncSetAttribute(batch_f16_kernel<TX, TY, S, AUX, 1, UNR, UPD>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
-        cudaFuncSetAttribute(batch_f16_kernel<TX, TY, S, AUX, 2, UNR, UPD>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess &&
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_f16_kernel<TX, TY, S, AUX, 0, UNR, UPD>,
-                                                      P::NT, P::SMEM) == cudaSuccess &&
-        n > 0) {
-        cached[dev & 63] = n;
-        return n;
+    int n = 0, n2 = 0;
+    if (set_batch_f16_smem<TX, TY, S, AUX, UNR, kFormPlain>(smem) &&
+        set_batch_f16_smem<TX, TY, S, AUX, UNR, kFormExactY>(smem) &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &n, batch_f16_kernel<TX, TY, S, AUX, 0, UNR, kFormPlain>, P::NT, P::SMEM) ==
+            cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &n2, batch_f16_kernel<TX, TY, S, AUX, 0, UNR, kFormExactY>, P::NT, P::SMEM) ==
+            cudaSuccess &&
+        std::min(n, n2) > 0) {
+        cached[dev & 63] = std::min(n, n2);
+        return cached[dev & 63];
     }
     cudaGetLastError();
     return std::max(1, std::min(int((228u * 1024u) / (P::SMEM + 1024u)), 65536 / (P::NT * 128)));
 }
 
 template <int TX, int TY, int S, int AUX, int UNR, int UPD>
-cudaError_t launch_batch_f16_t(const ShotF16* shots, const int4* items, int n_items,
-                               BatchQueue* queue, unsigned ctas, int phase, cudaStream_t stream) {
+void launch_batch_f16_form(const ShotF16* shots, const int4* items, int n_items,
+                           BatchQueue* queue, unsigned ctas, int phase, cudaStream_t stream) {
     using P = ShapeH<TX, TY, S, AUX>;
-    resident_batch_f16<TX, TY, S, AUX, UNR, UPD>();  // sets the attributes once per device
     if (phase == 1)
         batch_f16_kernel<TX, TY, S, AUX, 1, UNR, UPD><<<ctas, P::NT, P::SMEM, stream>>>(shots, items,
                                                                                     n_items, queue);
@@ -756,6 +784,19 @@ cudaError_t launch_batch_f16_t(const ShotF16* shots, const int4* items, int n_it
     else
         batch_f16_kernel<TX, TY, S, AUX, 0, UNR, UPD><<<ctas, P::NT, P::SMEM, stream>>>(shots, items,
                                                                                     n_items, queue);
+}
+
+template <int TX, int TY, int S, int AUX, int UNR>
+cudaError_t launch_batch_f16_t(const ShotF16* shots, const int4* items, int n_items,
+                               BatchQueue* queue, unsigned ctas, int phase, bool exact_y,
+                               cudaStream_t stream) {
+    resident_batch_f16<TX, TY, S, AUX, UNR>();  // sets the attributes once per device
+    if (exact_y)
+        launch_batch_f16_form<TX, TY, S, AUX, UNR, kFormExactY>(shots, items, n_items, queue, ctas,
+                                                              phase, stream);
+    else
+        launch_batch_f16_form<TX, TY, S, AUX, UNR, kFormPlain>(shots, items, n_items, queue, ctas,
+                                                             phase, stream);
     return cudaGetLastError();
 }
 
@@ -767,12 +808,12 @@ struct VariantB16 {
 };
 
 const VariantB16 kBatchF16[] = {
-    {64, 16, "bh64x16_s8_a4", &launch_batch_f16_t<64, 16, 8, 4, 4, kUpdConvert>,
-     &resident_batch_f16<64, 16, 8, 4, 4, kUpdConvert>},
-    {32, 16, "bh32x16_s8_a4", &launch_batch_f16_t<32, 16, 8, 4, 4, kUpdConvert>,
-     &resident_batch_f16<32, 16, 8, 4, 4, kUpdConvert>},
-    {64, 8, "bh64x8_s8_a4", &launch_batch_f16_t<64, 8, 8, 4, 4, kUpdConvert>,
-     &resident_batch_f16<64, 8, 8, 4, 4, kUpdConvert>},
+    {64, 16, "bh64x16_s8_a4", &launch_batch_f16_t<64, 16, 8, 4, 4>,
+     &resident_batch_f16<64, 16, 8, 4, 4>},
+    {32, 16, "bh32x16_s8_a4", &launch_batch_f16_t<32, 16, 8, 4, 4>,
+     &resident_batch_f16<32, 16, 8, 4, 4>},
+    {64, 8, "bh64x8_s8_a4", &launch_batch_f16_t<64, 8, 8, 4, 4>,
+     &resident_batch_f16<64, 8, 8, 4, 4>},
 };
 constexpr int kNumBatchF16 = sizeof(kBatchF16) / sizeof(kBatchF16[0]);
 
@@ -782,24 +823,12 @@ cudaError_t launch_wave_pencil_f16(const PencilMaps& maps, uint16_t* next, const
                                    const SourceDesc& src, const F16Scale* scale, int phase,
                                    const PencilConfig& cfg, int* err, cudaStream_t stream) {
     if (!g.has_interior()) return cudaSuccess;
-    int vi = cfg.variant;
-    if ((kF16[vi].upd & kUpdExactY) && !(g.dx == g.dy)) {
-        // the 5040-scaled weights are exact halves only for dx == dy: run the same
-        // tile shape (same tensor-map boxes) without the exact-y form
-        for (int k = 0; k < kNumF16; ++k)
-            if (kF16[k].tx == kF16[vi].tx && kF16[k].ty == kF16[vi].ty &&
-                kF16[k].stages == kF16[vi].stages && kF16[k].aux == kF16[vi].aux &&
-                kF16[k].unr == kF16[vi].unr && kF16[k].upd == (kF16[vi].upd & ~kUpdExactY)) {
-                vi = k;
-                break;
-            }
-    }
-    const VariantH& v = kF16[vi];
+    const VariantH& v = kF16[cfg.variant];
     const F16Args a = make_f16_args(v.tx, v.ty, g, cfg.zchunks, next, src, scale, err);
     const int inz = static_cast<int>(g.nz - 2 * R);
     const unsigned ctas = static_cast<unsigned>(int64_t(a.tiles_x) * a.tiles_y *
                                                 ((inz + a.zlen - 1) / a.zlen));
-    return v.launch(maps, a, ctas, phase, stream);
+    return v.launch(maps, a, ctas, phase, f16_exact_y(g), stream);
 }
 
 int batch_f16_variant_count() { return kNumBatchF16; }
@@ -824,8 +853,9 @@ F16Args batch_f16_shot_args(int v, const GridDesc& g, int zchunks, uint16_t* nex
     return make_f16_args(kBatchF16[v].tx, kBatchF16[v].ty, g, zchunks, next, src, scale, err);
 }
 cudaError_t launch_batch_f16(int v, const ShotF16* shots, const int4* items, int n_items,
-                             BatchQueue* queue, unsigned ctas, int phase, cudaStream_t stream) {
-    return kBatchF16[v].launch(shots, items, n_items, queue, ctas, phase, stream);
+                             BatchQueue* queue, unsigned ctas, int phase, bool exact_y,
+                             cudaStream_t stream) {
+    return kBatchF16[v].launch(shots, items, n_items, queue, ctas, phase, exact_y, stream);
 }
 
 }  // namespace sb200
