@@ -67,3 +67,30 @@ def test_time_to_solution_summary():
     sec["learned"]["judged"]["fallback_at_step"] = 100  # the judge fell back
     assert not bench.time_to_solution_summary(2.72, sec)["learned_within_1e-3"]
     assert bench.time_to_solution_summary(2.72, {}) == {"plain_fp32_1024^3_1000_steps_ms": 2720.0}
+
+
+def test_reference_arm_loads_only_the_oracle():
+    """bench.py --impl reference times the reference's CPU path through oracle/
+    alone: the process never imports the product package nor maps its library,
+    and its config is the workload description our arm prints."""
+    import json
+    import subprocess
+    import sys
+
+    code = (
+        "import sys, runpy\n"
+        "sys.argv = ['bench.py', '--impl', 'reference', '--n', '48', '--steps', '2',"
+        " '--warmup', '1']\n"
+        "runpy.run_path('bench.py', run_name='__main__')\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print('LOADED', 'libstencil_b200' in maps, 'stencil_solver_b200' in sys.modules)\n")
+    out = subprocess.run([sys.executable, "-c", code], cwd=str(bench.ROOT), capture_output=True,
+                         text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = out.stdout.strip().splitlines()
+    assert lines[-1] == "LOADED False False"
+    line = json.loads(lines[-2])
+    assert line["impl"] == "reference" and line["steps"] == 2 and line["value"] > 0
+    assert line["config"] == bench.workload_desc(48, line["config"]["dt_s"],
+                                                 line["config"]["v_max_mps"])
+    assert line["cpu_baseline"]["cores"] >= 1 and line["e2e"]["h2d_bytes_per_step"] == 0
