@@ -15,13 +15,11 @@ struct PencilArgs {
     const float* prev;  // acoustic, AUX = 0: p at t-dt (may alias next)
     const float* vel2;  // acoustic, AUX = 0: v^2
     float* next;
-    float* prev_out;    // prepass: p_prev + 2 beta dt^2 v^2 lap p (in place over p_prev)
     int nx, ny, nz;
     int64_t sy, sz;
     int tiles_x, tiles_y, zlen;
     Weights w;  // acoustic: weights * dt^2; heat: weights * alpha*dt
     float dt2;  // acoustic: dt^2 (source term)
-    float heat_c;  // heat: 1 + alpha*dt * (c0/dx^2 + c0/dy^2 + c0/dz^2), the centre's weight
     int src_x, src_y, src_z;  // -1 when there is no source
     float src_w;
     const float* src_wavelet;
@@ -29,6 +27,8 @@ struct PencilArgs {
     int src_off;
     float* trace;
     int* err;
+    float* prev_out;  // prepass: p_prev + 2 beta dt^2 v^2 lap p (in place over p_prev)
+    float heat_c;     // heat: 1 + alpha*dt * (c0/dx^2 + c0/dy^2 + c0/dz^2), the centre's weight
 };
 
 // Work queue of a batched launch.  `next` hands out work items, `done` counts

@@ -160,7 +160,6 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
         az2[r] = dup2(a.w.az[r]);
     }
     const float2 cx2 = dup2(a.w.cx), cy2 = dup2(a.w.cy), cz2 = dup2(a.w.cz), neg1 = dup2(-1.f);
-    const float2 hc2 = dup2(a.heat_c);
 
     float4 q[9][RPT];
     bool bad = false;
@@ -243,8 +242,8 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
                         const float2 ce = pair_of(c, h);
-                        const int e = 4 + 2 * h;  // window index of the pair's first lane
-                        if (HEAT) {
+                        if constexpr (HEAT) {
+                            const int e = 4 + 2 * h;  // window index of the pair's first lane
                             float2 txy = ya[j][h];
                             float2 tz = make_float2(0.f, 0.f);
 #pragma unroll
@@ -257,7 +256,7 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
                                                              win[e + 1 + r] + win[e + 1 - r]);
                                 txy = fma2(ax2[r - 1], s, txy);
                             }
-                            lap[j][h] = fma2(hc2, ce, add2(txy, tz));
+                            lap[j][h] = fma2(dup2(a.heat_c), ce, add2(txy, tz));
                         } else {
                             float2 tz = mul2(cz2, ce);
                             float2 tx = mul2(cx2, ce);
@@ -266,6 +265,7 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
                                 const float2 up = pair_of(q[(u + 4 + r) % 9][j], h);
                                 const float2 dn = pair_of(q[(u + 4 - r + 9) % 9][j], h);
                                 tz = fma2(az2[r - 1], add2(up, dn), tz);
+                                const int e = 4 + 2 * h;  // window index of the pair's first lane
                                 const float2 s = make_float2(win[e + r] + win[e - r],
                                                              win[e + 1 + r] + win[e + 1 - r]);
                                 tx = fma2(ax2[r - 1], s, tx);
