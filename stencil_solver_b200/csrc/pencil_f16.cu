@@ -179,9 +179,23 @@ __device__ __forceinline__ float xsum1(const float (&c)[8], uint2 lf, uint2 rt, 
 // sequence numbers of the next p plane and the next aux iteration.  Stage =
 // seq % ring size, phase parity = (seq / ring size) & 1, so its mbarriers are
 // initialised once and their phases continue across the tiles it sweeps.
+// pre_p / pre_aux: planes and aux iterations of the next tile already issued
+// (cross-tile prefetch; thread 0's view).
 struct RingH {
     uint32_t p = 0;
     uint32_t aux = 0;
+    int pre_p = 0;
+    int pre_aux = 0;
+};
+
+// The tile a persistent CTA sweeps next (thread 0 only): its maps, origin and
+// extent, so the current sweep can fill freed ring stages with its first planes.
+struct NextTileH {
+    const CUtensorMap* pmap;
+    const CUtensorMap* qmap;
+    const CUtensorMap* kmap;
+    int xa, y0, zb;  // first x (multiple of 8), first interior row, first plane
+    int nint;        // interior planes it computes
 };
 
 // Update formulas of the step (template parameter UPD):
@@ -208,7 +222,8 @@ template <int TX, int TY, int S, int AUX, int PHASE, int UNR, bool CARRY, int UP
 __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const CUtensorMap* qmap,
                                                 const CUtensorMap* kmap, const F16Args& a,
                                                 int tx, int ty, int zc, uint16_t* sm,
-                                                uint64_t* full, uint64_t* auxf, RingH& ring) {
+                                                uint64_t* full, uint64_t* auxf, RingH& ring,
+                                                const NextTileH* nxt = nullptr) {
     using P = ShapeH<TX, TY, S, AUX>;
     const uint32_t pb = CARRY ? ring.p : 0u;    // sequence number of plane 0
     const uint32_t ab = CARRY ? ring.aux : 0u;  // sequence number of aux iteration 0
@@ -245,12 +260,38 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
         aux_issued_hi = it;
     };
     auto wait_plane = [&](int j) { return mbar_wait(&full[(pb + j) % S], ((pb + j) / S) & 1u); };
+    // Cross-tile prefetch (CARRY, thread 0): plane / aux iteration jn of the next
+    // tile goes to the stage this sweep would refill next, at the sequence number
+    // pb + nplanes + jn (ab + nint + jn) the next sweep expects.
+    int next_p = 0, next_aux = 0;
+    auto prefetch_plane = [&](int jn) {
+        if (!CARRY || !nxt || jn != next_p || jn >= S || jn >= nxt->nint + 2 * R) return;
+        const uint32_t st = (pb + nplanes + jn) % S;
+        mbar_arrive_expect_tx(&full[st], P::PLANE_BYTES);
+        tma_load_3d(sm + st * P::PLANE, nxt->pmap, &full[st], nxt->xa - 8, nxt->y0 - R,
+                    nxt->zb - R + jn);
+        issued_hi = nplanes + jn;
+        ++next_p;
+    };
+    auto prefetch_aux = [&](int jn) {
+        if (!CARRY || !nxt || jn != next_aux || jn >= AUX || jn >= nxt->nint) return;
+        const uint32_t sa = (ab + nint + jn) % AUX;
+        uint16_t* st = aux + sa * 2 * P::TILE;
+        mbar_arrive_expect_tx(&auxf[sa], 2 * P::TILE_BYTES);
+        tma_load_3d(st, nxt->qmap, &auxf[sa], nxt->xa, nxt->y0, nxt->zb + jn);
+        tma_load_3d(st + P::TILE, nxt->kmap, &auxf[sa], nxt->xa, nxt->y0, nxt->zb + jn);
+        aux_issued_hi = nint + jn;
+        ++next_aux;
+    };
     auto wait_aux = [&](int it) {
         return mbar_wait(&auxf[(ab + it) % AUX], ((ab + it) / AUX) & 1u);
     };
     if (tid == 0) {
-        for (int s = 0; s < S && s < nplanes; ++s) issue_plane(s);
-        for (int it = 0; it < AUX && it < nint; ++it) issue_aux(it);
+        const int pre_p = CARRY ? ring.pre_p : 0, pre_a = CARRY ? ring.pre_aux : 0;
+        issued_hi = pre_p - 1;  // the previous sweep's prefetches are in flight
+        aux_issued_hi = pre_a - 1;
+        for (int s = pre_p; s < S && s < nplanes; ++s) issue_plane(s);
+        for (int it = pre_a; it < AUX && it < nint; ++it) issue_aux(it);
     }
 
     const int gx = xa + 8 * lx;  // first x of this thread's chunk
@@ -304,7 +345,10 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
     if (!abort_run && tid == 0) {
 #pragma unroll
         for (int p = 0; p < R; ++p)  // planes 0..3 are consumed: refill their stages
-            if (p + S < nplanes) issue_plane(p + S);
+            if (p + S < nplanes)
+                issue_plane(p + S);
+            else
+                prefetch_plane(p + S - nplanes);
     }
 
     // The plane loop is unrolled by UNR (4 or 8).  i0 is a multiple of 4 and so
@@ -461,8 +505,14 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                 goff += a.sz;
                 abort_run = __syncthreads_or(bad) != 0;
                 if (!abort_run && tid == 0) {
-                    if (i + 4 + S < nplanes) issue_plane(i + 4 + S);  // the centre's stage
-                    if (i + AUX < nint) issue_aux(i + AUX);
+                    if (i + 4 + S < nplanes)
+                        issue_plane(i + 4 + S);  // the centre's stage
+                    else
+                        prefetch_plane(i + 4 + S - nplanes);
+                    if (i + AUX < nint)
+                        issue_aux(i + AUX);
+                    else
+                        prefetch_aux(i + AUX - nint);
                 }
             }
         }
@@ -480,6 +530,8 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
     if (CARRY) {
         ring.p = pb + nplanes;
         ring.aux = ab + nint;
+        ring.pre_p = next_p;  // thread 0's counts (the only thread that issues)
+        ring.pre_aux = next_aux;
     }
     return true;
 }
@@ -532,8 +584,15 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
     uint16_t* sm = reinterpret_cast<uint16_t*>(smem_align<128>(dsmem));
     if (threadIdx.x == 0) init_rings_f16<S, AUX>(full, auxf);
     RingH ring;
+    // One item held in reserve per CTA: thread 0 fills the stages each sweep
+    // frees at its end with the next tile's first planes (NextTileH).
+    int next_it = 0;  // thread 0
+    if (threadIdx.x == 0) next_it = atomicAdd(&queue->next, 1);
     for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(&queue->next, 1);
+        if (threadIdx.x == 0) {
+            s_item = next_it;
+            if (next_it < n_items) next_it = atomicAdd(&queue->next, 1);
+        }
         __syncthreads();
         const int it = s_item;
         __syncthreads();  // every thread has read s_item before it is replaced
@@ -541,9 +600,24 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
         const int4 w = items[it];
         const ShotF16* sh = shots + w.x;
         const F16Args a = sh->args;
+        NextTileH nt{};
+        const NextTileH* ntp = nullptr;
+        if (threadIdx.x == 0 && next_it < n_items) {
+            const int4 wn = items[next_it];
+            const ShotF16* shn = shots + wn.x;
+            const int zlen = shn->args.zlen, nz = shn->args.nz;
+            nt.pmap = &shn->p;
+            nt.qmap = &shn->prev;
+            nt.kmap = &shn->k;
+            nt.xa = wn.y * TX;
+            nt.y0 = R + wn.z * TY;
+            nt.zb = R + wn.w * zlen;
+            nt.nint = min(nt.zb + zlen, nz - R) - nt.zb;
+            ntp = &nt;
+        }
         if (!pencil_f16_tile<TX, TY, S, AUX, PHASE, UNR, true, UPD>(&sh->p, &sh->prev, &sh->k, a,
                                                                     w.y, w.z, w.w, sm, full, auxf,
-                                                                    ring))
+                                                                    ring, ntp))
             break;
     }
     if (threadIdx.x == 0) {
