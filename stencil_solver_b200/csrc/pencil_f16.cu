@@ -107,11 +107,12 @@ __device__ __forceinline__ void stg_stream_u2(void* p, uint2 v) {
     asm volatile("st.global.cs.v2.u32 [%0], {%1, %2};" ::"l"(p), "r"(v.x), "r"(v.y) : "memory");
 }
 
-// f32(half) - b for both halves of a word (the sm_100 mixed-precision subtract).
-__device__ __forceinline__ float2 subhf2(uint32_t w, float2 b) {
+// b - f32(half) for both halves of a word: the sm_100 mixed-precision FMA
+// f32(half) * (-1) + b, whose product is exact, so one rounding of b - half.
+__device__ __forceinline__ float2 rsubhf2(uint32_t w, float2 b) {
     float x, y;
-    asm("{\n\t.reg .b16 lo, hi;\n\tmov.b32 {lo, hi}, %2;\n\t"
-        "sub.rn.f32.f16 %0, lo, %3;\n\tsub.rn.f32.f16 %1, hi, %4;\n\t}"
+    asm("{\n\t.reg .b16 lo, hi, m1;\n\tmov.b32 {lo, hi}, %2;\n\tmov.b16 m1, 0xBC00;\n\t"
+        "fma.rn.f32.f16 %0, lo, m1, %3;\n\tfma.rn.f32.f16 %1, hi, m1, %4;\n\t}"
         : "=f"(x), "=f"(y)
         : "r"(w), "f"(b.x), "f"(b.y));
     return make_float2(x, y);
@@ -179,30 +180,15 @@ __device__ __forceinline__ float xsum1(const float (&c)[8], uint2 lf, uint2 rt, 
 // sequence numbers of the next p plane and the next aux iteration.  Stage =
 // seq % ring size, phase parity = (seq / ring size) & 1, so its mbarriers are
 // initialised once and their phases continue across the tiles it sweeps.
-// pre_p / pre_aux: planes and aux iterations of the next tile already issued
-// (cross-tile prefetch; thread 0's view).
 struct RingH {
     uint32_t p = 0;
     uint32_t aux = 0;
-    int pre_p = 0;
-    int pre_aux = 0;
-};
-
-// The tile a persistent CTA sweeps next (thread 0 only): its maps, origin and
-// extent, so the current sweep can fill freed ring stages with its first planes.
-struct NextTileH {
-    const CUtensorMap* pmap;
-    const CUtensorMap* qmap;
-    const CUtensorMap* kmap;
-    int xa, y0, zb;  // first x (multiple of 8), first interior row, first plane
-    int nint;        // interior planes it computes
 };
 
 // Update formulas of the step (template parameter UPD):
 //   kUpdConvert:  p_prev converted to FP32, then fma(K, lap, fma(-m_q, pq, 2c));
-//   kUpdMixedSub: u = fma(K, lap, 2c), then the mixed subtract pq - u converts p_prev
-//                 on the way and gives -p_next, whose sign the rescale factor
-//                 (PHASE 1) or the packed halves' sign bits (PHASE 0) restore;
+//   kUpdMixedSub: u = fma(K, lap, 2c), then u - pq in one mixed-precision FMA
+//                 (pq x -1 + u) that converts p_prev on the way;
 //                 PHASE 2 (p_prev rescaled) uses kUpdConvert.
 // and, as a flag, the y pairs:
 //   kUpdExactY:   on a grid with dx == dy each y neighbour enters through one
@@ -222,8 +208,7 @@ template <int TX, int TY, int S, int AUX, int PHASE, int UNR, bool CARRY, int UP
 __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const CUtensorMap* qmap,
                                                 const CUtensorMap* kmap, const F16Args& a,
                                                 int tx, int ty, int zc, uint16_t* sm,
-                                                uint64_t* full, uint64_t* auxf, RingH& ring,
-                                                const NextTileH* nxt = nullptr) {
+                                                uint64_t* full, uint64_t* auxf, RingH& ring) {
     using P = ShapeH<TX, TY, S, AUX>;
     const uint32_t pb = CARRY ? ring.p : 0u;    // sequence number of plane 0
     const uint32_t ab = CARRY ? ring.aux : 0u;  // sequence number of aux iteration 0
@@ -260,38 +245,12 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
         aux_issued_hi = it;
     };
     auto wait_plane = [&](int j) { return mbar_wait(&full[(pb + j) % S], ((pb + j) / S) & 1u); };
-    // Cross-tile prefetch (CARRY, thread 0): plane / aux iteration jn of the next
-    // tile goes to the stage this sweep would refill next, at the sequence number
-    // pb + nplanes + jn (ab + nint + jn) the next sweep expects.
-    int next_p = 0, next_aux = 0;
-    auto prefetch_plane = [&](int jn) {
-        if (!CARRY || !nxt || jn != next_p || jn >= S || jn >= nxt->nint + 2 * R) return;
-        const uint32_t st = (pb + nplanes + jn) % S;
-        mbar_arrive_expect_tx(&full[st], P::PLANE_BYTES);
-        tma_load_3d(sm + st * P::PLANE, nxt->pmap, &full[st], nxt->xa - 8, nxt->y0 - R,
-                    nxt->zb - R + jn);
-        issued_hi = nplanes + jn;
-        ++next_p;
-    };
-    auto prefetch_aux = [&](int jn) {
-        if (!CARRY || !nxt || jn != next_aux || jn >= AUX || jn >= nxt->nint) return;
-        const uint32_t sa = (ab + nint + jn) % AUX;
-        uint16_t* st = aux + sa * 2 * P::TILE;
-        mbar_arrive_expect_tx(&auxf[sa], 2 * P::TILE_BYTES);
-        tma_load_3d(st, nxt->qmap, &auxf[sa], nxt->xa, nxt->y0, nxt->zb + jn);
-        tma_load_3d(st + P::TILE, nxt->kmap, &auxf[sa], nxt->xa, nxt->y0, nxt->zb + jn);
-        aux_issued_hi = nint + jn;
-        ++next_aux;
-    };
     auto wait_aux = [&](int it) {
         return mbar_wait(&auxf[(ab + it) % AUX], ((ab + it) / AUX) & 1u);
     };
     if (tid == 0) {
-        const int pre_p = CARRY ? ring.pre_p : 0, pre_a = CARRY ? ring.pre_aux : 0;
-        issued_hi = pre_p - 1;  // the previous sweep's prefetches are in flight
-        aux_issued_hi = pre_a - 1;
-        for (int s = pre_p; s < S && s < nplanes; ++s) issue_plane(s);
-        for (int it = pre_a; it < AUX && it < nint; ++it) issue_aux(it);
+        for (int s = 0; s < S && s < nplanes; ++s) issue_plane(s);
+        for (int it = 0; it < AUX && it < nint; ++it) issue_aux(it);
     }
 
     const int gx = xa + 8 * lx;  // first x of this thread's chunk
@@ -324,7 +283,7 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
     float m_out = 1.f, m_q = 1.f;
     if (PHASE == 1) m_out = a.scale->r;
     if (PHASE == 2) m_q = a.scale->r;
-    const float2 nmq2 = dup2(-m_q), mout2 = dup2(m_out), nmout2 = dup2(-m_out);
+    const float2 nmq2 = dup2(-m_q), mout2 = dup2(m_out);
 
     // Plane index p (z = zb - 4 + p) lives in slot p % 4 of both rings.
     uint4 hq[4];      // FP16: centre and the planes above it
@@ -345,10 +304,7 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
     if (!abort_run && tid == 0) {
 #pragma unroll
         for (int p = 0; p < R; ++p)  // planes 0..3 are consumed: refill their stages
-            if (p + S < nplanes)
-                issue_plane(p + S);
-            else
-                prefetch_plane(p + S - nplanes);
+            if (p + S < nplanes) issue_plane(p + S);
     }
 
     // The plane loop is unrolled by UNR (4 or 8).  i0 is a multiple of 4 and so
@@ -389,14 +345,17 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                 }
                 // lap = [c (cx+cy+cz) + sum_r (ax_r sx_r + ay_r sy_r)] + sum_r az_r sz_r,
                 // pair sums s = p[+r] + p[-r]; up operands of y and z enter FP16.
+                // z pair of radius r: up plane (slot (u + r) % 4) + down plane
+                auto zpair = [&](int r, int h) {
+                    return addhf2(get_word(hq[(u + r) % 4], h), dq[(u + 4 - r) % 4][h]);
+                };
                 float2 lap[4];
 #pragma unroll
                 for (int h = 0; h < 4; ++h) {
                     const float2 c = cv[h];
                     float2 txy = mul2(cxy2, c);
                     float2 ty = make_float2(0.f, 0.f);  // kUpdExactY: 5040 x the y pairs
-                    float2 tz = mul2(az2[0], addhf2(get_word(hq[(u + 1) % 4], h),
-                                                    dq[(u + 3) % 4][h]));
+                    float2 tz = mul2(az2[0], zpair(1, h));
 #pragma unroll
                     for (int r = 1; r <= R; ++r) {
                         // an aligned pair of own points (even r) adds as one pair
@@ -418,10 +377,7 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                         }
                         // up: plane z + r (FP16, slot (u + r) % 4; r = 4 is the plane
                         // just fed); down: plane z - r (FP32, slot (u + 4 - r) % 4)
-                        if (r > 1)
-                            tz = fma2(az2[r - 1], addhf2(get_word(hq[(u + r) % 4], h),
-                                                         dq[(u + 4 - r) % 4][h]),
-                                      tz);
+                        if (r > 1) tz = fma2(az2[r - 1], zpair(r, h), tz);
                     }
                     if (UPD & kUpdExactY) txy = fma2(dup2(kInv5040), ty, txy);
                     lap[h] = add2(txy, tz);
@@ -442,9 +398,7 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                 if (!aok) bad = true;
                 const uint4 qv = lds128h(st);
                 const uint4 kv = lds128h(st + P::TILE);
-                // kNeg: o holds -p_next (see kUpdMixedSub)
                 constexpr bool kMixed = (UPD & kUpdMixedSub) && PHASE != 2;
-                constexpr bool kNeg = kMixed && PHASE == 0;
                 float o[8];
 #pragma unroll
                 for (int h = 0; h < 4; ++h) {
@@ -454,8 +408,8 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                                                   __uint_as_float(kw & 0xffff0000u));
                     float2 ov;
                     if (kMixed) {
-                        ov = subhf2(get_word(qv, h), fma2(kk, lap[h], add2(c, c)));
-                        if (PHASE == 1) ov = mul2(ov, nmout2);
+                        ov = rsubhf2(get_word(qv, h), fma2(kk, lap[h], add2(c, c)));
+                        if (PHASE == 1) ov = mul2(ov, mout2);
                     } else {
                         // 2c - m_q pq in one rounding (2c is exact), then + K lap
                         const float2 pq = h2f2(get_word(qv, h));
@@ -475,10 +429,10 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
 #pragma unroll
                         for (int e = 0; e < 8; ++e)
                             if (e == src_e) {
-                                o[e] = kNeg ? o[e] - add : o[e] + add;
+                                o[e] += add;
                                 if (a.trace)
                                     a.trace[(a.src_step ? *a.src_step : 0) + a.src_off] =
-                                        __half2float(__float2half_rn(kNeg ? -o[e] : o[e])) / sa;
+                                        __half2float(__float2half_rn(o[e])) / sa;
                             }
                     }
                 }
@@ -489,12 +443,6 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                     pk.y = pack_h2(o[2], o[3]);
                     pk.z = pack_h2(o[4], o[5]);
                     pk.w = pack_h2(o[6], o[7]);
-                    if (kNeg) {  // -(-p_next): flip the sign bits (exact)
-                        pk.x ^= 0x80008000u;
-                        pk.y ^= 0x80008000u;
-                        pk.z ^= 0x80008000u;
-                        pk.w ^= 0x80008000u;
-                    }
                     if (xfull)
                         stg_stream_u4(dst, pk);
                     else if (gx < R)  // x = 4..7 of the first chunk
@@ -505,14 +453,8 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                 goff += a.sz;
                 abort_run = __syncthreads_or(bad) != 0;
                 if (!abort_run && tid == 0) {
-                    if (i + 4 + S < nplanes)
-                        issue_plane(i + 4 + S);  // the centre's stage
-                    else
-                        prefetch_plane(i + 4 + S - nplanes);
-                    if (i + AUX < nint)
-                        issue_aux(i + AUX);
-                    else
-                        prefetch_aux(i + AUX - nint);
+                    if (i + 4 + S < nplanes) issue_plane(i + 4 + S);  // the centre's stage
+                    if (i + AUX < nint) issue_aux(i + AUX);
                 }
             }
         }
@@ -530,8 +472,6 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
     if (CARRY) {
         ring.p = pb + nplanes;
         ring.aux = ab + nint;
-        ring.pre_p = next_p;  // thread 0's counts (the only thread that issues)
-        ring.pre_aux = next_aux;
     }
     return true;
 }
@@ -584,15 +524,8 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
     uint16_t* sm = reinterpret_cast<uint16_t*>(smem_align<128>(dsmem));
     if (threadIdx.x == 0) init_rings_f16<S, AUX>(full, auxf);
     RingH ring;
-    // One item held in reserve per CTA: thread 0 fills the stages each sweep
-    // frees at its end with the next tile's first planes (NextTileH).
-    int next_it = 0;  // thread 0
-    if (threadIdx.x == 0) next_it = atomicAdd(&queue->next, 1);
     for (;;) {
-        if (threadIdx.x == 0) {
-            s_item = next_it;
-            if (next_it < n_items) next_it = atomicAdd(&queue->next, 1);
-        }
+        if (threadIdx.x == 0) s_item = atomicAdd(&queue->next, 1);
         __syncthreads();
         const int it = s_item;
         __syncthreads();  // every thread has read s_item before it is replaced
@@ -600,24 +533,9 @@ __global__ void __launch_bounds__(ShapeH<TX, TY, S, AUX>::NT, ShapeH<TX, TY, S, 
         const int4 w = items[it];
         const ShotF16* sh = shots + w.x;
         const F16Args a = sh->args;
-        NextTileH nt{};
-        const NextTileH* ntp = nullptr;
-        if (threadIdx.x == 0 && next_it < n_items) {
-            const int4 wn = items[next_it];
-            const ShotF16* shn = shots + wn.x;
-            const int zlen = shn->args.zlen, nz = shn->args.nz;
-            nt.pmap = &shn->p;
-            nt.qmap = &shn->prev;
-            nt.kmap = &shn->k;
-            nt.xa = wn.y * TX;
-            nt.y0 = R + wn.z * TY;
-            nt.zb = R + wn.w * zlen;
-            nt.nint = min(nt.zb + zlen, nz - R) - nt.zb;
-            ntp = &nt;
-        }
         if (!pencil_f16_tile<TX, TY, S, AUX, PHASE, UNR, true, UPD>(&sh->p, &sh->prev, &sh->k, a,
                                                                     w.y, w.z, w.w, sm, full, auxf,
-                                                                    ring, ntp))
+                                                                    ring))
             break;
     }
     if (threadIdx.x == 0) {
@@ -718,7 +636,10 @@ struct VariantH {
 // Tile shapes.  Measured at 1024^3 (median of 5 interleaved rounds, random
 // fields, h64x16): the update with a separate p_prev conversion 1.86 ms, the
 // mixed subtract 1.83-1.86, exact y alone 1.80-1.82, both 1.78-1.80; not kept:
-// 64 x 8 tiles (2.08), 32 x 16 (2.12), the plane loop unrolled by 8 (1.82-2.14).
+// 64 x 8 tiles (2.08), 32 x 16 (2.12), the plane loop unrolled by 8 (1.82-2.14;
+// again 1.92-1.99 against 1.54-1.71 in one interleaved run), the planes above the
+// centre converted to FP32 when fed so that each z pair is one FP32 pair add
+// (2.39-2.48: 128 registers and spills; unrolled by 8, no spills, 1.98-2.21).
 const VariantH kF16[] = {
     SB200_VARIANT_H(64, 16, 8, 4, 4, "h64x16_s8_a4"),
     SB200_VARIANT_H(64, 32, 8, 4, 4, "h64x32_s8_a4"),

@@ -66,23 +66,9 @@ struct Shape {
 // the next p plane and the next aux iteration.  Stage = seq % ring size, phase
 // parity = (seq / ring size) & 1, so the mbarriers are initialised once per CTA
 // and their phases simply continue across the tiles a persistent CTA processes.
-// pre_p / pre_aux: planes and aux iterations of the next tile already issued
-// (cross-tile prefetch of a persistent CTA; thread 0's view).
 struct Ring {
     uint32_t p = 0;
     uint32_t aux = 0;
-    int pre_p = 0;
-    int pre_aux = 0;
-};
-
-// The tile a persistent CTA sweeps next (thread 0 only): its maps, origin and
-// extent, so the current sweep can fill freed ring stages with its first planes.
-struct NextTile {
-    const CUtensorMap* pmap;
-    const CUtensorMap* qmap;
-    const CUtensorMap* vmap;
-    int x0, y0, zb;  // interior origin of the tile and first plane of its z chunk
-    int nint;        // interior planes it computes
 };
 
 // One tile: columns [x0, x0+TX) x [y0, y0+TY) of the interior, marched over the
@@ -93,8 +79,7 @@ template <int TX, int TY, int RPT, int S, int AUX, int MODE>
 __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUtensorMap* qmap,
                                             const CUtensorMap* vmap, const PencilArgs& a,
                                             int tile_x, int tile_y, int zc, float* sm,
-                                            uint64_t* full, uint64_t* auxf, Ring& ring,
-                                            const NextTile* nxt = nullptr) {
+                                            uint64_t* full, uint64_t* auxf, Ring& ring) {
     using P = Shape<TX, TY, RPT, S, AUX>;
     constexpr bool HEAT = MODE == kModeHeat;
     constexpr bool PRE = MODE == kModePrepass;
@@ -130,29 +115,6 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
         tma_load_3d(st + P::TILE, vmap, &auxf[s], x0, y0, zb + it);
         aux_issued_hi = it;
     };
-    // Cross-tile prefetch (thread 0, persistent CTAs): plane jn / aux iteration jn
-    // of the next tile goes to the stage this sweep would refill next -- its
-    // sequence number, pb + nplanes + jn, is the one the next sweep expects.
-    int next_p = 0, next_aux = 0;  // how many of the next tile's were issued
-    auto prefetch_plane = [&](int jn) {
-        if (!nxt || jn != next_p || jn >= S || jn >= nxt->nint + 2 * R) return;
-        const uint32_t s = (pb + nplanes + jn) % S;
-        mbar_arrive_expect_tx(&full[s], P::PLANE_BYTES);
-        tma_load_3d(sm + s * P::PLANE, nxt->pmap, &full[s], nxt->x0 - R, nxt->y0 - R,
-                    nxt->zb - R + jn);
-        issued_hi = nplanes + jn;
-        ++next_p;
-    };
-    auto prefetch_aux = [&](int jn) {
-        if (!nxt || !kAuxTma || jn != next_aux || jn >= NAUX || jn >= nxt->nint) return;
-        const uint32_t s = (ab + nint + jn) % NAUX;
-        float* st = aux + s * 2 * P::TILE;
-        mbar_arrive_expect_tx(&auxf[s], 2 * P::TILE_BYTES);
-        tma_load_3d(st, nxt->qmap, &auxf[s], nxt->x0, nxt->y0, nxt->zb + jn);
-        tma_load_3d(st + P::TILE, nxt->vmap, &auxf[s], nxt->x0, nxt->y0, nxt->zb + jn);
-        aux_issued_hi = nint + jn;
-        ++next_aux;
-    };
     auto wait_plane = [&](int j) {
         return mbar_wait(&full[(pb + j) % S], ((pb + j) / S) & 1);
     };
@@ -167,12 +129,9 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
             prefetch_tmap(qmap);
             prefetch_tmap(vmap);
         }
-        // planes / aux iterations the previous sweep prefetched are in flight
-        issued_hi = ring.pre_p - 1;
-        aux_issued_hi = ring.pre_aux - 1;
-        for (int s = ring.pre_p; s < S && s < nplanes; ++s) issue_plane(s);
+        for (int s = 0; s < S && s < nplanes; ++s) issue_plane(s);
         if (kAuxTma)
-            for (int it = ring.pre_aux; it < NAUX && it < nint; ++it) issue_aux(it);
+            for (int it = 0; it < NAUX && it < nint; ++it) issue_aux(it);
     }
 
     const int gx = x0 + 4 * lx;
@@ -216,12 +175,8 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
     if (!abort_run && tid == 0) {
         // Planes 0..3 are only queue feed: their stages are free again.
 #pragma unroll
-        for (int jj = 0; jj < R; ++jj) {
-            if (jj + S < nplanes)
-                issue_plane(jj + S);
-            else
-                prefetch_plane(jj + S - nplanes);
-        }
+        for (int jj = 0; jj < R; ++jj)
+            if (jj + S < nplanes) issue_plane(jj + S);
     }
 
     for (int i0 = 0; i0 < nint && !abort_run; i0 += 9) {
@@ -378,14 +333,8 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
                 // refill them S planes / AUX iterations ahead.
                 abort_run = __syncthreads_or(bad) != 0;
                 if (!abort_run && tid == 0) {
-                    if (i + 4 + S < nplanes)
-                        issue_plane(i + 4 + S);
-                    else
-                        prefetch_plane(i + 4 + S - nplanes);
-                    if (kAuxTma && i + NAUX < nint)
-                        issue_aux(i + NAUX);
-                    else
-                        prefetch_aux(i + NAUX - nint);
+                    if (i + 4 + S < nplanes) issue_plane(i + 4 + S);
+                    if (kAuxTma && i + NAUX < nint) issue_aux(i + NAUX);
                 }
             }
         }
@@ -405,8 +354,6 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
     }
     ring.p = pb + nplanes;
     if (kAuxTma) ring.aux = ab + nint;
-    ring.pre_p = next_p;  // thread 0's counts (the only thread that issues)
-    ring.pre_aux = next_aux;
     return true;
 }
 
@@ -465,17 +412,8 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S, AUX>::NT, Shape<TX, TY, 
     __shared__ int s_item;
     float* sm = setup_rings<TX, TY, RPT, S, AUX>(dsmem, full, auxf);
     Ring ring;
-    // Each CTA holds one item in reserve: while it sweeps item `it`, thread 0
-    // knows the next one and fills the ring stages the sweep frees at its end
-    // with the next tile's first planes (NextTile), so the next sweep starts
-    // with its pipeline full.
-    int next_it = 0;  // thread 0
-    if (threadIdx.x == 0) next_it = atomicAdd(&queue->next, 1);
     for (;;) {
-        if (threadIdx.x == 0) {
-            s_item = next_it;
-            if (next_it < n_items) next_it = atomicAdd(&queue->next, 1);
-        }
+        if (threadIdx.x == 0) s_item = atomicAdd(&queue->next, 1);
         __syncthreads();
         const int it = s_item;
         __syncthreads();  // every thread has read s_item before it is replaced
@@ -483,23 +421,8 @@ __global__ void __launch_bounds__(Shape<TX, TY, RPT, S, AUX>::NT, Shape<TX, TY, 
         const int4 w = items[it];
         const ShotF32* sh = shots + w.x;
         const PencilArgs a = sh->args;
-        NextTile nt{};
-        const NextTile* ntp = nullptr;
-        if (threadIdx.x == 0 && next_it < n_items) {
-            const int4 wn = items[next_it];
-            const ShotF32* shn = shots + wn.x;
-            const int zlen = shn->args.zlen, nz = shn->args.nz;
-            nt.pmap = &shn->p;
-            nt.qmap = &shn->prev;
-            nt.vmap = &shn->vel2;
-            nt.x0 = R + wn.y * TX;
-            nt.y0 = R + wn.z * TY;
-            nt.zb = R + wn.w * zlen;
-            nt.nint = min(nt.zb + zlen, nz - R) - nt.zb;
-            ntp = &nt;
-        }
         if (!pencil_tile<TX, TY, RPT, S, AUX, kModeAcoustic>(&sh->p, &sh->prev, &sh->vel2, a, w.y, w.z,
-                                                     w.w, sm, full, auxf, ring, ntp))
+                                                     w.w, sm, full, auxf, ring))
             break;
     }
     if (threadIdx.x == 0) {
