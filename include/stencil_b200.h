@@ -100,6 +100,28 @@ int sb200_wave_step_dev_f32(const float* p, const float* p_prev, const float* ve
                             const float* wavelet, const int* step, int step_offset, int exact,
                             void* stream);
 
+/* No reference counterpart.  Two acoustic steps in one sweep over the grid
+ * (temporal blocking): p_next = the step of (p, p_prev) with source sample
+ * src_amp0, p_next2 = the step of (p_next, p) with src_amp1 -- the same bits as
+ * sb200_wave_step_f32(p, p_prev, vel2, p_prev, ...) followed by
+ * sb200_wave_step_f32(p_prev, p, vel2, p, ...), at 20 B of DRAM traffic per
+ * interior point for the pair instead of 32.  p, p_prev, vel2, p_next and
+ * p_next2 must be five distinct buffers (other tiles still read p and p_prev
+ * while a tile writes its results); the halo cells of p_next and p_next2 are not
+ * written and must hold the walls, as p_prev's and p's do (zeros for the
+ * reference's fixed walls).  nx % 4 == 0 and 16-byte aligned fields
+ * (SB200_ERR_UNSUPPORTED otherwise). */
+int sb200_wave_step2_f32(const float* p, const float* p_prev, const float* vel2, float* p_next,
+                         float* p_next2, const sb200_grid* grid, int64_t src_index,
+                         float src_amp0, float src_amp1, void* stream);
+
+/* sb200_wave_step2_f32 with the two source samples read on the device as
+ * wavelet[*step + step_offset] and wavelet[*step + step_offset + 1]. */
+int sb200_wave_step2_dev_f32(const float* p, const float* p_prev, const float* vel2,
+                             float* p_next, float* p_next2, const sb200_grid* grid,
+                             int64_t src_index, const float* wavelet, const int* step,
+                             int step_offset, void* stream);
+
 /* Writes value to the device int *dst (one-thread kernel, stream-ordered). */
 int sb200_set_device_int(int* dst, int value, void* stream);
 
@@ -212,6 +234,7 @@ int sb200_field_stats_f32_noalloc(const float* field, const sb200_grid* grid, do
 #define SB200_KIND_WAVE_F32 0
 #define SB200_KIND_HEAT_F32 1
 #define SB200_KIND_WAVE_F16 2
+#define SB200_KIND_WAVE2_F32 3 /* sb200_wave_step2_f32: two acoustic steps per sweep */
 int sb200_pencil_variant_count(int kind);
 const char* sb200_pencil_variant_name(int kind, int variant);
 /* Forces (variant, zchunks) for every later launch of `kind` on this process;

@@ -97,6 +97,7 @@ class sb200_f16_scale(C.Structure):
 PHYSICS_WAVE, PHYSICS_HEAT = 0, 1
 PRECISION_F32, PRECISION_F16 = 0, 1
 KIND_WAVE_F16 = 2
+KIND_WAVE2_F32 = 3  # wave_step2: two acoustic steps per sweep
 
 _lib: C.CDLL | None = None
 
@@ -115,6 +116,10 @@ _SIGNATURES = {
     "sb200_wave_step_dev_f32": ([C.c_void_p] * 4 + [C.POINTER(sb200_grid), C.c_int64,
                                     C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p],
                                    C.c_int),
+    "sb200_wave_step2_f32": ([C.c_void_p] * 5 + [C.POINTER(sb200_grid), C.c_int64, C.c_float,
+                                                 C.c_float, C.c_void_p], C.c_int),
+    "sb200_wave_step2_dev_f32": ([C.c_void_p] * 5 + [C.POINTER(sb200_grid), C.c_int64,
+                                     C.c_void_p, C.c_void_p, C.c_int, C.c_void_p], C.c_int),
     "sb200_set_device_int": ([C.c_void_p, C.c_int, C.c_void_p], C.c_int),
     "sb200_heat_step_exact_f32": ([C.c_void_p, C.c_void_p, C.POINTER(sb200_grid), C.c_float,
                                    C.c_void_p], C.c_int),
@@ -346,6 +351,22 @@ def wave_step_dev(p, p_prev, vel2, p_next, grid: Grid, src_index: int, wavelet, 
     _check(lib().sb200_wave_step_dev_f32(_ptr(p), _ptr(p_prev), _ptr(vel2), _ptr(p_next),
                                          _g(grid), src_index, _ptr(wavelet), _ptr(step),
                                          step_offset, 1 if exact else 0, _stream(stream)))
+
+
+def wave_step2(p, p_prev, vel2, p_next, p_next2, grid: Grid, src_index: int = -1,
+               src_amp0: float = 0.0, src_amp1: float = 0.0, stream=None) -> None:
+    """Two acoustic steps in one sweep: p_next = step(p, p_prev) with sample
+    src_amp0, p_next2 = step(p_next, p) with src_amp1 (five distinct buffers)."""
+    _check(lib().sb200_wave_step2_f32(_ptr(p), _ptr(p_prev), _ptr(vel2), _ptr(p_next),
+                                      _ptr(p_next2), _g(grid), src_index, src_amp0, src_amp1,
+                                      _stream(stream)))
+
+
+def wave_step2_dev(p, p_prev, vel2, p_next, p_next2, grid: Grid, src_index: int, wavelet, step,
+                   step_offset: int = 0, stream=None) -> None:
+    _check(lib().sb200_wave_step2_dev_f32(_ptr(p), _ptr(p_prev), _ptr(vel2), _ptr(p_next),
+                                          _ptr(p_next2), _g(grid), src_index, _ptr(wavelet),
+                                          _ptr(step), step_offset, _stream(stream)))
 
 
 def set_device_int(dst, value: int, stream=None) -> None:

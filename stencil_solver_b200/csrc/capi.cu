@@ -77,16 +77,23 @@ struct Override {
     int zchunks = 1;
 };
 std::mutex g_cfg_mu;
-Override g_override[3];
+Override g_override[4];
 
 bool valid_kind(int kind) {
     return kind == SB200_KIND_WAVE_F32 || kind == SB200_KIND_HEAT_F32 ||
-           kind == SB200_KIND_WAVE_F16;
+           kind == SB200_KIND_WAVE_F16 || kind == SB200_KIND_WAVE2_F32;
 }
 
 int variant_count(int kind) {
+    if (kind == SB200_KIND_WAVE2_F32) return leap2_variant_count();
     return kind == SB200_KIND_WAVE_F16 ? pencil_f16_variant_count()
                                        : pencil_f32_variant_count(kind == SB200_KIND_HEAT_F32);
+}
+
+const char* variant_name(int kind, int v) {
+    if (kind == SB200_KIND_WAVE2_F32) return leap2_variant_name(v);
+    if (kind == SB200_KIND_WAVE_F16) return pencil_f16_variant_name(v);
+    return pencil_f32_variant_name(kind == SB200_KIND_HEAT_F32, v);
 }
 
 int sm_count() {
@@ -100,14 +107,13 @@ int sm_count() {
 // (1024^3 acoustic: t64x32_r2_s8_a3; 512^3 heat: t64x16_r2_s8; FP16 1024^3:
 // h64x16_s8_a4), found by name so the tables can be reordered.
 int default_variant(int kind) {
-    const char* want = kind == SB200_KIND_WAVE_F32 ? "t64x32_r2_s8_a3"
+    const char* want = kind == SB200_KIND_WAVE_F32   ? "t64x32_r2_s8_a3"
                        : kind == SB200_KIND_HEAT_F32 ? "t64x16_r2_s8"
-                                                     : "h64x16_s8_a4";
+                       : kind == SB200_KIND_WAVE_F16 ? "h64x16_s8_a4"
+                                                     : "l32x32_s8";
     const int n = variant_count(kind);
     for (int v = 0; v < n; ++v) {
-        const char* name = kind == SB200_KIND_WAVE_F16
-                               ? pencil_f16_variant_name(v)
-                               : pencil_f32_variant_name(kind == SB200_KIND_HEAT_F32, v);
+        const char* name = variant_name(kind, v);
         if (name && std::strcmp(name, want) == 0) return v;
     }
     return 0;
@@ -198,6 +204,41 @@ int wave_step(const float* p, const float* p_prev, const float* vel2, float* p_n
     return finish_launch(launch_wave_naive(p, p_prev, vel2, p_next, g, src, st), where);
 }
 
+// Two acoustic steps in one sweep (leap2_f32.cu).  outputs_may_alias lets the
+// tuner time it with one scratch buffer for both outputs (their values unused).
+int wave_step2(const float* p, const float* p_prev, const float* vel2, float* out1, float* out2,
+               const sb200_grid* grid, const SourceDesc& src, float w1, void* stream,
+               bool outputs_may_alias, const char* where) {
+    GridDesc g;
+    if (int rc = to_desc(grid, &g)) return rc;
+    if (!p || !p_prev || !vel2 || !out1 || !out2)
+        return fail(SB200_ERR_INVALID, std::string(where) + ": NULL field pointer");
+    if (p == p_prev || (out1 == out2 && !outputs_may_alias))
+        return fail(SB200_ERR_INVALID, std::string(where) + ": the five fields must be distinct");
+    for (const float* o : {static_cast<const float*>(out1), static_cast<const float*>(out2)})
+        if (o == p || o == p_prev || o == vel2)
+            return fail(SB200_ERR_INVALID,
+                        std::string(where) + ": an output aliases an input (five distinct fields)");
+    if (src.idx >= g.size())
+        return fail(SB200_ERR_INVALID, std::string(where) + ": source index outside the grid");
+    if (!g.has_interior()) return SB200_OK;
+    if (!pencil_ok(g, {p, p_prev, vel2, out1, out2}))
+        return fail(SB200_ERR_UNSUPPORTED,
+                    std::string(where) + ": needs nx % 4 == 0 and 16-byte aligned fields");
+    const PencilConfig cfg = choose(SB200_KIND_WAVE2_F32, g);
+    const PencilBoxes b = leap2_boxes(cfg.variant);
+    PencilMaps maps;
+    int rc = tensor_map_3d(&maps.p, p, g.nx, g.ny, g.nz, 4, b.halo_x, b.halo_y);
+    if (!rc) rc = tensor_map_3d(&maps.prev, p_prev, g.nx, g.ny, g.nz, 4, b.tile_x, b.tile_y);
+    if (!rc) rc = tensor_map_3d(&maps.vel2, vel2, g.nx, g.ny, g.nz, 4, b.tile_x, b.tile_y);
+    if (rc)
+        return fail(SB200_ERR_CUDA, std::string(where) + ": tensor map encode failed (" +
+                                        std::to_string(rc) + ")");
+    return finish_launch(launch_leap2_f32(maps, out1, out2, g, src, w1, cfg, device_error_ptr(),
+                                          static_cast<cudaStream_t>(stream)),
+                         where);
+}
+
 SourceDesc host_source(int64_t idx, float amp) {
     SourceDesc s;
     s.idx = idx;
@@ -249,6 +290,13 @@ int dispatch_wave_f32(const float* p, const float* p_prev, const float* vel2, fl
                      exact ? "sb200_wave_step_exact_f32" : "sb200_wave_step_f32");
 }
 
+int dispatch_wave2_f32(const float* p, const float* p_prev, const float* vel2, float* out1,
+                       float* out2, const sb200_grid* grid, const SourceDesc& src, float w1,
+                       void* stream, bool outputs_may_alias) {
+    return wave_step2(p, p_prev, vel2, out1, out2, grid, src, w1, stream, outputs_may_alias,
+                      "sb200_wave_step2_f32");
+}
+
 int dispatch_wave_f16(const uint16_t* p, uint16_t* p_prev_next, const uint16_t* k,
                       const sb200_grid* grid, const SourceDesc& src, const sb200_f16_scale* scale,
                       int phase, void* stream) {
@@ -266,17 +314,23 @@ int* device_error_word() { return device_error_ptr(); }
 std::vector<int> zchunk_ranking(int kind, int v, const GridDesc& g, int max_n) {
     const bool f16 = kind == SB200_KIND_WAVE_F16;
     const bool heat = kind == SB200_KIND_HEAT_F32;
+    const bool two = kind == SB200_KIND_WAVE2_F32;
     const int inz = static_cast<int>(g.nz - 8);
-    const int resident = f16 ? pencil_f16_resident(v) : pencil_f32_resident(heat, v);
+    const int resident = two ? leap2_resident(v)
+                             : (f16 ? pencil_f16_resident(v) : pencil_f32_resident(heat, v));
     const double slots = double(sm_count()) * std::max(1, resident);
     std::vector<std::pair<double, int>> scored;
     for (int zc = 1; zc <= 16 && zc <= inz; ++zc) {
-        const double ctas = double(f16 ? pencil_f16_ctas(v, g, zc) : pencil_f32_ctas(heat, v, g, zc));
+        const double ctas = double(two ? leap2_ctas(v, g, zc)
+                                       : (f16 ? pencil_f16_ctas(v, g, zc)
+                                              : pencil_f32_ctas(heat, v, g, zc)));
         const double waves = std::ceil(ctas / slots);
         const double fill = ctas / (waves * slots);
         const int zlen = (inz + zc - 1) / zc;
-        const double pshare = heat ? 0.5 : 0.25;
-        const double halo = double(zlen) / double(zlen + 8) * pshare + (1.0 - pshare);
+        // two steps: p is 4 of the pair's 20 B and a chunk reads 16 halo planes
+        const double pshare = two ? 0.2 : (heat ? 0.5 : 0.25);
+        const int hplanes = two ? 16 : 8;
+        const double halo = double(zlen) / double(zlen + hplanes) * pshare + (1.0 - pshare);
         scored.emplace_back(-(fill * halo), zc);
     }
     std::stable_sort(scored.begin(), scored.end());
@@ -344,6 +398,28 @@ int sb200_wave_step_f32(const float* p, const float* p_prev, const float* vel2, 
                         void* stream) {
     return wave_step(p, p_prev, vel2, p_next, grid, host_source(src_index, src_amp), stream,
                      true, "sb200_wave_step_f32");
+}
+
+int sb200_wave_step2_f32(const float* p, const float* p_prev, const float* vel2, float* p_next,
+                         float* p_next2, const sb200_grid* grid, int64_t src_index,
+                         float src_amp0, float src_amp1, void* stream) {
+    return wave_step2(p, p_prev, vel2, p_next, p_next2, grid, host_source(src_index, src_amp0),
+                      src_amp1, stream, false, "sb200_wave_step2_f32");
+}
+
+int sb200_wave_step2_dev_f32(const float* p, const float* p_prev, const float* vel2,
+                             float* p_next, float* p_next2, const sb200_grid* grid,
+                             int64_t src_index, const float* wavelet, const int* step,
+                             int step_offset, void* stream) {
+    if (src_index >= 0 && (!wavelet || !step))
+        return fail(SB200_ERR_INVALID, "sb200_wave_step2_dev_f32: NULL wavelet / step pointer");
+    SourceDesc s;
+    s.idx = src_index;
+    s.wavelet = wavelet;
+    s.step = step;
+    s.step_offset = step_offset;
+    return wave_step2(p, p_prev, vel2, p_next, p_next2, grid, s, 0.f, stream, false,
+                      "sb200_wave_step2_dev_f32");
 }
 
 int sb200_wave_step_exact_f32(const float* p, const float* p_prev, const float* vel2,
@@ -539,8 +615,7 @@ int sb200_pencil_variant_count(int kind) {
 
 const char* sb200_pencil_variant_name(int kind, int variant) {
     if (!valid_kind(kind)) return nullptr;
-    if (kind == SB200_KIND_WAVE_F16) return pencil_f16_variant_name(variant);
-    return pencil_f32_variant_name(kind == SB200_KIND_HEAT_F32, variant);
+    return variant_name(kind, variant);
 }
 
 int sb200_set_pencil_override(int kind, int variant, int zchunks) {

@@ -12,6 +12,12 @@ namespace sb200 {
 
 int dispatch_wave_f32(const float* p, const float* p_prev, const float* vel2, float* p_next,
                       const sb200_grid* grid, const SourceDesc& src, void* stream, bool exact);
+// Two acoustic steps in one sweep (out1 = t+dt, out2 = t+2dt; w1 = the host
+// sample of the second step).  outputs_may_alias: out1 == out2 is accepted
+// (timing trials only: the values are then unusable).
+int dispatch_wave2_f32(const float* p, const float* p_prev, const float* vel2, float* out1,
+                       float* out2, const sb200_grid* grid, const SourceDesc& src, float w1,
+                       void* stream, bool outputs_may_alias);
 int dispatch_wave_f16(const uint16_t* p, uint16_t* p_prev_next, const uint16_t* k,
                       const sb200_grid* grid, const SourceDesc& src, const sb200_f16_scale* scale,
                       int phase, void* stream);

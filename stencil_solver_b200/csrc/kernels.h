@@ -118,6 +118,22 @@ cudaError_t launch_heat_pencil_f32(const PencilMaps& maps, float* u_next, const 
 cudaError_t launch_prepass_pencil_f32(const PencilMaps& maps, float* prev, const float* vel2,
                                       float* r, const GridDesc& g, float beta,
                                       const PencilConfig& cfg, int* err, cudaStream_t stream);
+// Two acoustic steps per sweep (leap2_f32.cu): out1 = p at t+dt, out2 = p at
+// t+2dt, the same bits as two launch_wave_pencil_f32 steps.  maps: p with the
+// leap2_boxes(v) halo box, p_prev and vel2 with its tile box.  p, p_prev, vel2,
+// out1 and out2 are distinct; out1 and out2 keep their halo cells (they must
+// hold the walls).  The source adds src's sample at step s and w1 at step s+1
+// (with a wavelet table: wavelet[*step + step_offset] and the next sample).
+int leap2_variant_count();
+const char* leap2_variant_name(int v);
+PencilBoxes leap2_boxes(int v);
+int leap2_resident(int v);
+void leap2_prepare();
+int64_t leap2_ctas(int v, const GridDesc& g, int zchunks);
+cudaError_t launch_leap2_f32(const PencilMaps& maps, float* out1, float* out2, const GridDesc& g,
+                             const SourceDesc& src, float w1, const PencilConfig& cfg, int* err,
+                             cudaStream_t stream);
+
 // Resident CTAs per SM of a variant (occupancy query; analytic if that fails).
 // The first call per device also sets the variant's shared-memory attribute.
 int pencil_f32_resident(bool heat, int v);

@@ -18,6 +18,7 @@
 #include <tuple>
 #include <vector>
 
+#include "dispatch.h"
 #include "kernels.h"
 #include "stencil_b200.h"
 
@@ -84,10 +85,12 @@ extern "C" {
 int sb200_tune(int kind, const sb200_grid* grid, const void* field, const void* prev,
                const void* vel2, void* scratch, int reps, int* variant, int* zchunks,
                float* best_ms) {
-    if (kind != SB200_KIND_WAVE_F32 && kind != SB200_KIND_HEAT_F32 && kind != SB200_KIND_WAVE_F16)
+    if (kind != SB200_KIND_WAVE_F32 && kind != SB200_KIND_HEAT_F32 && kind != SB200_KIND_WAVE_F16 &&
+        kind != SB200_KIND_WAVE2_F32)
         return SB200_ERR_INVALID;
     const bool heat = kind == SB200_KIND_HEAT_F32;
     const bool f16 = kind == SB200_KIND_WAVE_F16;
+    const bool two = kind == SB200_KIND_WAVE2_F32;
     if (!grid || !field || !scratch || (!heat && (!prev || !vel2))) return SB200_ERR_INVALID;
     if (scratch == field || scratch == prev || scratch == vel2) return SB200_ERR_INVALID;
     const int nvar = sb200_pencil_variant_count(kind);
@@ -121,6 +124,11 @@ int sb200_tune(int kind, const sb200_grid* grid, const void* field, const void* 
         for (int zc : zchunk_ranking(kind, v, gd, 3)) {
             sb200_set_pencil_override(kind, v, zc);
             auto launch = [&]() {
+                if (two)  // both outputs into scratch: only the time matters
+                    return dispatch_wave2_f32(
+                        static_cast<const float*>(field), static_cast<const float*>(prev),
+                        static_cast<const float*>(vel2), static_cast<float*>(scratch),
+                        static_cast<float*>(scratch), grid, SourceDesc(), 0.f, nullptr, true);
                 if (f16)
                     return sb200_wave_step_f16(static_cast<const uint16_t*>(field),
                                                static_cast<uint16_t*>(scratch),
@@ -192,8 +200,11 @@ int sb200_tune_load(const char* path) {
         std::string dev;
         if (!(s >> kind >> nx >> ny >> nz >> v >> zc >> ms >> dev)) continue;
         const bool heat = kind == SB200_KIND_HEAT_F32;
-        if ((kind != SB200_KIND_WAVE_F32 && !heat) || v < 0 ||
-            v >= pencil_f32_variant_count(heat) || zc < 1)
+        const int nvar = kind == SB200_KIND_WAVE2_F32 ? leap2_variant_count()
+                         : kind == SB200_KIND_WAVE_F16 ? pencil_f16_variant_count()
+                                                       : pencil_f32_variant_count(heat);
+        if ((kind != SB200_KIND_WAVE_F32 && !heat && kind != SB200_KIND_WAVE2_F32) || v < 0 ||
+            v >= nvar || zc < 1)
             continue;  // stale entry from another build
         Choice c;
         c.variant = v;
