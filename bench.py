@@ -62,7 +62,8 @@ def args_():
                     help="--kernel learned: an all-zero field (floor 2^-64)")
     ap.add_argument("--flags", action="store_true",
                     help="--kernel learned --zero: with activity flags (all clear: the plain path)")
-    ap.add_argument("--kernel", choices=["acoustic", "heat", "fp16", "batch", "mlp", "learned"],
+    ap.add_argument("--kernel", choices=["acoustic", "wave2", "heat", "fp16", "batch", "mlp",
+                                         "learned"],
                     help="run only a small case of one kernel (for profilers) and print its time")
     return ap.parse_args()
 
@@ -850,7 +851,7 @@ def run_kernel_probe(a):
     gen = torch.Generator(device="cuda")
     gen.manual_seed(SEED)
     e0, e1 = _events()
-    if a.kernel in ("acoustic", "fp16", "heat", "mlp", "learned"):
+    if a.kernel in ("acoustic", "wave2", "fp16", "heat", "mlp", "learned"):
         g, vel2, vmax, src = workload(n)
         v = torch.from_numpy(vel2).cuda()
         p = torch.randn(g.shape, generator=gen, device="cuda") * 0.1
@@ -858,6 +859,11 @@ def run_kernel_probe(a):
         q = p * 0.99
         sb.set_pencil_override(sb.KIND_WAVE_F32, max(a.variant, 0), a.zchunks)
         f = lambda: sb.wave_step(p, q, v, q, g)  # noqa: E731
+    elif a.kernel == "wave2":  # two steps per sweep (one launch = two steps)
+        q = p * 0.99
+        o1, o2 = torch.zeros_like(p), torch.zeros_like(p)
+        sb.set_pencil_override(sb.KIND_WAVE2_F32, max(a.variant, 0), a.zchunks)
+        f = lambda: sb.wave_step2(p, q, v, o1, o2, g)  # noqa: E731
     elif a.kernel == "heat":
         un = torch.empty_like(p)
         sb.set_pencil_override(sb.KIND_HEAT_F32, max(a.variant, 0), a.zchunks)

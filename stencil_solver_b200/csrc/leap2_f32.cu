@@ -400,381 +400,6 @@ __global__ void __launch_bounds__(Shape2<TX, TY, S, AQ, AV>::NT, 1)
     }
 }
 
-// ── warp-specialised form ────────────────────────────────────────────────────
-// The A warps hold the p queue and compute stage A over the widened region; the
-// B warps hold the q queue and compute stage B over the tile.  A hands each q
-// plane to B through a QS-slot shared-memory ring, together with p and vel2 of
-// the tile at that plane (stage B's p_prev and vel2): mbarrier qfull[s] (one
-// arrival per A warp) says a slot is written, bdone[s] (one arrival per B warp)
-// that B finished an iteration, bstart that B's queue start-up has read planes
-// 0..7.  A runs at most D = QS - 4 iterations ahead of B (B reads plane i as its
-// queue feed at iteration i and as its x-y plane at iteration i + 4).  Each role
-// keeps one 9-deep queue, so both fit in fewer registers and the SM holds more
-// warps.  Every wait is bounded; a wait that gives up raises a shared abort
-// flag, the A warps decide to stop together through a barrier reduction and the
-// B warps per warp, so no hardware barrier is ever left waiting.
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-    asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
-}
-
-// Named barrier `id` over `count` threads (a multiple of 32) returning the OR of
-// `pred` over them.
-__device__ __forceinline__ bool bar_red_or(int id, int count, bool pred) {
-    uint32_t r;
-    asm volatile(
-        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\t"
-        "bar.red.or.pred q, %2, %3, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
-        : "=r"(r)
-        : "r"(static_cast<uint32_t>(pred)), "r"(id), "r"(count)
-        : "memory");
-    return r != 0;
-}
-
-template <int TX, int TY, int S, int AQ, int AV, int QS>
-struct ShapeWS {
-    static_assert(TX % 4 == 0 && TY % 2 == 0, "float4 columns, row pairs");
-    static_assert(S >= 8, "the p ring holds the 8 planes the queue start-up reads");
-    static_assert(AQ >= 2 && AV >= 2, "aux rings");
-    // B's queue start-up reads q planes 0..7 before A may reuse a slot
-    static_assert(QS >= 8, "the q ring holds the 8 planes of stage B's queue start-up");
-    static constexpr int EX = TX + 2 * R, EY = TY + 2 * R;
-    static constexpr int SX0 = TX + 4 * R, SY0 = TY + 4 * R;
-    static_assert(SX0 <= 256 && SY0 <= 256, "TMA box extent is at most 256");
-    static constexpr int CX = EX / 4;
-    static constexpr int NB = (TX / 4) * (TY / 2);  // stage B tasks
-    static constexpr int NA = CX * (EY / 2);        // stage A tasks
-    static constexpr int NWA = (NA + 31) / 32, NWB = (NB + 31) / 32;
-    static constexpr int NT = 32 * (NWA + NWB);
-    static constexpr uint32_t P_BYTES = SX0 * SY0 * 4u;
-    static constexpr int PST = int(((P_BYTES + 127u) / 128u) * 32u);
-    static constexpr uint32_t E_BYTES = EX * EY * 4u;
-    static constexpr int EST = int(((E_BYTES + 127u) / 128u) * 32u);
-    static constexpr int TT = TX * TY;                                    // floats per tile field
-    static constexpr int BST = int(((2u * TT * 4u + 127u) / 128u) * 32u);  // p + vel2 slot
-    static constexpr int D = QS - 4;  // A's largest lead over B, iterations
-    static constexpr size_t SMEM =
-        (size_t(S) * PST + size_t(AQ + AV + QS) * EST + size_t(QS) * BST) * 4 + 128;
-    static_assert(SMEM + 512 <= 232448, "shared memory of one CTA");
-};
-
-template <int TX, int TY, int S, int AQ, int AV, int QS>
-__global__ void __launch_bounds__(ShapeWS<TX, TY, S, AQ, AV, QS>::NT, 1)
-    leap2ws_kernel(const __grid_constant__ CUtensorMap pmap,
-                   const __grid_constant__ CUtensorMap qmap,
-                   const __grid_constant__ CUtensorMap vmap, const Leap2Args a) {
-    using P = ShapeWS<TX, TY, S, AQ, AV, QS>;
-    extern __shared__ unsigned char dsmem[];
-    __shared__ __align__(8) uint64_t fullp[S];
-    __shared__ __align__(8) uint64_t fullq[AQ];
-    __shared__ __align__(8) uint64_t fullv[AV];
-    __shared__ __align__(8) uint64_t qfull[QS];
-    __shared__ __align__(8) uint64_t bdone[QS];
-    __shared__ __align__(8) uint64_t bstart;
-    __shared__ volatile int s_abort;
-    const int tid = threadIdx.x;
-    const int lane = tid & 31;
-    if (tid == 0) {
-#pragma unroll
-        for (int s = 0; s < S; ++s) mbar_init(&fullp[s], 1);
-#pragma unroll
-        for (int s = 0; s < AQ; ++s) mbar_init(&fullq[s], 1);
-#pragma unroll
-        for (int s = 0; s < AV; ++s) mbar_init(&fullv[s], 1);
-#pragma unroll
-        for (int s = 0; s < QS; ++s) {
-            mbar_init(&qfull[s], P::NWA);
-            mbar_init(&bdone[s], P::NWB);
-        }
-        mbar_init(&bstart, P::NWB);
-        fence_barrier_init();
-        s_abort = 0;
-    }
-    __syncthreads();
-    float* sp = reinterpret_cast<float*>(smem_align<128>(dsmem));  // S p planes
-    float* sq = sp + S * P::PST;                                   // AQ p_prev tiles
-    float* sv = sq + AQ * P::EST;                                  // AV vel2 tiles
-    float* s1 = sv + AV * P::EST;                                  // QS q planes
-    float* sb = s1 + QS * P::EST;                                  // QS (p, vel2) tiles for B
-
-    int b = blockIdx.x;
-    const int tile_x = b % a.tiles_x;
-    b /= a.tiles_x;
-    const int tile_y = b % a.tiles_y;
-    const int zc = b / a.tiles_y;
-    const int x0 = R + tile_x * TX;
-    const int y0 = R + tile_y * TY;
-    const int zb = R + zc * a.zlen;
-    const int ze = min(zb + a.zlen, a.nz - R);
-    const int nint = ze - zb;
-    const int nit = nint + 2 * R;
-    const int np = nint + 4 * R;
-    const Leap2Math m(a.w);
-
-    if (tid < 32 * P::NWA) {
-        // ───────────── A warps: stage A over the widened region ─────────────
-        const bool valid = tid < P::NA;
-        int ex = 0, ey = 0;
-        if (valid) task_of<TX, TY>(tid, ex, ey);
-        const bool inner = tid < P::NB;
-        const int gx = x0 - R + 4 * ex;
-        const int gy = y0 - R + ey;
-        const bool xin = valid && gx >= R && gx < a.nx - R;
-        bool rin[2];
-#pragma unroll
-        for (int r = 0; r < 2; ++r) rin[r] = xin && gy + r >= R && gy + r < a.ny - R;
-        const int poff = (ey + R) * P::SX0 + 4 * ex + R;
-        const int eoff = ey * P::EX + 4 * ex;
-        const int boff = (ey - R) * TX + 4 * (ex - 1);  // inner: the task in a B tile
-        int src_r = -1, src_e = 0;
-        if (xin && a.src_z >= 0 && a.src_x >= gx && a.src_x < gx + 4 && a.src_y >= gy &&
-            a.src_y < gy + 2) {
-            src_r = a.src_y - gy;
-            src_e = a.src_x - gx;
-        }
-        int hp = -1, hq = -1, hv = -1;
-        auto issue_p = [&](int j) {
-            const int s = j % S;
-            mbar_arrive_expect_tx(&fullp[s], P::P_BYTES);
-            tma_load_3d(sp + s * P::PST, &pmap, &fullp[s], x0 - 2 * R, y0 - 2 * R, zb - 2 * R + j);
-            hp = j;
-        };
-        auto issue_q = [&](int i) {
-            const int s = i % AQ;
-            mbar_arrive_expect_tx(&fullq[s], P::E_BYTES);
-            tma_load_3d(sq + s * P::EST, &qmap, &fullq[s], x0 - R, y0 - R, zb - R + i);
-            hq = i;
-        };
-        auto issue_v = [&](int i) {
-            const int s = i % AV;
-            mbar_arrive_expect_tx(&fullv[s], P::E_BYTES);
-            tma_load_3d(sv + s * P::EST, &vmap, &fullv[s], x0 - R, y0 - R, zb - R + i);
-            hv = i;
-        };
-        auto wait_p = [&](int j) { return mbar_wait(&fullp[j % S], (j / S) & 1); };
-        auto wait_q = [&](int i) { return mbar_wait(&fullq[i % AQ], (i / AQ) & 1); };
-        auto wait_v = [&](int i) { return mbar_wait(&fullv[i % AV], (i / AV) & 1); };
-        if (tid == 0) {
-            prefetch_tmap(&pmap);
-            prefetch_tmap(&qmap);
-            prefetch_tmap(&vmap);
-            for (int j = 0; j < S && j < np; ++j) issue_p(j);
-            for (int i = 0; i < AQ && i < nit; ++i) issue_q(i);
-            for (int i = 0; i < AV && i < nit; ++i) issue_v(i);
-        }
-        float4 qp[9][2];
-        bool bad = false;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            if (!wait_p(j)) bad = true;
-            const float* pl = sp + (j % S) * P::PST + poff;
-            if (valid) {
-                qp[j][0] = lds128(pl);
-                qp[j][1] = lds128(pl + P::SX0);
-            }
-        }
-        bool abort_run = bar_red_or(1, 32 * P::NWA, bad);
-        if (!abort_run && tid == 0)
-#pragma unroll
-            for (int j = 0; j < R; ++j)
-                if (j + S < np) issue_p(j + S);
-        int64_t goff = static_cast<int64_t>(zb - R) * a.sz + static_cast<int64_t>(gy) * a.sy + gx;
-        for (int i0 = 0; i0 < nit && !abort_run; i0 += 9) {
-#pragma unroll
-            for (int u = 0; u < 9; ++u) {
-                const int i = i0 + u;
-                if (i < nit && !abort_run) {
-                    const int za = zb - R + i;
-                    if (!wait_p(i + 8)) bad = true;
-                    if (valid) {
-                        const float* pf = sp + ((i + 8) % S) * P::PST + poff;
-                        qp[(u + 8) % 9][0] = lds128(pf);
-                        qp[(u + 8) % 9][1] = lds128(pf + P::SX0);
-                    }
-                    if (!wait_q(i)) bad = true;
-                    if (!wait_v(i)) bad = true;
-                    // slot i % QS: B is done with plane i - QS -- read by its queue
-                    // start-up (planes 0..7) or, from plane 4 on, as the x-y plane of
-                    // iteration i - QS + 4 = i - D
-                    if (i - P::D >= 2 * R) {
-                        const int k = i - P::D - 2 * R;
-                        if (!mbar_wait(&bdone[k % QS], (k / QS) & 1)) bad = true;
-                    } else if (i == QS) {
-                        if (!mbar_wait(&bstart, 0)) bad = true;
-                    }
-                    if (valid) {
-                        const float* qt = sq + (i % AQ) * P::EST + eoff;
-                        const float* vt = sv + (i % AV) * P::EST + eoff;
-                        const float4 pv[2] = {lds128(qt), lds128(qt + P::EX)};
-                        float4 qn[2] = {pv[0], pv[1]};
-                        if (za >= R && za < a.nz - R) {
-                            const float4 vv[2] = {lds128(vt), lds128(vt + P::EX)};
-                            const float4 c[2] = {qp[(u + 4) % 9][0], qp[(u + 4) % 9][1]};
-                            float2 lap[2][2];
-                            m.laplacian(
-                                sp + ((i + 4) % S) * P::PST + poff, P::SX0, c,
-                                [&](int r, int j) -> const float4& { return qp[(u + 4 + r) % 9][j]; },
-                                [&](int r, int j) -> const float4& {
-                                    return qp[(u + 4 - r + 9) % 9][j];
-                                },
-                                lap);
-#pragma unroll
-                            for (int r = 0; r < 2; ++r) {
-                                float4 o = m.update(c[r], pv[r], vv[r], lap[r]);
-                                if (src_r == r && za == a.src_z) {
-                                    Leap2Math::add_source(o, vv[r], a.dt2, source_sample(a, 0), src_e);
-                                    if (inner && za >= zb && za < ze)
-                                        record_trace(a, 0, f4get(o, src_e));
-                                }
-                                if (rin[r]) qn[r] = o;
-                            }
-                            if (inner && za >= zb && za < ze) {  // stage B's p_prev and vel2
-                                float* bt = sb + (i % QS) * P::BST + boff;
-                                sts128(bt, c[0]);
-                                sts128(bt + TX, c[1]);
-                                sts128(bt + P::TT, vv[0]);
-                                sts128(bt + P::TT + TX, vv[1]);
-                            }
-                        }
-                        float* qs = s1 + (i % QS) * P::EST + eoff;
-                        sts128(qs, qn[0]);
-                        sts128(qs + P::EX, qn[1]);
-                        if (inner && za >= zb && za < ze) {
-#pragma unroll
-                            for (int r = 0; r < 2; ++r)
-                                if (rin[r]) stg_stream(a.out1 + goff + r * a.sy, qn[r]);
-                        }
-                    }
-                    goff += a.sz;
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(&qfull[i % QS]);
-                    abort_run = bar_red_or(1, 32 * P::NWA, bad || s_abort != 0);
-                    if (!abort_run && tid == 0) {
-                        if (i + 4 + S < np) issue_p(i + 4 + S);
-                        if (i + AQ < nit) issue_q(i + AQ);
-                        if (i + AV < nit) issue_v(i + AV);
-                    }
-                }
-            }
-        }
-        if (abort_run && tid == 0) {
-            s_abort = 1;
-            record_error(a.err, kDevWaitTimeout);
-            for (int j = max(0, hp - S + 1); j <= hp; ++j) (void)wait_p(j);
-            for (int k = max(0, hq - AQ + 1); k <= hq; ++k) (void)wait_q(k);
-            for (int k = max(0, hv - AV + 1); k <= hv; ++k) (void)wait_v(k);
-        }
-    } else {
-        // ───────────── B warps: stage B over the tile ─────────────
-        const int bt = tid - 32 * P::NWA;
-        const bool valid = bt < P::NB;
-        const int ix = bt % (TX / 4), iy = bt / (TX / 4);
-        const int ex = 1 + ix, ey = R + 2 * iy;  // the same task as A thread bt
-        const int gx = x0 - R + 4 * ex;
-        const int gy = y0 - R + ey;
-        const bool xin = valid && gx < a.nx - R;
-        bool rin[2];
-#pragma unroll
-        for (int r = 0; r < 2; ++r) rin[r] = xin && gy + r < a.ny - R;
-        const int eoff = ey * P::EX + 4 * ex;
-        const int boff = 2 * iy * TX + 4 * ix;
-        int src_r = -1, src_e = 0;
-        if (xin && a.src_z >= 0 && a.src_x >= gx && a.src_x < gx + 4 && a.src_y >= gy &&
-            a.src_y < gy + 2) {
-            src_r = a.src_y - gy;
-            src_e = a.src_x - gx;
-        }
-        float4 q1[9][2];
-        bool bad = false;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            if (!mbar_wait(&qfull[j % QS], (j / QS) & 1)) bad = true;
-            if (valid) {
-                const float* qs = s1 + (j % QS) * P::EST + eoff;
-                q1[j][0] = lds128(qs);
-                q1[j][1] = lds128(qs + P::EX);
-            }
-        }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&bstart);
-        bool stop = __any_sync(0xffffffffu, bad || s_abort != 0);
-        int64_t goff = static_cast<int64_t>(zb) * a.sz + static_cast<int64_t>(gy) * a.sy + gx;
-        for (int j0 = 0; j0 < nit && !stop; j0 += 9) {
-#pragma unroll
-            for (int u = 0; u < 9; ++u) {
-                const int j = j0 + u;
-                if (j >= 2 * R && j < nit && !stop) {
-                    if (!mbar_wait(&qfull[j % QS], (j / QS) & 1)) bad = true;
-                    if (valid) {
-                        const float* qs = s1 + (j % QS) * P::EST + eoff;
-                        q1[u][0] = lds128(qs);
-                        q1[u][1] = lds128(qs + P::EX);
-                        const float* bp = sb + ((j - R) % QS) * P::BST + boff;
-                        const float4 pv[2] = {lds128(bp), lds128(bp + TX)};
-                        const float4 vv[2] = {lds128(bp + P::TT), lds128(bp + P::TT + TX)};
-                        const float4 c[2] = {q1[(u + 5) % 9][0], q1[(u + 5) % 9][1]};
-                        float2 lap[2][2];
-                        m.laplacian(
-                            s1 + ((j - R) % QS) * P::EST + eoff, P::EX, c,
-                            [&](int r, int k) -> const float4& { return q1[(u + 5 + r) % 9][k]; },
-                            [&](int r, int k) -> const float4& { return q1[(u + 5 - r + 9) % 9][k]; },
-                            lap);
-                        const int zbb = zb - 2 * R + j;
-#pragma unroll
-                        for (int r = 0; r < 2; ++r) {
-                            float4 o = m.update(c[r], pv[r], vv[r], lap[r]);
-                            if (src_r == r && zbb == a.src_z) {
-                                Leap2Math::add_source(o, vv[r], a.dt2, source_sample(a, 1), src_e);
-                                record_trace(a, 1, f4get(o, src_e));
-                            }
-                            if (rin[r]) stg_stream(a.out2 + goff + r * a.sy, o);
-                        }
-                    }
-                    goff += a.sz;
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(&bdone[(j - 2 * R) % QS]);
-                    stop = __any_sync(0xffffffffu, bad || s_abort != 0);
-                    if (stop && lane == 0 && bad) {
-                        s_abort = 1;
-                        record_error(a.err, kDevWaitTimeout);
-                    }
-                }
-            }
-        }
-    }
-}
-
-template <int TX, int TY, int S, int AQ, int AV, int QS>
-int resident_leap2ws() {
-    using P = ShapeWS<TX, TY, S, AQ, AV, QS>;
-    static int cached[64] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (cached[dev & 63] > 0) return cached[dev & 63];
-    auto kern = leap2ws_kernel<TX, TY, S, AQ, AV, QS>;
-    int n = 0;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(P::SMEM)) == cudaSuccess &&
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, P::NT, P::SMEM) == cudaSuccess &&
-        n > 0) {
-        cached[dev & 63] = n;
-        return n;
-    }
-    cudaGetLastError();
-    return 1;
-}
-
-template <int TX, int TY, int S, int AQ, int AV, int QS>
-cudaError_t launch_leap2ws(const PencilMaps& m, const Leap2Args& a, unsigned ctas,
-                           cudaStream_t stream) {
-    using P = ShapeWS<TX, TY, S, AQ, AV, QS>;
-    resident_leap2ws<TX, TY, S, AQ, AV, QS>();
-    leap2ws_kernel<TX, TY, S, AQ, AV, QS><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev, m.vel2,
-                                                                            a);
-    return cudaGetLastError();
-}
-
 template <int TX, int TY, int S, int AQ, int AV>
 int resident_leap2() {
     using P = Shape2<TX, TY, S, AQ, AV>;
@@ -814,17 +439,15 @@ struct Leap2Variant {
 #define SB200_LEAP2(TX, TY, S, AQ, AV, NAME) \
     Leap2Variant { TX, TY, NAME, &launch_leap2<TX, TY, S, AQ, AV>, &resident_leap2<TX, TY, S, AQ, AV> }
 
-#define SB200_LEAP2WS(TX, TY, S, AQ, AV, QS, NAME)                                   \
-    Leap2Variant {                                                                   \
-        TX, TY, NAME, &launch_leap2ws<TX, TY, S, AQ, AV, QS>,                        \
-            &resident_leap2ws<TX, TY, S, AQ, AV, QS>                                 \
-    }
-
+// Measured at 1024^3 (ms per step, one-step kernel 2.73): l64x16 3.95-3.98,
+// l32x32 3.97-4.12 (z split 2-4).  Not kept: a warp-specialised form (A warps
+// holding the p queue, B warps the q queue, q planes handed over through an
+// mbarrier ring; 158-161 registers, 11 warps per SM) at 7.26-7.48 -- its two
+// 9x-unrolled loops run side by side and stall on instruction fetch (6.1 stalls
+// per issue against 1.3).
 const Leap2Variant kLeap2[] = {
     SB200_LEAP2(32, 32, 8, 3, 8, "l32x32_s8"),
     SB200_LEAP2(64, 16, 8, 3, 8, "l64x16_s8"),
-    SB200_LEAP2WS(32, 32, 8, 3, 3, 8, "w32x32_s8_q8"),
-    SB200_LEAP2WS(64, 16, 8, 2, 2, 8, "w64x16_s8_q8"),
 };
 constexpr int kNumLeap2 = sizeof(kLeap2) / sizeof(kLeap2[0]);
 
