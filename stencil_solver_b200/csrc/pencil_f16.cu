@@ -329,14 +329,22 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                 // own 8 points (the centre) are converted once.
                 const uint2 lf = lds64(pc - 4);
                 const uint2 rt = lds64(pc + 8);
-                float2 cv[4];
-#pragma unroll
-                for (int h = 0; h < 4; ++h) cv[h] = h2f2(get_word(hq[u % 4], h));
-                const float cf[8] = {cv[0].x, cv[0].y, cv[1].x, cv[1].y,
-                                     cv[2].x, cv[2].y, cv[3].x, cv[3].y};
-                // feed: plane i + 8 (z + 4) replaces the centre in slot u
+                // feed: plane i + 8 (z + 4) replaces the centre in slot u; the z pair
+                // of radius 4 is formed at once, so plane z - 4 (FP32 slot u) is dead
+                // before the centre is converted into that slot -- the two never
+                // hold registers at the same time and the slots need no copies.
+                const uint4 c16 = hq[u % 4];
                 if (!mbar_wait(&full[fst], fph)) bad = true;
                 hq[u % 4] = lds128h(sm + fst * P::PLANE + soff);
+                float2 z4[4];
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    z4[h] = addhf2(get_word(hq[u % 4], h), dq[u % 4][h]);
+                    dq[u % 4][h] = h2f2(get_word(c16, h));
+                }
+                const float2(&cv)[4] = dq[u % 4];  // the centre, FP32
+                const float cf[8] = {cv[0].x, cv[0].y, cv[1].x, cv[1].y,
+                                     cv[2].x, cv[2].y, cv[3].x, cv[3].y};
                 uint4 yu[R], yd[R];  // staged rows y +- d of the centre plane
 #pragma unroll
                 for (int d = 1; d <= R; ++d) {
@@ -347,7 +355,8 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                 // pair sums s = p[+r] + p[-r]; up operands of y and z enter FP16.
                 // z pair of radius r: up plane (slot (u + r) % 4) + down plane
                 auto zpair = [&](int r, int h) {
-                    return addhf2(get_word(hq[(u + r) % 4], h), dq[(u + 4 - r) % 4][h]);
+                    return r == R ? z4[h]
+                                  : addhf2(get_word(hq[(u + r) % 4], h), dq[(u + 4 - r) % 4][h]);
                 };
                 float2 lap[4];
 #pragma unroll
@@ -382,9 +391,6 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                     if (UPD & kUpdExactY) txy = fma2(dup2(kInv5040), ty, txy);
                     lap[h] = add2(txy, tz);
                 }
-                // plane z - 4 is no longer needed: its slot takes the centre (z).
-#pragma unroll
-                for (int h = 0; h < 4; ++h) dq[u % 4][h] = cv[h];
 
                 bool aok;
                 const uint16_t* st;
