@@ -351,8 +351,9 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                     yu[d - 1] = lds128h(pc + d * P::SX);
                     yd[d - 1] = lds128h(pc - d * P::SX);
                 }
-                // lap = [c (cx+cy+cz) + sum_r (ax_r sx_r + ay_r sy_r)] + sum_r az_r sz_r,
-                // pair sums s = p[+r] + p[-r]; up operands of y and z enter FP16.
+                // lap = c (cx+cy+cz) + sum_r (ax_r sx_r [+ ay_r sy_r] + az_r sz_r) in one
+                // chain (+ sy5040 / 5040 with exact y), pair sums s = p[+r] + p[-r];
+                // up operands of y and z enter FP16.
                 // z pair of radius r: up plane (slot (u + r) % 4) + down plane
                 auto zpair = [&](int r, int h) {
                     return r == R ? z4[h]
@@ -362,9 +363,10 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
 #pragma unroll
                 for (int h = 0; h < 4; ++h) {
                     const float2 c = cv[h];
+                    // one chain: centre, then per radius the x pair and the z pair
+                    // (and the y pair without exact y); 5040 x the y pairs apart
                     float2 txy = mul2(cxy2, c);
                     float2 ty = make_float2(0.f, 0.f);  // kUpdExactY: 5040 x the y pairs
-                    float2 tz = mul2(az2[0], zpair(1, h));
 #pragma unroll
                     for (int r = 1; r <= R; ++r) {
                         // an aligned pair of own points (even r) adds as one pair
@@ -386,10 +388,10 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                         }
                         // up: plane z + r (FP16, slot (u + r) % 4; r = 4 is the plane
                         // just fed); down: plane z - r (FP32, slot (u + 4 - r) % 4)
-                        if (r > 1) tz = fma2(az2[r - 1], zpair(r, h), tz);
+                        txy = fma2(az2[r - 1], zpair(r, h), txy);
                     }
                     if (UPD & kUpdExactY) txy = fma2(dup2(kInv5040), ty, txy);
-                    lap[h] = add2(txy, tz);
+                    lap[h] = txy;
                 }
 
                 bool aok;
