@@ -112,3 +112,22 @@ def test_tune_cache_load_skips_bad_lines(tmp_path):
     lines = out.read_text().split("\n")
     assert any(l.startswith("0 1024 1024 1024 1 4") for l in lines)
     assert any(l.startswith("1 512 512 512 0 2") for l in lines)
+
+
+def test_two_step_argument_checks():
+    """sb200_wave_step2_f32 wants five distinct fields: every aliasing of an output
+    with an input, the two outputs with each other and p with p_prev is refused
+    before any device work (the pointers are never dereferenced)."""
+    g = sb.Grid(32, 32, 32)
+    p, q, v, o1, o2 = 256, 512, 768, 1024, 1280
+    for args in ((p, q, v, q, o2), (p, q, v, o1, p), (p, q, v, v, o2), (p, q, v, o1, o1),
+                 (p, p, v, o1, o2)):
+        with pytest.raises(sb.StencilError) as e:
+            sb.wave_step2(*args, g)
+        assert e.value.status == sb.SB200_ERR_INVALID
+    with pytest.raises(sb.StencilError, match="NULL"):
+        sb.wave_step2(p, q, None, o1, o2, g)
+    with pytest.raises(sb.StencilError, match="source"):
+        sb.wave_step2(p, q, v, o1, o2, g, src_index=g.size)
+    sb.wave_step2(p, q, v, o1, o2, sb.Grid(8, 8, 8))  # no interior: nothing to do
+    assert sb.variant_names(sb.KIND_WAVE2_F32)
