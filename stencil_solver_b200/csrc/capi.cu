@@ -110,7 +110,7 @@ int default_variant(int kind) {
     const char* want = kind == SB200_KIND_WAVE_F32   ? "t64x32_r2_s8_a3"
                        : kind == SB200_KIND_HEAT_F32 ? "t64x16_r2_s8"
                        : kind == SB200_KIND_WAVE_F16 ? "h64x16_s8_a4"
-                                                     : "l64x16_s8";
+                                                     : "l32x32_r1_s8";
     const int n = variant_count(kind);
     for (int v = 0; v < n; ++v) {
         const char* name = variant_name(kind, v);

@@ -17,7 +17,7 @@
 //     last five iterations (a shared-memory ring, x-y neighbours) and a 9-deep
 //     register queue of q for the z neighbours; p_prev of that step is p itself,
 //     still in the first queue, and vel2 is still in its ring.
-// Each thread owns a float4 of x in two rows of the widened region; the threads
+// Each thread owns a float4 of x in RPT (1 or 2) rows of the widened region; the threads
 // whose rows lie in the tile run both stages, the others (the 4-cell ring around
 // the tile) stage A only.  Points of the widened region outside the grid's
 // interior keep p_prev's value (a one-step launch never writes them, and it runs
@@ -53,9 +53,10 @@ struct Leap2Args {
     int* err;
 };
 
-template <int TX, int TY, int S, int AQ, int AV>
+template <int TX, int TY, int RPT, int S, int AQ, int AV>
 struct Shape2 {
-    static_assert(TX % 4 == 0 && TY % 2 == 0, "float4 columns, row pairs");
+    static_assert(RPT == 1 || RPT == 2, "one or two rows per thread");
+    static_assert(TX % 4 == 0 && TY % RPT == 0, "float4 columns, RPT-row tasks");
     static_assert(S >= 8, "the p ring holds the 8 planes the queue start-up reads");
     static_assert(AV >= 6, "vel2 stays staged for stage B, 4 iterations later");
     static_assert(AQ >= 2, "p_prev ring");
@@ -63,8 +64,8 @@ struct Shape2 {
     static constexpr int SX0 = TX + 4 * R, SY0 = TY + 4 * R;  // p box
     static_assert(SX0 <= 256 && SY0 <= 256, "TMA box extent is at most 256");
     static constexpr int CX = EX / 4;                 // float4 columns of the widened region
-    static constexpr int NB = (TX / 4) * (TY / 2);    // tasks in the tile (both stages)
-    static constexpr int NT = CX * (EY / 2);          // threads: every task of the widened region
+    static constexpr int NB = (TX / 4) * (TY / RPT);  // tasks in the tile (both stages)
+    static constexpr int NT = CX * (EY / RPT);        // threads: every task of the widened region
     static constexpr uint32_t P_BYTES = SX0 * SY0 * 4u;
     static constexpr int PST = int(((P_BYTES + 127u) / 128u) * 32u);  // stage stride, floats
     static constexpr uint32_t E_BYTES = EX * EY * 4u;
@@ -75,7 +76,7 @@ struct Shape2 {
 
 __device__ __forceinline__ void sts128(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
 
-// The one-step kernel's per-point arithmetic on two rows of a float4 column
+// The one-step kernel's per-point arithmetic on RPT rows of a float4 column
 // (pencil_f32.cu, acoustic mode): y rows accumulated in row order, x and z pairs
 // with the centre cancelled first, combined as (x + y) + z; the update rounds
 // 2c - p_prev once, then adds vel2 * lap.  Packed f32x2 lanes round as scalars.
@@ -94,18 +95,18 @@ struct Leap2Math {
         neg1 = dup2(-1.f);
     }
     // pc: the task's first point in a staged plane of row stride SX; c: its own
-    // two rows; up(r, row) / dn(r, row): the z neighbours at +-r.
-    template <class Up, class Dn>
-    __device__ __forceinline__ void laplacian(const float* pc, int SX, const float4 (&c)[2],
-                                              Up&& up, Dn&& dn, float2 (&lap)[2][2]) const {
-        float2 ya[2][2];
+    // RPT rows; up(r, row) / dn(r, row): the z neighbours at +-r.
+    template <int RPT, class Up, class Dn>
+    __device__ __forceinline__ void laplacian(const float* pc, int SX, const float4 (&c)[RPT],
+                                              Up&& up, Dn&& dn, float2 (&lap)[RPT][2]) const {
+        float2 ya[RPT][2];
 #pragma unroll
-        for (int j = 0; j < 2; ++j) ya[j][0] = ya[j][1] = make_float2(0.f, 0.f);
+        for (int j = 0; j < RPT; ++j) ya[j][0] = ya[j][1] = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int k = -R; k < 2 + R; ++k) {
-            const float4 row = (k >= 0 && k < 2) ? c[k] : lds128(pc + k * SX);
+        for (int k = -R; k < RPT + R; ++k) {
+            const float4 row = (k >= 0 && k < RPT) ? c[k] : lds128(pc + k * SX);
 #pragma unroll
-            for (int j = 0; j < 2; ++j) {
+            for (int j = 0; j < RPT; ++j) {
                 const int d = k > j ? k - j : j - k;
                 if (d >= 1 && d <= R) {
                     ya[j][0] = fma2(ay2[d - 1], pair_of(row, 0), ya[j][0]);
@@ -114,7 +115,7 @@ struct Leap2Math {
             }
         }
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
+        for (int j = 0; j < RPT; ++j) {
             const float4 cc = c[j];
             const float4 lf = lds128(pc + j * SX - 4);
             const float4 rt = lds128(pc + j * SX + 4);
@@ -166,41 +167,41 @@ __device__ __forceinline__ void record_trace(const Leap2Args& a, int k, float v)
     if (a.trace) a.trace[(a.src_step ? *a.src_step : 0) + a.src_off + k] = v;
 }
 
-// Thread t -> its task: float4 column ex and first row ey of the widened region.
-// Threads [0, NB) take the tile row-major; the rest take the ring: the two row
-// pairs above the tile, the two below, then the left / right column of each row
-// pair beside it.
-template <int TX, int TY>
+// Thread t -> its task: float4 column ex and first row ey (of RPT) of the widened
+// region.  Threads [0, NB) take the tile row-major; the rest take the ring: the
+// 4 rows above the tile, the 4 below, then the left / right column of each task
+// row beside it.
+template <int TX, int TY, int RPT>
 __device__ __forceinline__ void task_of(int t, int& ex, int& ey) {
-    constexpr int CX = (TX + 2 * R) / 4, EY = TY + 2 * R, NB = (TX / 4) * (TY / 2);
+    constexpr int CX = (TX + 2 * R) / 4, EY = TY + 2 * R, NB = (TX / 4) * (TY / RPT);
     if (t < NB) {
         ex = 1 + t % (TX / 4);
-        ey = R + 2 * (t / (TX / 4));
+        ey = R + RPT * (t / (TX / 4));
         return;
     }
     int k = t - NB;
-    constexpr int band = 2 * CX;
+    constexpr int band = (R / RPT) * CX;  // the 4 rows above (below) the tile
     if (k < band) {
         ex = k % CX;
-        ey = 2 * (k / CX);
+        ey = RPT * (k / CX);
         return;
     }
     k -= band;
     if (k < band) {
         ex = k % CX;
-        ey = EY - R + 2 * (k / CX);
+        ey = EY - R + RPT * (k / CX);
         return;
     }
     k -= band;
     ex = (k & 1) ? CX - 1 : 0;
-    ey = R + 2 * (k >> 1);
+    ey = R + RPT * (k >> 1);
 }
 
-template <int TX, int TY, int S, int AQ, int AV>
-__global__ void __launch_bounds__(Shape2<TX, TY, S, AQ, AV>::NT, 1)
+template <int TX, int TY, int RPT, int S, int AQ, int AV>
+__global__ void __launch_bounds__(Shape2<TX, TY, RPT, S, AQ, AV>::NT, 1)
     leap2_kernel(const __grid_constant__ CUtensorMap pmap, const __grid_constant__ CUtensorMap qmap,
                  const __grid_constant__ CUtensorMap vmap, const Leap2Args a) {
-    using P = Shape2<TX, TY, S, AQ, AV>;
+    using P = Shape2<TX, TY, RPT, S, AQ, AV>;
     extern __shared__ unsigned char dsmem[];
     __shared__ __align__(8) uint64_t fullp[S];
     __shared__ __align__(8) uint64_t fullq[AQ];
@@ -267,20 +268,20 @@ __global__ void __launch_bounds__(Shape2<TX, TY, S, AQ, AV>::NT, 1)
     }
 
     int ex, ey;
-    task_of<TX, TY>(tid, ex, ey);
+    task_of<TX, TY, RPT>(tid, ex, ey);
     const bool inner = tid < P::NB;  // the task lies in the tile: stage B too
     const int gx = x0 - R + 4 * ex;  // first x of the task (a multiple of 4)
     const int gy = y0 - R + ey;      // first row of the task
     const bool xin = gx >= R && gx < a.nx - R;  // the float4 is interior or halo as a whole
-    bool rin[2];
+    bool rin[RPT];
 #pragma unroll
-    for (int r = 0; r < 2; ++r) rin[r] = xin && gy + r >= R && gy + r < a.ny - R;
+    for (int r = 0; r < RPT; ++r) rin[r] = xin && gy + r >= R && gy + r < a.ny - R;
     const int poff = (ey + R) * P::SX0 + 4 * ex + R;  // task in a p plane
     const int eoff = ey * P::EX + 4 * ex;             // task in a widened-region tile
 
     // Source ownership (row, element) within the task.
     int src_r = -1, src_e = 0;
-    if (a.src_z >= 0 && a.src_x >= gx && a.src_x < gx + 4 && a.src_y >= gy && a.src_y < gy + 2 &&
+    if (a.src_z >= 0 && a.src_x >= gx && a.src_x < gx + 4 && a.src_y >= gy && a.src_y < gy + RPT &&
         xin) {
         src_r = a.src_y - gy;
         src_e = a.src_x - gx;
@@ -288,15 +289,15 @@ __global__ void __launch_bounds__(Shape2<TX, TY, S, AQ, AV>::NT, 1)
 
     const Leap2Math m(a.w);
 
-    float4 qp[9][2];  // p: planes z-4 .. z+4 of stage A (slot = plane index % 9)
-    float4 q1[9][2];  // q: planes z-8 .. z of stage B's z neighbours (slot = iteration % 9)
+    float4 qp[9][RPT];  // p: planes z-4 .. z+4 of stage A (slot = plane index % 9)
+    float4 q1[9][RPT];  // q: planes z-8 .. z of stage B's z neighbours (slot = iteration % 9)
     bool bad = false;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         if (!wait_p(j)) bad = true;
         const float* pl = sp + (j % S) * P::PST + poff;
-        qp[j][0] = lds128(pl);
-        qp[j][1] = lds128(pl + P::SX0);
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) qp[j][r] = lds128(pl + r * P::SX0);
     }
     bool abort_run = __syncthreads_or(bad) != 0;
     if (!abort_run && tid == 0)
@@ -315,26 +316,31 @@ __global__ void __launch_bounds__(Shape2<TX, TY, S, AQ, AV>::NT, 1)
                 {
                     if (!wait_p(i + 8)) bad = true;
                     const float* pf = sp + ((i + 8) % S) * P::PST + poff;
-                    qp[(u + 8) % 9][0] = lds128(pf);
-                    qp[(u + 8) % 9][1] = lds128(pf + P::SX0);
+#pragma unroll
+                    for (int r = 0; r < RPT; ++r) qp[(u + 8) % 9][r] = lds128(pf + r * P::SX0);
                 }
                 // ── stage A: q at za over the widened region ──
                 if (!wait_q(i)) bad = true;
                 if (!wait_v(i)) bad = true;
                 const float* qt = sq + (i % AQ) * P::EST + eoff;
                 const float* vt = sv + (i % AV) * P::EST + eoff;
-                const float4 pv[2] = {lds128(qt), lds128(qt + P::EX)};
-                float4 qn[2] = {pv[0], pv[1]};
+                float4 pv[RPT], qn[RPT];
+#pragma unroll
+                for (int r = 0; r < RPT; ++r) qn[r] = pv[r] = lds128(qt + r * P::EX);
                 if (za >= R && za < a.nz - R) {  // CTA-uniform
-                    const float4 vv[2] = {lds128(vt), lds128(vt + P::EX)};
-                    const float4 c[2] = {qp[(u + 4) % 9][0], qp[(u + 4) % 9][1]};
-                    float2 lap[2][2];
+                    float4 vv[RPT], c[RPT];
+#pragma unroll
+                    for (int r = 0; r < RPT; ++r) {
+                        vv[r] = lds128(vt + r * P::EX);
+                        c[r] = qp[(u + 4) % 9][r];
+                    }
+                    float2 lap[RPT][2];
                     m.laplacian(sp + ((i + 4) % S) * P::PST + poff, P::SX0, c,
                               [&](int r, int j) -> const float4& { return qp[(u + 4 + r) % 9][j]; },
                               [&](int r, int j) -> const float4& { return qp[(u + 4 - r + 9) % 9][j]; },
                               lap);
 #pragma unroll
-                    for (int r = 0; r < 2; ++r) {
+                    for (int r = 0; r < RPT; ++r) {
                         float4 o = m.update(c[r], pv[r], vv[r], lap[r]);
                         if (src_r == r && za == a.src_z) {
                             Leap2Math::add_source(o, vv[r], a.dt2, source_sample(a, 0), src_e);
@@ -343,14 +349,14 @@ __global__ void __launch_bounds__(Shape2<TX, TY, S, AQ, AV>::NT, 1)
                         if (rin[r]) qn[r] = o;  // halo points keep p_prev
                     }
                 }
-                sts128(s1 + (i % P::QS) * P::EST + eoff, qn[0]);
-                sts128(s1 + (i % P::QS) * P::EST + eoff + P::EX, qn[1]);
+#pragma unroll
+                for (int r = 0; r < RPT; ++r) sts128(s1 + (i % P::QS) * P::EST + eoff + r * P::EX, qn[r]);
                 if (inner) {
-                    q1[u][0] = qn[0];
-                    q1[u][1] = qn[1];
+#pragma unroll
+                    for (int r = 0; r < RPT; ++r) q1[u][r] = qn[r];
                     if (za >= zb && za < ze) {
 #pragma unroll
-                        for (int r = 0; r < 2; ++r)
+                        for (int r = 0; r < RPT; ++r)
                             if (rin[r]) stg_stream(a.out1 + goff + r * a.sy, qn[r]);
                     }
                 }
@@ -358,18 +364,22 @@ __global__ void __launch_bounds__(Shape2<TX, TY, S, AQ, AV>::NT, 1)
                 // (no barrier: it reads the q plane written 4 iterations ago and
                 // this thread's own q of za from its queue)
                 if (inner && i >= 2 * R) {
-                    const float4 c[2] = {q1[(u + 5) % 9][0], q1[(u + 5) % 9][1]};
-                    const float4 pv[2] = {qp[u % 9][0], qp[u % 9][1]};  // p at za - 4
                     const float* vb = sv + ((i - R) % AV) * P::EST + eoff;
-                    const float4 vv[2] = {lds128(vb), lds128(vb + P::EX)};
-                    float2 lap[2][2];
+                    float4 c[RPT], pv[RPT], vv[RPT];  // pv: p at za - 4
+#pragma unroll
+                    for (int r = 0; r < RPT; ++r) {
+                        c[r] = q1[(u + 5) % 9][r];
+                        pv[r] = qp[u % 9][r];
+                        vv[r] = lds128(vb + r * P::EX);
+                    }
+                    float2 lap[RPT][2];
                     m.laplacian(s1 + ((i - R) % P::QS) * P::EST + eoff, P::EX, c,
                               [&](int r, int j) -> const float4& { return q1[(u + 5 + r) % 9][j]; },
                               [&](int r, int j) -> const float4& { return q1[(u + 5 - r + 9) % 9][j]; },
                               lap);
                     const int zbb = za - R;
 #pragma unroll
-                    for (int r = 0; r < 2; ++r) {
+                    for (int r = 0; r < RPT; ++r) {
                         float4 o = m.update(c[r], pv[r], vv[r], lap[r]);
                         if (src_r == r && zbb == a.src_z) {
                             Leap2Math::add_source(o, vv[r], a.dt2, source_sample(a, 1), src_e);
@@ -400,14 +410,14 @@ __global__ void __launch_bounds__(Shape2<TX, TY, S, AQ, AV>::NT, 1)
     }
 }
 
-template <int TX, int TY, int S, int AQ, int AV>
+template <int TX, int TY, int RPT, int S, int AQ, int AV>
 int resident_leap2() {
-    using P = Shape2<TX, TY, S, AQ, AV>;
+    using P = Shape2<TX, TY, RPT, S, AQ, AV>;
     static int cached[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (cached[dev & 63] > 0) return cached[dev & 63];
-    auto kern = leap2_kernel<TX, TY, S, AQ, AV>;
+    auto kern = leap2_kernel<TX, TY, RPT, S, AQ, AV>;
     int n = 0;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(P::SMEM)) == cudaSuccess &&
@@ -420,12 +430,12 @@ int resident_leap2() {
     return 1;
 }
 
-template <int TX, int TY, int S, int AQ, int AV>
+template <int TX, int TY, int RPT, int S, int AQ, int AV>
 cudaError_t launch_leap2(const PencilMaps& m, const Leap2Args& a, unsigned ctas,
                          cudaStream_t stream) {
-    using P = Shape2<TX, TY, S, AQ, AV>;
-    resident_leap2<TX, TY, S, AQ, AV>();  // sets the shared-memory attribute once per device
-    leap2_kernel<TX, TY, S, AQ, AV><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev, m.vel2, a);
+    using P = Shape2<TX, TY, RPT, S, AQ, AV>;
+    resident_leap2<TX, TY, RPT, S, AQ, AV>();  // sets the shared-memory attribute once per device
+    leap2_kernel<TX, TY, RPT, S, AQ, AV><<<ctas, P::NT, P::SMEM, stream>>>(m.p, m.prev, m.vel2, a);
     return cudaGetLastError();
 }
 
@@ -436,18 +446,22 @@ struct Leap2Variant {
     int (*resident)();
 };
 
-#define SB200_LEAP2(TX, TY, S, AQ, AV, NAME) \
-    Leap2Variant { TX, TY, NAME, &launch_leap2<TX, TY, S, AQ, AV>, &resident_leap2<TX, TY, S, AQ, AV> }
+#define SB200_LEAP2(TX, TY, RPT, S, AQ, AV, NAME)                                      \
+    Leap2Variant {                                                                     \
+        TX, TY, NAME, &launch_leap2<TX, TY, RPT, S, AQ, AV>,                           \
+            &resident_leap2<TX, TY, RPT, S, AQ, AV>                                    \
+    }
 
-// Measured at 1024^3 (ms per step, one-step kernel 2.73): l64x16 3.95-3.98,
-// l32x32 3.97-4.12 (z split 2-4).  Not kept: a warp-specialised form (A warps
+// Measured at 1024^3 (ms per step, one-step kernel 2.72-2.73): l64x16 3.94-3.96,
+// l32x32 one row per thread (400 threads, 126 registers, 13 warps per SM) 3.90-3.96,
+// and not kept: l32x32 two rows 3.97-4.07, l64x16 one row 3.95-4.01 (z split 2-4).  Not kept: a warp-specialised form (A warps
 // holding the p queue, B warps the q queue, q planes handed over through an
 // mbarrier ring; 158-161 registers, 11 warps per SM) at 7.26-7.48 -- its two
 // 9x-unrolled loops run side by side and stall on instruction fetch (6.1 stalls
 // per issue against 1.3).
 const Leap2Variant kLeap2[] = {
-    SB200_LEAP2(32, 32, 8, 3, 8, "l32x32_s8"),
-    SB200_LEAP2(64, 16, 8, 3, 8, "l64x16_s8"),
+    SB200_LEAP2(64, 16, 2, 8, 3, 8, "l64x16_s8"),
+    SB200_LEAP2(32, 32, 1, 8, 3, 8, "l32x32_r1_s8"),
 };
 constexpr int kNumLeap2 = sizeof(kLeap2) / sizeof(kLeap2[0]);
 
