@@ -223,3 +223,34 @@ def test_batch_monitor_limit():
             b.synchronize()
         assert e.value.status == sb.SB200_ERR_MONITOR
         assert b.monitor_flags().sum() >= 1
+
+
+THIN = ((12, 9, 9), (40, 12, 10), (16, 33, 9), (40, 36, 36))  # nx, ny, nz
+
+
+@pytest.mark.parametrize("precision", [sb.PRECISION_F32, sb.PRECISION_F16])
+def test_batch_thin_shots_match_single_grid_runs(precision):
+    """Minimal shots (four interior columns, one interior plane, one tile row)
+    beside a normal one, every tile variant and z-chunk length: each shot bit for
+    bit the single-grid run engine on that grid alone."""
+    f16 = precision == sb.PRECISION_F16
+    steps = 24
+    dims = tuple((max(16, nx) if f16 else nx, ny, nz) for nx, ny, nz in THIN)
+    shots = [(g, s, v, w[:steps]) for g, s, v, w in make_shots(seed=31, dims=dims)]
+    refs = []
+    for g, src, v, w in shots:
+        z = np.zeros(g.shape, np.float32)
+        with sb.Run(g, src_index=src, graph_chunk=0, precision=precision) as r:
+            r.set_fields(z, z, v)
+            r.set_wavelet(np.pad(w, (0, 1)))
+            r.steps(steps)
+            refs.append((r.field(), r.trace(steps)))
+    nvar = (sb.lib().sb200_batch_variant_count_f16() if f16
+            else sb.lib().sb200_batch_variant_count())
+    runner = run_batch_f16 if f16 else run_batch
+    for v in range(nvar):
+        for zlen in (0, 1):
+            got = runner(shots, steps=steps, chunk=0, choice=(v, zlen), split=(5, steps - 5))
+            for (p, tr), (rp, rtr) in zip(got, refs):
+                assert np.array_equal(p, rp), (v, zlen)
+                assert np.array_equal(tr, rtr), (v, zlen)
