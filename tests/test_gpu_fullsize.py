@@ -4,7 +4,8 @@ grid (2^30 cells, byte offsets past 2^32) and of the 2048^3 FP16 grid (2^33
 cells) at 4096 sampled interior points against a float64 restatement of the
 stencil from the gathered stars (tolerance: FP32 rounding of the terms, plus
 one FP16 ulp for the stored halves), linearity of the FP32 step under a
-power-of-two scaling (bit for bit), and one heat step of the 512^3 grid."""
+power-of-two scaling (bit for bit), two steps per sweep at 1024^3 against two
+one-step launches (bit for bit), and one heat step of the 512^3 grid."""
 from __future__ import annotations
 
 import numpy as np
@@ -83,6 +84,28 @@ def test_acoustic_1024_sampled_and_linear(torch_cuda):
     out2 = torch.zeros_like(out)
     sb.wave_step(p * 4.0, q * 4.0, v, out2, g)
     assert torch.equal(out2, out * 4.0)
+
+
+def test_two_step_1024_equals_two_one_step_launches(torch_cuda):
+    """Two steps per sweep on the 1024^3 grid (byte offsets past 2^32, random
+    halos): bit for bit two in-place one-step launches, the outputs' halos
+    started as the walls they stand for (p_prev's for t+dt, p's for t+2dt)."""
+    torch = torch_cuda
+    n = 1024
+    g = sb.Grid(n, n, n, 10.0, 10.0, 10.0, 8.5e-4)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(21)
+    p = torch.randn(g.shape, generator=gen, device="cuda")
+    q = torch.randn(g.shape, generator=gen, device="cuda")
+    v = torch.rand(g.shape, generator=gen, device="cuda") * (4500.0 ** 2 - 1500.0 ** 2) + 1500.0 ** 2
+    src = g.index(512, 500, 700)
+    o1, o2 = q.clone(), p.clone()
+    sb.wave_step2(p, q, v, o1, o2, g, src, 0.75, -0.5)
+    a, b = q.clone(), p.clone()
+    sb.wave_step(p, a, v, a, g, src, 0.75)
+    sb.wave_step(a, b, v, b, g, src, -0.5)
+    torch.cuda.synchronize()
+    assert torch.equal(o1, a) and torch.equal(o2, b)
 
 
 def test_fp16_2048_sampled(torch_cuda):
