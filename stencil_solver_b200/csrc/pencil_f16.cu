@@ -103,8 +103,21 @@ __device__ __forceinline__ uint4 lds128h(const uint16_t* p) {
     return *reinterpret_cast<const uint4*>(p);
 }
 
-__device__ __forceinline__ void stg_stream_u2(void* p, uint2 v) {
-    asm volatile("st.global.cs.v2.u32 [%0], {%1, %2};" ::"l"(p), "r"(v.x), "r"(v.y) : "memory");
+// Streaming stores under a predicate (no branch: the three store shapes of a
+// chunk -- whole, upper half, lower half -- are issued with per-thread predicates).
+__device__ __forceinline__ void stg_stream_u4_if(void* p, uint4 v, bool pred) {
+    asm volatile(
+        "{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %5, 0;\n\t"
+        "@q st.global.cs.v4.u32 [%0], {%1, %2, %3, %4};\n\t}" ::"l"(p),
+        "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w), "r"(static_cast<uint32_t>(pred))
+        : "memory");
+}
+__device__ __forceinline__ void stg_stream_u2_if(void* p, uint2 v, bool pred) {
+    asm volatile(
+        "{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %3, 0;\n\t"
+        "@q st.global.cs.v2.u32 [%0], {%1, %2};\n\t}" ::"l"(p),
+        "r"(v.x), "r"(v.y), "r"(static_cast<uint32_t>(pred))
+        : "memory");
 }
 
 // b - f32(half) for both halves of a word: the sm_100 mixed-precision FMA
@@ -261,6 +274,9 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
     const bool xfull = gx >= R && gx + 8 <= a.nx - R;
     const bool xany = gx + 8 > R && gx < a.nx - R;
     const bool rin = xany && gy < a.ny - R;
+    const bool st_full = rin && xfull;           // the whole chunk is interior
+    const bool st_upper = rin && !xfull && gx < R;  // first chunk: x = 4..7
+    const bool st_lower = rin && !xfull && gx >= R;  // last chunk: x = nx-8 .. nx-5
     const int soff = (ly + R) * P::SX + 8 + 8 * lx;
     const int aoff = ly * TX + 8 * lx;
     int64_t goff = static_cast<int64_t>(zb) * a.sz + static_cast<int64_t>(gy) * a.sy + gx;
@@ -444,19 +460,17 @@ __device__ __forceinline__ bool pencil_f16_tile(const CUtensorMap* pmap, const C
                             }
                     }
                 }
-                if (rin) {
-                    uint16_t* dst = a.next + goff;
+                {
+                    uint16_t* dst = a.next + goff;  // used only under the predicates
                     uint4 pk;
                     pk.x = pack_h2(o[0], o[1]);
                     pk.y = pack_h2(o[2], o[3]);
                     pk.z = pack_h2(o[4], o[5]);
                     pk.w = pack_h2(o[6], o[7]);
-                    if (xfull)
-                        stg_stream_u4(dst, pk);
-                    else if (gx < R)  // x = 4..7 of the first chunk
-                        stg_stream_u2(dst + 4, make_uint2(pk.z, pk.w));
-                    else  // x = nx-8 .. nx-5 of the last chunk
-                        stg_stream_u2(dst, make_uint2(pk.x, pk.y));
+                    stg_stream_u4_if(dst, pk, st_full);
+                    // x = 4..7 of the first chunk; x = nx-8 .. nx-5 of the last
+                    stg_stream_u2_if(dst + 4, make_uint2(pk.z, pk.w), st_upper);
+                    stg_stream_u2_if(dst, make_uint2(pk.x, pk.y), st_lower);
                 }
                 goff += a.sz;
                 abort_run = __syncthreads_or(bad) != 0;
