@@ -326,7 +326,17 @@ __device__ __forceinline__ bool pencil_tile(const CUtensorMap* pmap, const CUten
                                     f4get(o, src_i);
                         }
                     }
-                    if (rin[j]) stg_stream(a.next + goff + j * a.sy, o);
+                    if constexpr (HEAT) {  // predicated: no branch per row
+                        float* dst = a.next + goff + j * a.sy;  // used only if rin[j]
+                        asm volatile(
+                            "{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %5, 0;\n\t"
+                            "@q st.global.cs.v4.f32 [%0], {%1, %2, %3, %4};\n\t}" ::"l"(dst),
+                            "f"(o.x), "f"(o.y), "f"(o.z), "f"(o.w),
+                            "r"(static_cast<uint32_t>(rin[j]))
+                            : "memory");
+                    } else if (rin[j]) {
+                        stg_stream(a.next + goff + j * a.sy, o);
+                    }
                 }
                 goff += a.sz;
                 // The stages of plane z (p) and of iteration i (aux) are free now:
