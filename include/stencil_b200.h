@@ -116,11 +116,13 @@ int sb200_wave_step2_f32(const float* p, const float* p_prev, const float* vel2,
                          float src_amp0, float src_amp1, void* stream);
 
 /* sb200_wave_step2_f32 with the two source samples read on the device as
- * wavelet[*step + step_offset] and wavelet[*step + step_offset + 1]. */
+ * wavelet[*step + step_offset] and wavelet[*step + step_offset + 1].  trace
+ * (optional device array, NULL for none) receives the source cell's value after
+ * each of the two steps at trace[*step + step_offset] and at the next index. */
 int sb200_wave_step2_dev_f32(const float* p, const float* p_prev, const float* vel2,
                              float* p_next, float* p_next2, const sb200_grid* grid,
                              int64_t src_index, const float* wavelet, const int* step,
-                             int step_offset, void* stream);
+                             int step_offset, float* trace, void* stream);
 
 /* Writes value to the device int *dst (one-thread kernel, stream-ordered). */
 int sb200_set_device_int(int* dst, int value, void* stream);

@@ -119,7 +119,8 @@ _SIGNATURES = {
     "sb200_wave_step2_f32": ([C.c_void_p] * 5 + [C.POINTER(sb200_grid), C.c_int64, C.c_float,
                                                  C.c_float, C.c_void_p], C.c_int),
     "sb200_wave_step2_dev_f32": ([C.c_void_p] * 5 + [C.POINTER(sb200_grid), C.c_int64,
-                                     C.c_void_p, C.c_void_p, C.c_int, C.c_void_p], C.c_int),
+                                     C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p],
+                                    C.c_int),
     "sb200_set_device_int": ([C.c_void_p, C.c_int, C.c_void_p], C.c_int),
     "sb200_heat_step_exact_f32": ([C.c_void_p, C.c_void_p, C.POINTER(sb200_grid), C.c_float,
                                    C.c_void_p], C.c_int),
@@ -363,10 +364,11 @@ def wave_step2(p, p_prev, vel2, p_next, p_next2, grid: Grid, src_index: int = -1
 
 
 def wave_step2_dev(p, p_prev, vel2, p_next, p_next2, grid: Grid, src_index: int, wavelet, step,
-                   step_offset: int = 0, stream=None) -> None:
+                   step_offset: int = 0, trace=None, stream=None) -> None:
     _check(lib().sb200_wave_step2_dev_f32(_ptr(p), _ptr(p_prev), _ptr(vel2), _ptr(p_next),
                                           _ptr(p_next2), _g(grid), src_index, _ptr(wavelet),
-                                          _ptr(step), step_offset, _stream(stream)))
+                                          _ptr(step), step_offset, _ptr(trace),
+                                          _stream(stream)))
 
 
 def set_device_int(dst, value: int, stream=None) -> None:

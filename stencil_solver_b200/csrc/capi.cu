@@ -410,7 +410,7 @@ int sb200_wave_step2_f32(const float* p, const float* p_prev, const float* vel2,
 int sb200_wave_step2_dev_f32(const float* p, const float* p_prev, const float* vel2,
                              float* p_next, float* p_next2, const sb200_grid* grid,
                              int64_t src_index, const float* wavelet, const int* step,
-                             int step_offset, void* stream) {
+                             int step_offset, float* trace, void* stream) {
     if (src_index >= 0 && (!wavelet || !step))
         return fail(SB200_ERR_INVALID, "sb200_wave_step2_dev_f32: NULL wavelet / step pointer");
     SourceDesc s;
@@ -418,6 +418,7 @@ int sb200_wave_step2_dev_f32(const float* p, const float* p_prev, const float* v
     s.wavelet = wavelet;
     s.step = step;
     s.step_offset = step_offset;
+    s.trace = trace;
     return wave_step2(p, p_prev, vel2, p_next, p_next2, grid, s, 0.f, stream, false,
                       "sb200_wave_step2_dev_f32");
 }

@@ -80,17 +80,29 @@ def test_twenty_steps_match(torch_cuda):
 
 
 def test_device_wavelet_and_trace_match(torch_cuda):
-    """The device-sample form reads wavelet[*step + off] and wavelet[... + 1]."""
+    """The device-sample form reads wavelet[*step + off] and the next sample, and
+    records the source cell after each step: the same field and trace as the run
+    engine's two one-step launches."""
     g = sb.Grid(48, 40, 36, 10.0, 10.0, 10.0, 7e-4)
     p, q, v = fields(torch_cuda, g, 11)
     src = g.index(20, 21, 17)
     wav = torch_cuda.tensor([0.1, 0.2, 0.9, -0.4, 0.3], device="cuda")
     step = torch_cuda.tensor([1], dtype=torch_cuda.int32, device="cuda")
+    trace = torch_cuda.full((5,), -7.0, device="cuda")
     o1, o2 = torch_cuda.zeros_like(p), torch_cuda.zeros_like(p)
-    sb.wave_step2_dev(p, q, v, o1, o2, g, src, wav, step, 1)
+    sb.wave_step2_dev(p, q, v, o1, o2, g, src, wav, step, 1, trace=trace)
     r1, r2 = one_step_pair(torch_cuda, p, q, v, g, src, 0.9, -0.4)
     torch_cuda.cuda.synchronize()
     assert torch_cuda.equal(o1, r1) and torch_cuda.equal(o2, r2)
+    t = trace.cpu().numpy()
+    assert t[0] == -7.0 and t[1] == -7.0 and t[4] == -7.0  # only indices 2 and 3 written
+    with sb.Run(g, src_index=src, graph_chunk=0) as run:
+        run.set_fields(p.cpu().numpy(), q.cpu().numpy(), v.cpu().numpy())
+        run.set_wavelet(np.array([0.9, -0.4, 0.0], np.float32))
+        run.steps(2)
+        field, tr = run.field(), run.trace(2)
+    assert np.array_equal(field, o2.cpu().numpy())
+    assert np.array_equal(t[2:4], tr)
 
 
 def test_argument_checks(torch_cuda):
