@@ -17,9 +17,9 @@
 //     last five iterations (a shared-memory ring, x-y neighbours) and a 9-deep
 //     register queue of q for the z neighbours; p_prev of that step is p itself,
 //     still in the first queue, and vel2 is still in its ring.
-// Each thread owns a float4 of x in RPT (1 or 2) rows of the widened region; the threads
-// whose rows lie in the tile run both stages, the others (the 4-cell ring around
-// the tile) stage A only.  Points of the widened region outside the grid's
+// Each thread owns a float4 of x in RPT (1 or 2) rows of the widened region; the
+// threads whose rows lie in the tile run both stages, the others (the 4-cell ring
+// around the tile) stage A only.  Points of the widened region outside the grid's
 // interior keep p_prev's value (a one-step launch never writes them, and it runs
 // in place over p_prev).  The z chunk is widened by 4 planes on each side for
 // stage A (q at z-4..z+4 of every output plane), so the chunk reads 16 halo
@@ -453,12 +453,12 @@ struct Leap2Variant {
     }
 
 // Measured at 1024^3 (ms per step, one-step kernel 2.72-2.73): l64x16 3.94-3.96,
-// l32x32 one row per thread (400 threads, 126 registers, 13 warps per SM) 3.90-3.96,
-// and not kept: l32x32 two rows 3.97-4.07, l64x16 one row 3.95-4.01 (z split 2-4).  Not kept: a warp-specialised form (A warps
-// holding the p queue, B warps the q queue, q planes handed over through an
-// mbarrier ring; 158-161 registers, 11 warps per SM) at 7.26-7.48 -- its two
-// 9x-unrolled loops run side by side and stall on instruction fetch (6.1 stalls
-// per issue against 1.3).
+// l32x32 one row per thread (400 threads, 126 registers, 13 warps per SM; the
+// default) 3.90-3.96.  Not kept: l32x32 two rows 3.97-4.07, l64x16 one row
+// 3.95-4.01 (z split 2-4); a warp-specialised form (A warps holding the p queue,
+// B warps the q queue, q planes handed over through an mbarrier ring; 158-161
+// registers, 11 warps per SM) at 7.26-7.48 -- its two 9x-unrolled loops run side
+// by side and stall on instruction fetch (6.1 stalls per issue against 1.3).
 const Leap2Variant kLeap2[] = {
     SB200_LEAP2(64, 16, 2, 8, 3, 8, "l64x16_s8"),
     SB200_LEAP2(32, 32, 1, 8, 3, 8, "l32x32_r1_s8"),
